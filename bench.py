@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the residual-and-update step (one JSON line).
+
+Metric: cell-RK-stage updates/s = active cells x RK stages x steps / device
+time of the step loop (SURVEY/BASELINE metric of the reference solver).
+
+Workload (N=1): viscous air flow past a cylinder, O-grid 160 x 256 x 20 hexes
+split into 6 tets (4,915,200 cells), Mach 0.3, Re_D 150, SSP-RK3, CFL 0.5,
+32 water-rich droplets; synthetic, generated in the reference's formats.
+Every rank runs its own replica (the path does not shard across GPUs here):
+value = cells x stages x steps summed over ranks / max-over-ranks time.
+
+Arms:
+  default          the CUDA engine through its C ABI (libhydraphase.so)
+  --impl reference the reference algorithm on the host cores (the FP64 CPU
+                   restatement in oracle/, since the Fortran reference cannot
+                   be built here), on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "multiphase-code_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "cell-RK-stage updates/s"
+UNIT = "cell-stage/s"
+
+# Compulsory bytes per cell and RK stage (each array crossing HBM once):
+# SURVEY's figure for the whole step (FP64) and the flux kernel's own set.
+STEP_BYTES_FP64 = 772
+STEP_BYTES_MIXED = 566
+
+
+def flux_kernel_bytes(grad_bytes: int, rk_scheme: int) -> float:
+    """Bytes the fused flux + source + RK-update kernel must move per cell:
+    14 primitives, 33 gradient components, phi, centroid, vol, dl, 12 face
+    vectors, 12 face centroids, 4 neighbour ids, face kinds, iblank, d24 (10),
+    vis (8), cu (10) read; cn (10) written; cn read on stages 2.. and cn1
+    traffic of the reference scheme, averaged over the stages."""
+    reads = 14 * 8 + 33 * grad_bytes + 8 + 24 + 16 + 96 + 96 + 16 + 4 + 4 + 80 + 64 + 80
+    if rk_scheme == 1:
+        reads += 80 * 2 / 3
+        writes = 80
+    else:
+        reads += 80 * 3 / 4 + 80 / 4
+        writes = 80 + 80 / 4
+    return reads + writes
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(prefix="clocks_", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        for line in open(self.out.name).read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+def make_workload(name: str, seed_offset: int = 0):
+    from hydraphase import cases
+    if name == "cylinder":
+        return cases.cylinder(seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+    if name == "cylinder_small":
+        return cases.cylinder(nr=40, nt=64, nz=8, seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+    if name == "shock_bubble":
+        return cases.shock_bubble(n=20, alpha_min=0.1, reference_scheme=True, seed=seed_offset)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def workload_config(spec, name):
+    m = spec.mesh
+    return {"workload": name, "cells": m.neles, "boundary_ghosts": m.nghosts,
+            "rk_stages_per_step": 3 if spec.extra.get("rk_scheme", 0) == 1 else 4,
+            "scheme": "SSP-RK3" if spec.extra.get("rk_scheme", 0) == 1 else "ESSPRK-4",
+            "flux": "HLLC-Batten", "limiter_K": spec.extra.get("venkat_k", 0.3),
+            "viscous": not spec.extra.get("inviscid", 0),
+            "l2_policy": "state larger than L2 (about 10 GB resident per replica)"}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group(backend="nccl" if os.environ.get("BENCH_BACKEND", "nccl") == "nccl" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier_max(pg, value: float, device) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier_sum(pg, value: float, device) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_oracle_sample(name: str, threads: int, seconds_target: float = 15.0):
+    """The CPU restatement on a bounded sample: same physics and scheme on a
+    coarser O-grid, timed over whole steps."""
+    import oracle as O
+    from hydraphase import cases
+    spec = cases.cylinder(nr=40, nt=64, nz=8, seed=1, alpha_w_drop=1e-5, alpha_w_bg=1e-6) \
+        if name.startswith("cylinder") else cases.shock_bubble(n=8, alpha_min=0.1, reference_scheme=True)
+    m = spec.mesh
+    O.set_threads(threads)
+    orc = O.Oracle(O.params_from_flow(spec.flow, **spec.extra), O.Mesh(m.x, m.y, m.z, m.elem, m.ghost))
+    orc.set_state(0.0, spec.cu, spec.ghost_prims)
+    orc.run(1)   # warm-up
+    stages = 3 if spec.extra.get("rk_scheme", 0) == 1 else 4
+    steps, t_used = 0, 0.0
+    while t_used < seconds_target and steps < 200:
+        t0 = time.perf_counter()
+        orc.run(1)
+        t_used += time.perf_counter() - t0
+        steps += 1
+    return {"value": m.neles * stages * steps / t_used, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{m.neles} cells (O-grid 40x64x8, same physics), {steps} steps, {t_used:.1f} s"}
+
+
+def run_reference_arm(args, world, rank, pg):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    res = cpu_oracle_sample(args.workload, threads, seconds_target=max(5.0, min(60.0, 3.0 * args.steps)))
+    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "impl": "reference", "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "note": "CPU restatement of the reference on a bounded sample"},
+            "cpu_baseline": res,
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def measure_variant(spec, precision, steps, warmup, pg, device):
+    """Device-timed steps of one precision variant; returns numbers and the
+    final state (for accuracy comparison)."""
+    from hydraphase import Case
+    p = spec.params(precision=precision)
+    c = Case(spec.mesh, p)
+    c.set_state(0.0, spec.cu, spec.ghost_prims)
+    c.step(warmup, diagnostics=False)
+    c.sync()
+    if pg is not None:
+        pg.barrier()
+    ms = c.step_timed(steps)
+    if pg is not None:
+        pg.barrier()
+    info = c.info()
+    prof = c.profile(2)
+    d = c.step(1)
+    t, cu, _ = c.state()
+    c.close()
+    return ms, info, prof, cu, d
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+    from hydraphase import PREC_FP64_PARITY, PREC_MIXED, Case
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    spec = make_workload(args.workload, seed_offset=rank)
+    m = spec.mesh
+    stages = 3 if spec.extra.get("rk_scheme", 0) == 1 else 4
+    cells = m.neles
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    # --- headline: plain FP64 (bit-parity) path, device-timed -------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms64, info, prof64, cu64, d64 = measure_variant(spec, PREC_FP64_PARITY, args.steps, args.warmup, pg, device)
+    clk = clocks.stop()
+    t_max = barrier_max(pg, ms64, device) / 1e3
+    total_updates = barrier_sum(pg, float(cells * stages * args.steps), device)
+    value = total_updates / t_max
+
+    # --- mixed precision variant ----------------------------------------
+    msmx, infomx, profmx, cumx, dmx = measure_variant(spec, PREC_MIXED, args.steps, args.warmup, pg, device)
+    tmx = barrier_max(pg, msmx, device) / 1e3
+    value_mx = barrier_sum(pg, float(cells * stages * args.steps), device) / tmx
+    rel = np.linalg.norm(cumx - cu64, axis=1) / np.linalg.norm(cu64, axis=1)
+
+    # --- end to end through the public API with host buffers -------------
+    from hydraphase import Case as _Case
+    cu_host = np.ascontiguousarray(spec.cu)
+    gp_host = np.ascontiguousarray(spec.ghost_prims)
+    c = _Case(m, spec.params(precision=PREC_FP64_PARITY))
+    c.set_state(0.0, cu_host, gp_host)
+    c.step(args.warmup, diagnostics=False)
+    c.sync()
+    if pg is not None:
+        pg.barrier()
+    t0 = time.perf_counter()
+    c.set_state(0.0, cu_host, gp_host)
+    diag = c.step(args.steps, diagnostics=True)
+    _, cu_out, gp_out = c.state()
+    e2e_s = time.perf_counter() - t0
+    c.close()
+    e2e_max = barrier_max(pg, e2e_s, device)
+    e2e_value = total_updates / e2e_max
+    h2d = (cu_host.nbytes + gp_host.nbytes) / args.steps
+    d2h = (cu_out.nbytes + gp_out.nbytes) / args.steps + 64
+
+    # --- roofline of the dominant kernel (fused flux + source + update) ---
+    kinds = prof64["kinds"]
+    flux_ms = prof64["ms"][kinds.index("flux")] / max(prof64["launches"][kinds.index("flux")], 1)
+    fb = flux_kernel_bytes(8, spec.extra.get("rk_scheme", 0))
+    achieved = fb * cells / (flux_ms / 1e3) / 1e9
+    step_ms = ms64 / args.steps
+    achieved_step = STEP_BYTES_FP64 * cells * stages / (step_ms / 1e3) / 1e9
+    share = {k: round(v / sum(prof64["ms"]), 4) for k, v in zip(kinds, prof64["ms"]) if v > 0}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (O-grid cylinder generated in the reference's formats)",
+        "config": {**workload_config(spec, args.workload), "parallelism": f"replicas x{world}",
+                   "precision": "fp64 bit-parity (no FMA)"},
+        "gpu_launches": int(info["kernels_per_step"]) * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "k_flux (HLLC faces + sources + RK update)",
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "peak_source": peak_src, "bytes_per_cell": fb, "traffic": None,
+                     "step_level": {"bytes_per_cell_stage": STEP_BYTES_FP64, "achieved": achieved_step,
+                                    "frac": achieved_step / hbm_peak}},
+        "kernel_share": share,
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "note": "set_state (H2D) + steps with per-step diagnostics + get_state (D2H), wall clock"},
+        "mixed": {"value": value_mx, "ms_per_step": msmx / args.steps, "speedup_vs_fp64": value_mx / value,
+                  "rel_l2_vs_fp64_after_steps": {"rho_g_alpha_g": float(rel[0]), "rho_p_alpha_p": float(rel[5]),
+                                                 "max_air_vars": float(rel[:5].max())},
+                  "dtype": "f32 fluxes/gradients, f64 state/EOS/reductions"},
+        "nan_cells_after": float(d64["nan_cells"][0]),
+    }
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_oracle_sample(args.workload, os.cpu_count() or 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cylinder")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            rc = run_reference_arm(args, world, rank, pg)
+        else:
+            rc = run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,165 @@
+/*
+ * hydraphase.h -- C ABI of the B200 residual-and-update engine for the
+ * two-phase six-equation solver (reference: GauthamBijoy23/Multiphase-code,
+ * project HydraPhase_60_FPC_5mill, Fortran 90 + OpenACC).
+ *
+ * The reference has no library API: its time loop (src/main.F90:511-657)
+ * calls argument-less subroutines that share module globals
+ * (src/mod_GlobalVariables.F90).  This header replaces that loop.  A Fortran
+ * host keeps its own Read_flow, mesh reader and restart/Tecplot writers and
+ * calls these entry points through ISO_C_BINDING interfaces (see
+ * INTEGRATION.md); plain pointers and sizes only, 1-based cell ids as the
+ * reference stores them, column-major conserved state.
+ *
+ * Conventions: every entry point returns 0 on success and a negative
+ * HP_E_* code on failure (never exits or stops); hp_last_error() gives the
+ * message.  One host thread per handle; each handle owns one CUDA stream and
+ * all of its device memory.
+ */
+#ifndef HYDRAPHASE_H
+#define HYDRAPHASE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    HP_OK = 0,
+    HP_E_ARG = -1,        /* bad argument / malformed mesh or parameters */
+    HP_E_CUDA = -2,       /* CUDA runtime failure */
+    HP_E_NOMEM = -3,      /* device allocation failed or over the HBM budget */
+    HP_E_IO = -4,         /* file could not be opened / parsed */
+    HP_E_STATE = -5,      /* call out of order (e.g. step before set_state) */
+    HP_E_UNSUPPORTED = -6 /* feature outside this build (partition ghosts) */
+};
+
+/* Arithmetic of the hot kernels. */
+enum {
+    HP_PREC_FP64_PARITY = 0, /* FP64, no FMA contraction: bit-parity path */
+    HP_PREC_FP64 = 1,        /* FP64 with FMA */
+    HP_PREC_MIXED = 2        /* FP32 gradients/limiter/fluxes, FP64 state,
+                                EOS recovery and reductions */
+};
+
+/* flow.in in file order (src/sr_Read_flow.F90:19-268) plus the switches of
+ * this build.  Field meanings and units are those of flow.in. */
+typedef struct hp_params {
+    double pmax, pmin, tgmax, tgmin;
+    double ugmax, ugmin, vgmax, vgmin, wgmax, wgmin;
+    double upmax, upmin, vpmax, vpmin, wpmax, wpmin;
+    double tpmax, tpmin;
+    double pinf, gamap, gamag, cpp, cpg, amolg, prg, epslnmax;
+    double epslnmin, epslninf, phipzero;
+    double cfl;
+    int32_t niter, itersub;
+    int32_t istart;
+    double diap;
+    double surfacetension;
+    int32_t myflux;          /* 2 = HLLC-Batten (the only flux of this build) */
+    int32_t myorder;         /* 1 or 2 */
+    double as, ts;           /* Sutherland constants */
+    /* --- additions; zero-initialised values reproduce the reference --- */
+    int32_t reserved0;
+    double venkat_k;         /* limiter eps^2 = (K*dl)^3; 0 selects 0.3 */
+    int32_t rk_scheme;       /* 0: reference 4-stage ESSPRK; 1: SSP-RK3 */
+    int32_t inviscid;        /* 1: viscous face fluxes off */
+    double twall;            /* isothermal wall temperature (BC type 6) */
+    int32_t precision;       /* HP_PREC_* */
+    int32_t renumber;        /* 1: space-filling-curve cell order on device */
+    int32_t block_size;      /* 0: autotuned */
+    int32_t use_graph;       /* 1: capture each step in a CUDA graph */
+    double pad_[4];
+} hp_params;
+
+/* Mesh as the reference reads it (src/sr_geometry.F90:101-139):
+ *   x, y, z[nodes]                   node coordinates
+ *   elem[neles*9] row-major          nod1..nod4, nc1..nc4, iblank (1-based)
+ *   ghost[nghosts*4] row-major       nparent, nghost, ntype, nside
+ * Partition ghosts (proc_bc) must be zero: one partition per GPU. */
+typedef struct hp_mesh {
+    int32_t nodes, neles, nghosts, pghosts;
+    const double *x, *y, *z;
+    const int32_t *elem;
+    const int32_t *ghost;
+} hp_mesh;
+
+/* Per-step diagnostics (src/main.F90:646-654). */
+typedef struct hp_diag {
+    double time;      /* simulation time after the step */
+    double dt;        /* time step used */
+    double velmag;    /* |u_g| of cell 1 (Velocity.dat) */
+    double diff[4];   /* max |cn - cu| of variables 1..4 (diffp,diffu,diffv,diffw) */
+    double nan_cells; /* elements whose state is NaN after the step */
+} hp_diag;
+
+typedef struct hp_handle hp_handle;
+
+/* --- lifecycle --------------------------------------------------------- */
+/* Replaces the setup half of src/main.F90:47-499: computes the geometry of
+ * src/sr_geometry.F90:147-347 (bit-identical to the reference), builds the
+ * device layout, and allocates all device memory on the current device. */
+int hp_create(const hp_mesh *mesh, const hp_params *params, hp_handle **out);
+int hp_destroy(hp_handle *h);
+const char *hp_last_error(const hp_handle *h);
+/* Message of the last failed hp_create (no handle exists then). */
+const char *hp_create_error(void);
+
+/* src/sr_init_cond.F90:177-226 (uniform state) and cn = cu. */
+int hp_init_uniform(hp_handle *h);
+/* Restart injection, src/main.F90:427-441: cu_elem is cu(1:neles,1:10)
+ * column-major; ghost_prims (may be NULL) is ug,vg,wg,pg,tg,rog at the ghost
+ * ids in ghost-list order (6 x nghosts).  Host pointers. */
+int hp_set_state(hp_handle *h, double time, const double *cu_elem,
+                 const double *ghost_prims);
+
+/* nsteps of src/main.F90:515-654.  diag may be NULL or hold nsteps entries.
+ * Asynchronous with respect to the host unless diag != NULL. */
+int hp_step(hp_handle *h, int32_t nsteps, hp_diag *diag);
+/* Blocks until the handle's stream is idle. */
+int hp_sync(hp_handle *h);
+/* nsteps without diagnostics; *device_ms is the device time of those steps
+ * measured with CUDA events on the handle's stream. */
+int hp_step_timed(hp_handle *h, int32_t nsteps, double *device_ms);
+/* nsteps launched eagerly with a CUDA event between every two kernels;
+ * accumulates device time and launch counts per kernel kind (nkinds >= 13:
+ * prim_start, step_begin, smooth1, smooth2, bc_visc, visc, prim_stage, bc,
+ * grad, flux, prim_end, step_end, serial). */
+int hp_profile_steps(hp_handle *h, int32_t nsteps, double *ms_per_kind,
+                     int64_t *launches_per_kind, int32_t nkinds);
+
+/* State read-back in the restart layout (src/main.F90:817-824). */
+int hp_get_state(hp_handle *h, double *time, double *cu_elem,
+                 double *ghost_prims);
+/* Cell primitives after the last step (ug,vg,wg,tg,pg,pp,phig,phip,up,vp,wp,
+ * tp,rog,rop; 14 x neles, reference cell order). */
+int hp_get_prims(hp_handle *h, double *prims);
+
+/* --- device-resident access (for callers that keep data in HBM) --------- */
+/* Device pointer of the conserved state cu (10 x ld, internal cell order)
+ * and the leading dimension; valid until hp_destroy. */
+int hp_device_state(hp_handle *h, double **cu_dev, int64_t *ld);
+/* Number of kernels one step launches and the device bytes the handle
+ * holds. */
+int hp_info(const hp_handle *h, int64_t *kernels_per_step, int64_t *device_bytes,
+            int64_t *aliased);
+
+/* --- reference file formats (drop-in inputs/outputs) -------------------- */
+/* flow.in parser, src/sr_Read_flow.F90:19-268. */
+int hp_read_flow(const char *path, hp_params *out);
+/* Mesh files of one rank: geometry_files/{grid_procNNNN.dat, bc_procNNNN.in,
+ * proc_bcNNNN.in}.  Arrays are malloc'ed; free with hp_free_mesh. */
+int hp_read_mesh(const char *case_dir, int32_t rank, hp_mesh *out);
+void hp_free_mesh(hp_mesh *m);
+/* Restart file, src/main.F90:427-441 / 812-828. */
+int hp_read_restart(const char *path, int32_t neles, int32_t nghosts,
+                    double *time, double *cu_elem, double *ghost_prims);
+int hp_write_restart(const char *path, int32_t neles, int32_t nghosts,
+                     double time, const double *cu_elem, const double *ghost_prims);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

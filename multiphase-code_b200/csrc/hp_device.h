@@ -1,0 +1,110 @@
+// hp_device.h -- device-side layout of one case (mesh + state) and the
+// per-variant kernel entry table.  Shared by the host code (hp_host.cu) and
+// every precision variant (hp_variant_*.cu).
+//
+// Layout in HBM: structure of arrays, one column per variable, leading
+// dimension `ld` (= ntot rounded up to 64 cells) so each column starts on a
+// 512-byte boundary.  Cell ids are 0-based internally: elements [0, neles),
+// boundary ghosts [neles, neles + nghosts) -- the reference's 1-based ids
+// minus one (src/main.F90:103).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hp {
+
+enum { NEQ = 10, NPR = 14, NGR = 33 };
+
+// primitive columns (the reference's ug,vg,wg,tg,pg,pp,phig,phip,up,vp,wp,
+// tp,rog,rop of src/mod_GlobalVariables.F90:13)
+enum { P_UG = 0, P_VG, P_WG, P_TG, P_PG, P_PP, P_PHIG, P_PHIP, P_UP, P_VP,
+       P_WP, P_TP, P_ROG, P_ROP };
+// stored gradient columns (x,y,z per field), src/sr_derivative.F90:259-309
+enum { G_UG = 0, G_VG = 3, G_WG = 6, G_TG = 9, G_UP = 12, G_VP = 15,
+       G_WP = 18, G_TP = 21, G_PG = 24, G_PP = 27, G_PHIG = 30 };
+
+// face kind bits per cell, 4 bits per face: bit 0 = wall (ghost type 5),
+// bit 1 = MUSCL-reconstruct across the face (interior or partition ghost).
+enum { FK_WALL = 1, FK_RECON = 2 };
+
+struct DevParams {
+    double gamag, gamap, pinf, cpp, cpg, prg, rrg, prp;
+    double emin, emax, phipzero;
+    double ugmin, vgmin, wgmin, upmin, vpmin, wpmin, tgmin, tpmin, pmin;
+    double as, ts, c23, co2, co4, fsd;   // fsd = 4 sigma / d
+    double cfl, venkat_k, twall, amup;
+    int rk_scheme, inviscid, myorder, nstage;
+};
+
+struct DevMesh {
+    int neles, nghosts, ntot, aliased;
+    long long ld;
+    int cell1;              // internal id of the reference's cell 1
+    const int* nc;          // [4][ld] face neighbours
+    const int* snb;         // [4][ld] neighbours as smoothing sees them
+    const unsigned* fk;     // [ld] face kind nibbles
+    const int* iblank;      // [ld]
+    const double *xc, *yc, *zc, *vol, *dl, *dd;   // [ld]
+    const double* sc;       // [12][ld] face area vectors sc1x..sc4z
+    const double* fch;      // [12][ld] face centroids, 0.3333 factor (HLLC, VK)
+    const double* fcv;      // [12][ld] face centroids, /3 (viscous)
+    const int *g_par, *g_id, *g_type;   // [nghosts] ghost list (reference order)
+};
+
+struct DevScalars {
+    unsigned long long dtmin_bits;    // running min of dl/(a+|u|), skips NaN
+    unsigned long long diff_bits[4];  // running max |cn - cu|, skips NaN
+    unsigned long long nan_count;
+    double dt, time, velmag;
+    int total;                        // step counter (src/main.F90:522)
+    int step_in_call;
+    double fcarry[10];                // stale-flux carry (aliased meshes)
+    int err_flags;
+};
+
+template <class R>
+struct DevState {
+    double *cn, *cu, *cn1;   // [10][ld]
+    double* pr;              // [14][ld]
+    R* gr;                   // [33][ld]
+    double* phi;             // [ld]
+    double *anu, *d2q;       // [2][ld], [10][ld]
+    double *d24, *vis;       // [10][ld], [8][ld]
+    double* egt;             // [2][ld] ghost egtotal/eptotal (aliased meshes)
+    DevScalars* s;
+    double* diag;            // [max_steps][8]
+    int max_diag;
+};
+
+// Kernel kinds, for per-kernel timing (hp_profile_steps).
+enum KernelKind {
+    KK_PRIM_START = 0, KK_STEP_BEGIN, KK_SMOOTH1, KK_SMOOTH2, KK_BC_VISC, KK_VISC,
+    KK_PRIM_STAGE, KK_BC, KK_GRAD, KK_FLUX, KK_PRIM_END, KK_STEP_END, KK_SERIAL,
+    KK_COUNT
+};
+
+// Optional hook called before every launch (and with KK_COUNT after the
+// last one) so the host can bracket each kernel with CUDA events.
+struct StepHook {
+    void (*mark)(void* ctx, int kind);
+    void* ctx;
+};
+
+// What one precision variant provides to the host.
+struct Variant {
+    const char* name;
+    size_t grad_bytes;  // sizeof(R) of the gradient columns
+    // enqueue the start-of-step primitive recovery + dt contributions
+    void (*enqueue_start)(const DevMesh&, const void* st, const DevParams&,
+                          cudaStream_t, int block, const StepHook* hook);
+    // enqueue one full step (after enqueue_start of the same step)
+    void (*enqueue_step)(const DevMesh&, const void* st, const DevParams&,
+                         cudaStream_t, int block, const StepHook* hook);
+    int kernels_per_step;
+};
+
+extern const Variant variant_fp64_parity;
+extern const Variant variant_fp64;
+extern const Variant variant_mixed;
+
+}  // namespace hp

@@ -1,0 +1,691 @@
+// hp_host.cu -- C ABI of the engine (include/hydraphase.h): mesh setup,
+// geometry, device layout, state transfer and the step loop.
+//
+// Geometry is set-up work the reference also does on the host
+// (src/sr_geometry.F90 has no device regions); it is restated here with the
+// reference's operand order so face vectors, volumes, centroids and dl are
+// bit-identical.  The time step itself runs only on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/hydraphase.h"
+#include "hp_device.h"
+
+using namespace hp;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0, used = 0;
+    void* take(size_t bytes) {
+        size_t off = (used + 255) & ~size_t(255);
+        used = off + bytes;
+        return base ? base + off : nullptr;
+    }
+};
+
+inline double mn2(double a, double b) { return (b < a || a != a) ? b : a; }
+inline double mx2(double a, double b) { return (b > a || a != a) ? b : a; }
+inline double sq(double a) { return a * a; }
+inline double det3(double A11, double A21, double A31, double A12, double A22, double A32,
+                   double A13, double A23, double A33) {
+    return A11 * (A22 * A33 - A23 * A32) - A21 * (A12 * A33 - A13 * A32) +
+           A31 * (A12 * A23 - A13 * A22);
+}
+
+const int GEO_FACE[4][3] = {{2, 3, 4}, {4, 3, 1}, {2, 4, 1}, {3, 2, 1}};
+const int HLL_FACE[4][3] = {{2, 4, 3}, {3, 4, 1}, {4, 2, 1}, {2, 3, 1}};
+const int VIS_FACE[4][3] = {{2, 3, 4}, {1, 3, 4}, {1, 2, 4}, {1, 2, 3}};
+
+}  // namespace
+
+struct hp_handle {
+    hp_params prm{};
+    DevParams dp{};
+    DevMesh dm{};
+    DevState<double> ds{};
+    const Variant* var = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    Arena arena;
+    int device = 0;
+    int neles = 0, nghosts = 0, ntot = 0;
+    long long ld = 0;
+    std::vector<int> perm;      // reference element (0-based) -> internal id
+    std::vector<int> ghost_id;  // ghost-list position -> internal slot id
+    bool started = false, have_state = false;
+    int aliased = 0;
+    int max_diag = 4096;
+    std::string err;
+    double* h_diag = nullptr;   // pinned
+    DevScalars* h_scal = nullptr;
+};
+
+static int fail(hp_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define CUDA_OK(h, call)                                                                  \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(h, HP_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// 30-bit Morton key of a point in the unit cube (10 bits per axis).
+static inline uint32_t spread10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+extern "C" const char* hp_create_error(void) { return g_create_error.c_str(); }
+
+extern "C" const char* hp_last_error(const hp_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle** out) {
+    g_create_error.clear();
+    if (!mesh || !params || !out) return fail(nullptr, HP_E_ARG, "null argument");
+    *out = nullptr;
+    const int nodes = mesh->nodes, neles = mesh->neles, nghosts = mesh->nghosts;
+    if (mesh->pghosts != 0)
+        return fail(nullptr, HP_E_UNSUPPORTED, "partition ghosts: one partition per GPU only");
+    if (nodes <= 0 || neles <= 0 || nghosts < 0 || !mesh->x || !mesh->y || !mesh->z || !mesh->elem ||
+        (nghosts > 0 && !mesh->ghost))
+        return fail(nullptr, HP_E_ARG, "empty or incomplete mesh");
+    if (params->myflux != 2)
+        return fail(nullptr, HP_E_UNSUPPORTED, "myflux must be 2 (HLLC-Batten)");
+    if (params->myorder != 1 && params->myorder != 2)
+        return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
+    const int ntot = neles + nghosts;
+    // --- validate connectivity (1-based as read) ---
+    for (long long e = 0; e < neles; e++) {
+        const int32_t* r = mesh->elem + 9 * e;
+        for (int k = 0; k < 4; k++)
+            if (r[k] < 1 || r[k] > nodes)
+                return fail(nullptr, HP_E_ARG, "element " + std::to_string(e + 1) + ": node id out of range");
+        for (int k = 4; k < 8; k++)
+            if (r[k] < 1 || r[k] > ntot)
+                return fail(nullptr, HP_E_ARG, "element " + std::to_string(e + 1) + ": neighbour id out of range");
+    }
+    for (long long g = 0; g < nghosts; g++) {
+        const int32_t* r = mesh->ghost + 4 * g;
+        if (r[0] < 1 || r[0] > ntot || r[1] < 1 || r[1] > ntot || r[3] < 1 || r[3] > 4)
+            return fail(nullptr, HP_E_ARG, "ghost " + std::to_string(g + 1) + ": bad parent/id/side");
+    }
+
+    auto* h = new hp_handle();
+    h->prm = *params;
+    h->neles = neles; h->nghosts = nghosts; h->ntot = ntot;
+
+    // --- geometry, src/sr_geometry.F90:112-347 (1-based work arrays) ---
+    std::vector<double> x(nodes + 1), y(nodes + 1), z(nodes + 1);
+    for (int n = 1; n <= nodes; n++) { x[n] = mesh->x[n - 1]; y[n] = mesh->y[n - 1]; z[n] = mesh->z[n - 1]; }
+    double xmax = -1.0e30, ymax = -1.0e30, zmax = -1.0e30, ymin = 1.0e30, zmin = 1.0e30;
+    for (int n = 1; n <= nodes; n++) {
+        xmax = mx2(xmax, x[n]); ymax = mx2(ymax, y[n]); zmax = mx2(zmax, z[n]);
+        ymin = mn2(ymin, y[n]); zmin = mn2(zmin, z[n]);
+    }
+    std::vector<int> nod[4], nc[4];
+    for (int k = 0; k < 4; k++) { nod[k].assign(ntot + 1, 0); nc[k].assign(ntot + 1, 0); }
+    std::vector<int> iblank(ntot + 1, 0);
+    for (int e = 1; e <= neles; e++) {
+        const int32_t* r = mesh->elem + 9 * (size_t)(e - 1);
+        for (int k = 0; k < 4; k++) { nod[k][e] = r[k]; nc[k][e] = r[4 + k]; }
+        iblank[e] = r[8];
+    }
+    std::vector<double> xcel(ntot + 1, 0.0), ycel(ntot + 1, 0.0), zcel(ntot + 1, 0.0), vol(ntot + 1, 0.0),
+        dl(ntot + 1, 0.0), dd(ntot + 1, 0.0);
+    std::vector<double> sc(12 * (size_t)(ntot + 1), 0.0), fch(12 * (size_t)(ntot + 1), 0.0),
+        fcv(12 * (size_t)(ntot + 1), 0.0);
+    auto SC = [&](int k, int i) -> double& { return sc[(size_t)k * (ntot + 1) + i]; };
+    auto FCH = [&](int k, int i) -> double& { return fch[(size_t)k * (ntot + 1) + i]; };
+    auto FCV = [&](int k, int i) -> double& { return fcv[(size_t)k * (ntot + 1) + i]; };
+    for (int i = 1; i <= neles; i++) {
+        for (int f = 0; f < 4; f++) {
+            int n1 = nod[GEO_FACE[f][0] - 1][i], n2 = nod[GEO_FACE[f][1] - 1][i], n3 = nod[GEO_FACE[f][2] - 1][i];
+            double dxyA = (x[n1] - x[n2]) * (y[n1] + y[n2]);
+            double dxyB = (x[n2] - x[n3]) * (y[n2] + y[n3]);
+            double dxyC = (x[n3] - x[n1]) * (y[n3] + y[n1]);
+            double dyzA = (y[n1] - y[n2]) * (z[n1] + z[n2]);
+            double dyzB = (y[n2] - y[n3]) * (z[n2] + z[n3]);
+            double dyzC = (y[n3] - y[n1]) * (z[n3] + z[n1]);
+            double dzxA = (z[n1] - z[n2]) * (x[n1] + x[n2]);
+            double dzxB = (z[n2] - z[n3]) * (x[n2] + x[n3]);
+            double dzxC = (z[n3] - z[n1]) * (x[n3] + x[n1]);
+            SC(3 * f + 0, i) = 0.5 * (dyzA + dyzB + dyzC);
+            SC(3 * f + 1, i) = 0.5 * (dzxA + dzxB + dzxC);
+            SC(3 * f + 2, i) = 0.5 * (dxyA + dxyB + dxyC);
+            int a = nod[HLL_FACE[f][0] - 1][i], b = nod[HLL_FACE[f][1] - 1][i], c = nod[HLL_FACE[f][2] - 1][i];
+            FCH(f, i) = (x[a] + x[b] + x[c]) * 0.3333;
+            FCH(4 + f, i) = (y[a] + y[b] + y[c]) * 0.3333;
+            FCH(8 + f, i) = (z[a] + z[b] + z[c]) * 0.3333;
+            a = nod[VIS_FACE[f][0] - 1][i]; b = nod[VIS_FACE[f][1] - 1][i]; c = nod[VIS_FACE[f][2] - 1][i];
+            FCV(f, i) = (x[a] + x[b] + x[c]) / 3.0;
+            FCV(4 + f, i) = (y[a] + y[b] + y[c]) / 3.0;
+            FCV(8 + f, i) = (z[a] + z[b] + z[c]) / 3.0;
+        }
+        int n1 = nod[0][i], n2 = nod[1][i], n3 = nod[2][i], n4 = nod[3][i];
+        double x1 = x[n1], x2 = x[n2], x3 = x[n3], x4 = x[n4];
+        double y1 = y[n1], y2 = y[n2], y3 = y[n3], y4 = y[n4];
+        double z1 = z[n1], z2 = z[n2], z3 = z[n3], z4 = z[n4];
+        xcel[i] = 0.25 * (x1 + x2 + x3 + x4);
+        ycel[i] = 0.25 * (y1 + y2 + y3 + y4);
+        zcel[i] = 0.25 * (z1 + z2 + z3 + z4);
+        double dl12 = std::sqrt(sq(x1 - x2) + sq(y1 - y2) + sq(z1 - z2));
+        double dl13 = std::sqrt(sq(x1 - x3) + sq(y1 - y3) + sq(z1 - z3));
+        double dl14 = std::sqrt(sq(x1 - x4) + sq(y1 - y4) + sq(z1 - z4));
+        double dl23 = std::sqrt(sq(x2 - x3) + sq(y2 - y3) + sq(z2 - z3));
+        double dl42 = std::sqrt(sq(x4 - x2) + sq(y4 - y2) + sq(z4 - z2));
+        double dl43 = std::sqrt(sq(x4 - x3) + sq(y4 - y3) + sq(z4 - z3));
+        dl[i] = mn2(mn2(mn2(mn2(mn2(dl12, dl13), dl14), dl23), dl42), dl43);
+        double v6 = det3(x2, x3, x4, y2, y3, y4, z2, z3, z4) - det3(x1, x3, x4, y1, y3, y4, z1, z3, z4) +
+                    det3(x1, x2, x4, y1, y2, y4, z1, z2, z4) - det3(x1, x2, x3, y1, y2, y3, z1, z2, z3);
+        vol[i] = std::fabs(v6) / 6.0;
+    }
+    std::vector<int> gpar(nghosts), gid(nghosts), gtyp(nghosts), gside(nghosts);
+    for (int g = 0; g < nghosts; g++) {
+        const int32_t* r = mesh->ghost + 4 * (size_t)g;
+        gpar[g] = r[0]; gid[g] = r[1]; gtyp[g] = r[2]; gside[g] = r[3];
+    }
+    for (int g = 0; g < nghosts; g++) {   // mirrored ghost centroids, sequential
+        int np = gpar[g], ng = gid[g], ns = gside[g];
+        int n1 = nod[GEO_FACE[ns - 1][0] - 1][np], n2 = nod[GEO_FACE[ns - 1][1] - 1][np],
+            n3 = nod[GEO_FACE[ns - 1][2] - 1][np];
+        double xcf = (x[n1] + x[n2] + x[n3]) / 3.0;
+        double ycf = (y[n1] + y[n2] + y[n3]) / 3.0;
+        double zcf = (z[n1] + z[n2] + z[n3]) / 3.0;
+        xcel[ng] = 2.0 * xcf - xcel[np];
+        ycel[ng] = 2.0 * ycf - ycel[np];
+        zcel[ng] = 2.0 * zcf - zcel[np];
+        vol[ng] = vol[np];
+        nc[0][ng] = ng; nc[1][ng] = ng; nc[2][ng] = ng; nc[3][ng] = ng;
+    }
+    for (int g = 0; g < nghosts; g++) {   // wave-transmissive distance
+        int np = gpar[g], nt = gtyp[g];
+        int n1 = nod[0][np], n2 = nod[1][np], n3 = nod[2][np], n4 = nod[3][np];
+        if (nt == 3) {
+            double xc = (x[n1] + x[n2] + x[n3] + x[n4]) * 0.25;
+            dd[np] = std::fabs(xmax - xc);
+        } else if (nt == 51) {
+            double yc = (y[n1] + y[n2] + y[n3] + y[n4]) * 0.25;
+            dd[np] = (yc > 0) ? std::fabs(ymax - yc) : std::fabs(ymin - yc);
+        } else if (nt == 53) {
+            double zc = (z[n1] + z[n2] + z[n3] + z[n4]) * 0.25;
+            dd[np] = (zc > (double)0.1f) ? std::fabs(zmax - zc) : std::fabs(zmin - zc);
+        }
+    }
+    // --- aliasing: ghost slots that are elements, repeated, or ghost parents ---
+    {
+        std::vector<char> seen(ntot + 1, 0);
+        int al = 0;
+        for (int g = 0; g < nghosts && !al; g++) {
+            if (gid[g] <= neles || seen[gid[g]]) al = 1;
+            seen[gid[g]] = 1;
+        }
+        for (int g = 0; g < nghosts && !al; g++)
+            if (gpar[g] > neles || seen[gpar[g]]) al = 1;
+        // neighbours in the ghost range must be ghost slots that exist
+        for (int e = 1; e <= neles && !al; e++)
+            for (int k = 0; k < 4; k++)
+                if (nc[k][e] > neles && !seen[nc[k][e]]) { al = 1; break; }
+        h->aliased = al;
+    }
+    // --- internal order: space-filling curve over element centroids ---
+    std::vector<int> perm(neles + 1);   // 1-based reference id -> 0-based internal
+    std::iota(perm.begin(), perm.end(), -1);
+    if (params->renumber && !h->aliased) {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int i = 1; i <= neles; i++) {
+            double p[3] = {xcel[i], ycel[i], zcel[i]};
+            for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], p[d]); hi[d] = std::max(hi[d], p[d]); }
+        }
+        std::vector<std::pair<uint32_t, int>> key(neles);
+        for (int i = 1; i <= neles; i++) {
+            double p[3] = {xcel[i], ycel[i], zcel[i]};
+            uint32_t q[3];
+            for (int d = 0; d < 3; d++) {
+                double t = (hi[d] > lo[d]) ? (p[d] - lo[d]) / (hi[d] - lo[d]) : 0.0;
+                q[d] = (uint32_t)std::min(1023.0, std::max(0.0, t * 1023.0));
+            }
+            key[i - 1] = {spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2), i};
+        }
+        std::stable_sort(key.begin(), key.end());
+        for (int r = 0; r < neles; r++) perm[key[r].second] = r;
+    }
+    auto map = [&](int id1) -> int { return id1 <= neles ? perm[id1] : id1 - 1; };
+    h->perm.assign(neles, 0);
+    for (int i = 1; i <= neles; i++) h->perm[i - 1] = perm[i];
+    h->ghost_id.resize(nghosts);
+    for (int g = 0; g < nghosts; g++) h->ghost_id[g] = map(gid[g]);
+
+    // --- device layout ---
+    const long long ld = ((long long)ntot + 63) / 64 * 64;
+    h->ld = ld;
+    std::vector<int> hnc(4 * ld, 0), hsnb(4 * ld, 0), hib(ld, 0), hgpar(nghosts), hgid(nghosts), hgtyp(nghosts);
+    std::vector<unsigned> hfk(ld, 0u);
+    std::vector<double> hx(ld, 0.0), hy(ld, 0.0), hz(ld, 0.0), hvol(ld, 0.0), hdl(ld, 0.0), hdd(ld, 0.0);
+    std::vector<double> hsc(12 * ld, 0.0), hfch(12 * ld, 0.0), hfcv(12 * ld, 0.0);
+    std::vector<int> slot_parent(ntot + 1, 0);
+    for (int g = 0; g < nghosts; g++) slot_parent[gid[g]] = gpar[g];
+    for (int i = 1; i <= ntot; i++) {
+        int t = map(i);
+        hx[t] = xcel[i]; hy[t] = ycel[i]; hz[t] = zcel[i]; hvol[t] = vol[i]; hdd[t] = dd[i];
+        if (i <= neles) {
+            hdl[t] = dl[i];
+            hib[t] = iblank[i];
+            unsigned fk = 0;
+            for (int k = 0; k < 4; k++) {
+                int nb = nc[k][i];
+                hnc[k * ld + t] = map(nb);
+                int snb = nb;
+                if (!h->aliased && nb > neles) snb = slot_parent[nb];
+                hsnb[k * ld + t] = h->aliased ? map(nb) : map(snb);
+                int nt = 0;
+                if (nb > neles && nb <= neles + nghosts) nt = gtyp[nb - neles - 1];
+                unsigned kind = 0;
+                if (nt == 5) kind |= FK_WALL;
+                if (nb <= neles || nb > neles + nghosts) kind |= FK_RECON;
+                fk |= kind << (4 * k);
+            }
+            hfk[t] = fk;
+            for (int k = 0; k < 12; k++) {
+                hsc[k * ld + t] = SC(k, i); hfch[k * ld + t] = FCH(k, i); hfcv[k * ld + t] = FCV(k, i);
+            }
+        } else {
+            for (int k = 0; k < 4; k++) { hnc[k * ld + t] = map(nc[k][i]); hsnb[k * ld + t] = map(nc[k][i]); }
+        }
+    }
+    for (int g = 0; g < nghosts; g++) { hgpar[g] = map(gpar[g]); hgid[g] = map(gid[g]); hgtyp[g] = gtyp[g]; }
+
+    // --- parameters ---
+    const hp_params& p = h->prm;
+    DevParams& P = h->dp;
+    P.gamag = p.gamag; P.gamap = p.gamap; P.pinf = p.pinf; P.cpp = p.cpp; P.cpg = p.cpg; P.prg = p.prg;
+    P.rrg = 287.0; P.prp = 10.0;
+    P.emin = p.epslnmin; P.emax = p.epslnmax; P.phipzero = p.phipzero;
+    P.ugmin = p.ugmin; P.vgmin = p.vgmin; P.wgmin = p.wgmin;
+    P.upmin = p.upmin; P.vpmin = p.vpmin; P.wpmin = p.wpmin;
+    P.tgmin = p.tgmin; P.tpmin = p.tpmin; P.pmin = p.pmin;
+    P.as = p.as; P.ts = p.ts;
+    P.c23 = (double)(2.00f / 3.00f); P.co2 = (double)(1.00f / 16.00f); P.co4 = (double)(1.00f / 1024.00f);
+    P.fsd = 4.0 * p.surfacetension / p.diap;
+    P.cfl = p.cfl; P.venkat_k = p.venkat_k > 0 ? p.venkat_k : 0.3; P.twall = p.twall; P.amup = 0.001;
+    P.rk_scheme = p.rk_scheme; P.inviscid = p.inviscid; P.myorder = p.myorder;
+    P.nstage = p.rk_scheme == 0 ? 4 : 3;
+    switch (p.precision) {
+        case HP_PREC_FP64_PARITY: h->var = &variant_fp64_parity; break;
+        case HP_PREC_FP64: h->var = &variant_fp64; break;
+        case HP_PREC_MIXED: h->var = &variant_mixed; break;
+        default: delete h; return fail(nullptr, HP_E_ARG, "unknown precision mode");
+    }
+
+    // --- device memory: one arena ---
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { delete h; return fail(nullptr, HP_E_CUDA, "no CUDA device"); }
+    h->device = dev;
+    const size_t D = sizeof(double), I = sizeof(int), gb = h->var->grad_bytes;
+    Arena& A = h->arena;
+    auto plan = [&](Arena& a) {
+        DevMesh& m = h->dm;
+        m.nc = (int*)a.take(4 * ld * I); m.snb = (int*)a.take(4 * ld * I);
+        m.fk = (unsigned*)a.take(ld * sizeof(unsigned)); m.iblank = (int*)a.take(ld * I);
+        m.xc = (double*)a.take(ld * D); m.yc = (double*)a.take(ld * D); m.zc = (double*)a.take(ld * D);
+        m.vol = (double*)a.take(ld * D); m.dl = (double*)a.take(ld * D); m.dd = (double*)a.take(ld * D);
+        m.sc = (double*)a.take(12 * ld * D); m.fch = (double*)a.take(12 * ld * D);
+        m.fcv = (double*)a.take(12 * ld * D);
+        m.g_par = (int*)a.take((nghosts + 1) * (size_t)I); m.g_id = (int*)a.take((nghosts + 1) * (size_t)I);
+        m.g_type = (int*)a.take((nghosts + 1) * (size_t)I);
+        DevState<double>& s = h->ds;
+        s.cn = (double*)a.take(10 * ld * D); s.cu = (double*)a.take(10 * ld * D);
+        s.cn1 = (double*)a.take(10 * ld * D); s.pr = (double*)a.take(NPR * ld * D);
+        s.gr = (double*)a.take(NGR * ld * gb); s.phi = (double*)a.take(ld * D);
+        s.anu = (double*)a.take(2 * ld * D); s.d2q = (double*)a.take(10 * ld * D);
+        s.d24 = (double*)a.take(10 * ld * D); s.vis = (double*)a.take(8 * ld * D);
+        s.egt = (double*)a.take(2 * ld * D);
+        s.s = (DevScalars*)a.take(sizeof(DevScalars));
+        s.diag = (double*)a.take((size_t)h->max_diag * 8 * D);
+        s.max_diag = h->max_diag;
+    };
+    Arena probe;
+    plan(probe);
+    A.size = probe.used + 256;
+    size_t freeb = 0, totalb = 0;
+    cudaMemGetInfo(&freeb, &totalb);
+    if (A.size > freeb) {
+        delete h;
+        return fail(nullptr, HP_E_NOMEM, "case needs " + std::to_string(A.size >> 20) + " MiB, " +
+                                             std::to_string(freeb >> 20) + " MiB free");
+    }
+    if (cudaMalloc((void**)&A.base, A.size) != cudaSuccess) {
+        delete h;
+        return fail(nullptr, HP_E_NOMEM, "cudaMalloc of the case arena failed");
+    }
+    A.used = 0;
+    plan(A);
+    DevMesh& m = h->dm;
+    m.neles = neles; m.nghosts = nghosts; m.ntot = ntot; m.aliased = h->aliased; m.ld = ld;
+    m.cell1 = perm[1];
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaFree(A.base);
+        delete h;
+        return fail(nullptr, HP_E_CUDA, "stream creation failed");
+    }
+    cudaStream_t st = h->stream;
+    auto up = [&](const void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, st);
+    };
+    cudaError_t e = cudaMemsetAsync(A.base, 0, A.size, st);
+    if (e == cudaSuccess) e = up(m.nc, hnc.data(), 4 * ld * I);
+    if (e == cudaSuccess) e = up(m.snb, hsnb.data(), 4 * ld * I);
+    if (e == cudaSuccess) e = up(m.fk, hfk.data(), ld * sizeof(unsigned));
+    if (e == cudaSuccess) e = up(m.iblank, hib.data(), ld * I);
+    if (e == cudaSuccess) e = up(m.xc, hx.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.yc, hy.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.zc, hz.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.vol, hvol.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.dl, hdl.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.dd, hdd.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.sc, hsc.data(), 12 * ld * D);
+    if (e == cudaSuccess) e = up(m.fch, hfch.data(), 12 * ld * D);
+    if (e == cudaSuccess) e = up(m.fcv, hfcv.data(), 12 * ld * D);
+    if (e == cudaSuccess && nghosts) e = up(m.g_par, hgpar.data(), nghosts * (size_t)I);
+    if (e == cudaSuccess && nghosts) e = up(m.g_id, hgid.data(), nghosts * (size_t)I);
+    if (e == cudaSuccess && nghosts) e = up(m.g_type, hgtyp.data(), nghosts * (size_t)I);
+    if (e == cudaSuccess) {
+        DevScalars s0{};
+        s0.dtmin_bits = 0;
+        double v = 1.0e8;
+        std::memcpy(&s0.dtmin_bits, &v, 8);
+        e = cudaMemcpy(h->ds.s, &s0, sizeof s0, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_diag, (size_t)h->max_diag * 8 * D);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_scal, sizeof(DevScalars));
+    if (e != cudaSuccess) {
+        std::string msg = std::string("device upload failed: ") + cudaGetErrorString(e);
+        hp_destroy(h);
+        return fail(nullptr, HP_E_CUDA, msg);
+    }
+    *out = h;
+    return HP_OK;
+}
+
+extern "C" int hp_destroy(hp_handle* h) {
+    if (!h) return HP_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->arena.base) cudaFree(h->arena.base);
+    if (h->h_diag) cudaFreeHost(h->h_diag);
+    if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return HP_OK;
+}
+
+// Upload cu (elements, reference order, column-major) and set cn = cu.
+static int upload_state(hp_handle* h, double time, const double* cu_elem, const double* ghost_prims) {
+    const long long ld = h->ld;
+    const int ne = h->neles, ng = h->nghosts;
+    std::vector<double> cu(10 * ld, 0.0);
+    for (int k = 0; k < 10; k++)
+        for (int i = 0; i < ne; i++) cu[k * ld + h->perm[i]] = cu_elem[(size_t)k * ne + i];
+    cudaStream_t st = h->stream;
+    CUDA_OK(h, cudaStreamSynchronize(st));
+    CUDA_OK(h, cudaMemcpyAsync(h->ds.cu, cu.data(), 10 * ld * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(h, cudaMemcpyAsync(h->ds.cn, cu.data(), 10 * ld * sizeof(double), cudaMemcpyHostToDevice, st));
+    // primitives: zero, then the restart's ghost values (src/main.F90:433-438)
+    std::vector<double> pr(NPR * ld, 0.0);
+    if (ghost_prims) {
+        const int cols[6] = {P_UG, P_VG, P_WG, P_PG, P_TG, P_ROG};
+        for (int v = 0; v < 6; v++)
+            for (int g = 0; g < ng; g++) pr[cols[v] * ld + h->ghost_id[g]] = ghost_prims[(size_t)v * ng + g];
+    }
+    CUDA_OK(h, cudaMemcpyAsync(h->ds.pr, pr.data(), NPR * ld * sizeof(double), cudaMemcpyHostToDevice, st));
+    DevScalars s0{};
+    double v = 1.0e8;
+    std::memcpy(&s0.dtmin_bits, &v, 8);
+    s0.time = time;
+    *h->h_scal = s0;
+    CUDA_OK(h, cudaMemcpyAsync(h->ds.s, h->h_scal, sizeof s0, cudaMemcpyHostToDevice, st));
+    CUDA_OK(h, cudaStreamSynchronize(st));
+    h->started = false;
+    h->have_state = true;
+    return HP_OK;
+}
+
+extern "C" int hp_init_uniform(hp_handle* h) {
+    if (!h) return HP_E_ARG;
+    const hp_params& p = h->prm;
+    const double rrg = 287.0;
+    // src/main.F90:397-402 and src/sr_init_cond.F90:177-195
+    double rogmin = p.pmin / (rrg * p.tgmin);
+    double ropmin = (p.pmin + p.pinf) * p.gamap / ((p.gamap - 1.0) * p.cpp * p.tpmin);
+    double egtmin = rrg * p.tgmin / (p.gamag - 1.0) + 0.5 * (sq(p.ugmin) + sq(p.vgmin) + sq(p.wgmin));
+    double eptmin = (p.cpp * p.tpmin) / p.gamap + p.pinf / ropmin + 0.5 * (sq(p.upmin) + sq(p.vpmin) + sq(p.wpmin));
+    const int ne = h->neles;
+    std::vector<double> cu(10 * (size_t)ne);
+    double phip = p.epslninf, phig = 1 - p.epslninf;
+    double v[10] = {phig * rogmin, phig * rogmin * p.ugmin, phig * rogmin * p.vgmin, phig * rogmin * p.wgmin,
+                    phig * rogmin * egtmin, phip * ropmin, phip * ropmin * p.upmin, phip * ropmin * p.vpmin,
+                    phip * ropmin * p.wpmin, phip * ropmin * eptmin};
+    for (int k = 0; k < 10; k++)
+        for (int i = 0; i < ne; i++) cu[(size_t)k * ne + i] = v[k];
+    return upload_state(h, 0.0, cu.data(), nullptr);
+}
+
+extern "C" int hp_set_state(hp_handle* h, double time, const double* cu_elem, const double* ghost_prims) {
+    if (!h || !cu_elem) return HP_E_ARG;
+    return upload_state(h, time, cu_elem, ghost_prims);
+}
+
+static int run_steps(hp_handle* h, int n) {
+    cudaStream_t st = h->stream;
+    const int block = h->prm.block_size;
+    if (!h->started) {
+        h->var->enqueue_start(h->dm, &h->ds, h->dp, st, block, nullptr);
+        h->started = true;
+    }
+    if (h->prm.use_graph) {
+        if (!h->gexec) {
+            CUDA_OK(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            h->var->enqueue_step(h->dm, &h->ds, h->dp, st, block, nullptr);
+            CUDA_OK(h, cudaStreamEndCapture(st, &h->graph));
+            CUDA_OK(h, cudaGraphInstantiate(&h->gexec, h->graph, 0));
+        }
+        for (int k = 0; k < n; k++) CUDA_OK(h, cudaGraphLaunch(h->gexec, st));
+    } else {
+        for (int k = 0; k < n; k++) h->var->enqueue_step(h->dm, &h->ds, h->dp, st, block, nullptr);
+    }
+    CUDA_OK(h, cudaGetLastError());
+    return HP_OK;
+}
+
+extern "C" int hp_step(hp_handle* h, int32_t nsteps, hp_diag* diag) {
+    if (!h || nsteps < 0) return HP_E_ARG;
+    if (!h->have_state) return fail(h, HP_E_STATE, "hp_step before hp_init_uniform/hp_set_state");
+    int done = 0;
+    while (done < nsteps) {
+        int chunk = std::min(nsteps - done, h->max_diag);
+        CUDA_OK(h, cudaMemsetAsync(&h->ds.s->step_in_call, 0, sizeof(int), h->stream));
+        int rc = run_steps(h, chunk);
+        if (rc) return rc;
+        if (diag) {
+            CUDA_OK(h, cudaMemcpyAsync(h->h_diag, h->ds.diag, (size_t)chunk * 8 * sizeof(double),
+                                       cudaMemcpyDeviceToHost, h->stream));
+            CUDA_OK(h, cudaStreamSynchronize(h->stream));
+            for (int k = 0; k < chunk; k++) {
+                const double* d = h->h_diag + 8 * (size_t)k;
+                hp_diag& o = diag[done + k];
+                o.time = d[0]; o.dt = d[1]; o.velmag = d[2];
+                for (int j = 0; j < 4; j++) o.diff[j] = d[3 + j];
+                o.nan_cells = d[7];
+            }
+        }
+        done += chunk;
+    }
+    return HP_OK;
+}
+
+extern "C" int hp_step_timed(hp_handle* h, int32_t nsteps, double* device_ms) {
+    if (!h || nsteps < 0 || !device_ms) return HP_E_ARG;
+    if (!h->have_state) return fail(h, HP_E_STATE, "hp_step_timed before the state is set");
+    cudaEvent_t a, b;
+    CUDA_OK(h, cudaEventCreate(&a));
+    CUDA_OK(h, cudaEventCreate(&b));
+    if (!h->started) {   // the first step's start-of-step pass is not timed
+        h->var->enqueue_start(h->dm, &h->ds, h->dp, h->stream, h->prm.block_size, nullptr);
+        h->started = true;
+    }
+    CUDA_OK(h, cudaMemsetAsync(&h->ds.s->step_in_call, 0, sizeof(int), h->stream));
+    CUDA_OK(h, cudaEventRecord(a, h->stream));
+    int rc = run_steps(h, nsteps);
+    CUDA_OK(h, cudaEventRecord(b, h->stream));
+    CUDA_OK(h, cudaEventSynchronize(b));
+    float ms = 0.f;
+    CUDA_OK(h, cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *device_ms = ms;
+    return rc;
+}
+
+namespace {
+struct ProfCtx {
+    cudaStream_t st;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;
+    cudaError_t err = cudaSuccess;
+};
+void prof_mark(void* c, int kind) {
+    auto* p = static_cast<ProfCtx*>(c);
+    cudaEvent_t e;
+    cudaError_t r = cudaEventCreate(&e);
+    if (r == cudaSuccess) r = cudaEventRecord(e, p->st);
+    if (r != cudaSuccess) { p->err = r; return; }
+    p->ev.push_back(e);
+    p->kind.push_back(kind);
+}
+}  // namespace
+
+extern "C" int hp_profile_steps(hp_handle* h, int32_t nsteps, double* ms_per_kind, int64_t* launches_per_kind,
+                                int32_t nkinds) {
+    if (!h || nsteps <= 0 || !ms_per_kind || !launches_per_kind || nkinds < (int)KK_COUNT) return HP_E_ARG;
+    if (!h->have_state) return fail(h, HP_E_STATE, "hp_profile_steps before the state is set");
+    for (int k = 0; k < nkinds; k++) { ms_per_kind[k] = 0.0; launches_per_kind[k] = 0; }
+    ProfCtx ctx;
+    ctx.st = h->stream;
+    StepHook hook{prof_mark, &ctx};
+    if (!h->started) {
+        h->var->enqueue_start(h->dm, &h->ds, h->dp, h->stream, h->prm.block_size, nullptr);
+        h->started = true;
+    }
+    CUDA_OK(h, cudaMemsetAsync(&h->ds.s->step_in_call, 0, sizeof(int), h->stream));
+    for (int k = 0; k < nsteps; k++) {
+        h->var->enqueue_step(h->dm, &h->ds, h->dp, h->stream, h->prm.block_size, &hook);
+        if (ctx.err != cudaSuccess) break;
+    }
+    CUDA_OK(h, ctx.err);
+    CUDA_OK(h, cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i + 1 < ctx.ev.size(); i++) {
+        int kd = ctx.kind[i];
+        if (kd >= (int)KK_COUNT) continue;
+        float ms = 0.f;
+        CUDA_OK(h, cudaEventElapsedTime(&ms, ctx.ev[i], ctx.ev[i + 1]));
+        ms_per_kind[kd] += ms;
+        launches_per_kind[kd] += 1;
+    }
+    for (auto e : ctx.ev) cudaEventDestroy(e);
+    return HP_OK;
+}
+
+extern "C" int hp_sync(hp_handle* h) {
+    if (!h) return HP_E_ARG;
+    CUDA_OK(h, cudaStreamSynchronize(h->stream));
+    return HP_OK;
+}
+
+extern "C" int hp_get_state(hp_handle* h, double* time, double* cu_elem, double* ghost_prims) {
+    if (!h) return HP_E_ARG;
+    const long long ld = h->ld;
+    const int ne = h->neles, ng = h->nghosts;
+    cudaStream_t st = h->stream;
+    if (time) {
+        CUDA_OK(h, cudaMemcpyAsync(h->h_scal, h->ds.s, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    }
+    std::vector<double> cu, pr;
+    if (cu_elem) {
+        cu.resize(10 * ld);
+        CUDA_OK(h, cudaMemcpyAsync(cu.data(), h->ds.cu, 10 * ld * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    if (ghost_prims) {
+        pr.resize(NPR * ld);
+        CUDA_OK(h, cudaMemcpyAsync(pr.data(), h->ds.pr, NPR * ld * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_OK(h, cudaStreamSynchronize(st));
+    if (time) *time = h->h_scal->time;
+    if (cu_elem)
+        for (int k = 0; k < 10; k++)
+            for (int i = 0; i < ne; i++) cu_elem[(size_t)k * ne + i] = cu[k * ld + h->perm[i]];
+    if (ghost_prims) {
+        const int cols[6] = {P_UG, P_VG, P_WG, P_PG, P_TG, P_ROG};
+        for (int v = 0; v < 6; v++)
+            for (int g = 0; g < ng; g++) ghost_prims[(size_t)v * ng + g] = pr[cols[v] * ld + h->ghost_id[g]];
+    }
+    return HP_OK;
+}
+
+extern "C" int hp_get_prims(hp_handle* h, double* prims) {
+    if (!h || !prims) return HP_E_ARG;
+    const long long ld = h->ld;
+    const int ne = h->neles;
+    std::vector<double> pr(NPR * ld);
+    CUDA_OK(h, cudaMemcpyAsync(pr.data(), h->ds.pr, NPR * ld * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OK(h, cudaStreamSynchronize(h->stream));
+    for (int v = 0; v < NPR; v++)
+        for (int i = 0; i < ne; i++) prims[(size_t)v * ne + i] = pr[v * ld + h->perm[i]];
+    return HP_OK;
+}
+
+extern "C" int hp_device_state(hp_handle* h, double** cu_dev, int64_t* ld) {
+    if (!h) return HP_E_ARG;
+    if (cu_dev) *cu_dev = h->ds.cu;
+    if (ld) *ld = h->ld;
+    return HP_OK;
+}
+
+extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* device_bytes, int64_t* aliased) {
+    if (!h) return HP_E_ARG;
+    if (kernels_per_step) {
+        // k_step_begin, smooth x2, bc, visc, stages x (prim, bc, grad, flux), prim end,
+        // k_step_end, prim start
+        int64_t n = 1 + 2 + (h->nghosts ? 1 : 0) + (h->prm.inviscid ? 0 : 1);
+        int64_t per_stage = 1 + (h->nghosts ? 1 : 0) + (h->prm.myorder == 2 ? 1 : 0) + 1;
+        if (h->aliased) per_stage += (h->prm.myorder == 2 ? 1 : 0) + 1;
+        n += (int64_t)h->dp.nstage * per_stage + 3;
+        if (h->aliased) n += 2;
+        *kernels_per_step = n;
+    }
+    if (device_bytes) *device_bytes = (int64_t)h->arena.size;
+    if (aliased) *aliased = h->aliased;
+    return HP_OK;
+}

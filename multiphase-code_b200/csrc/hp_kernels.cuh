@@ -1,0 +1,1193 @@
+// hp_kernels.cuh -- sm_100a kernels of the explicit residual-and-update step.
+//
+// Included once per precision variant with HP_NS (namespace) and HP_R (the
+// arithmetic type of gradients, limiter, reconstruction, HLLC, sources and
+// viscous fluxes) defined.  Primitive recovery through the stiffened-gas
+// pressure-equilibrium quadratic, the RK state update and the dt / residual
+// reductions are FP64 in every variant.
+//
+// Every kernel is cell-centric: one thread owns one cell, evaluates its own 4
+// faces in local face order 1..4 and writes only that cell.  This keeps the
+// reference's per-cell summation order (src/sr_hllcbatten.F90:77-555), so the
+// parity variant (compiled with -fmad=false) reproduces the CPU reference
+// bit for bit, and it needs no atomics.
+#include <cfloat>
+#include <cmath>
+
+#include "hp_device.h"
+
+namespace hp {
+namespace HP_NS {
+
+using R = HP_R;
+
+// ---------------------------------------------------------------------------
+// Fortran MIN/MAX as the reference's build evaluates them: a NaN argument is
+// skipped unless it is the first (pinned by the shipped Velocity.dat).
+template <class T> __device__ __forceinline__ T mn2(T a, T b) { return (b < a || a != a) ? b : a; }
+template <class T> __device__ __forceinline__ T mx2(T a, T b) { return (b > a || a != a) ? b : a; }
+
+// det() of src/mod_MatrixOps.F90:4-9
+template <class T>
+__device__ __forceinline__ T det3(T A11, T A21, T A31, T A12, T A22, T A32, T A13, T A23, T A33) {
+    return A11 * (A22 * A33 - A23 * A32) - A21 * (A12 * A33 - A13 * A32) + A31 * (A12 * A23 - A13 * A22);
+}
+// fvenkat() of src/mod_MatrixOps.F90:12-18
+template <class T>
+__device__ __forceinline__ T fvenkat(T delp, T delm, T epssq) {
+    return (((delp * delp + epssq) * delm + T(2) * delm * delm * delp) /
+            (delp * delp + T(2) * delm * delm + delp * delm + epssq)) / delm;
+}
+
+// (K dl)^3 rounded once: Dekker's exact product splits a*a and (a*a)*a into
+// head + tail with fma, then one final rounding of the sum.  Matches a
+// correctly rounded pow(a, 3) except in near-tie cases.
+__device__ __forceinline__ double cube_rn(double a) {
+    double p = a * a;
+    double pe = fma(a, a, -p);
+    double h = p * a;
+    double he = fma(p, a, -h);
+    return h + (he + pe * a);
+}
+__device__ __forceinline__ float cube_rn(float a) { return (float)cube_rn((double)a); }
+
+template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
+
+#define COL(ptr, k) ((ptr) + (size_t)(k) * (size_t)m.ld)
+
+// ---------------------------------------------------------------------------
+// Primitive recovery, src/sr_primitive.F90:23-161 (== the element loop of
+// src/sr_primitiveplusbc.F90:36-172 without ag/ap).  c[] is renormalised.
+struct PrimV {
+    double ug, vg, wg, tg, pg, pp, phig, phip, up, vp, wp, tp, rog, rop;
+};
+
+__device__ __forceinline__ void blend_phases(const DevParams& P, double& phig, double& phip,
+                                             double& ug, double& vg, double& wg, double& tg,
+                                             double& pg, double& up, double& vp, double& wp,
+                                             double& tp, double& pp) {
+    const double emin = P.emin, emax = P.emax;
+    if (phig < emin) {
+        phig = emin; phip = 1.0 - phig;
+        ug = up; vg = vp; wg = wp; tg = tp; pg = pp;
+    }
+    if (phip < emin) {
+        phip = emin; phig = 1.0 - phip;
+        up = ug; vp = vg; wp = wg; tp = tg; pp = pg;
+    }
+    if (phig >= emin && phig <= emax) {
+        double psig = (phig - emin) / (emax - emin);
+        double f = -(psig * psig * (2.0 * psig - 3.0));
+        ug = f * ug + (1.0 - f) * up;
+        vg = f * vg + (1.0 - f) * vp;
+        wg = f * wg + (1.0 - f) * wp;
+        tg = f * tg + (1.0 - f) * tp;
+        pg = f * pg + (1.0 - f) * pp;
+    }
+    if (phip >= emin && phip <= emax) {
+        double psig = (phip - emin) / (emax - emin);
+        double f = -(psig * psig * (2.0 * psig - 3.0));
+        up = f * up + (1.0 - f) * ug;
+        vp = f * vp + (1.0 - f) * vg;
+        wp = f * wp + (1.0 - f) * wg;
+        tp = f * tp + (1.0 - f) * tg;
+        pp = f * pp + (1.0 - f) * pg;
+    }
+}
+
+__device__ __forceinline__ void prim_full(double c[10], PrimV& q, const DevParams& P) {
+    const double gamag = P.gamag, gamap = P.gamap, pinf = P.pinf;
+    q.ug = c[1] / c[0]; q.vg = c[2] / c[0]; q.wg = c[3] / c[0];
+    q.up = c[6] / c[5]; q.vp = c[7] / c[5]; q.wp = c[8] / c[5];
+    double eg = c[4] / c[0] - 0.5 * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+    double ep = c[9] / c[5] - 0.5 * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
+    double bbb = (P.fsd + pinf * gamap) - (c[0] * (gamag - 1.0) * eg) - (c[5] * (gamap - 1.0) * ep);
+    double ccc = c[0] * (gamag - 1.0) * eg * (P.fsd + pinf * gamap);
+    q.pg = (-bbb + sqrt(bbb * bbb + 4.0 * ccc)) * 0.5;
+    q.pp = q.pg + P.fsd;
+    q.phig = (c[0] * (gamag - 1.0) * eg) / q.pg;
+    q.phip = 1.0 - q.phig;
+    q.rog = c[0] / q.phig;
+    q.rop = c[5] / q.phip;
+    q.tg = q.pg / (q.rog * P.rrg);
+    q.tp = ((q.pp + pinf) * gamap) / ((gamap - 1.0) * q.rop * P.cpp);
+    blend_phases(P, q.phig, q.phip, q.ug, q.vg, q.wg, q.tg, q.pg, q.up, q.vp, q.wp, q.tp, q.pp);
+    q.rog = q.pg / (P.rrg * q.tg);
+    q.rop = (q.pp + pinf) * gamap / ((gamap - 1.0) * P.cpp * q.tp);
+    double eg2 = q.pg / ((gamag - 1.0) * q.rog);
+    double ep2 = (q.pp + gamap * pinf) / ((gamap - 1.0) * q.rop);
+    double egt = eg2 + 0.5 * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+    double ept = ep2 + 0.5 * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
+    c[0] = q.phig * q.rog;
+    c[1] = q.phig * q.rog * q.ug;
+    c[2] = q.phig * q.rog * q.vg;
+    c[3] = q.phig * q.rog * q.wg;
+    c[4] = q.phig * q.rog * egt;
+    c[5] = q.phip * q.rop;
+    c[6] = q.phip * q.rop * q.up;
+    c[7] = q.phip * q.rop * q.vp;
+    c[8] = q.phip * q.rop * q.wp;
+    c[9] = q.phip * q.rop * ept;
+}
+
+__device__ __forceinline__ void store_prims(const DevMesh& m, double* pr, int i, const PrimV& q) {
+    COL(pr, P_UG)[i] = q.ug; COL(pr, P_VG)[i] = q.vg; COL(pr, P_WG)[i] = q.wg;
+    COL(pr, P_TG)[i] = q.tg; COL(pr, P_PG)[i] = q.pg; COL(pr, P_PP)[i] = q.pp;
+    COL(pr, P_PHIG)[i] = q.phig; COL(pr, P_PHIP)[i] = q.phip;
+    COL(pr, P_UP)[i] = q.up; COL(pr, P_VP)[i] = q.vp; COL(pr, P_WP)[i] = q.wp;
+    COL(pr, P_TP)[i] = q.tp; COL(pr, P_ROG)[i] = q.rog; COL(pr, P_ROP)[i] = q.rop;
+}
+
+// Block-wide min / max of 64-bit keys, then one atomic per block.
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+
+enum { PM_STAGE = 0, PM_START = 1, PM_END = 2 };
+
+// Element primitive pass.  PM_START adds the dt contribution of
+// src/main.F90:529-546; PM_END adds the max-norm residual of :605-611, the
+// cu = cn copy of :619-625 and |u_g(1)| of :641.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_prim(DevMesh m, DevState<R> s, DevParams P) {
+    __shared__ unsigned long long red[4][8];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long kmin = ~0ull, kd[4] = {0, 0, 0, 0}, nanc = 0;
+    if (i < m.neles) {
+        double c[10];
+#pragma unroll
+        for (int k = 0; k < 10; k++) c[k] = COL(s.cn, k)[i];
+        PrimV q;
+        prim_full(c, q, P);
+#pragma unroll
+        for (int k = 0; k < 10; k++) COL(s.cn, k)[i] = c[k];
+        store_prims(m, s.pr, i, q);
+        if (MODE == PM_START) {
+            double ag = sqrt((P.gamag * q.pg) / q.rog);
+            double ap = sqrt((P.gamap * (q.pp + P.pinf)) / q.rop);
+            double qg = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+            double qp = sqrt(q.up * q.up + q.vp * q.vp + q.wp * q.wp);
+            double x = ldg(m.dl + i) / (mx2(ag, ap) + mx2(qg, qp));
+            if (x == x) kmin = (unsigned long long)__double_as_longlong(x);
+        }
+        if (MODE == PM_END) {
+            bool bad = false;
+#pragma unroll
+            for (int k = 0; k < 10; k++) {
+                double u = COL(s.cu, k)[i];
+                if (k < 4) {
+                    double d = fabs(c[k] - u);
+                    if (d == d) kd[k] = (unsigned long long)__double_as_longlong(d);
+                }
+                bad |= (c[k] != c[k]);
+                COL(s.cu, k)[i] = c[k];
+            }
+            nanc = bad ? 1 : 0;
+            if (i == m.cell1) s.s->velmag = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+        }
+    }
+    if (MODE == PM_STAGE) return;
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (MODE == PM_START) {
+        kmin = warp_min_u64(kmin);
+        if (lane == 0) red[0][wid] = kmin;
+        __syncthreads();
+        if (wid == 0) {
+            unsigned long long v = lane < (int)(blockDim.x >> 5) ? red[0][lane] : ~0ull;
+            v = warp_min_u64(v);
+            if (lane == 0 && v != ~0ull) atomicMin(&s.s->dtmin_bits, v);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) kd[k] = warp_max_u64(kd[k]);
+        for (int o = 16; o > 0; o >>= 1) nanc += __shfl_xor_sync(0xffffffffu, nanc, o);
+        if (lane == 0) {
+            for (int k = 0; k < 4; k++) red[k][wid] = kd[k];
+        }
+        __shared__ unsigned long long nred[8];
+        if (lane == 0) nred[wid] = nanc;
+        __syncthreads();
+        if (wid == 0) {
+            int nw = blockDim.x >> 5;
+            for (int k = 0; k < 4; k++) {
+                unsigned long long v = lane < nw ? red[k][lane] : 0ull;
+                v = warp_max_u64(v);
+                if (lane == 0 && v) atomicMax(&s.s->diff_bits[k], v);
+            }
+            unsigned long long c = lane < nw ? nred[lane] : 0ull;
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0 && c) atomicAdd(&s.s->nan_count, c);
+        }
+    }
+}
+
+// dt = cfl * dtmin, time += dt (src/main.F90:521-556); one thread.
+__global__ void k_step_begin(DevState<R> s, DevParams P) {
+    DevScalars* S = s.s;
+    double dtmin = __longlong_as_double((long long)S->dtmin_bits);
+    S->dt = dtmin * P.cfl;
+    S->time = S->time + S->dt;
+    S->total = S->total + 1;
+    S->dtmin_bits = (unsigned long long)__double_as_longlong(1.0e8);
+}
+
+// per-step diagnostics and reset of the residual accumulators; one thread.
+__global__ void k_step_end(DevState<R> s) {
+    DevScalars* S = s.s;
+    int k = S->step_in_call;
+    if (k < s.max_diag) {
+        double* d = s.diag + 8 * (size_t)k;
+        d[0] = S->time; d[1] = S->dt; d[2] = S->velmag;
+        for (int j = 0; j < 4; j++) d[3 + j] = __longlong_as_double((long long)S->diff_bits[j]);
+        d[7] = (double)S->nan_count;
+    }
+    S->step_in_call = k + 1;
+    for (int j = 0; j < 4; j++) S->diff_bits[j] = 0ull;
+    S->nan_count = 0ull;
+}
+
+// ---------------------------------------------------------------------------
+// Ghost states per boundary type, src/sr_primitiveplusbc.F90:198-592
+// (VISC = false) and src/sr_viscousgp.F90:71-446 (VISC = true).  Types 6
+// (isothermal no-slip wall) and 7 (far field) are additions of this build.
+// Operates on one ghost-list entry; reads the parent's primitives and the
+// ghost's previous primitives.
+template <bool VISC>
+__device__ __forceinline__ void bc_one(const DevMesh& m, double* pr, double* egt, const DevParams& P,
+                                       int gidx, double dt, int total) {
+    const int np = m.g_par[gidx], ng = m.g_id[gidx], nt = m.g_type[gidx];
+    double* ug = COL(pr, P_UG); double* vg = COL(pr, P_VG); double* wg = COL(pr, P_WG);
+    double* tg = COL(pr, P_TG); double* pg = COL(pr, P_PG); double* pp = COL(pr, P_PP);
+    double* phig = COL(pr, P_PHIG); double* phip = COL(pr, P_PHIP);
+    double* up = COL(pr, P_UP); double* vp = COL(pr, P_VP); double* wp = COL(pr, P_WP);
+    double* tp = COL(pr, P_TP); double* rog = COL(pr, P_ROG); double* rop = COL(pr, P_ROP);
+    const double rrg = P.rrg, gamag = P.gamag, gamap = P.gamap, pinf = P.pinf, cpp = P.cpp;
+    if (nt == 2) {
+        phip[ng] = P.phipzero;
+        phig[ng] = 1.0 - phip[ng];
+        ug[ng] = P.ugmin; vg[ng] = P.vgmin; wg[ng] = P.wgmin;
+        tg[ng] = P.tgmin;
+        pg[ng] = pg[np];
+        rog[ng] = pg[ng] / (rrg * tg[ng]);
+        up[ng] = 0.99 * P.ugmin; vp[ng] = 0.99 * P.vgmin; wp[ng] = 0.99 * P.wgmin;
+        tp[ng] = P.tgmin;
+        pp[ng] = pp[np];
+        rop[ng] = gamap * (pg[ng] + pinf) / ((gamap - 1.0) * cpp * tp[ng]);
+    } else if (nt == 3) {
+        phig[ng] = phig[np];
+        phip[ng] = phip[np];
+        double dd = m.dd[np];
+        double wT = ug[np];
+        double wU = ug[np] + sqrt(gamag * pg[np] / rog[np]);
+        double alphaT = wT * dt / dd, alphaU = wU * dt / dd;
+        double fracT = 1 / (1 + alphaT), fracU = 1 / (1 + alphaU);
+        if (total == 1) {
+            ug[ng] = ug[np]; vg[ng] = vg[np]; wg[ng] = wg[np]; tg[ng] = tg[np]; pg[ng] = P.pmin;
+        }
+        if (ug[np] > ug[ng]) {
+            ug[ng] = ug[ng] * fracU + (1 - fracU) * (2.0 * ug[np] - ug[ng]);
+            vg[ng] = vg[ng] * fracT + (1 - fracT) * (2.0 * vg[np] - vg[ng]);
+            wg[ng] = wg[ng] * fracT + (1 - fracT) * (2.0 * wg[np] - wg[ng]);
+            tg[ng] = tg[ng] * fracT + (1 - fracT) * (2.0 * tg[np] - tg[ng]);
+        } else {
+            ug[ng] = ug[np]; vg[ng] = vg[np]; wg[ng] = wg[np]; tg[ng] = tg[np];
+        }
+        pg[ng] = P.pmin;
+        rog[ng] = pg[ng] / (rrg * tg[ng]);
+        vp[ng] = vp[np]; up[ng] = up[np]; wp[ng] = wp[np];
+        pp[ng] = P.pmin;
+        tp[ng] = tp[np];
+        rop[ng] = gamap * (pp[ng] + pinf) / ((gamap - 1.0) * cpp * tp[ng]);
+    } else if (nt == 5) {
+        phig[ng] = phig[np];
+        ug[ng] = -ug[np]; vg[ng] = -vg[np]; wg[ng] = -wg[np];
+        tg[ng] = tg[np];
+        phip[ng] = phip[np];
+        up[ng] = -up[np]; vp[ng] = -vp[np]; wp[ng] = -wp[np];
+        tp[ng] = tp[np];
+        pg[ng] = pg[np]; pp[ng] = pp[np];
+        rog[ng] = pg[ng] / (rrg * tg[ng]);
+        rop[ng] = gamap * (pp[ng] + pinf) / ((gamap - 1.0) * cpp * tp[ng]);
+    } else if (nt == 51 || nt == 53) {
+        const bool ylat = (nt == 51);
+        double* vn = ylat ? vg : wg;
+        double* t2 = ylat ? wg : vg;
+        double dd = m.dd[np];
+        double wT = vn[np];
+        double alphaT = wT * dt / dd;
+        double fracT = 1 / (1 + alphaT);
+        if (vn[np] > vn[ng]) {
+            if (VISC && !ylat) vn[ng] = -vn[ng];   // src/sr_viscousgp.F90:408
+            else vn[ng] = -vn[np];
+            ug[ng] = ug[ng] * fracT + (1 - fracT) * (2.0 * ug[np] - ug[ng]);
+            t2[ng] = t2[ng] * fracT + (1 - fracT) * (2.0 * t2[np] - t2[ng]);
+            tg[ng] = tg[ng] * fracT + (1 - fracT) * (2.0 * tg[np] - tg[ng]);
+        } else {
+            ug[ng] = ug[np]; vn[ng] = -vn[np]; t2[ng] = t2[np]; tg[ng] = tg[np];
+        }
+        pg[ng] = pg[np];
+        phig[ng] = phig[np];
+        phip[ng] = phip[np];
+        up[ng] = up[np]; vp[ng] = vp[np]; wp[ng] = wp[np];
+        if (ylat) vp[ng] = -vp[np]; else wp[ng] = -wp[np];
+        tp[ng] = tp[np];
+        pp[ng] = pp[np];
+        rog[ng] = pg[ng] / (rrg * tg[ng]);
+        rop[ng] = gamap * (pp[ng] + pinf) / ((gamap - 1.0) * cpp * tp[ng]);
+    } else if (nt == 6) {
+        phig[ng] = phig[np]; phip[ng] = phip[np];
+        ug[ng] = -ug[np]; vg[ng] = -vg[np]; wg[ng] = -wg[np];
+        up[ng] = -up[np]; vp[ng] = -vp[np]; wp[ng] = -wp[np];
+        tg[ng] = 2.0 * P.twall - tg[np];
+        tp[ng] = 2.0 * P.twall - tp[np];
+        pg[ng] = pg[np]; pp[ng] = pp[np];
+        rog[ng] = pg[ng] / (rrg * tg[ng]);
+        rop[ng] = gamap * (pp[ng] + pinf) / ((gamap - 1.0) * cpp * tp[ng]);
+    } else if (nt == 7) {
+        phip[ng] = P.phipzero; phig[ng] = 1.0 - phip[ng];
+        ug[ng] = P.ugmin; vg[ng] = P.vgmin; wg[ng] = P.wgmin;
+        up[ng] = P.upmin; vp[ng] = P.vpmin; wp[ng] = P.wpmin;
+        tg[ng] = P.tgmin; tp[ng] = P.tpmin;
+        pg[ng] = P.pmin; pp[ng] = P.pmin + P.fsd;
+        rog[ng] = pg[ng] / (rrg * tg[ng]);
+        rop[ng] = gamap * (pp[ng] + pinf) / ((gamap - 1.0) * cpp * tp[ng]);
+    }
+    if (!VISC && egt != nullptr && (nt == 2 || nt == 3 || nt == 5 || nt == 51 || nt == 53 || nt == 6 || nt == 7)) {
+        // egtotal / eptotal of the ghost as the BC loop that wrote it last
+        // defines them (src/sr_primitiveplusbc.F90:255-258 for type 2,
+        // :342-345 and siblings for the others)
+        double eg, ep;
+        if (nt == 2) {
+            eg = pg[ng] / (rog[ng] * (gamag - 1.0));
+            ep = (pp[ng] + gamap * pinf) / (rop[ng] * (gamap - 1.0));
+        } else {
+            eg = rrg * tg[ng] / (gamag - 1.0);
+            ep = cpp * tp[ng] / gamap + pinf / rop[ng];
+        }
+        egt[ng] = eg + 0.5 * (ug[ng] * ug[ng] + vg[ng] * vg[ng] + wg[ng] * wg[ng]);
+        egt[m.ld + ng] = ep + 0.5 * (up[ng] * up[ng] + vp[ng] * vp[ng] + wp[ng] * wp[ng]);
+    }
+}
+
+// ghost cn, src/sr_primitiveplusbc.F90:602-631 (energies as the BC loops
+// define them; only observable when ghost ids alias element ids)
+__device__ __forceinline__ void ghost_cn_one(const DevMesh& m, double* pr, double* cn,
+                                             const double* egtp, int gidx) {
+    const int ng = m.g_id[gidx];
+    double ug = COL(pr, P_UG)[ng], vg = COL(pr, P_VG)[ng], wg = COL(pr, P_WG)[ng];
+    double up = COL(pr, P_UP)[ng], vp = COL(pr, P_VP)[ng], wp = COL(pr, P_WP)[ng];
+    double phig = COL(pr, P_PHIG)[ng], phip = COL(pr, P_PHIP)[ng];
+    double rog = COL(pr, P_ROG)[ng], rop = COL(pr, P_ROP)[ng];
+    double egt = egtp[ng], ept = egtp[m.ld + ng];
+    COL(cn, 0)[ng] = phig * rog; COL(cn, 1)[ng] = phig * rog * ug;
+    COL(cn, 2)[ng] = phig * rog * vg; COL(cn, 3)[ng] = phig * rog * wg;
+    COL(cn, 4)[ng] = phig * rog * egt; COL(cn, 5)[ng] = phip * rop;
+    COL(cn, 6)[ng] = phip * rop * up; COL(cn, 7)[ng] = phip * rop * vp;
+    COL(cn, 8)[ng] = phip * rop * wp; COL(cn, 9)[ng] = phip * rop * ept;
+}
+
+// Parallel ghost fill: valid when every ghost id is its own slot and every
+// parent is an element (no aliasing), so ghost entries are independent.
+template <bool VISC>
+__global__ void __launch_bounds__(256) k_bc(DevMesh m, DevState<R> s, DevParams P) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= m.nghosts) return;
+    bc_one<VISC>(m, s.pr, nullptr, P, g, s.s->dt, s.s->total);
+}
+
+// Sequential ghost fill in the reference's exact order (type lists 2, 3, 5,
+// 51, 53, then ghost cn for every ghost) for meshes whose ghost ids alias
+// element ids or each other (e.g. merged overset meshes).  One thread.
+template <bool VISC>
+__global__ void k_bc_serial(DevMesh m, DevState<R> s, DevParams P) {
+    const int order[7] = {2, 3, 5, 51, 53, 6, 7};
+    double dt = s.s->dt;
+    int total = s.s->total;
+    for (int t = 0; t < 7; t++)
+        for (int g = 0; g < m.nghosts; g++)
+            if (m.g_type[g] == order[t]) bc_one<VISC>(m, s.pr, VISC ? nullptr : s.egt, P, g, dt, total);
+    if (!VISC)
+        for (int g = 0; g < m.nghosts; g++) ghost_cn_one(m, s.pr, s.cn, s.egt, g);
+}
+
+// src/sr_smooth.F90:19-41 and :164-187 ghost copies (aliased meshes only;
+// otherwise the smoothing kernels read the parent through m.snb).
+__global__ void k_smooth_copy_serial(DevMesh m, DevState<R> s, int which) {
+    for (int g = 0; g < m.nghosts; g++) {
+        int ng = m.g_id[g], np = m.g_par[g];
+        if (which == 0) {
+            COL(s.pr, P_PG)[ng] = COL(s.pr, P_PG)[np];
+            COL(s.pr, P_PP)[ng] = COL(s.pr, P_PP)[np];
+            for (int k = 0; k < 10; k++) COL(s.cn, k)[ng] = COL(s.cn, k)[np];
+        } else {
+            for (int k = 0; k < 10; k++) COL(s.d2q, k)[ng] = COL(s.d2q, k)[np];
+            COL(s.anu, 0)[ng] = COL(s.anu, 0)[np];
+            COL(s.anu, 1)[ng] = COL(s.anu, 1)[np];
+        }
+    }
+}
+
+// phi(ghost) = phi(parent), src/sr_VK.F90:299-301 (aliased meshes only).
+__global__ void k_phi_copy_serial(DevMesh m, DevState<R> s) {
+    for (int g = 0; g < m.nghosts; g++) s.phi[m.g_id[g]] = s.phi[m.g_par[g]];
+}
+
+// ---------------------------------------------------------------------------
+// JST dissipation, src/sr_smooth.F90:52-154: switches anu and Laplacian d2q.
+__global__ void __launch_bounds__(256) k_smooth1(DevMesh m, DevState<R> s) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles) return;
+    const int a = ldg(COL(m.snb, 0) + i), b = ldg(COL(m.snb, 1) + i);
+    const int c = ldg(COL(m.snb, 2) + i), d = ldg(COL(m.snb, 3) + i);
+    const double* pg = COL(s.pr, P_PG);
+    const double* pp = COL(s.pr, P_PP);
+    const double e6 = (double)1.0e-6f;
+    double pgi = pg[i];
+    double anun = fabs(pg[a] - pgi) + fabs(pg[b] - pgi) + fabs(pg[c] - pgi) + fabs(pg[d] - pgi);
+    double anud = fabs(pg[a] + pgi) + fabs(pg[b] + pgi) + fabs(pg[c] + pgi) + fabs(pg[d] + pgi);
+    double anupg = anun / anud;
+    double cv[10][5];
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+        const double* col = COL(s.cn, k);
+        cv[k][0] = col[i]; cv[k][1] = col[a]; cv[k][2] = col[b]; cv[k][3] = col[c]; cv[k][4] = col[d];
+    }
+#define SW(K)                                                                                    \
+    anun = fabs(cv[K][1] - cv[K][0]) + fabs(cv[K][2] - cv[K][0]) + fabs(cv[K][3] - cv[K][0]) +   \
+           fabs(cv[K][4] - cv[K][0]);                                                            \
+    anud = fabs(cv[K][1] + cv[K][0]) + fabs(cv[K][2] + cv[K][0]) + fabs(cv[K][3] + cv[K][0]) +   \
+           fabs(cv[K][4] + cv[K][0]);
+    SW(4);
+    double anu1 = anupg + anun / (anud + e6);
+    SW(0);
+    anu1 = anu1 + anun / (anud + e6);
+    double ppi = pp[i];
+    anun = fabs(pp[a] - ppi) + fabs(pp[b] - ppi) + fabs(pp[c] - ppi) + fabs(pp[d] - ppi);
+    anud = fabs(pp[a] + ppi) + fabs(pp[b] + ppi) + fabs(pp[c] + ppi) + fabs(pp[d] + ppi);
+    double anupp = anun / anud;
+    SW(5);
+    double anu2 = anupp + anun / (anud + e6);
+    SW(9);
+    anu2 = anu2 + anun / (anud + e6);
+#undef SW
+    COL(s.anu, 0)[i] = anu1;
+    COL(s.anu, 1)[i] = anu2;
+#pragma unroll
+    for (int k = 0; k < 10; k++)
+        COL(s.d2q, k)[i] = cv[k][1] - cv[k][0] + cv[k][2] - cv[k][0] + cv[k][3] - cv[k][0] +
+                           cv[k][4] - cv[k][0];
+}
+
+// src/sr_smooth.F90:200-374: blended 2nd/4th difference d24.
+__global__ void __launch_bounds__(256) k_smooth2(DevMesh m, DevState<R> s, DevParams P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles) return;
+    const double dt = s.s->dt;
+    int nb[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) nb[f] = ldg(COL(m.snb, f) + i);
+    const double voli = ldg(m.vol + i);
+#pragma unroll
+    for (int set = 0; set < 2; set++) {
+        const double* anu = COL(s.anu, set);
+        double ai = anu[i];
+        double d2c[4], d4c[4];
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            double e2 = P.co2 * mx2(ai, anu[nb[f]]);
+            double e4 = mx2(0.0, P.co4 - e2);
+            double d24nc = 0.5 * (voli / dt + ldg(m.vol + nb[f]) / dt);
+            d2c[f] = e2 * d24nc;
+            d4c[f] = e4 * d24nc;
+        }
+#pragma unroll
+        for (int k = 5 * set; k < 5 * set + 5; k++) {
+            const double* cn = COL(s.cn, k);
+            const double* dq = COL(s.d2q, k);
+            double ci = cn[i], qi = dq[i];
+            double d2 = d2c[0] * (cn[nb[0]] - ci) + d2c[1] * (cn[nb[1]] - ci) +
+                        d2c[2] * (cn[nb[2]] - ci) + d2c[3] * (cn[nb[3]] - ci);
+            double d4 = d4c[0] * (dq[nb[0]] - qi) + d4c[1] * (dq[nb[1]] - qi) +
+                        d4c[2] * (dq[nb[2]] - qi) + d4c[3] * (dq[nb[3]] - qi);
+            COL(s.d24, k)[i] = d2 - d4;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LSQ gradients (src/sr_derivative.F90:45-322) fused with the
+// Venkatakrishnan limiter (src/sr_VK.F90:32-272).  iblank == 1 cells.
+__global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParams P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles) return;
+    if (ldg(m.iblank + i) != 1) return;
+    int n[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
+    const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
+    R xa[4], ya[4], za[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        xa[f] = (R)(ldg(m.xc + n[f]) - x0);
+        ya[f] = (R)(ldg(m.yc + n[f]) - y0);
+        za[f] = (R)(ldg(m.zc + n[f]) - z0);
+    }
+    R wt[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) wt[f] = xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f];
+    R a1 = xa[0] * xa[0] / wt[0] + xa[1] * xa[1] / wt[1] + xa[2] * xa[2] / wt[2] + xa[3] * xa[3] / wt[3];
+    R a2 = ya[0] * ya[0] / wt[0] + ya[1] * ya[1] / wt[1] + ya[2] * ya[2] / wt[2] + ya[3] * ya[3] / wt[3];
+    R a3 = za[0] * za[0] / wt[0] + za[1] * za[1] / wt[1] + za[2] * za[2] / wt[2] + za[3] * za[3] / wt[3];
+    R b1 = xa[0] * ya[0] / wt[0] + xa[1] * ya[1] / wt[1] + xa[2] * ya[2] / wt[2] + xa[3] * ya[3] / wt[3];
+    R b2 = xa[0] * za[0] / wt[0] + xa[1] * za[1] / wt[1] + xa[2] * za[2] / wt[2] + xa[3] * za[3] / wt[3];
+    R b3 = za[0] * ya[0] / wt[0] + za[1] * ya[1] / wt[1] + za[2] * ya[2] / wt[2] + za[3] * ya[3] / wt[3];
+    R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+    // fields in the order of the stored gradient columns, then rog, rop
+    const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
+    R gv[13][3];
+#pragma unroll
+    for (int v = 0; v < 13; v++) {
+        const double* q = COL(s.pr, pcol[v]);
+        double qi = q[i];
+        R qa = (R)(q[n[0]] - qi), qb = (R)(q[n[1]] - qi), qc = (R)(q[n[2]] - qi), qd = (R)(q[n[3]] - qi);
+        R c1 = qa * xa[0] / wt[0] + qb * xa[1] / wt[1] + qc * xa[2] / wt[2] + qd * xa[3] / wt[3];
+        R c2;
+        if (v == 7)   // cTp2 lacks the /wt4 (src/sr_derivative.F90:225)
+            c2 = qa * ya[0] / wt[0] + qb * ya[1] / wt[1] + qc * ya[2] / wt[2] + qd * ya[3];
+        else
+            c2 = qa * ya[0] / wt[0] + qb * ya[1] / wt[1] + qc * ya[2] / wt[2] + qd * ya[3] / wt[3];
+        R c3 = qa * za[0] / wt[0] + qb * za[1] / wt[1] + qc * za[2] / wt[2] + qd * za[3] / wt[3];
+        gv[v][0] = det3(c1, c2, c3, b1, a2, b3, b2, b3, a3) / dnr;
+        gv[v][1] = det3(a1, b1, b2, c1, c2, c3, b2, b3, a3) / dnr;
+        gv[v][2] = det3(a1, b1, b2, b1, a2, b3, c1, c2, c3) / dnr;
+    }
+#pragma unroll
+    for (int v = 0; v < 11; v++) {
+        COL(s.gr, 3 * v + 0)[i] = gv[v][0];
+        COL(s.gr, 3 * v + 1)[i] = gv[v][1];
+        COL(s.gr, 3 * v + 2)[i] = gv[v][2];
+    }
+    // limiter: phi_i = min over {pg, pp, rog, rop} x 4 faces
+    const R epssq = (R)cube_rn((double)(P.venkat_k * ldg(m.dl + i)));
+    R fx[4], fy[4], fz[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        fx[f] = (R)(ldg(COL(m.fch, f) + i) - x0);
+        fy[f] = (R)(ldg(COL(m.fch, 4 + f) + i) - y0);
+        fz[f] = (R)(ldg(COL(m.fch, 8 + f) + i) - z0);
+    }
+    const int lv[4] = {8, 9, 11, 12};   // pg, pp, rog, rop rows of gv
+    R phi = R(0);
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        const double* q = COL(s.pr, pcol[lv[t]]);
+        double qi = q[i];
+        double vmax = mx2(mx2(mx2(mx2(qi, q[n[0]]), q[n[1]]), q[n[2]]), q[n[3]]);
+        double vmin = mn2(mn2(mn2(mn2(qi, q[n[0]]), q[n[1]]), q[n[2]]), q[n[3]]);
+        R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
+        R gx = gv[lv[t]][0], gy = gv[lv[t]][1], gz = gv[lv[t]][2];
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            R d = fx[f] * gx + fy[f] * gy + fz[f] * gz;
+            R ph;
+            if (d > R(0)) ph = fvenkat(dmax, d, epssq);
+            else if (d < R(0)) ph = fvenkat(dmin, d, epssq);
+            else ph = R(1);
+            phi = (t == 0 && f == 0) ? ph : mn2(phi, ph);
+        }
+    }
+    s.phi[i] = (double)phi;
+}
+
+// ---------------------------------------------------------------------------
+// One face of cell i: MUSCL reconstruction, phase blending and HLLC-Batten
+// (src/sr_hllcbatten.F90:79-529).  Wall faces return the pressure terms.
+struct FaceOut {
+    R F[10];
+    R w[6];
+    bool wall, takeg, takep;
+};
+
+__device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& phip, R& ug, R& vg,
+                                               R& wg, R& tg, R& pg, R& up, R& vp, R& wp, R& tp,
+                                               R& pp) {
+    const R emin = (R)P.emin, emax = (R)P.emax;
+    if (phig < emin) {
+        phig = emin; phip = R(1) - phig;
+        ug = up; vg = vp; wg = wp; tg = tp; pg = pp;
+    }
+    if (phip < emin) {
+        phip = emin; phig = R(1) - phip;
+        up = ug; vp = vg; wp = wg; tp = tg; pp = pg;
+    }
+    if (phig >= emin && phig <= emax) {
+        R psig = (phig - emin) / (emax - emin);
+        R f = -(psig * psig * (R(2) * psig - R(3)));
+        ug = f * ug + (R(1) - f) * up; vg = f * vg + (R(1) - f) * vp;
+        wg = f * wg + (R(1) - f) * wp; tg = f * tg + (R(1) - f) * tp;
+        pg = f * pg + (R(1) - f) * pp;
+    }
+    if (phip >= emin && phip <= emax) {
+        R psig = (phip - emin) / (emax - emin);
+        R f = -(psig * psig * (R(2) * psig - R(3)));
+        up = f * up + (R(1) - f) * ug; vp = f * vp + (R(1) - f) * vg;
+        wp = f * wp + (R(1) - f) * wg; tp = f * tp + (R(1) - f) * tg;
+        pp = f * pp + (R(1) - f) * pg;
+    }
+}
+
+__device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s, const DevParams& P,
+                                          int i, int f, FaceOut& o) {
+    const int neigh = ldg(COL(m.nc, f) + i);
+    const unsigned kind = (ldg(m.fk + i) >> (4 * f)) & 0xFu;
+    const double scxd = ldg(COL(m.sc, 3 * f) + i), scyd = ldg(COL(m.sc, 3 * f + 1) + i),
+                 sczd = ldg(COL(m.sc, 3 * f + 2) + i);
+    const R scx = (R)scxd, scy = (R)scyd, scz = (R)sczd;
+    const R area = sqrt(scx * scx + scy * scy + scz * scz);
+    const R enx = scx / area, eny = scy / area, enz = scz / area;
+    const double* pr = s.pr;
+    R ugL = (R)COL(pr, P_UG)[i], vgL = (R)COL(pr, P_VG)[i], wgL = (R)COL(pr, P_WG)[i];
+    R tgL = (R)COL(pr, P_TG)[i], phigL = (R)COL(pr, P_PHIG)[i];
+    R upL = (R)COL(pr, P_UP)[i], vpL = (R)COL(pr, P_VP)[i], wpL = (R)COL(pr, P_WP)[i];
+    R tpL = (R)COL(pr, P_TP)[i], pgL = (R)COL(pr, P_PG)[i], ppL = (R)COL(pr, P_PP)[i];
+    R ugR = (R)COL(pr, P_UG)[neigh], vgR = (R)COL(pr, P_VG)[neigh], wgR = (R)COL(pr, P_WG)[neigh];
+    R tgR = (R)COL(pr, P_TG)[neigh], phigR = (R)COL(pr, P_PHIG)[neigh];
+    R upR = (R)COL(pr, P_UP)[neigh], vpR = (R)COL(pr, P_VP)[neigh], wpR = (R)COL(pr, P_WP)[neigh];
+    R tpR = (R)COL(pr, P_TP)[neigh], pgR = (R)COL(pr, P_PG)[neigh], ppR = (R)COL(pr, P_PP)[neigh];
+    if (P.myorder == 2 && (kind & FK_RECON)) {
+        const R phimin = (R)mn2(s.phi[i], s.phi[neigh]);
+        const double xf = ldg(COL(m.fch, f) + i), yf = ldg(COL(m.fch, 4 + f) + i),
+                     zf = ldg(COL(m.fch, 8 + f) + i);
+        const R xf0 = (R)(xf - ldg(m.xc + i)), yf0 = (R)(yf - ldg(m.yc + i)), zf0 = (R)(zf - ldg(m.zc + i));
+        const R xfn = (R)(xf - ldg(m.xc + neigh)), yfn = (R)(yf - ldg(m.yc + neigh)),
+                zfn = (R)(zf - ldg(m.zc + neigh));
+        const R* g = s.gr;
+#define REC(v, X, Y, Z, G, c) \
+    v = v + phimin * (X * COL(g, G)[c] + Y * COL(g, G + 1)[c] + Z * COL(g, G + 2)[c])
+        REC(phigL, xf0, yf0, zf0, G_PHIG, i); REC(ugL, xf0, yf0, zf0, G_UG, i);
+        REC(vgL, xf0, yf0, zf0, G_VG, i); REC(wgL, xf0, yf0, zf0, G_WG, i);
+        REC(tgL, xf0, yf0, zf0, G_TG, i); REC(pgL, xf0, yf0, zf0, G_PG, i);
+        REC(phigR, xfn, yfn, zfn, G_PHIG, neigh); REC(ugR, xfn, yfn, zfn, G_UG, neigh);
+        REC(vgR, xfn, yfn, zfn, G_VG, neigh); REC(wgR, xfn, yfn, zfn, G_WG, neigh);
+        REC(tgR, xfn, yfn, zfn, G_TG, neigh); REC(pgR, xfn, yfn, zfn, G_PG, neigh);
+        REC(upL, xf0, yf0, zf0, G_UP, i); REC(vpL, xf0, yf0, zf0, G_VP, i);
+        REC(wpL, xf0, yf0, zf0, G_WP, i); REC(tpL, xf0, yf0, zf0, G_TP, i);
+        REC(ppL, xf0, yf0, zf0, G_PP, i);
+        REC(upR, xfn, yfn, zfn, G_UP, neigh); REC(vpR, xfn, yfn, zfn, G_VP, neigh);
+        REC(wpR, xfn, yfn, zfn, G_WP, neigh); REC(tpR, xfn, yfn, zfn, G_TP, neigh);
+        REC(ppR, xfn, yfn, zfn, G_PP, neigh);
+#undef REC
+    }
+    const R rrg = (R)P.rrg, gamag = (R)P.gamag, gamap = (R)P.gamap, pinf = (R)P.pinf, cpp = (R)P.cpp;
+    R phipL = R(1) - phigL, phipR = R(1) - phigR;
+    blend_phases_r(P, phigL, phipL, ugL, vgL, wgL, tgL, pgL, upL, vpL, wpL, tpL, ppL);
+    R rogL = pgL / (rrg * tgL);
+    R ropL = gamap * (ppL + pinf) / ((gamap - R(1)) * cpp * tpL);
+    blend_phases_r(P, phigR, phipR, ugR, vgR, wgR, tgR, pgR, upR, vpR, wpR, tpR, ppR);
+    R rogR = pgR / (rrg * tgR);
+    R ropR = gamap * (ppR + pinf) / ((gamap - R(1)) * cpp * tpR);
+    o.wall = (kind & FK_WALL) != 0;
+    if (o.wall) {
+        o.w[0] = phigL * pgL * enx * area;
+        o.w[1] = phigL * pgL * eny * area;
+        o.w[2] = phigL * pgL * enz * area;
+        o.w[3] = phipL * ppL * enx * area;
+        o.w[4] = phipL * ppL * eny * area;
+        o.w[5] = phipL * ppL * enz * area;
+        o.takeg = o.takep = false;
+        return;
+    }
+    const R eps8 = (R)(double)1.0e-8f, eps6 = (R)(double)1.0e-6f;
+    R egL = rrg * tgL / (gamag - R(1)) + R(0.5) * (ugL * ugL + vgL * vgL + wgL * wgL);
+    R hgL = egL + pgL / rogL;
+    R qgL = ugL * enx + vgL * eny + wgL * enz;
+    R agL = sqrt(gamag * pgL / rogL);
+    R egR = rrg * tgR / (gamag - R(1)) + R(0.5) * (ugR * ugR + vgR * vgR + wgR * wgR);
+    R hgR = egR + pgR / rogR;
+    R qgR = ugR * enx + vgR * eny + wgR * enz;
+    R agR = sqrt(gamag * pgR / rogR);
+    R epL = (cpp * tpL) / gamap + pinf / ropL + R(0.5) * (upL * upL + vpL * vpL + wpL * wpL);
+    R hpL = epL + ppL / ropL;
+    R qpL = upL * enx + vpL * eny + wpL * enz;
+    R apL = sqrt(gamap * (ppL + pinf) / ropL);
+    R epR = (cpp * tpR) / gamap + pinf / ropR + R(0.5) * (upR * upR + vpR * vpR + wpR * wpR);
+    R hpR = epR + ppR / ropR;
+    R qpR = upR * enx + vpR * eny + wpR * enz;
+    R apR = sqrt(gamap * (ppR + pinf) / ropR);
+    R sgl = mn2(mn2(qgL - agL, qgR - agR), eps8);
+    R spl = mn2(mn2(qpL - apL, qpR - apR), eps8);
+    R sgr = mx2(mx2(qgL + agL, qgR + agR), eps8);
+    R spr = mx2(mx2(qpL + apL, qpR + apR), eps8);
+    R sgstar = (pgR - pgL + rogL * qgL * (sgl - qgL) - rogR * qgR * (sgr - qgR)) /
+               ((rogL * (sgl - qgL) - rogR * (sgr - qgR)) + eps8);
+    R spstar = (ppR - ppL + ropL * qpL * (spl - qpL) - ropR * qpR * (spr - qpR)) /
+               ((ropL * (spl - qpL) - ropR * (spr - qpR)) + eps8);
+    R pgstar = mx2(pgL + rogL * (qgL - sgl) * (qgL - sgstar), eps6 * mn2(pgL, pgR));
+    R ppstar = mx2(ppL + ropL * (qpL - spl) * (qpL - spstar), eps6 * mn2(ppL, ppR));
+    // gas phase
+    {
+        int br = (sgl > R(0)) ? 1 : (sgl <= R(0) && sgstar > R(0)) ? 2
+                 : (sgstar <= R(0) && sgr >= R(0)) ? 3 : (sgr < R(0)) ? 4 : 0;
+        o.takeg = br != 0;
+        if (br == 1 || br == 2) {
+            R cn0 = phigL * rogL, cn1 = phigL * rogL * ugL, cn2 = phigL * rogL * vgL;
+            R cn3 = phigL * rogL * wgL, cn4 = phigL * rogL * egL;
+            R fl0 = phigL * rogL * qgL;
+            R fl1 = phigL * rogL * qgL * ugL + phigL * pgL * enx;
+            R fl2 = phigL * rogL * qgL * vgL + phigL * pgL * eny;
+            R fl3 = phigL * rogL * qgL * wgL + phigL * pgL * enz;
+            R fl4 = phigL * rogL * qgL * hgL;
+            if (br == 1) {
+                o.F[0] = fl0 * area; o.F[1] = fl1 * area; o.F[2] = fl2 * area;
+                o.F[3] = fl3 * area; o.F[4] = fl4 * area;
+            } else {
+                R dnrg = (sgstar - sgl) + eps6;
+                R cs0 = (qgL - sgl) * cn0 / dnrg;
+                R cs1 = ((qgL - sgl) * cn1 + phigL * (pgL * enx - pgstar * enx)) / dnrg;
+                R cs2 = ((qgL - sgl) * cn2 + phigL * (pgL * eny - pgstar * eny)) / dnrg;
+                R cs3 = ((qgL - sgl) * cn3 + phigL * (pgL * enz - pgstar * enz)) / dnrg;
+                R cs4 = ((qgL - sgl) * cn4 + phigL * (pgL * qgL - pgstar * sgstar)) / dnrg;
+                o.F[0] = (fl0 + sgl * (cs0 - cn0)) * area;
+                o.F[1] = (fl1 + sgl * (cs1 - cn1)) * area;
+                o.F[2] = (fl2 + sgl * (cs2 - cn2)) * area;
+                o.F[3] = (fl3 + sgl * (cs3 - cn3)) * area;
+                o.F[4] = (fl4 + sgl * (cs4 - cn4)) * area;
+            }
+        } else if (br == 3 || br == 4) {
+            R cn0 = phigR * rogR, cn1 = phigR * rogR * ugR, cn2 = phigR * rogR * vgR;
+            R cn3 = phigR * rogR * wgR, cn4 = phigR * rogR * egR;
+            R fr0 = phigR * rogR * qgR;
+            R fr1 = phigR * rogR * qgR * ugR + phigR * pgR * enx;
+            R fr2 = phigR * rogR * qgR * vgR + phigR * pgR * eny;
+            R fr3 = phigR * rogR * qgR * wgR + phigR * pgR * enz;
+            R fr4 = phigR * rogR * qgR * hgR;
+            if (br == 4) {
+                o.F[0] = fr0 * area; o.F[1] = fr1 * area; o.F[2] = fr2 * area;
+                o.F[3] = fr3 * area; o.F[4] = fr4 * area;
+            } else {
+                R dnrg = (sgstar - sgr) + eps6;
+                R cs0 = (qgR - sgr) * cn0 / dnrg;
+                R cs1 = ((qgR - sgr) * cn1 + phigR * (pgR * enx - pgstar * enx)) / dnrg;
+                R cs2 = ((qgR - sgr) * cn2 + phigR * (pgR * eny - pgstar * eny)) / dnrg;
+                R cs3 = ((qgR - sgr) * cn3 + phigR * (pgR * enz - pgstar * enz)) / dnrg;
+                R cs4 = ((qgR - sgr) * cn4 + phigR * (pgR * qgR - pgstar * sgstar)) / dnrg;
+                o.F[0] = (fr0 + sgr * (cs0 - cn0)) * area;
+                o.F[1] = (fr1 + sgr * (cs1 - cn1)) * area;
+                o.F[2] = (fr2 + sgr * (cs2 - cn2)) * area;
+                o.F[3] = (fr3 + sgr * (cs3 - cn3)) * area;
+                o.F[4] = (fr4 + sgr * (cs4 - cn4)) * area;
+            }
+        }
+    }
+    // liquid phase
+    {
+        int br = (spl > R(0)) ? 1 : (spl <= R(0) && spstar > R(0)) ? 2
+                 : (spstar <= R(0) && spr >= R(0)) ? 3 : (spr < R(0)) ? 4 : 0;
+        o.takep = br != 0;
+        if (br == 1 || br == 2) {
+            R cn0 = phipL * ropL, cn1 = phipL * ropL * upL, cn2 = phipL * ropL * vpL;
+            R cn3 = phipL * ropL * wpL, cn4 = phipL * ropL * epL;
+            R fl0 = phipL * ropL * qpL;
+            R fl1 = phipL * ropL * qpL * upL + phipL * ppL * enx;
+            R fl2 = phipL * ropL * qpL * vpL + phipL * ppL * eny;
+            R fl3 = phipL * ropL * qpL * wpL + phipL * ppL * enz;
+            R fl4 = phipL * ropL * qpL * hpL;
+            if (br == 1) {
+                o.F[5] = fl0 * area; o.F[6] = fl1 * area; o.F[7] = fl2 * area;
+                o.F[8] = fl3 * area; o.F[9] = fl4 * area;
+            } else {
+                R dnrp = (spstar - spl) + eps6;
+                R cs0 = (qpL - spl) * cn0 / dnrp;
+                R cs1 = ((qpL - spl) * cn1 + phipL * (ppL * enx - ppstar * enx)) / dnrp;
+                R cs2 = ((qpL - spl) * cn2 + phipL * (ppL * eny - ppstar * eny)) / dnrp;
+                R cs3 = ((qpL - spl) * cn3 + phipL * (ppL * enz - ppstar * enz)) / dnrp;
+                R cs4 = ((qpL - spl) * cn4 + phipL * (ppL * qpL - ppstar * spstar)) / dnrp;
+                o.F[5] = (fl0 + spl * (cs0 - cn0)) * area;
+                o.F[6] = (fl1 + spl * (cs1 - cn1)) * area;
+                o.F[7] = (fl2 + spl * (cs2 - cn2)) * area;
+                o.F[8] = (fl3 + spl * (cs3 - cn3)) * area;
+                o.F[9] = (fl4 + spl * (cs4 - cn4)) * area;
+            }
+        } else if (br == 3 || br == 4) {
+            R cn0 = phipR * ropR, cn1 = phipR * ropR * upR, cn2 = phipR * ropR * vpR;
+            R cn3 = phipR * ropR * wpR, cn4 = phipR * ropR * epR;
+            R fr0 = phipR * ropR * qpR;
+            R fr1 = phipR * ropR * qpR * upR + phipR * ppR * enx;
+            R fr2 = phipR * ropR * qpR * vpR + phipR * ppR * eny;
+            R fr3 = phipR * ropR * qpR * wpR + phipR * ppR * enz;
+            R fr4 = phipR * ropR * qpR * hpR;
+            if (br == 4) {
+                o.F[5] = fr0 * area; o.F[6] = fr1 * area; o.F[7] = fr2 * area;
+                o.F[8] = fr3 * area; o.F[9] = fr4 * area;
+            } else {
+                R dnrp = (spstar - spr) + eps6;
+                R cs0 = (qpR - spr) * cn0 / dnrp;
+                R cs1 = ((qpR - spr) * cn1 + phipR * (ppR * enx - ppstar * enx)) / dnrp;
+                R cs2 = ((qpR - spr) * cn2 + phipR * (ppR * eny - ppstar * eny)) / dnrp;
+                R cs3 = ((qpR - spr) * cn3 + phipR * (ppR * enz - ppstar * enz)) / dnrp;
+                R cs4 = ((qpR - spr) * cn4 + phipR * (ppR * qpR - ppstar * spstar)) / dnrp;
+                o.F[5] = (fr0 + spr * (cs0 - cn0)) * area;
+                o.F[6] = (fr1 + spr * (cs1 - cn1)) * area;
+                o.F[7] = (fr2 + spr * (cs2 - cn2)) * area;
+                o.F[8] = (fr3 + spr * (cs3 - cn3)) * area;
+                o.F[9] = (fr4 + spr * (cs4 - cn4)) * area;
+            }
+        }
+    }
+}
+
+// Flux of the most recently evaluated face, in the reference's sequential
+// cell order, whose wave branch was taken -- what the reference's FSTARA
+// variables hold when a NaN state leaves every branch untaken.  Scans
+// backwards from (i, f); falls back to the carry of the previous call.
+__device__ __noinline__ void stale_flux(const DevMesh& m, const DevState<R>& s, const DevParams& P,
+                                        int i, int f, bool gas, R* out) {
+    int cell = i, face = f - 1;
+    for (int guard = 0; guard < (1 << 20); guard++) {
+        if (face < 0) {
+            cell--;
+            while (cell >= 0 && ldg(m.iblank + cell) != 1) cell--;
+            if (cell < 0) break;
+            face = 3;
+        }
+        FaceOut o;
+        face_eval(m, s, P, cell, face, o);
+        if (!o.wall && (gas ? o.takeg : o.takep)) {
+            for (int k = 0; k < 5; k++) out[k] = o.F[(gas ? 0 : 5) + k];
+            return;
+        }
+        face--;
+    }
+    for (int k = 0; k < 5; k++) out[k] = (R)s.s->fcarry[(gas ? 0 : 5) + k];
+}
+
+// Updates the stale-flux carry with the last taken face of the sweep; one
+// thread, aliased meshes only.
+__global__ void k_flux_carry(DevMesh m, DevState<R> s, DevParams P) {
+    R tmp[5];
+    int last = m.neles - 1;
+    while (last >= 0 && ldg(m.iblank + last) != 1) last--;
+    if (last < 0) return;
+    stale_flux(m, s, P, last, 4, true, tmp);
+    for (int k = 0; k < 5; k++) s.s->fcarry[k] = (double)tmp[k];
+    stale_flux(m, s, P, last, 4, false, tmp);
+    for (int k = 0; k < 5; k++) s.s->fcarry[5 + k] = (double)tmp[k];
+}
+
+// Residual (4 faces + interphase sources, src/sr_source.F90:42-155) and the
+// RK stage update of src/sr_RK.F90 fused; iblank == 1 cells.
+template <bool ALIASED>
+__global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParams P, int stage) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles) return;
+    if (ldg(m.iblank + i) != 1) return;
+    double rhs[10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) rhs[k] = 0.0;
+    R Fg[5] = {R(0), R(0), R(0), R(0), R(0)}, Fp[5] = {R(0), R(0), R(0), R(0), R(0)};
+    bool haveg = false, havep = false;
+#pragma unroll 1
+    for (int f = 0; f < 4; f++) {
+        FaceOut o;
+        face_eval(m, s, P, i, f, o);
+        if (o.wall) {
+            rhs[1] = rhs[1] + (double)o.w[0]; rhs[2] = rhs[2] + (double)o.w[1];
+            rhs[3] = rhs[3] + (double)o.w[2]; rhs[6] = rhs[6] + (double)o.w[3];
+            rhs[7] = rhs[7] + (double)o.w[4]; rhs[8] = rhs[8] + (double)o.w[5];
+            continue;
+        }
+        if (o.takeg) {
+            for (int k = 0; k < 5; k++) Fg[k] = o.F[k];
+            haveg = true;
+        } else if (ALIASED && !haveg) {
+            stale_flux(m, s, P, i, f, true, Fg);
+            haveg = true;
+        }
+        if (o.takep) {
+            for (int k = 0; k < 5; k++) Fp[k] = o.F[5 + k];
+            havep = true;
+        } else if (ALIASED && !havep) {
+            stale_flux(m, s, P, i, f, false, Fp);
+            havep = true;
+        }
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            rhs[k] = rhs[k] + (double)Fg[k];
+            rhs[5 + k] = rhs[5 + k] + (double)Fp[k];
+        }
+    }
+    // interphase sources with the 1/r-weighted LSQ gradient of alpha_g
+    {
+        const double* pr = s.pr;
+        const R tg = (R)COL(pr, P_TG)[i], phig = (R)COL(pr, P_PHIG)[i], rog = (R)COL(pr, P_ROG)[i];
+        const R rop = (R)COL(pr, P_ROP)[i], phip = (R)COL(pr, P_PHIP)[i];
+        const R ug = (R)COL(pr, P_UG)[i], vg = (R)COL(pr, P_VG)[i], wg = (R)COL(pr, P_WG)[i];
+        const R up = (R)COL(pr, P_UP)[i], vp = (R)COL(pr, P_VP)[i], wp = (R)COL(pr, P_WP)[i];
+        const R tp = (R)COL(pr, P_TP)[i], pg = (R)COL(pr, P_PG)[i];
+        const R dl = (R)ldg(m.dl + i), voli = (R)ldg(m.vol + i);
+        const R amug = (R)P.as * sqrt(tg) / (R(1) + (R)P.ts / tg);
+        const R du = ug - up, dv = vg - vp, dw = wg - wp;
+        const R drag = R(0.44) * phig * (phig - R(1)) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        const R fdgx = drag * du, fdgy = drag * dv, fdgz = drag * dw;
+        const R qsource = R(6) * phip * amug * (R)P.cpg * R(2) * (tp - tg) / ((R)P.prg * (dl * dl));
+        const R delpstar = R(2) * (phig * rog * phip * rop) / (phig * rop + phip * rog) *
+                           (du * du + dv * dv + dw * dw);
+        const R pint = pg - mn2(delpstar, R(0.01) * pg);
+        const R den = phig * rog + (R(1) - phig) * rop;
+        const R uint_ = (phig * rog * ug + (R(1) - phig) * rop * up) / den;
+        const R vint = (phig * rog * vg + (R(1) - phig) * rop * vp) / den;
+        const R wint = (phig * rog * wg + (R(1) - phig) * rop * wp) / den;
+        const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
+        R xa[4], ya[4], za[4], pa[4], wt[4];
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            int n = ldg(COL(m.nc, f) + i);
+            xa[f] = (R)(ldg(m.xc + n) - x0);
+            ya[f] = (R)(ldg(m.yc + n) - y0);
+            za[f] = (R)(ldg(m.zc + n) - z0);
+            pa[f] = (R)(COL(pr, P_PHIG)[n] - COL(pr, P_PHIG)[i]);
+            wt[f] = sqrt(xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]);
+        }
+        R a1 = xa[0] * xa[0] / wt[0] + xa[1] * xa[1] / wt[1] + xa[2] * xa[2] / wt[2] + xa[3] * xa[3] / wt[3];
+        R a2 = ya[0] * ya[0] / wt[0] + ya[1] * ya[1] / wt[1] + ya[2] * ya[2] / wt[2] + ya[3] * ya[3] / wt[3];
+        R a3 = za[0] * za[0] / wt[0] + za[1] * za[1] / wt[1] + za[2] * za[2] / wt[2] + za[3] * za[3] / wt[3];
+        R b1 = xa[0] * ya[0] / wt[0] + xa[1] * ya[1] / wt[1] + xa[2] * ya[2] / wt[2] + xa[3] * ya[3] / wt[3];
+        R b2 = xa[0] * za[0] / wt[0] + xa[1] * za[1] / wt[1] + xa[2] * za[2] / wt[2] + xa[3] * za[3] / wt[3];
+        R b3 = ya[0] * za[0] / wt[0] + ya[1] * za[1] / wt[1] + ya[2] * za[2] / wt[2] + ya[3] * za[3] / wt[3];
+        R c1 = pa[0] * xa[0] / wt[0] + pa[1] * xa[1] / wt[1] + pa[2] * xa[2] / wt[2] + pa[3] * xa[3] / wt[3];
+        R c2 = pa[0] * ya[0] / wt[0] + pa[1] * ya[1] / wt[1] + pa[2] * ya[2] / wt[2] + pa[3] * ya[3] / wt[3];
+        R c3 = pa[0] * za[0] / wt[0] + pa[1] * za[1] / wt[1] + pa[2] * za[2] / wt[2] + pa[3] * za[3] / wt[3];
+        R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+        R dpx = det3(c1, c2, c3, b1, a2, b3, b2, b3, a3) / dnr;
+        R dpy = det3(a1, b1, b2, c1, c2, c3, b2, b3, a3) / dnr;
+        R dpz = det3(a1, b1, b2, b1, a2, b3, c1, c2, c3) / dnr;
+        const R g = R(0);   // gravity (src/main.F90:341)
+        R en = pint * (uint_ * dpx + vint * dpy + wint * dpz) + uint_ * fdgx + vint * fdgy + wint * fdgz + qsource;
+        const double* vis = s.vis;
+        rhs[1] = rhs[1] - (double)((fdgx + pint * dpx + phig * rog * g) * voli) - COL(vis, 0)[i];
+        rhs[2] = rhs[2] - (double)((fdgy + pint * dpy) * voli) - COL(vis, 1)[i];
+        rhs[3] = rhs[3] - (double)((fdgz + pint * dpz) * voli) - COL(vis, 2)[i];
+        rhs[4] = rhs[4] - (double)(en * voli) - COL(vis, 3)[i];
+        rhs[6] = rhs[6] + (double)((fdgx + pint * dpx - phip * rop * g) * voli) - COL(vis, 4)[i];
+        rhs[7] = rhs[7] + (double)((fdgy + pint * dpy) * voli) - COL(vis, 5)[i];
+        rhs[8] = rhs[8] + (double)((fdgz + pint * dpz) * voli) - COL(vis, 6)[i];
+        rhs[9] = rhs[9] + (double)(en * voli) - COL(vis, 7)[i];
+    }
+    // RK stage update (FP64)
+    const double dtbyvol = s.s->dt / ldg(m.vol + i);
+#pragma unroll
+    for (int j = 0; j < 10; j++) {
+        const double r = rhs[j] - COL(s.d24, j)[i];
+        const double cu = COL(s.cu, j)[i];
+        double* cnp = COL(s.cn, j) + i;
+        if (P.rk_scheme == 0) {
+            if (stage == 1) {
+                double v = cu - (11.0 / 20.0) * dtbyvol * r;
+                *cnp = v;
+                COL(s.cn1, j)[i] = v;
+            } else {
+                double upd = *cnp - (11.0 / 20.0) * dtbyvol * r;
+                if (stage == 2) *cnp = (3.0 / 8.0) * cu + (5.0 / 8.0) * upd;
+                else if (stage == 3) *cnp = (4.0 / 9.0) * cu + (5.0 / 9.0) * upd;
+                else *cnp = (111.0 / 1331.0) * cu + (260.0 / 1331.0) * COL(s.cn1, j)[i] + (960.0 / 1331.0) * upd;
+            }
+        } else {
+            if (stage == 1) *cnp = cu - dtbyvol * r;
+            else {
+                double upd = *cnp - dtbyvol * r;
+                if (stage == 2) *cnp = 0.75 * cu + 0.25 * upd;
+                else *cnp = (1.0 / 3.0) * cu + (2.0 / 3.0) * upd;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Face-centred viscous fluxes, src/sr_viscousgp.F90:488-1138 (AMUP constant).
+__global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParams P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles) return;
+    if (ldg(m.iblank + i) != 1) return;
+    const double* pr = s.pr;
+    const int fcol[8] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP};
+    double acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = 0.0;
+    int nci[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) nci[f] = ldg(COL(m.nc, f) + i);
+    const R c23 = (R)P.c23;
+#pragma unroll 1
+    for (int f = 0; f < 4; f++) {
+        const R scx = (R)ldg(COL(m.sc, 3 * f) + i), scy = (R)ldg(COL(m.sc, 3 * f + 1) + i),
+                scz = (R)ldg(COL(m.sc, 3 * f + 2) + i);
+        const double xf = ldg(COL(m.fcv, f) + i), yf = ldg(COL(m.fcv, 4 + f) + i),
+                     zf = ldg(COL(m.fcv, 8 + f) + i);
+        const int neigh = nci[f];
+        R ff[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) ff[v] = (R)((COL(pr, fcol[v])[i] + COL(pr, fcol[v])[neigh]) * 0.5);
+        const R phigf = (R)((COL(pr, P_PHIG)[i] + COL(pr, P_PHIG)[neigh]) * 0.5);
+        const R phipf = (R)((COL(pr, P_PHIP)[i] + COL(pr, P_PHIP)[neigh]) * 0.5);
+        const R tgf = ff[3];
+        const R amug = (R)P.as * sqrt(tgf) / (R(1) + (R)P.ts / tgf);
+        const R akg = amug * (R)P.cpg / (R)P.prg;
+        const R amup = (R)P.amup;
+        const R akp = amup * (R)P.cpp / (R)P.prp;
+        int mm[8];
+        int nm;
+        mm[0] = nci[0]; mm[1] = nci[1]; mm[2] = nci[2]; mm[3] = nci[3];
+        if (neigh >= m.neles) {
+            mm[4] = i; nm = 5;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) mm[4 + k] = ldg(COL(m.nc, k) + neigh);
+            nm = 8;
+        }
+        R dx[8], dy[8], dz[8];
+        for (int k = 0; k < nm; k++) {
+            dx[k] = (R)(ldg(m.xc + mm[k]) - xf);
+            dy[k] = (R)(ldg(m.yc + mm[k]) - yf);
+            dz[k] = (R)(ldg(m.zc + mm[k]) - zf);
+        }
+        R a11 = dx[0] * dx[0], a22 = dy[0] * dy[0], a33 = dz[0] * dz[0];
+        R a12 = dx[0] * dy[0], a13 = dx[0] * dz[0], a23 = dy[0] * dz[0];
+        for (int k = 1; k < nm; k++) {
+            a11 = a11 + dx[k] * dx[k]; a22 = a22 + dy[k] * dy[k]; a33 = a33 + dz[k] * dz[k];
+            a12 = a12 + dx[k] * dy[k]; a13 = a13 + dx[k] * dz[k]; a23 = a23 + dy[k] * dz[k];
+        }
+        const R dnr = det3(a11, a12, a13, a12, a22, a23, a13, a23, a33);
+        R gr[8][3];
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            const double* q = COL(pr, fcol[v]);
+            R d0 = (R)q[mm[0]] - ff[v];
+            R b1 = d0 * dx[0], b2 = d0 * dy[0], b3 = d0 * dz[0];
+            for (int k = 1; k < nm; k++) {
+                R dk = (R)q[mm[k]] - ff[v];
+                b1 = b1 + dk * dx[k]; b2 = b2 + dk * dy[k]; b3 = b3 + dk * dz[k];
+            }
+            gr[v][0] = det3(b1, b2, b3, a12, a22, a23, a13, a23, a33) / dnr;
+            gr[v][1] = det3(a11, a12, a13, b1, b2, b3, a13, a23, a33) / dnr;
+            gr[v][2] = det3(a11, a12, a13, a12, a22, a23, b1, b2, b3) / dnr;
+        }
+        const R ugf = ff[0], vgf = ff[1], wgf = ff[2], upf = ff[4], vpf = ff[5], wpf = ff[6];
+        R delvg = gr[0][0] + gr[1][1] + gr[2][2];
+        R txxg = amug * (R(2) * gr[0][0] - c23 * delvg);
+        R tyyg = amug * (R(2) * gr[1][1] - c23 * delvg);
+        R tzzg = amug * (R(2) * gr[2][2] - c23 * delvg);
+        R txyg = amug * (gr[1][0] + gr[0][1]);
+        R txzg = amug * (gr[2][0] + gr[0][2]);
+        R tyzg = amug * (gr[1][2] + gr[2][1]);
+        R qxxg = ugf * txxg + vgf * txyg + wgf * txzg + akg * gr[3][0];
+        R qyyg = ugf * txyg + vgf * tyyg + wgf * tyzg + akg * gr[3][1];
+        R qzzg = ugf * txzg + vgf * tyzg + wgf * tzzg + akg * gr[3][2];
+        R delvp = gr[4][0] + gr[5][1] + gr[6][2];
+        R txxp = amup * (R(2) * gr[4][0] - c23 * delvp);
+        R tyyp = amup * (R(2) * gr[5][1] - c23 * delvp);
+        R tzzp = amup * (R(2) * gr[6][2] - c23 * delvp);
+        R txyp = amup * (gr[5][0] + gr[4][1]);
+        R txzp = amup * (gr[6][0] + gr[4][2]);
+        R tyzp = amup * (gr[5][2] + gr[6][1]);
+        R qxxp = upf * txxp + vpf * txyp + wpf * txzp + akp * gr[7][0];
+        R qyyp = upf * txyp + vpf * tyyp + wpf * tyzp + akp * gr[7][1];
+        R qzzp = upf * txzp + vpf * tyzp + wpf * tzzp + akp * gr[7][2];
+        acc[0] = acc[0] + (double)(phigf * (txxg * scx + txyg * scy + txzg * scz));
+        acc[1] = acc[1] + (double)(phigf * (txyg * scx + tyyg * scy + tyzg * scz));
+        acc[2] = acc[2] + (double)(phigf * (txzg * scx + tyzg * scy + tzzg * scz));
+        acc[3] = acc[3] + (double)(phigf * (qxxg * scx + qyyg * scy + qzzg * scz));
+        acc[4] = acc[4] + (double)(phipf * (txxp * scx + txyp * scy + txzp * scz));
+        acc[5] = acc[5] + (double)(phipf * (txyp * scx + tyyp * scy + tyzp * scz));
+        acc[6] = acc[6] + (double)(phipf * (txzp * scx + tyzp * scy + tzzp * scz));
+        acc[7] = acc[7] + (double)(phipf * (qxxp * scx + qyyp * scy + qzzp * scz));
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) COL(s.vis, k)[i] = acc[k];
+}
+
+// ---------------------------------------------------------------------------
+static inline unsigned grid_for(long long n, int block) {
+    return (unsigned)((n + block - 1) / block);
+}
+
+#define MARK(k) do { if (hook) hook->mark(hook->ctx, (k)); } while (0)
+
+static void enqueue_start(const DevMesh& m, const void* stp, const DevParams& P, cudaStream_t st,
+                          int block, const StepHook* hook) {
+    const DevState<R>& s = *static_cast<const DevState<R>*>(stp);
+    MARK(KK_PRIM_START);
+    k_prim<PM_START><<<grid_for(m.neles, 256), 256, 0, st>>>(m, s, P);
+    MARK(KK_COUNT);
+}
+
+// One time step of src/main.F90:520-654 (after enqueue_start).
+static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, cudaStream_t st,
+                         int block, const StepHook* hook) {
+    const DevState<R>& s = *static_cast<const DevState<R>*>(stp);
+    const int b = block > 0 ? block : 128;
+    const unsigned ge = grid_for(m.neles, 256), gf = grid_for(m.neles, b);
+    const unsigned gg = grid_for(m.nghosts > 0 ? m.nghosts : 1, 256);
+    MARK(KK_STEP_BEGIN);
+    k_step_begin<<<1, 1, 0, st>>>(s, P);
+    // JST dissipation, src/sr_smooth.F90 (once per step)
+    if (m.aliased) { MARK(KK_SERIAL); k_smooth_copy_serial<<<1, 1, 0, st>>>(m, s, 0); }
+    MARK(KK_SMOOTH1);
+    k_smooth1<<<ge, 256, 0, st>>>(m, s);
+    if (m.aliased) { MARK(KK_SERIAL); k_smooth_copy_serial<<<1, 1, 0, st>>>(m, s, 1); }
+    MARK(KK_SMOOTH2);
+    k_smooth2<<<ge, 256, 0, st>>>(m, s, P);
+    // viscous fluxes, src/sr_viscousgp.F90 (stage 1 of each step)
+    if (m.nghosts > 0) {
+        MARK(KK_BC_VISC);
+        if (m.aliased) k_bc_serial<true><<<1, 1, 0, st>>>(m, s, P);
+        else k_bc<true><<<gg, 256, 0, st>>>(m, s, P);
+    }
+    if (!P.inviscid) { MARK(KK_VISC); k_visc<<<gf, b, 0, st>>>(m, s, P); }
+    for (int stage = 1; stage <= P.nstage; stage++) {
+        // src/sr_hllcbatten.F90:29-33: primitiveplusbc, derivative, limiter
+        MARK(KK_PRIM_STAGE);
+        k_prim<PM_STAGE><<<ge, 256, 0, st>>>(m, s, P);
+        if (m.nghosts > 0) {
+            MARK(KK_BC);
+            if (m.aliased) k_bc_serial<false><<<1, 1, 0, st>>>(m, s, P);
+            else k_bc<false><<<gg, 256, 0, st>>>(m, s, P);
+        }
+        if (P.myorder == 2) {
+            MARK(KK_GRAD);
+            k_grad<<<gf, b, 0, st>>>(m, s, P);
+            if (m.aliased) { MARK(KK_SERIAL); k_phi_copy_serial<<<1, 1, 0, st>>>(m, s); }
+        }
+        MARK(KK_FLUX);
+        if (m.aliased) {
+            k_flux<true><<<gf, b, 0, st>>>(m, s, P, stage);
+            MARK(KK_SERIAL);
+            k_flux_carry<<<1, 1, 0, st>>>(m, s, P);
+        } else {
+            k_flux<false><<<gf, b, 0, st>>>(m, s, P, stage);
+        }
+    }
+    // src/main.F90:595-641: primitive, residual norms, cu = cn
+    MARK(KK_PRIM_END);
+    k_prim<PM_END><<<ge, 256, 0, st>>>(m, s, P);
+    MARK(KK_STEP_END);
+    k_step_end<<<1, 1, 0, st>>>(s);
+    // start of the next step: primitive + dt contributions
+    MARK(KK_PRIM_START);
+    k_prim<PM_START><<<ge, 256, 0, st>>>(m, s, P);
+    MARK(KK_COUNT);
+}
+#undef MARK
+
+}  // namespace HP_NS
+}  // namespace hp

@@ -1,0 +1,8 @@
+// Precision variant "mixed": flux/gradient arithmetic in float.
+#define HP_NS v_mixed
+#define HP_R float
+#include "hp_kernels.cuh"
+
+namespace hp {
+const Variant variant_mixed = {"mixed", sizeof(float), &v_mixed::enqueue_start, &v_mixed::enqueue_step, 0};
+}

@@ -1,0 +1,211 @@
+"""Python mirror of the engine's C ABI: one ``Case`` per mesh on the GPU.
+
+The method names follow the reference's time loop (src/main.F90:511-657):
+``init_uniform`` is INIT_COND, ``set_state`` is the restart read,
+``step`` runs main-loop iterations, ``state`` is what the restart writer
+dumps.  Arrays use the reference's layout: conserved state column-major
+(10, neles) in reference cell order, ghost primitives (6, nghosts) in
+ghost-list order.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import (KERNEL_KINDS, HpDiag, HpMesh, HpParams, HydraError, PREC_FP64_PARITY, lib)
+
+FLOW_FIELDS = (
+    "pmax", "pmin", "tgmax", "tgmin", "ugmax", "ugmin", "vgmax", "vgmin", "wgmax", "wgmin",
+    "upmax", "upmin", "vpmax", "vpmin", "wpmax", "wpmin", "tpmax", "tpmin", "pinf", "gamap",
+    "gamag", "cpp", "cpg", "amolg", "prg", "epslnmax", "epslnmin", "epslninf", "phipzero", "cfl",
+    "niter", "itersub", "istart", "diap", "surfacetension", "myflux", "myorder", "as_", "ts")
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _check(rc: int, h=None):
+    if rc != 0:
+        L = lib()
+        msg = (L.hp_last_error(h) if h else L.hp_create_error()) or b""
+        raise HydraError(rc, msg.decode(errors="replace"))
+
+
+def make_params(flow: dict | None = None, **over) -> HpParams:
+    """hp_params from a flow.in dict (names as in the reference, ``as_`` for
+    ``as``) plus engine switches (precision, renumber, use_graph, ...)."""
+    p = HpParams()
+    p.venkat_k = 0.3
+    p.myflux = 2
+    p.myorder = 2
+    p.renumber = 1
+    p.use_graph = 1
+    p.precision = PREC_FP64_PARITY
+    for src in (flow or {}), over:
+        for k, v in src.items():
+            if k == "as":
+                k = "as_"
+            setattr(p, k, v)
+    return p
+
+
+@dataclass
+class MeshArrays:
+    """Mesh in the reference's in-memory form (sr_geometry.F90:101-139)."""
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    elem: np.ndarray    # (neles, 9) int32: nod1..4, nc1..4, iblank
+    ghost: np.ndarray   # (nghosts, 4) int32: nparent, nghost, ntype, nside
+
+    @property
+    def nodes(self):
+        return int(self.x.shape[0])
+
+    @property
+    def neles(self):
+        return int(self.elem.shape[0])
+
+    @property
+    def nghosts(self):
+        return int(self.ghost.shape[0])
+
+
+class Case:
+    """One mesh + solution resident on the current CUDA device."""
+
+    def __init__(self, mesh: MeshArrays, params: HpParams):
+        self.L = lib()
+        self.mesh = mesh
+        self.params = params
+        self._keep = [np.ascontiguousarray(mesh.x, np.float64), np.ascontiguousarray(mesh.y, np.float64),
+                      np.ascontiguousarray(mesh.z, np.float64), np.ascontiguousarray(mesh.elem, np.int32),
+                      np.ascontiguousarray(mesh.ghost, np.int32)]
+        x, y, z, el, gh = self._keep
+        hm = HpMesh(mesh.nodes, mesh.neles, mesh.nghosts, 0, _dp(x), _dp(y), _dp(z), _ip(el), _ip(gh))
+        h = ctypes.c_void_p()
+        _check(self.L.hp_create(ctypes.byref(hm), ctypes.byref(params), ctypes.byref(h)))
+        self.h = h
+        self.neles = mesh.neles
+        self.nghosts = mesh.nghosts
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def init_uniform(self):
+        _check(self.L.hp_init_uniform(self.h), self.h)
+
+    def set_state(self, time: float, cu: np.ndarray, ghost_prims: np.ndarray | None = None):
+        cu = np.ascontiguousarray(cu, np.float64).reshape(-1)
+        if cu.size != 10 * self.neles:
+            raise ValueError("cu must hold 10 x neles values")
+        gp = None if ghost_prims is None else np.ascontiguousarray(ghost_prims, np.float64).reshape(-1)
+        _check(self.L.hp_set_state(self.h, float(time), _dp(cu), _dp(gp)), self.h)
+
+    def step(self, nsteps: int, diagnostics: bool = True):
+        """Run nsteps; returns a dict of per-step arrays (or None)."""
+        if not diagnostics:
+            _check(self.L.hp_step(self.h, int(nsteps), None), self.h)
+            return None
+        d = (HpDiag * max(int(nsteps), 1))()
+        _check(self.L.hp_step(self.h, int(nsteps), d), self.h)
+        arr = np.frombuffer(d, dtype=np.float64).reshape(-1, 8)[:nsteps]
+        return {"time": arr[:, 0].copy(), "dt": arr[:, 1].copy(), "velmag": arr[:, 2].copy(),
+                "diff": arr[:, 3:7].copy(), "nan_cells": arr[:, 7].copy()}
+
+    def sync(self):
+        _check(self.L.hp_sync(self.h), self.h)
+
+    def step_timed(self, nsteps: int) -> float:
+        """Run nsteps; device milliseconds from CUDA events on the case's stream."""
+        ms = ctypes.c_double()
+        _check(self.L.hp_step_timed(self.h, int(nsteps), ctypes.byref(ms)), self.h)
+        return ms.value
+
+    def profile(self, nsteps: int) -> dict:
+        """Per-kernel-kind device time of nsteps launched eagerly with events."""
+        n = len(KERNEL_KINDS)
+        ms = np.zeros(n)
+        cnt = np.zeros(n, np.int64)
+        _check(self.L.hp_profile_steps(self.h, int(nsteps), _dp(ms),
+                                       cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n), self.h)
+        return {"kinds": list(KERNEL_KINDS), "ms": ms.tolist(), "launches": cnt.tolist()}
+
+    def state(self):
+        t = ctypes.c_double()
+        cu = np.zeros(10 * self.neles)
+        gp = np.zeros(6 * max(self.nghosts, 1))
+        _check(self.L.hp_get_state(self.h, ctypes.byref(t), _dp(cu), _dp(gp)), self.h)
+        return t.value, cu.reshape(10, self.neles), gp[:6 * self.nghosts].reshape(6, self.nghosts)
+
+    def prims(self):
+        out = np.zeros(14 * self.neles)
+        _check(self.L.hp_get_prims(self.h, _dp(out)), self.h)
+        return out.reshape(14, self.neles)
+
+    def info(self):
+        k, b, a = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(self.L.hp_info(self.h, ctypes.byref(k), ctypes.byref(b), ctypes.byref(a)), self.h)
+        return {"kernels_per_step": k.value, "device_bytes": b.value, "aliased": bool(a.value)}
+
+
+# --- reference file formats through the C ABI --------------------------------
+def read_flow(path: str) -> HpParams:
+    p = HpParams()
+    _check(lib().hp_read_flow(path.encode(), ctypes.byref(p)))
+    return p
+
+
+def read_mesh(case_dir: str, rank: int = 0) -> MeshArrays:
+    L = lib()
+    m = HpMesh()
+    _check(L.hp_read_mesh(case_dir.encode(), rank, ctypes.byref(m)))
+    try:
+        if m.pghosts:
+            raise HydraError(-6, "partition ghosts are not supported (one partition per GPU)")
+        x = np.ctypeslib.as_array(m.x, (m.nodes,)).copy()
+        y = np.ctypeslib.as_array(m.y, (m.nodes,)).copy()
+        z = np.ctypeslib.as_array(m.z, (m.nodes,)).copy()
+        el = np.ctypeslib.as_array(m.elem, (m.neles * 9,)).reshape(m.neles, 9).copy()
+        gh = (np.ctypeslib.as_array(m.ghost, (m.nghosts * 4,)).reshape(m.nghosts, 4).copy()
+              if m.nghosts else np.zeros((0, 4), np.int32))
+    finally:
+        L.hp_free_mesh(ctypes.byref(m))
+    return MeshArrays(x, y, z, el, gh)
+
+
+def read_restart(path: str, neles: int, nghosts: int):
+    t = ctypes.c_double()
+    cu = np.zeros(10 * neles)
+    gp = np.zeros(6 * max(nghosts, 1))
+    _check(lib().hp_read_restart(path.encode(), neles, nghosts, ctypes.byref(t), _dp(cu), _dp(gp)))
+    return t.value, cu.reshape(10, neles), gp[:6 * nghosts].reshape(6, nghosts)
+
+
+def write_restart(path: str, time: float, cu: np.ndarray, ghost_prims: np.ndarray):
+    cu = np.ascontiguousarray(cu, np.float64)
+    gp = np.ascontiguousarray(ghost_prims, np.float64)
+    neles = cu.size // 10
+    nghosts = gp.size // 6
+    _check(lib().hp_write_restart(path.encode(), neles, nghosts, float(time), _dp(cu), _dp(gp)))

@@ -48,7 +48,12 @@ struct or_case {
     double time, dt, dtmin;
     int total;
     double fstar[10];                        /* stale HLLC flux carry */
+    int aliased;                             /* ghost ids alias elements/each other */
 };
+
+/* Cell loops run in parallel only when the result cannot depend on the
+ * order (no aliased ghosts); ghost loops always run in reference order. */
+#define PAR(S) ((S)->aliased == 0 && g_threads > 1)
 
 /* ------------------------------------------------------------------ */
 /* Fortran MIN/MAX.  nan_mode 0: the pre-GCC-9 gfortran expansion
@@ -56,6 +61,9 @@ struct or_case {
  * which skips a NaN argument unless it comes first.  nan_mode 1: MIN_EXPR
  * as expanded on x86-64 SSE, (a < b ? a : b), returning b on NaN.        */
 static int g_nan_mode = 0;
+static int g_threads = 1;       /* OpenMP threads for non-aliased meshes */
+
+void or_set_threads(int n) { g_threads = n > 0 ? n : 1; }
 static inline double mn2(double a, double b) {
     if (g_nan_mode == 0) return (b < a || isnan(a)) ? b : a;
     return (a < b) ? a : b;
@@ -223,6 +231,17 @@ or_case *or_create(const or_params *p, int32_t nodes, int32_t neles,
         S->nparent[i] = r[0]; S->nghost[i] = r[1]; S->ntype[i] = r[2]; S->nside[i] = r[3];
         for (int t = 0; t < 7; t++)
             if (r[2] == types[t]) S->bcl[t][++S->nbc[t]] = i;   /* main.F90:239-275 */
+    }
+    {
+        char *seen = (char *)calloc(nt1, 1);
+        for (int i = 1; i <= nghosts && !S->aliased; i++) {
+            int g = S->nghost[i];
+            if (g <= neles || seen[g]) S->aliased = 1;
+            seen[g] = 1;
+        }
+        for (int i = 1; i <= nghosts && !S->aliased; i++)
+            if (S->nparent[i] > neles || seen[S->nparent[i]]) S->aliased = 1;
+        free(seen);
     }
     S->xcel = dalloc(nt1); S->ycel = dalloc(nt1); S->zcel = dalloc(nt1);
     S->vol = dalloc(nt1); S->dl = dalloc(nt1); S->dd = dalloc(nt1);
@@ -401,6 +420,7 @@ static void prim_head(or_case *S, int i, int with_sound) {
 }
 
 void or_primitive(or_case *S) {          /* src/sr_primitive.F90:18-178 */
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= S->neles; i++) { prim_head(S, i, 0); prim_tail(S, i); }
 }
 
@@ -578,6 +598,7 @@ static void bc_fill(or_case *S, int viscous) {
 }
 
 void or_primitiveplusbc(or_case *S) {    /* src/sr_primitiveplusbc.F90 */
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= S->neles; i++) { prim_head(S, i, 1); prim_tail(S, i); }
     bc_fill(S, 0);
     /* ghost cn, src/sr_primitiveplusbc.F90:602-631 */
@@ -604,6 +625,7 @@ void or_derivative(or_case *S) {
                        S->pg, S->pp, S->phig, S->rog, S->rop};
     static const int gidx[13] = {G_UG, G_VG, G_WG, G_TG, G_UP, G_VP, G_WP, G_TP,
                                  G_PG, G_PP, G_PHIG, G_ROG, G_ROP};
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= S->neles; i++) {
         if (S->iblank[i] != 1) continue;
         int n1 = S->nc[0][i], n2 = S->nc[1][i], n3 = S->nc[2][i], n4 = S->nc[3][i];
@@ -650,6 +672,7 @@ static double venk_face(double dface, double vmax, double vmin, double vi, doubl
 void or_venkat(or_case *S) {
     const double *x = S->x, *y = S->y, *z = S->z;
     double K = S->p.venkat_k;
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= S->neles; i++) {
         if (S->iblank[i] != 1) continue;
         double epssq = pow(K * S->dl[i], 3.0);
@@ -695,6 +718,7 @@ void or_smooth(or_case *S) {
         for (int k = 1; k <= 10; k++) CN(ng, k) = CN(np, k);
     }
     const double e6 = R4(1.0e-6);
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= S->neles; i++) {
         int a = S->nc[0][i], b = S->nc[1][i], c = S->nc[2][i], d = S->nc[3][i];
         double *pg = S->pg, *pp = S->pp;
@@ -729,6 +753,7 @@ void or_smooth(or_case *S) {
         ANU(ng, 2) = ANU(np, 2);
     }
     double dt = S->dt;
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= S->neles; i++) {
         int nb[4] = {S->nc[0][i], S->nc[1][i], S->nc[2][i], S->nc[3][i]};
         for (int set = 0; set < 2; set++) {
@@ -792,9 +817,12 @@ static void hllc_batten(or_case *S) {
     const double eps8 = R4(1.0e-8), eps6 = R4(1.0e-6);
     double rrg = S->rrg, gamag = p->gamag, gamap = p->gamap, pinf = p->pinf, cpp = p->cpp;
     int neles = S->neles, nghosts = S->nghosts;
-    double *F = S->fstar;
+    const int par = PAR(S);
+#pragma omp parallel for num_threads(g_threads) if (par) schedule(static)
     for (int i = 1; i <= neles; i++) {
         if (S->iblank[i] != 1) continue;
+        double Floc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double *F = par ? Floc : S->fstar;
         for (int k = 1; k <= 10; k++) RHS(i, k) = 0.0;
         for (int f = 0; f < 4; f++) {
             int n1 = S->nod[HLL_FACE[f][0] - 1][i], n2 = S->nod[HLL_FACE[f][1] - 1][i],
@@ -955,6 +983,7 @@ static void hllc_batten(or_case *S) {
 /* Interphase sources, src/sr_source.F90:42-178 */
 static void source(or_case *S) {
     const or_params *p = &S->p;
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= S->neles; i++) {
         if (S->iblank[i] != 1) continue;
         double voli = S->vol[i];
@@ -1031,6 +1060,7 @@ void or_viscous(or_case *S) {
     if (p->inviscid) return;
     double *fld[8] = {S->ug, S->vg, S->wg, S->tg, S->up, S->vp, S->wp, S->tp};
     double c23 = S->c23;
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= S->neles; i++) {
         if (S->iblank[i] != 1) continue;
         for (int f = 0; f < 4; f++) {
@@ -1127,6 +1157,7 @@ void or_viscous(or_case *S) {
 /* RK stages, src/sr_RK.F90:19-164 (rk_scheme 0) or Shu-Osher SSP-RK3 */
 static void stage(or_case *S, int st) {
     int ne = S->neles;
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
     for (int i = 1; i <= ne; i++) {
         if (S->iblank[i] != 1) continue;
         double dtbyvol = S->dt / S->vol[i];
@@ -1172,13 +1203,24 @@ static void one_step(or_case *S, double *diff4, double *velmag) {
     S->total++;
     or_primitive(S);
     S->dtmin = 1.0e8;
-    for (int i = 1; i <= S->neles; i++) {
-        S->ag[i] = sqrt((p->gamag * S->pg[i]) / S->rog[i]);
-        S->ap[i] = sqrt((p->gamap * (S->pp[i] + p->pinf)) / S->rop[i]);
-        double qgi = sqrt(sq(S->ug[i]) + sq(S->vg[i]) + sq(S->wg[i]));
-        double qpi = sqrt(sq(S->up[i]) + sq(S->vp[i]) + sq(S->wp[i]));
-        S->dtmin = mn2(S->dtmin, S->dl[i] / (mx2(S->ag[i], S->ap[i]) + mx2(qgi, qpi)));
+    /* min over cells skipping NaN: exact in any order, so chunks are
+     * reduced per thread and combined */
+    double dtmin = 1.0e8;
+#pragma omp parallel num_threads(g_threads) if (PAR(S))
+    {
+        double loc = 1.0e8;
+#pragma omp for schedule(static)
+        for (int i = 1; i <= S->neles; i++) {
+            S->ag[i] = sqrt((p->gamag * S->pg[i]) / S->rog[i]);
+            S->ap[i] = sqrt((p->gamap * (S->pp[i] + p->pinf)) / S->rop[i]);
+            double qgi = sqrt(sq(S->ug[i]) + sq(S->vg[i]) + sq(S->wg[i]));
+            double qpi = sqrt(sq(S->up[i]) + sq(S->vp[i]) + sq(S->wp[i]));
+            loc = mn2(loc, S->dl[i] / (mx2(S->ag[i], S->ap[i]) + mx2(qgi, qpi)));
+        }
+#pragma omp critical
+        dtmin = mn2(dtmin, loc);
     }
+    S->dtmin = dtmin;
     S->dt = S->dtmin * p->cfl;
     S->time = S->time + S->dt;
     or_smooth(S);

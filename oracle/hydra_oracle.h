@@ -90,6 +90,10 @@ void or_get_vis(const or_case *c, double *out);         /* 8 x neles */
 void or_get_grad(const or_case *c, double *out);        /* 33 x ntot + phi */
 double or_last_dt(const or_case *c);
 
+/* OpenMP threads for the cell loops of meshes without aliased ghost ids
+ * (results are identical for any thread count). */
+void or_set_threads(int n);
+
 /* Individual phases of one step for unit checks of single kernels. */
 void or_primitive(or_case *c);
 void or_primitiveplusbc(or_case *c);

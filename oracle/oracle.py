@@ -232,7 +232,13 @@ def lib():
                    "or_smooth", "or_viscous", "or_flux"):
             getattr(L, fn).argtypes = [ctypes.c_void_p]
         L.or_set_dt.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.or_set_threads.argtypes = [ctypes.c_int]
     return _lib
+
+
+def set_threads(n: int) -> None:
+    """Threads for the cell loops (meshes without aliased ghosts only)."""
+    lib().or_set_threads(int(n))
 
 
 def _dp(a):
