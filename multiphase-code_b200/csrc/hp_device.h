@@ -33,6 +33,8 @@ struct DevParams {
     double ugmin, vgmin, wgmin, upmin, vpmin, wpmin, tgmin, tpmin, pmin;
     double as, ts, c23, co2, co4, fsd;   // fsd = 4 sigma / d
     double cfl, venkat_k, twall, amup;
+    // correctly rounded reciprocals of constant divisors
+    double r_emm, r_gm1, r_gamap, r_prg, r_prp;
     int rk_scheme, inviscid, myorder, nstage;
 };
 
@@ -48,6 +50,13 @@ struct DevMesh {
     const double* sc;       // [12][ld] face area vectors sc1x..sc4z
     const double* fch;      // [12][ld] face centroids, 0.3333 factor (HLLC, VK)
     const double* fcv;      // [12][ld] face centroids, /3 (viscous)
+    // geometry-only least-squares terms, evaluated once at set-up with the
+    // reference's expressions: [0..3] weights, [4..9] a1 a2 a3 b1 b2 b3,
+    // [10] the determinant; LSQA for the 1/r^2 cell gradients
+    // (src/sr_derivative.F90:163-176,255), LSQB for the 1/r gradient of
+    // alpha_g in the sources (src/sr_source.F90:100-117)
+    const double* lsqa;     // [11][ld]
+    const double* lsqb;     // [11][ld]
     const int *g_par, *g_id, *g_type;   // [nghosts] ghost list (reference order)
 };
 

@@ -233,6 +233,41 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
             dd[np] = (zc > (double)0.1f) ? std::fabs(zmax - zc) : std::fabs(zmin - zc);
         }
     }
+    // --- static least-squares terms of the gradient and source operators ---
+    std::vector<double> lsqa(11 * (size_t)(neles + 1), 0.0), lsqb(11 * (size_t)(neles + 1), 0.0);
+    auto LA = [&](int k, int i) -> double& { return lsqa[(size_t)k * (neles + 1) + i]; };
+    auto LB = [&](int k, int i) -> double& { return lsqb[(size_t)k * (neles + 1) + i]; };
+    for (int i = 1; i <= neles; i++) {
+        double xa[4], ya[4], za[4], wa[4], wb[4];
+        for (int f = 0; f < 4; f++) {
+            int nb = nc[f][i];
+            xa[f] = xcel[nb] - xcel[i];
+            ya[f] = ycel[nb] - ycel[i];
+            za[f] = zcel[nb] - zcel[i];
+            wa[f] = sq(xa[f]) + sq(ya[f]) + sq(za[f]);
+            wb[f] = std::sqrt(sq(xa[f]) + sq(ya[f]) + sq(za[f]));
+        }
+        // src/sr_derivative.F90:163-176 and :255
+        double a1 = sq(xa[0]) / wa[0] + sq(xa[1]) / wa[1] + sq(xa[2]) / wa[2] + sq(xa[3]) / wa[3];
+        double a2 = sq(ya[0]) / wa[0] + sq(ya[1]) / wa[1] + sq(ya[2]) / wa[2] + sq(ya[3]) / wa[3];
+        double a3 = sq(za[0]) / wa[0] + sq(za[1]) / wa[1] + sq(za[2]) / wa[2] + sq(za[3]) / wa[3];
+        double b1 = xa[0] * ya[0] / wa[0] + xa[1] * ya[1] / wa[1] + xa[2] * ya[2] / wa[2] + xa[3] * ya[3] / wa[3];
+        double b2 = xa[0] * za[0] / wa[0] + xa[1] * za[1] / wa[1] + xa[2] * za[2] / wa[2] + xa[3] * za[3] / wa[3];
+        double b3 = za[0] * ya[0] / wa[0] + za[1] * ya[1] / wa[1] + za[2] * ya[2] / wa[2] + za[3] * ya[3] / wa[3];
+        for (int f = 0; f < 4; f++) LA(f, i) = wa[f];
+        LA(4, i) = a1; LA(5, i) = a2; LA(6, i) = a3; LA(7, i) = b1; LA(8, i) = b2; LA(9, i) = b3;
+        LA(10, i) = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+        // src/sr_source.F90:100-117
+        a1 = sq(xa[0]) / wb[0] + sq(xa[1]) / wb[1] + sq(xa[2]) / wb[2] + sq(xa[3]) / wb[3];
+        a2 = sq(ya[0]) / wb[0] + sq(ya[1]) / wb[1] + sq(ya[2]) / wb[2] + sq(ya[3]) / wb[3];
+        a3 = sq(za[0]) / wb[0] + sq(za[1]) / wb[1] + sq(za[2]) / wb[2] + sq(za[3]) / wb[3];
+        b1 = xa[0] * ya[0] / wb[0] + xa[1] * ya[1] / wb[1] + xa[2] * ya[2] / wb[2] + xa[3] * ya[3] / wb[3];
+        b2 = xa[0] * za[0] / wb[0] + xa[1] * za[1] / wb[1] + xa[2] * za[2] / wb[2] + xa[3] * za[3] / wb[3];
+        b3 = ya[0] * za[0] / wb[0] + ya[1] * za[1] / wb[1] + ya[2] * za[2] / wb[2] + ya[3] * za[3] / wb[3];
+        for (int f = 0; f < 4; f++) LB(f, i) = wb[f];
+        LB(4, i) = a1; LB(5, i) = a2; LB(6, i) = a3; LB(7, i) = b1; LB(8, i) = b2; LB(9, i) = b3;
+        LB(10, i) = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+    }
     // --- aliasing: ghost slots that are elements, repeated, or ghost parents ---
     {
         std::vector<char> seen(ntot + 1, 0);
@@ -284,6 +319,7 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     std::vector<unsigned> hfk(ld, 0u);
     std::vector<double> hx(ld, 0.0), hy(ld, 0.0), hz(ld, 0.0), hvol(ld, 0.0), hdl(ld, 0.0), hdd(ld, 0.0);
     std::vector<double> hsc(12 * ld, 0.0), hfch(12 * ld, 0.0), hfcv(12 * ld, 0.0);
+    std::vector<double> hla(11 * ld, 0.0), hlb(11 * ld, 0.0);
     std::vector<int> slot_parent(ntot + 1, 0);
     for (int g = 0; g < nghosts; g++) slot_parent[gid[g]] = gpar[g];
     for (int i = 1; i <= ntot; i++) {
@@ -310,6 +346,7 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
             for (int k = 0; k < 12; k++) {
                 hsc[k * ld + t] = SC(k, i); hfch[k * ld + t] = FCH(k, i); hfcv[k * ld + t] = FCV(k, i);
             }
+            for (int k = 0; k < 11; k++) { hla[k * ld + t] = LA(k, i); hlb[k * ld + t] = LB(k, i); }
         } else {
             for (int k = 0; k < 4; k++) { hnc[k * ld + t] = map(nc[k][i]); hsnb[k * ld + t] = map(nc[k][i]); }
         }
@@ -330,6 +367,11 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     P.fsd = 4.0 * p.surfacetension / p.diap;
     P.cfl = p.cfl; P.venkat_k = p.venkat_k > 0 ? p.venkat_k : 0.3; P.twall = p.twall; P.amup = 0.001;
     P.rk_scheme = p.rk_scheme; P.inviscid = p.inviscid; P.myorder = p.myorder;
+    P.r_emm = 1.0 / (P.emax - P.emin);
+    P.r_gm1 = 1.0 / (P.gamag - 1.0);
+    P.r_gamap = 1.0 / P.gamap;
+    P.r_prg = 1.0 / P.prg;
+    P.r_prp = 1.0 / P.prp;
     P.nstage = p.rk_scheme == 0 ? 4 : 3;
     switch (p.precision) {
         case HP_PREC_FP64_PARITY: h->var = &variant_fp64_parity; break;
@@ -352,6 +394,8 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
         m.vol = (double*)a.take(ld * D); m.dl = (double*)a.take(ld * D); m.dd = (double*)a.take(ld * D);
         m.sc = (double*)a.take(12 * ld * D); m.fch = (double*)a.take(12 * ld * D);
         m.fcv = (double*)a.take(12 * ld * D);
+        m.lsqa = (double*)a.take(11 * ld * D);
+        m.lsqb = (double*)a.take(11 * ld * D);
         m.g_par = (int*)a.take((nghosts + 1) * (size_t)I); m.g_id = (int*)a.take((nghosts + 1) * (size_t)I);
         m.g_type = (int*)a.take((nghosts + 1) * (size_t)I);
         DevState<double>& s = h->ds;
@@ -407,6 +451,8 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     if (e == cudaSuccess) e = up(m.sc, hsc.data(), 12 * ld * D);
     if (e == cudaSuccess) e = up(m.fch, hfch.data(), 12 * ld * D);
     if (e == cudaSuccess) e = up(m.fcv, hfcv.data(), 12 * ld * D);
+    if (e == cudaSuccess) e = up(m.lsqa, hla.data(), 11 * ld * D);
+    if (e == cudaSuccess) e = up(m.lsqb, hlb.data(), 11 * ld * D);
     if (e == cudaSuccess && nghosts) e = up(m.g_par, hgpar.data(), nghosts * (size_t)I);
     if (e == cudaSuccess && nghosts) e = up(m.g_id, hgid.data(), nghosts * (size_t)I);
     if (e == cudaSuccess && nghosts) e = up(m.g_type, hgtyp.data(), nghosts * (size_t)I);

@@ -53,6 +53,49 @@ __device__ __forceinline__ float cube_rn(float a) { return (float)cube_rn((doubl
 
 template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 
+// a / b when RN(1/b) = rb is already known (divisors reused within a cell):
+// two FMA correction steps after q0 = RN(a * rb) give the IEEE
+// round-to-nearest quotient (Markstein's theorem: rb correctly rounded and q1
+// within one ulp make RN(q1 + (a - b q1) rb) = RN(a / b)).  Operands near the
+// overflow / underflow range take the hardware division.  The XU pipe that
+// IEEE division uses for its reciprocal seed is the bottleneck of these
+// kernels; this form runs on the FP64 pipe only.
+__device__ __noinline__ double div_slow(double a, double b) { return a / b; }
+#ifndef HP_DIV_MARKSTEIN
+#define HP_DIV_MARKSTEIN 0
+#endif
+__device__ __forceinline__ double div_rn(double a, double b, double rb) {
+#if HP_DIV_MARKSTEIN
+    double q0 = a * rb;
+    double r0 = fma(-b, q0, a);
+    double q1 = fma(r0, rb, q0);
+    double r1 = fma(-b, q1, a);
+    double q2 = fma(r1, rb, q1);
+    // results outside [2^-960, 2^960) (zero, denormal, inf, NaN, or operands
+    // near the range limits) take the hardware division
+    const unsigned eq = (unsigned)(__double2hiint(q2) >> 20) & 0x7ffu;
+    if (__builtin_expect(eq - 63u > 1919u, 0)) q2 = div_slow(a, b);
+    return q2;
+#else
+    (void)rb;
+    return a / b;
+#endif
+}
+// the mixed variant divides approximately
+__device__ __forceinline__ float div_rn(float a, float b, float rb) { return a * rb; }
+#if HP_DIV_MARKSTEIN
+template <class T> __device__ __forceinline__ T rcp(T b) { return T(1) / b; }
+#else
+__device__ __forceinline__ double rcp(double) { return 0.0; }
+__device__ __forceinline__ float rcp(float b) { return 1.0f / b; }
+#endif
+
+// Value of lane q of this thread's group of four consecutive lanes.
+template <class T>
+__device__ __forceinline__ T qshfl(T v, int q) {
+    return __shfl_sync(0xffffffffu, v, (int)((threadIdx.x & 31) & ~3u) + q);
+}
+
 #define COL(ptr, k) ((ptr) + (size_t)(k) * (size_t)m.ld)
 
 // ---------------------------------------------------------------------------
@@ -76,7 +119,7 @@ __device__ __forceinline__ void blend_phases(const DevParams& P, double& phig, d
         up = ug; vp = vg; wp = wg; tp = tg; pp = pg;
     }
     if (phig >= emin && phig <= emax) {
-        double psig = (phig - emin) / (emax - emin);
+        double psig = div_rn(phig - emin, emax - emin, P.r_emm);
         double f = -(psig * psig * (2.0 * psig - 3.0));
         ug = f * ug + (1.0 - f) * up;
         vg = f * vg + (1.0 - f) * vp;
@@ -85,7 +128,7 @@ __device__ __forceinline__ void blend_phases(const DevParams& P, double& phig, d
         pg = f * pg + (1.0 - f) * pp;
     }
     if (phip >= emin && phip <= emax) {
-        double psig = (phip - emin) / (emax - emin);
+        double psig = div_rn(phip - emin, emax - emin, P.r_emm);
         double f = -(psig * psig * (2.0 * psig - 3.0));
         up = f * up + (1.0 - f) * ug;
         vp = f * vp + (1.0 - f) * vg;
@@ -97,10 +140,11 @@ __device__ __forceinline__ void blend_phases(const DevParams& P, double& phig, d
 
 __device__ __forceinline__ void prim_full(double c[10], PrimV& q, const DevParams& P) {
     const double gamag = P.gamag, gamap = P.gamap, pinf = P.pinf;
-    q.ug = c[1] / c[0]; q.vg = c[2] / c[0]; q.wg = c[3] / c[0];
-    q.up = c[6] / c[5]; q.vp = c[7] / c[5]; q.wp = c[8] / c[5];
-    double eg = c[4] / c[0] - 0.5 * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
-    double ep = c[9] / c[5] - 0.5 * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
+    const double r0 = rcp(c[0]), r5 = rcp(c[5]);
+    q.ug = div_rn(c[1], c[0], r0); q.vg = div_rn(c[2], c[0], r0); q.wg = div_rn(c[3], c[0], r0);
+    q.up = div_rn(c[6], c[5], r5); q.vp = div_rn(c[7], c[5], r5); q.wp = div_rn(c[8], c[5], r5);
+    double eg = div_rn(c[4], c[0], r0) - 0.5 * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+    double ep = div_rn(c[9], c[5], r5) - 0.5 * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
     double bbb = (P.fsd + pinf * gamap) - (c[0] * (gamag - 1.0) * eg) - (c[5] * (gamap - 1.0) * ep);
     double ccc = c[0] * (gamag - 1.0) * eg * (P.fsd + pinf * gamap);
     q.pg = (-bbb + sqrt(bbb * bbb + 4.0 * ccc)) * 0.5;
@@ -494,6 +538,7 @@ __global__ void __launch_bounds__(256) k_smooth2(DevMesh m, DevState<R> s, DevPa
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     const double dt = s.s->dt;
+    const double rdt = rcp(dt);
     int nb[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) nb[f] = ldg(COL(m.snb, f) + i);
@@ -507,7 +552,7 @@ __global__ void __launch_bounds__(256) k_smooth2(DevMesh m, DevState<R> s, DevPa
         for (int f = 0; f < 4; f++) {
             double e2 = P.co2 * mx2(ai, anu[nb[f]]);
             double e4 = mx2(0.0, P.co4 - e2);
-            double d24nc = 0.5 * (voli / dt + ldg(m.vol + nb[f]) / dt);
+            double d24nc = 0.5 * (div_rn(voli, dt, rdt) + div_rn(ldg(m.vol + nb[f]), dt, rdt));
             d2c[f] = e2 * d24nc;
             d4c[f] = e4 * d24nc;
         }
@@ -543,16 +588,28 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParam
         ya[f] = (R)(ldg(m.yc + n[f]) - y0);
         za[f] = (R)(ldg(m.zc + n[f]) - z0);
     }
-    R wt[4];
+    // geometry-only terms (wt, a1..b3, dnr of src/sr_derivative.F90:163-176,
+    // 255), evaluated once at set-up with the same expressions
+    R wt[4], rw[4];
+#define DW(x, f) div_rn((x), wt[f], rw[f])
+#if HP_LSQ_TABLE
 #pragma unroll
-    for (int f = 0; f < 4; f++) wt[f] = xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f];
-    R a1 = xa[0] * xa[0] / wt[0] + xa[1] * xa[1] / wt[1] + xa[2] * xa[2] / wt[2] + xa[3] * xa[3] / wt[3];
-    R a2 = ya[0] * ya[0] / wt[0] + ya[1] * ya[1] / wt[1] + ya[2] * ya[2] / wt[2] + ya[3] * ya[3] / wt[3];
-    R a3 = za[0] * za[0] / wt[0] + za[1] * za[1] / wt[1] + za[2] * za[2] / wt[2] + za[3] * za[3] / wt[3];
-    R b1 = xa[0] * ya[0] / wt[0] + xa[1] * ya[1] / wt[1] + xa[2] * ya[2] / wt[2] + xa[3] * ya[3] / wt[3];
-    R b2 = xa[0] * za[0] / wt[0] + xa[1] * za[1] / wt[1] + xa[2] * za[2] / wt[2] + xa[3] * za[3] / wt[3];
-    R b3 = za[0] * ya[0] / wt[0] + za[1] * ya[1] / wt[1] + za[2] * ya[2] / wt[2] + za[3] * ya[3] / wt[3];
-    R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+    for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqa, f) + i); rw[f] = rcp(wt[f]); }
+    const R a1 = (R)ldg(COL(m.lsqa, 4) + i), a2 = (R)ldg(COL(m.lsqa, 5) + i), a3 = (R)ldg(COL(m.lsqa, 6) + i);
+    const R b1 = (R)ldg(COL(m.lsqa, 7) + i), b2 = (R)ldg(COL(m.lsqa, 8) + i), b3 = (R)ldg(COL(m.lsqa, 9) + i);
+    const R dnr = (R)ldg(COL(m.lsqa, 10) + i);
+#else
+#pragma unroll
+    for (int f = 0; f < 4; f++) { wt[f] = xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]; rw[f] = rcp(wt[f]); }
+    const R a1 = DW(xa[0] * xa[0], 0) + DW(xa[1] * xa[1], 1) + DW(xa[2] * xa[2], 2) + DW(xa[3] * xa[3], 3);
+    const R a2 = DW(ya[0] * ya[0], 0) + DW(ya[1] * ya[1], 1) + DW(ya[2] * ya[2], 2) + DW(ya[3] * ya[3], 3);
+    const R a3 = DW(za[0] * za[0], 0) + DW(za[1] * za[1], 1) + DW(za[2] * za[2], 2) + DW(za[3] * za[3], 3);
+    const R b1 = DW(xa[0] * ya[0], 0) + DW(xa[1] * ya[1], 1) + DW(xa[2] * ya[2], 2) + DW(xa[3] * ya[3], 3);
+    const R b2 = DW(xa[0] * za[0], 0) + DW(xa[1] * za[1], 1) + DW(xa[2] * za[2], 2) + DW(xa[3] * za[3], 3);
+    const R b3 = DW(za[0] * ya[0], 0) + DW(za[1] * ya[1], 1) + DW(za[2] * ya[2], 2) + DW(za[3] * ya[3], 3);
+    const R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+#endif
+    const R rdnr = rcp(dnr);
     // fields in the order of the stored gradient columns, then rog, rop
     const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
     R gv[13][3];
@@ -561,16 +618,16 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParam
         const double* q = COL(s.pr, pcol[v]);
         double qi = q[i];
         R qa = (R)(q[n[0]] - qi), qb = (R)(q[n[1]] - qi), qc = (R)(q[n[2]] - qi), qd = (R)(q[n[3]] - qi);
-        R c1 = qa * xa[0] / wt[0] + qb * xa[1] / wt[1] + qc * xa[2] / wt[2] + qd * xa[3] / wt[3];
+        R c1 = DW(qa * xa[0], 0) + DW(qb * xa[1], 1) + DW(qc * xa[2], 2) + DW(qd * xa[3], 3);
         R c2;
         if (v == 7)   // cTp2 lacks the /wt4 (src/sr_derivative.F90:225)
-            c2 = qa * ya[0] / wt[0] + qb * ya[1] / wt[1] + qc * ya[2] / wt[2] + qd * ya[3];
+            c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + qd * ya[3];
         else
-            c2 = qa * ya[0] / wt[0] + qb * ya[1] / wt[1] + qc * ya[2] / wt[2] + qd * ya[3] / wt[3];
-        R c3 = qa * za[0] / wt[0] + qb * za[1] / wt[1] + qc * za[2] / wt[2] + qd * za[3] / wt[3];
-        gv[v][0] = det3(c1, c2, c3, b1, a2, b3, b2, b3, a3) / dnr;
-        gv[v][1] = det3(a1, b1, b2, c1, c2, c3, b2, b3, a3) / dnr;
-        gv[v][2] = det3(a1, b1, b2, b1, a2, b3, c1, c2, c3) / dnr;
+            c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + DW(qd * ya[3], 3);
+        R c3 = DW(qa * za[0], 0) + DW(qb * za[1], 1) + DW(qc * za[2], 2) + DW(qd * za[3], 3);
+        gv[v][0] = div_rn(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr);
+        gv[v][1] = div_rn(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr);
+        gv[v][2] = div_rn(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr);
     }
 #pragma unroll
     for (int v = 0; v < 11; v++) {
@@ -632,14 +689,14 @@ __device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& p
         up = ug; vp = vg; wp = wg; tp = tg; pp = pg;
     }
     if (phig >= emin && phig <= emax) {
-        R psig = (phig - emin) / (emax - emin);
+        R psig = div_rn(phig - emin, emax - emin, (R)P.r_emm);
         R f = -(psig * psig * (R(2) * psig - R(3)));
         ug = f * ug + (R(1) - f) * up; vg = f * vg + (R(1) - f) * vp;
         wg = f * wg + (R(1) - f) * wp; tg = f * tg + (R(1) - f) * tp;
         pg = f * pg + (R(1) - f) * pp;
     }
     if (phip >= emin && phip <= emax) {
-        R psig = (phip - emin) / (emax - emin);
+        R psig = div_rn(phip - emin, emax - emin, (R)P.r_emm);
         R f = -(psig * psig * (R(2) * psig - R(3)));
         up = f * up + (R(1) - f) * ug; vp = f * vp + (R(1) - f) * vg;
         wp = f * wp + (R(1) - f) * wg; tp = f * tp + (R(1) - f) * tg;
@@ -655,7 +712,8 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                  sczd = ldg(COL(m.sc, 3 * f + 2) + i);
     const R scx = (R)scxd, scy = (R)scyd, scz = (R)sczd;
     const R area = sqrt(scx * scx + scy * scy + scz * scz);
-    const R enx = scx / area, eny = scy / area, enz = scz / area;
+    const R rarea = rcp(area);
+    const R enx = div_rn(scx, area, rarea), eny = div_rn(scy, area, rarea), enz = div_rn(scz, area, rarea);
     const double* pr = s.pr;
     R ugL = (R)COL(pr, P_UG)[i], vgL = (R)COL(pr, P_VG)[i], wgL = (R)COL(pr, P_WG)[i];
     R tgL = (R)COL(pr, P_TG)[i], phigL = (R)COL(pr, P_PHIG)[i];
@@ -709,22 +767,26 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
         return;
     }
     const R eps8 = (R)(double)1.0e-8f, eps6 = (R)(double)1.0e-6f;
-    R egL = rrg * tgL / (gamag - R(1)) + R(0.5) * (ugL * ugL + vgL * vgL + wgL * wgL);
+    const R rgm1 = (R)P.r_gm1, rgamap = (R)P.r_gamap;
+    const R rropL = rcp(ropL), rropR = rcp(ropR);
+    R egL = div_rn(rrg * tgL, gamag - R(1), rgm1) + R(0.5) * (ugL * ugL + vgL * vgL + wgL * wgL);
     R hgL = egL + pgL / rogL;
     R qgL = ugL * enx + vgL * eny + wgL * enz;
     R agL = sqrt(gamag * pgL / rogL);
-    R egR = rrg * tgR / (gamag - R(1)) + R(0.5) * (ugR * ugR + vgR * vgR + wgR * wgR);
+    R egR = div_rn(rrg * tgR, gamag - R(1), rgm1) + R(0.5) * (ugR * ugR + vgR * vgR + wgR * wgR);
     R hgR = egR + pgR / rogR;
     R qgR = ugR * enx + vgR * eny + wgR * enz;
     R agR = sqrt(gamag * pgR / rogR);
-    R epL = (cpp * tpL) / gamap + pinf / ropL + R(0.5) * (upL * upL + vpL * vpL + wpL * wpL);
-    R hpL = epL + ppL / ropL;
+    R epL = div_rn(cpp * tpL, gamap, rgamap) + div_rn(pinf, ropL, rropL) +
+            R(0.5) * (upL * upL + vpL * vpL + wpL * wpL);
+    R hpL = epL + div_rn(ppL, ropL, rropL);
     R qpL = upL * enx + vpL * eny + wpL * enz;
-    R apL = sqrt(gamap * (ppL + pinf) / ropL);
-    R epR = (cpp * tpR) / gamap + pinf / ropR + R(0.5) * (upR * upR + vpR * vpR + wpR * wpR);
-    R hpR = epR + ppR / ropR;
+    R apL = sqrt(div_rn(gamap * (ppL + pinf), ropL, rropL));
+    R epR = div_rn(cpp * tpR, gamap, rgamap) + div_rn(pinf, ropR, rropR) +
+            R(0.5) * (upR * upR + vpR * vpR + wpR * wpR);
+    R hpR = epR + div_rn(ppR, ropR, rropR);
     R qpR = upR * enx + vpR * eny + wpR * enz;
-    R apR = sqrt(gamap * (ppR + pinf) / ropR);
+    R apR = sqrt(div_rn(gamap * (ppR + pinf), ropR, rropR));
     R sgl = mn2(mn2(qgL - agL, qgR - agR), eps8);
     R spl = mn2(mn2(qpL - apL, qpR - apR), eps8);
     R sgr = mx2(mx2(qgL + agL, qgR + agR), eps8);
@@ -753,11 +815,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 o.F[3] = fl3 * area; o.F[4] = fl4 * area;
             } else {
                 R dnrg = (sgstar - sgl) + eps6;
-                R cs0 = (qgL - sgl) * cn0 / dnrg;
-                R cs1 = ((qgL - sgl) * cn1 + phigL * (pgL * enx - pgstar * enx)) / dnrg;
-                R cs2 = ((qgL - sgl) * cn2 + phigL * (pgL * eny - pgstar * eny)) / dnrg;
-                R cs3 = ((qgL - sgl) * cn3 + phigL * (pgL * enz - pgstar * enz)) / dnrg;
-                R cs4 = ((qgL - sgl) * cn4 + phigL * (pgL * qgL - pgstar * sgstar)) / dnrg;
+                const R rd = rcp(dnrg);
+                R cs0 = div_rn((qgL - sgl) * cn0, dnrg, rd);
+                R cs1 = div_rn((qgL - sgl) * cn1 + phigL * (pgL * enx - pgstar * enx), dnrg, rd);
+                R cs2 = div_rn((qgL - sgl) * cn2 + phigL * (pgL * eny - pgstar * eny), dnrg, rd);
+                R cs3 = div_rn((qgL - sgl) * cn3 + phigL * (pgL * enz - pgstar * enz), dnrg, rd);
+                R cs4 = div_rn((qgL - sgl) * cn4 + phigL * (pgL * qgL - pgstar * sgstar), dnrg, rd);
                 o.F[0] = (fl0 + sgl * (cs0 - cn0)) * area;
                 o.F[1] = (fl1 + sgl * (cs1 - cn1)) * area;
                 o.F[2] = (fl2 + sgl * (cs2 - cn2)) * area;
@@ -777,11 +840,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 o.F[3] = fr3 * area; o.F[4] = fr4 * area;
             } else {
                 R dnrg = (sgstar - sgr) + eps6;
-                R cs0 = (qgR - sgr) * cn0 / dnrg;
-                R cs1 = ((qgR - sgr) * cn1 + phigR * (pgR * enx - pgstar * enx)) / dnrg;
-                R cs2 = ((qgR - sgr) * cn2 + phigR * (pgR * eny - pgstar * eny)) / dnrg;
-                R cs3 = ((qgR - sgr) * cn3 + phigR * (pgR * enz - pgstar * enz)) / dnrg;
-                R cs4 = ((qgR - sgr) * cn4 + phigR * (pgR * qgR - pgstar * sgstar)) / dnrg;
+                const R rd = rcp(dnrg);
+                R cs0 = div_rn((qgR - sgr) * cn0, dnrg, rd);
+                R cs1 = div_rn((qgR - sgr) * cn1 + phigR * (pgR * enx - pgstar * enx), dnrg, rd);
+                R cs2 = div_rn((qgR - sgr) * cn2 + phigR * (pgR * eny - pgstar * eny), dnrg, rd);
+                R cs3 = div_rn((qgR - sgr) * cn3 + phigR * (pgR * enz - pgstar * enz), dnrg, rd);
+                R cs4 = div_rn((qgR - sgr) * cn4 + phigR * (pgR * qgR - pgstar * sgstar), dnrg, rd);
                 o.F[0] = (fr0 + sgr * (cs0 - cn0)) * area;
                 o.F[1] = (fr1 + sgr * (cs1 - cn1)) * area;
                 o.F[2] = (fr2 + sgr * (cs2 - cn2)) * area;
@@ -808,11 +872,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 o.F[8] = fl3 * area; o.F[9] = fl4 * area;
             } else {
                 R dnrp = (spstar - spl) + eps6;
-                R cs0 = (qpL - spl) * cn0 / dnrp;
-                R cs1 = ((qpL - spl) * cn1 + phipL * (ppL * enx - ppstar * enx)) / dnrp;
-                R cs2 = ((qpL - spl) * cn2 + phipL * (ppL * eny - ppstar * eny)) / dnrp;
-                R cs3 = ((qpL - spl) * cn3 + phipL * (ppL * enz - ppstar * enz)) / dnrp;
-                R cs4 = ((qpL - spl) * cn4 + phipL * (ppL * qpL - ppstar * spstar)) / dnrp;
+                const R rd = rcp(dnrp);
+                R cs0 = div_rn((qpL - spl) * cn0, dnrp, rd);
+                R cs1 = div_rn((qpL - spl) * cn1 + phipL * (ppL * enx - ppstar * enx), dnrp, rd);
+                R cs2 = div_rn((qpL - spl) * cn2 + phipL * (ppL * eny - ppstar * eny), dnrp, rd);
+                R cs3 = div_rn((qpL - spl) * cn3 + phipL * (ppL * enz - ppstar * enz), dnrp, rd);
+                R cs4 = div_rn((qpL - spl) * cn4 + phipL * (ppL * qpL - ppstar * spstar), dnrp, rd);
                 o.F[5] = (fl0 + spl * (cs0 - cn0)) * area;
                 o.F[6] = (fl1 + spl * (cs1 - cn1)) * area;
                 o.F[7] = (fl2 + spl * (cs2 - cn2)) * area;
@@ -832,11 +897,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 o.F[8] = fr3 * area; o.F[9] = fr4 * area;
             } else {
                 R dnrp = (spstar - spr) + eps6;
-                R cs0 = (qpR - spr) * cn0 / dnrp;
-                R cs1 = ((qpR - spr) * cn1 + phipR * (ppR * enx - ppstar * enx)) / dnrp;
-                R cs2 = ((qpR - spr) * cn2 + phipR * (ppR * eny - ppstar * eny)) / dnrp;
-                R cs3 = ((qpR - spr) * cn3 + phipR * (ppR * enz - ppstar * enz)) / dnrp;
-                R cs4 = ((qpR - spr) * cn4 + phipR * (ppR * qpR - ppstar * spstar)) / dnrp;
+                const R rd = rcp(dnrp);
+                R cs0 = div_rn((qpR - spr) * cn0, dnrp, rd);
+                R cs1 = div_rn((qpR - spr) * cn1 + phipR * (ppR * enx - ppstar * enx), dnrp, rd);
+                R cs2 = div_rn((qpR - spr) * cn2 + phipR * (ppR * eny - ppstar * eny), dnrp, rd);
+                R cs3 = div_rn((qpR - spr) * cn3 + phipR * (ppR * enz - ppstar * enz), dnrp, rd);
+                R cs4 = div_rn((qpR - spr) * cn4 + phipR * (ppR * qpR - ppstar * spstar), dnrp, rd);
                 o.F[5] = (fr0 + spr * (cs0 - cn0)) * area;
                 o.F[6] = (fr1 + spr * (cs1 - cn1)) * area;
                 o.F[7] = (fr2 + spr * (cs2 - cn2)) * area;
@@ -945,9 +1011,10 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
                            (du * du + dv * dv + dw * dw);
         const R pint = pg - mn2(delpstar, R(0.01) * pg);
         const R den = phig * rog + (R(1) - phig) * rop;
-        const R uint_ = (phig * rog * ug + (R(1) - phig) * rop * up) / den;
-        const R vint = (phig * rog * vg + (R(1) - phig) * rop * vp) / den;
-        const R wint = (phig * rog * wg + (R(1) - phig) * rop * wp) / den;
+        const R rden = rcp(den);
+        const R uint_ = div_rn(phig * rog * ug + (R(1) - phig) * rop * up, den, rden);
+        const R vint = div_rn(phig * rog * vg + (R(1) - phig) * rop * vp, den, rden);
+        const R wint = div_rn(phig * rog * wg + (R(1) - phig) * rop * wp, den, rden);
         const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
         R xa[4], ya[4], za[4], pa[4], wt[4];
 #pragma unroll
@@ -957,21 +1024,35 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
             ya[f] = (R)(ldg(m.yc + n) - y0);
             za[f] = (R)(ldg(m.zc + n) - z0);
             pa[f] = (R)(COL(pr, P_PHIG)[n] - COL(pr, P_PHIG)[i]);
-            wt[f] = sqrt(xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]);
         }
-        R a1 = xa[0] * xa[0] / wt[0] + xa[1] * xa[1] / wt[1] + xa[2] * xa[2] / wt[2] + xa[3] * xa[3] / wt[3];
-        R a2 = ya[0] * ya[0] / wt[0] + ya[1] * ya[1] / wt[1] + ya[2] * ya[2] / wt[2] + ya[3] * ya[3] / wt[3];
-        R a3 = za[0] * za[0] / wt[0] + za[1] * za[1] / wt[1] + za[2] * za[2] / wt[2] + za[3] * za[3] / wt[3];
-        R b1 = xa[0] * ya[0] / wt[0] + xa[1] * ya[1] / wt[1] + xa[2] * ya[2] / wt[2] + xa[3] * ya[3] / wt[3];
-        R b2 = xa[0] * za[0] / wt[0] + xa[1] * za[1] / wt[1] + xa[2] * za[2] / wt[2] + xa[3] * za[3] / wt[3];
-        R b3 = ya[0] * za[0] / wt[0] + ya[1] * za[1] / wt[1] + ya[2] * za[2] / wt[2] + ya[3] * za[3] / wt[3];
-        R c1 = pa[0] * xa[0] / wt[0] + pa[1] * xa[1] / wt[1] + pa[2] * xa[2] / wt[2] + pa[3] * xa[3] / wt[3];
-        R c2 = pa[0] * ya[0] / wt[0] + pa[1] * ya[1] / wt[1] + pa[2] * ya[2] / wt[2] + pa[3] * ya[3] / wt[3];
-        R c3 = pa[0] * za[0] / wt[0] + pa[1] * za[1] / wt[1] + pa[2] * za[2] / wt[2] + pa[3] * za[3] / wt[3];
-        R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
-        R dpx = det3(c1, c2, c3, b1, a2, b3, b2, b3, a3) / dnr;
-        R dpy = det3(a1, b1, b2, c1, c2, c3, b2, b3, a3) / dnr;
-        R dpz = det3(a1, b1, b2, b1, a2, b3, c1, c2, c3) / dnr;
+        R rw[4];
+#if HP_LSQ_TABLE
+#pragma unroll
+        for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqb, f) + i); rw[f] = rcp(wt[f]); }
+        const R a1 = (R)ldg(COL(m.lsqb, 4) + i), a2 = (R)ldg(COL(m.lsqb, 5) + i), a3 = (R)ldg(COL(m.lsqb, 6) + i);
+        const R b1 = (R)ldg(COL(m.lsqb, 7) + i), b2 = (R)ldg(COL(m.lsqb, 8) + i), b3 = (R)ldg(COL(m.lsqb, 9) + i);
+#else
+#pragma unroll
+        for (int f = 0; f < 4; f++) { wt[f] = sqrt(xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]); rw[f] = rcp(wt[f]); }
+        const R a1 = DW(xa[0] * xa[0], 0) + DW(xa[1] * xa[1], 1) + DW(xa[2] * xa[2], 2) + DW(xa[3] * xa[3], 3);
+        const R a2 = DW(ya[0] * ya[0], 0) + DW(ya[1] * ya[1], 1) + DW(ya[2] * ya[2], 2) + DW(ya[3] * ya[3], 3);
+        const R a3 = DW(za[0] * za[0], 0) + DW(za[1] * za[1], 1) + DW(za[2] * za[2], 2) + DW(za[3] * za[3], 3);
+        const R b1 = DW(xa[0] * ya[0], 0) + DW(xa[1] * ya[1], 1) + DW(xa[2] * ya[2], 2) + DW(xa[3] * ya[3], 3);
+        const R b2 = DW(xa[0] * za[0], 0) + DW(xa[1] * za[1], 1) + DW(xa[2] * za[2], 2) + DW(xa[3] * za[3], 3);
+        const R b3 = DW(ya[0] * za[0], 0) + DW(ya[1] * za[1], 1) + DW(ya[2] * za[2], 2) + DW(ya[3] * za[3], 3);
+#endif
+        R c1 = DW(pa[0] * xa[0], 0) + DW(pa[1] * xa[1], 1) + DW(pa[2] * xa[2], 2) + DW(pa[3] * xa[3], 3);
+        R c2 = DW(pa[0] * ya[0], 0) + DW(pa[1] * ya[1], 1) + DW(pa[2] * ya[2], 2) + DW(pa[3] * ya[3], 3);
+        R c3 = DW(pa[0] * za[0], 0) + DW(pa[1] * za[1], 1) + DW(pa[2] * za[2], 2) + DW(pa[3] * za[3], 3);
+#if HP_LSQ_TABLE
+        const R dnr = (R)ldg(COL(m.lsqb, 10) + i);
+#else
+        const R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+#endif
+        const R rdnr = rcp(dnr);
+        R dpx = div_rn(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr);
+        R dpy = div_rn(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr);
+        R dpz = div_rn(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr);
         const R g = R(0);   // gravity (src/main.F90:341)
         R en = pint * (uint_ * dpx + vint * dpy + wint * dpz) + uint_ * fdgx + vint * fdgy + wint * fdgz + qsource;
         const double* vis = s.vis;
@@ -1014,106 +1095,422 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
 }
 
 // ---------------------------------------------------------------------------
+// k_grad with four lanes per cell: lane q computes the LSQ gradients of
+// fields q, q+4, q+8, q+12 and the limiter of one of pg, pp, rog, rop; phi is
+// the in-order minimum over the lanes (equal to the reference's chain when no
+// value is NaN).
+__global__ void __launch_bounds__(128, 4) k_grad4(DevMesh m, DevState<R> s, DevParams P) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (int)(gt & 3);
+    int i = (int)(gt >> 2);
+    const bool valid = i < m.neles;
+    if (!valid) i = m.neles - 1;
+    const bool active = valid && ldg(m.iblank + i) == 1;
+    int n[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
+    const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
+    R xa[4], ya[4], za[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        xa[f] = (R)(ldg(m.xc + n[f]) - x0);
+        ya[f] = (R)(ldg(m.yc + n[f]) - y0);
+        za[f] = (R)(ldg(m.zc + n[f]) - z0);
+    }
+    // geometry-only terms (wt, a1..b3, dnr of src/sr_derivative.F90:163-176,
+    // 255), evaluated once at set-up with the same expressions
+    R wt[4], rw[4];
+#define DW(x, f) div_rn((x), wt[f], rw[f])
+#if HP_LSQ_TABLE
+#pragma unroll
+    for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqa, f) + i); rw[f] = rcp(wt[f]); }
+    const R a1 = (R)ldg(COL(m.lsqa, 4) + i), a2 = (R)ldg(COL(m.lsqa, 5) + i), a3 = (R)ldg(COL(m.lsqa, 6) + i);
+    const R b1 = (R)ldg(COL(m.lsqa, 7) + i), b2 = (R)ldg(COL(m.lsqa, 8) + i), b3 = (R)ldg(COL(m.lsqa, 9) + i);
+    const R dnr = (R)ldg(COL(m.lsqa, 10) + i);
+#else
+#pragma unroll
+    for (int f = 0; f < 4; f++) { wt[f] = xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]; rw[f] = rcp(wt[f]); }
+    const R a1 = DW(xa[0] * xa[0], 0) + DW(xa[1] * xa[1], 1) + DW(xa[2] * xa[2], 2) + DW(xa[3] * xa[3], 3);
+    const R a2 = DW(ya[0] * ya[0], 0) + DW(ya[1] * ya[1], 1) + DW(ya[2] * ya[2], 2) + DW(ya[3] * ya[3], 3);
+    const R a3 = DW(za[0] * za[0], 0) + DW(za[1] * za[1], 1) + DW(za[2] * za[2], 2) + DW(za[3] * za[3], 3);
+    const R b1 = DW(xa[0] * ya[0], 0) + DW(xa[1] * ya[1], 1) + DW(xa[2] * ya[2], 2) + DW(xa[3] * ya[3], 3);
+    const R b2 = DW(xa[0] * za[0], 0) + DW(xa[1] * za[1], 1) + DW(xa[2] * za[2], 2) + DW(xa[3] * za[3], 3);
+    const R b3 = DW(za[0] * ya[0], 0) + DW(za[1] * ya[1], 1) + DW(za[2] * ya[2], 2) + DW(za[3] * ya[3], 3);
+    const R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+#endif
+    const R rdnr = rcp(dnr);
+    const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
+    // limiter field of this lane: pg (grad field 8), pp (9), rog (11), rop (12)
+    R lg[3] = {R(0), R(0), R(0)};     // gradient of the lane's limiter field
+    R sg[3] = {R(0), R(0), R(0)};     // gradient this lane forwards to another lane
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int v = q + 4 * r;
+        if (v >= 13) break;
+        const double* qq = COL(s.pr, pcol[v]);
+        double qi = qq[i];
+        R qa = (R)(qq[n[0]] - qi), qb = (R)(qq[n[1]] - qi), qc = (R)(qq[n[2]] - qi), qd = (R)(qq[n[3]] - qi);
+        R c1 = DW(qa * xa[0], 0) + DW(qb * xa[1], 1) + DW(qc * xa[2], 2) + DW(qd * xa[3], 3);
+        R c2;
+        if (v == 7)   // cTp2 lacks the /wt4 (src/sr_derivative.F90:225)
+            c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + qd * ya[3];
+        else
+            c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + DW(qd * ya[3], 3);
+        R c3 = DW(qa * za[0], 0) + DW(qb * za[1], 1) + DW(qc * za[2], 2) + DW(qd * za[3], 3);
+        R gx = div_rn(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr);
+        R gy = div_rn(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr);
+        R gz = div_rn(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr);
+        if (v < 11 && active) {
+            COL(s.gr, 3 * v + 0)[i] = gx;
+            COL(s.gr, 3 * v + 1)[i] = gy;
+            COL(s.gr, 3 * v + 2)[i] = gz;
+        }
+        if (v == 8 || v == 9) { lg[0] = gx; lg[1] = gy; lg[2] = gz; }          // lanes 0, 1
+        if (v == 11 || v == 12) { sg[0] = gx; sg[1] = gy; sg[2] = gz; }        // lanes 3, 0
+    }
+    // lane 2 takes rog from lane 3, lane 3 takes rop from lane 0
+    const int src = q == 2 ? 3 : (q == 3 ? 0 : q);
+    R fx0 = qshfl(sg[0], src), fy0 = qshfl(sg[1], src), fz0 = qshfl(sg[2], src);
+    if (q >= 2) { lg[0] = fx0; lg[1] = fy0; lg[2] = fz0; }
+    const int lcol = q == 0 ? P_PG : q == 1 ? P_PP : q == 2 ? P_ROG : P_ROP;
+    const R epssq = (R)cube_rn((double)(P.venkat_k * ldg(m.dl + i)));
+    const double* qq = COL(s.pr, lcol);
+    double qi = qq[i];
+    double vmax = mx2(mx2(mx2(mx2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
+    double vmin = mn2(mn2(mn2(mn2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
+    R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
+    R phl = R(0);
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        R fx = (R)(ldg(COL(m.fch, f) + i) - x0);
+        R fy = (R)(ldg(COL(m.fch, 4 + f) + i) - y0);
+        R fz = (R)(ldg(COL(m.fch, 8 + f) + i) - z0);
+        R d = fx * lg[0] + fy * lg[1] + fz * lg[2];
+        R ph;
+        if (d > R(0)) ph = fvenkat(dmax, d, epssq);
+        else if (d < R(0)) ph = fvenkat(dmin, d, epssq);
+        else ph = R(1);
+        phl = (f == 0) ? ph : mn2(phl, ph);
+    }
+    R p0 = qshfl(phl, 0), p1 = qshfl(phl, 1), p2 = qshfl(phl, 2), p3 = qshfl(phl, 3);
+    if (q == 0 && active) s.phi[i] = (double)mn2(mn2(mn2(p0, p1), p2), p3);
+}
+
+// Residual + sources + RK update with four lanes per cell: lane q evaluates
+// face q; every lane re-assembles the residual in face order and computes
+// the sources; lane q writes variables q, q+4, q+8.
+__global__ void __launch_bounds__(128, 4) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (int)(gt & 3);
+    int i = (int)(gt >> 2);
+    const bool valid = i < m.neles;
+    if (!valid) i = m.neles - 1;
+    const bool active = valid && ldg(m.iblank + i) == 1;
+    const double* pr = s.pr;
+    // this lane's face
+    R eff[10];
+    int flags;
+    {
+        FaceOut o;
+        face_eval(m, s, P, i, q, o);
+        if (o.wall) {
+#pragma unroll
+            for (int k = 0; k < 10; k++) eff[k] = R(0);
+            eff[1] = o.w[0]; eff[2] = o.w[1]; eff[3] = o.w[2];
+            eff[6] = o.w[3]; eff[7] = o.w[4]; eff[8] = o.w[5];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 10; k++) eff[k] = o.F[k];
+        }
+        flags = (o.wall ? 1 : 0) | (o.takeg ? 2 : 0) | (o.takep ? 4 : 0);
+    }
+    // neighbour data for the alpha_g gradient of the sources
+    const int nq = ldg(COL(m.nc, q) + i);
+    const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
+    const R xq = (R)(ldg(m.xc + nq) - x0), yq = (R)(ldg(m.yc + nq) - y0), zq = (R)(ldg(m.zc + nq) - z0);
+    const R pq = (R)(COL(pr, P_PHIG)[nq] - COL(pr, P_PHIG)[i]);
+    // residual in face order 1..4 (src/sr_hllcbatten.F90:534-552)
+    double rhs[10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) rhs[k] = 0.0;
+    R Fg[5] = {R(0), R(0), R(0), R(0), R(0)}, Fp[5] = {R(0), R(0), R(0), R(0), R(0)};
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        R e[10];
+#pragma unroll
+        for (int k = 0; k < 10; k++) e[k] = qshfl(eff[k], f);
+        const int fl = qshfl(flags, f);
+        if (fl & 1) {
+            rhs[1] = rhs[1] + (double)e[1]; rhs[2] = rhs[2] + (double)e[2]; rhs[3] = rhs[3] + (double)e[3];
+            rhs[6] = rhs[6] + (double)e[6]; rhs[7] = rhs[7] + (double)e[7]; rhs[8] = rhs[8] + (double)e[8];
+        } else {
+            if (fl & 2) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) Fg[k] = e[k];
+            }
+            if (fl & 4) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) Fp[k] = e[5 + k];
+            }
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                rhs[k] = rhs[k] + (double)Fg[k];
+                rhs[5 + k] = rhs[5 + k] + (double)Fp[k];
+            }
+        }
+    }
+    R xa[4], ya[4], za[4], pa[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        xa[f] = qshfl(xq, f); ya[f] = qshfl(yq, f); za[f] = qshfl(zq, f); pa[f] = qshfl(pq, f);
+    }
+    // interphase sources (src/sr_source.F90:46-155)
+    {
+        const R tg = (R)COL(pr, P_TG)[i], phig = (R)COL(pr, P_PHIG)[i], rog = (R)COL(pr, P_ROG)[i];
+        const R rop = (R)COL(pr, P_ROP)[i], phip = (R)COL(pr, P_PHIP)[i];
+        const R ug = (R)COL(pr, P_UG)[i], vg = (R)COL(pr, P_VG)[i], wg = (R)COL(pr, P_WG)[i];
+        const R up = (R)COL(pr, P_UP)[i], vp = (R)COL(pr, P_VP)[i], wp = (R)COL(pr, P_WP)[i];
+        const R tp = (R)COL(pr, P_TP)[i], pg = (R)COL(pr, P_PG)[i];
+        const R dl = (R)ldg(m.dl + i), voli = (R)ldg(m.vol + i);
+        const R amug = (R)P.as * sqrt(tg) / (R(1) + (R)P.ts / tg);
+        const R du = ug - up, dv = vg - vp, dw = wg - wp;
+        const R drag = R(0.44) * phig * (phig - R(1)) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        const R fdgx = drag * du, fdgy = drag * dv, fdgz = drag * dw;
+        const R qsource = R(6) * phip * amug * (R)P.cpg * R(2) * (tp - tg) / ((R)P.prg * (dl * dl));
+        const R delpstar = R(2) * (phig * rog * phip * rop) / (phig * rop + phip * rog) *
+                           (du * du + dv * dv + dw * dw);
+        const R pint = pg - mn2(delpstar, R(0.01) * pg);
+        const R den = phig * rog + (R(1) - phig) * rop;
+        // lane q < 3 evaluates component q of the interface velocity, of the
+        // right-hand side of the alpha_g LSQ system and of its solution; the
+        // results are exchanged with shuffles
+        const R gq = q == 0 ? ug : (q == 1 ? vg : wg);
+        const R pq_ = q == 0 ? up : (q == 1 ? vp : wp);
+        const R vq_int = (phig * rog * gq + (R(1) - phig) * rop * pq_) / den;
+        const R uint_ = qshfl(vq_int, 0), vint = qshfl(vq_int, 1), wint = qshfl(vq_int, 2);
+        // geometry-only terms (src/sr_source.F90:100-117), evaluated at set-up
+        R wt[4], rw[4];
+#if HP_LSQ_TABLE
+#pragma unroll
+        for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqb, f) + i); rw[f] = rcp(wt[f]); }
+        const R a1 = (R)ldg(COL(m.lsqb, 4) + i), a2 = (R)ldg(COL(m.lsqb, 5) + i), a3 = (R)ldg(COL(m.lsqb, 6) + i);
+        const R b1 = (R)ldg(COL(m.lsqb, 7) + i), b2 = (R)ldg(COL(m.lsqb, 8) + i), b3 = (R)ldg(COL(m.lsqb, 9) + i);
+#else
+#pragma unroll
+        for (int f = 0; f < 4; f++) { wt[f] = sqrt(xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]); rw[f] = rcp(wt[f]); }
+        const R a1 = DW(xa[0] * xa[0], 0) + DW(xa[1] * xa[1], 1) + DW(xa[2] * xa[2], 2) + DW(xa[3] * xa[3], 3);
+        const R a2 = DW(ya[0] * ya[0], 0) + DW(ya[1] * ya[1], 1) + DW(ya[2] * ya[2], 2) + DW(ya[3] * ya[3], 3);
+        const R a3 = DW(za[0] * za[0], 0) + DW(za[1] * za[1], 1) + DW(za[2] * za[2], 2) + DW(za[3] * za[3], 3);
+        const R b1 = DW(xa[0] * ya[0], 0) + DW(xa[1] * ya[1], 1) + DW(xa[2] * ya[2], 2) + DW(xa[3] * ya[3], 3);
+        const R b2 = DW(xa[0] * za[0], 0) + DW(xa[1] * za[1], 1) + DW(xa[2] * za[2], 2) + DW(xa[3] * za[3], 3);
+        const R b3 = DW(ya[0] * za[0], 0) + DW(ya[1] * za[1], 1) + DW(ya[2] * za[2], 2) + DW(ya[3] * za[3], 3);
+#endif
+#if HP_LSQ_TABLE
+        const R dnr = (R)ldg(COL(m.lsqb, 10) + i);
+#else
+        const R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+#endif
+        R dir[4];
+#pragma unroll
+        for (int f = 0; f < 4; f++) dir[f] = q == 0 ? xa[f] : (q == 1 ? ya[f] : za[f]);
+        const R cq = DW(pa[0] * dir[0], 0) + DW(pa[1] * dir[1], 1) + DW(pa[2] * dir[2], 2) + DW(pa[3] * dir[3], 3);
+        const R c1 = qshfl(cq, 0), c2 = qshfl(cq, 1), c3 = qshfl(cq, 2);
+        // Cramer: lane 0 replaces the first column by c, lane 1 the second,
+        // lane 2 the third
+        const R A11 = q == 0 ? c1 : a1, A21 = q == 0 ? c2 : b1, A31 = q == 0 ? c3 : b2;
+        const R A12 = q == 1 ? c1 : b1, A22 = q == 1 ? c2 : a2, A32 = q == 1 ? c3 : b3;
+        const R A13 = q >= 2 ? c1 : b2, A23 = q >= 2 ? c2 : b3, A33 = q >= 2 ? c3 : a3;
+        const R dq = det3(A11, A21, A31, A12, A22, A32, A13, A23, A33) / dnr;
+        const R dpx = qshfl(dq, 0), dpy = qshfl(dq, 1), dpz = qshfl(dq, 2);
+        const R g = R(0);
+        R en = pint * (uint_ * dpx + vint * dpy + wint * dpz) + uint_ * fdgx + vint * fdgy + wint * fdgz + qsource;
+        const double* vis = s.vis;
+        rhs[1] = rhs[1] - (double)((fdgx + pint * dpx + phig * rog * g) * voli) - COL(vis, 0)[i];
+        rhs[2] = rhs[2] - (double)((fdgy + pint * dpy) * voli) - COL(vis, 1)[i];
+        rhs[3] = rhs[3] - (double)((fdgz + pint * dpz) * voli) - COL(vis, 2)[i];
+        rhs[4] = rhs[4] - (double)(en * voli) - COL(vis, 3)[i];
+        rhs[6] = rhs[6] + (double)((fdgx + pint * dpx - phip * rop * g) * voli) - COL(vis, 4)[i];
+        rhs[7] = rhs[7] + (double)((fdgy + pint * dpy) * voli) - COL(vis, 5)[i];
+        rhs[8] = rhs[8] + (double)((fdgz + pint * dpz) * voli) - COL(vis, 6)[i];
+        rhs[9] = rhs[9] + (double)(en * voli) - COL(vis, 7)[i];
+    }
+    if (!active) return;
+    const double dtbyvol = s.s->dt / ldg(m.vol + i);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const int j = q + 4 * r;
+        if (j >= 10) break;
+        const double rr = rhs[j] - COL(s.d24, j)[i];
+        const double cu = COL(s.cu, j)[i];
+        double* cnp = COL(s.cn, j) + i;
+        if (P.rk_scheme == 0) {
+            if (stage == 1) {
+                double v = cu - (11.0 / 20.0) * dtbyvol * rr;
+                *cnp = v;
+                COL(s.cn1, j)[i] = v;
+            } else {
+                double upd = *cnp - (11.0 / 20.0) * dtbyvol * rr;
+                if (stage == 2) *cnp = (3.0 / 8.0) * cu + (5.0 / 8.0) * upd;
+                else if (stage == 3) *cnp = (4.0 / 9.0) * cu + (5.0 / 9.0) * upd;
+                else *cnp = (111.0 / 1331.0) * cu + (260.0 / 1331.0) * COL(s.cn1, j)[i] + (960.0 / 1331.0) * upd;
+            }
+        } else {
+            if (stage == 1) *cnp = cu - dtbyvol * rr;
+            else {
+                double upd = *cnp - dtbyvol * rr;
+                if (stage == 2) *cnp = 0.75 * cu + 0.25 * upd;
+                else *cnp = (1.0 / 3.0) * cu + (2.0 / 3.0) * upd;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Face-centred viscous fluxes, src/sr_viscousgp.F90:488-1138 (AMUP constant).
+// One face f of cell i: face-centred LSQ over 5 (boundary) or 8 (interior)
+// cell centres, Newtonian stresses and heat flux; c[8] = the face's
+// contribution to visug..vistp.
+__device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s, const DevParams& P,
+                                          int i, int f, const int nci[4], double c[8]) {
+    const double* pr = s.pr;
+    const int fcol[8] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP};
+    const R c23 = (R)P.c23;
+    const R scx = (R)ldg(COL(m.sc, 3 * f) + i), scy = (R)ldg(COL(m.sc, 3 * f + 1) + i),
+            scz = (R)ldg(COL(m.sc, 3 * f + 2) + i);
+    const double xf = ldg(COL(m.fcv, f) + i), yf = ldg(COL(m.fcv, 4 + f) + i),
+                 zf = ldg(COL(m.fcv, 8 + f) + i);
+    const int neigh = nci[f];
+    R ff[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) ff[v] = (R)((COL(pr, fcol[v])[i] + COL(pr, fcol[v])[neigh]) * 0.5);
+    const R phigf = (R)((COL(pr, P_PHIG)[i] + COL(pr, P_PHIG)[neigh]) * 0.5);
+    const R phipf = (R)((COL(pr, P_PHIP)[i] + COL(pr, P_PHIP)[neigh]) * 0.5);
+    const R tgf = ff[3];
+    const R amug = (R)P.as * sqrt(tgf) / (R(1) + (R)P.ts / tgf);
+    const R akg = div_rn(amug * (R)P.cpg, (R)P.prg, (R)P.r_prg);
+    const R amup = (R)P.amup;
+    const R akp = div_rn(amup * (R)P.cpp, (R)P.prp, (R)P.r_prp);
+    int mm[8];
+    int nm;
+    mm[0] = nci[0]; mm[1] = nci[1]; mm[2] = nci[2]; mm[3] = nci[3];
+    if (neigh >= m.neles) {
+        mm[4] = i; nm = 5;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) mm[4 + k] = ldg(COL(m.nc, k) + neigh);
+        nm = 8;
+    }
+    R dx[8], dy[8], dz[8];
+    for (int k = 0; k < nm; k++) {
+        dx[k] = (R)(ldg(m.xc + mm[k]) - xf);
+        dy[k] = (R)(ldg(m.yc + mm[k]) - yf);
+        dz[k] = (R)(ldg(m.zc + mm[k]) - zf);
+    }
+    R a11 = dx[0] * dx[0], a22 = dy[0] * dy[0], a33 = dz[0] * dz[0];
+    R a12 = dx[0] * dy[0], a13 = dx[0] * dz[0], a23 = dy[0] * dz[0];
+    for (int k = 1; k < nm; k++) {
+        a11 = a11 + dx[k] * dx[k]; a22 = a22 + dy[k] * dy[k]; a33 = a33 + dz[k] * dz[k];
+        a12 = a12 + dx[k] * dy[k]; a13 = a13 + dx[k] * dz[k]; a23 = a23 + dy[k] * dz[k];
+    }
+    const R dnr = det3(a11, a12, a13, a12, a22, a23, a13, a23, a33);
+    const R rdnr = rcp(dnr);
+    R gr[8][3];
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        const double* q = COL(pr, fcol[v]);
+        R d0 = (R)q[mm[0]] - ff[v];
+        R b1 = d0 * dx[0], b2 = d0 * dy[0], b3 = d0 * dz[0];
+        for (int k = 1; k < nm; k++) {
+            R dk = (R)q[mm[k]] - ff[v];
+            b1 = b1 + dk * dx[k]; b2 = b2 + dk * dy[k]; b3 = b3 + dk * dz[k];
+        }
+        gr[v][0] = div_rn(det3(b1, b2, b3, a12, a22, a23, a13, a23, a33), dnr, rdnr);
+        gr[v][1] = div_rn(det3(a11, a12, a13, b1, b2, b3, a13, a23, a33), dnr, rdnr);
+        gr[v][2] = div_rn(det3(a11, a12, a13, a12, a22, a23, b1, b2, b3), dnr, rdnr);
+    }
+    const R ugf = ff[0], vgf = ff[1], wgf = ff[2], upf = ff[4], vpf = ff[5], wpf = ff[6];
+    R delvg = gr[0][0] + gr[1][1] + gr[2][2];
+    R txxg = amug * (R(2) * gr[0][0] - c23 * delvg);
+    R tyyg = amug * (R(2) * gr[1][1] - c23 * delvg);
+    R tzzg = amug * (R(2) * gr[2][2] - c23 * delvg);
+    R txyg = amug * (gr[1][0] + gr[0][1]);
+    R txzg = amug * (gr[2][0] + gr[0][2]);
+    R tyzg = amug * (gr[1][2] + gr[2][1]);
+    R qxxg = ugf * txxg + vgf * txyg + wgf * txzg + akg * gr[3][0];
+    R qyyg = ugf * txyg + vgf * tyyg + wgf * tyzg + akg * gr[3][1];
+    R qzzg = ugf * txzg + vgf * tyzg + wgf * tzzg + akg * gr[3][2];
+    R delvp = gr[4][0] + gr[5][1] + gr[6][2];
+    R txxp = amup * (R(2) * gr[4][0] - c23 * delvp);
+    R tyyp = amup * (R(2) * gr[5][1] - c23 * delvp);
+    R tzzp = amup * (R(2) * gr[6][2] - c23 * delvp);
+    R txyp = amup * (gr[5][0] + gr[4][1]);
+    R txzp = amup * (gr[6][0] + gr[4][2]);
+    R tyzp = amup * (gr[5][2] + gr[6][1]);
+    R qxxp = upf * txxp + vpf * txyp + wpf * txzp + akp * gr[7][0];
+    R qyyp = upf * txyp + vpf * tyyp + wpf * tyzp + akp * gr[7][1];
+    R qzzp = upf * txzp + vpf * tyzp + wpf * tzzp + akp * gr[7][2];
+    c[0] = (double)(phigf * (txxg * scx + txyg * scy + txzg * scz));
+    c[1] = (double)(phigf * (txyg * scx + tyyg * scy + tyzg * scz));
+    c[2] = (double)(phigf * (txzg * scx + tyzg * scy + tzzg * scz));
+    c[3] = (double)(phigf * (qxxg * scx + qyyg * scy + qzzg * scz));
+    c[4] = (double)(phipf * (txxp * scx + txyp * scy + txzp * scz));
+    c[5] = (double)(phipf * (txyp * scx + tyyp * scy + tyzp * scz));
+    c[6] = (double)(phipf * (txzp * scx + tyzp * scy + tzzp * scz));
+    c[7] = (double)(phipf * (qxxp * scx + qyyp * scy + qzzp * scz));
+}
+
+// one thread per cell (aliased meshes)
 __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParams P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     if (ldg(m.iblank + i) != 1) return;
-    const double* pr = s.pr;
-    const int fcol[8] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP};
     double acc[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) acc[k] = 0.0;
     int nci[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) nci[f] = ldg(COL(m.nc, f) + i);
-    const R c23 = (R)P.c23;
 #pragma unroll 1
     for (int f = 0; f < 4; f++) {
-        const R scx = (R)ldg(COL(m.sc, 3 * f) + i), scy = (R)ldg(COL(m.sc, 3 * f + 1) + i),
-                scz = (R)ldg(COL(m.sc, 3 * f + 2) + i);
-        const double xf = ldg(COL(m.fcv, f) + i), yf = ldg(COL(m.fcv, 4 + f) + i),
-                     zf = ldg(COL(m.fcv, 8 + f) + i);
-        const int neigh = nci[f];
-        R ff[8];
+        double c[8];
+        visc_face(m, s, P, i, f, nci, c);
 #pragma unroll
-        for (int v = 0; v < 8; v++) ff[v] = (R)((COL(pr, fcol[v])[i] + COL(pr, fcol[v])[neigh]) * 0.5);
-        const R phigf = (R)((COL(pr, P_PHIG)[i] + COL(pr, P_PHIG)[neigh]) * 0.5);
-        const R phipf = (R)((COL(pr, P_PHIP)[i] + COL(pr, P_PHIP)[neigh]) * 0.5);
-        const R tgf = ff[3];
-        const R amug = (R)P.as * sqrt(tgf) / (R(1) + (R)P.ts / tgf);
-        const R akg = amug * (R)P.cpg / (R)P.prg;
-        const R amup = (R)P.amup;
-        const R akp = amup * (R)P.cpp / (R)P.prp;
-        int mm[8];
-        int nm;
-        mm[0] = nci[0]; mm[1] = nci[1]; mm[2] = nci[2]; mm[3] = nci[3];
-        if (neigh >= m.neles) {
-            mm[4] = i; nm = 5;
-        } else {
-#pragma unroll
-            for (int k = 0; k < 4; k++) mm[4 + k] = ldg(COL(m.nc, k) + neigh);
-            nm = 8;
-        }
-        R dx[8], dy[8], dz[8];
-        for (int k = 0; k < nm; k++) {
-            dx[k] = (R)(ldg(m.xc + mm[k]) - xf);
-            dy[k] = (R)(ldg(m.yc + mm[k]) - yf);
-            dz[k] = (R)(ldg(m.zc + mm[k]) - zf);
-        }
-        R a11 = dx[0] * dx[0], a22 = dy[0] * dy[0], a33 = dz[0] * dz[0];
-        R a12 = dx[0] * dy[0], a13 = dx[0] * dz[0], a23 = dy[0] * dz[0];
-        for (int k = 1; k < nm; k++) {
-            a11 = a11 + dx[k] * dx[k]; a22 = a22 + dy[k] * dy[k]; a33 = a33 + dz[k] * dz[k];
-            a12 = a12 + dx[k] * dy[k]; a13 = a13 + dx[k] * dz[k]; a23 = a23 + dy[k] * dz[k];
-        }
-        const R dnr = det3(a11, a12, a13, a12, a22, a23, a13, a23, a33);
-        R gr[8][3];
-#pragma unroll
-        for (int v = 0; v < 8; v++) {
-            const double* q = COL(pr, fcol[v]);
-            R d0 = (R)q[mm[0]] - ff[v];
-            R b1 = d0 * dx[0], b2 = d0 * dy[0], b3 = d0 * dz[0];
-            for (int k = 1; k < nm; k++) {
-                R dk = (R)q[mm[k]] - ff[v];
-                b1 = b1 + dk * dx[k]; b2 = b2 + dk * dy[k]; b3 = b3 + dk * dz[k];
-            }
-            gr[v][0] = det3(b1, b2, b3, a12, a22, a23, a13, a23, a33) / dnr;
-            gr[v][1] = det3(a11, a12, a13, b1, b2, b3, a13, a23, a33) / dnr;
-            gr[v][2] = det3(a11, a12, a13, a12, a22, a23, b1, b2, b3) / dnr;
-        }
-        const R ugf = ff[0], vgf = ff[1], wgf = ff[2], upf = ff[4], vpf = ff[5], wpf = ff[6];
-        R delvg = gr[0][0] + gr[1][1] + gr[2][2];
-        R txxg = amug * (R(2) * gr[0][0] - c23 * delvg);
-        R tyyg = amug * (R(2) * gr[1][1] - c23 * delvg);
-        R tzzg = amug * (R(2) * gr[2][2] - c23 * delvg);
-        R txyg = amug * (gr[1][0] + gr[0][1]);
-        R txzg = amug * (gr[2][0] + gr[0][2]);
-        R tyzg = amug * (gr[1][2] + gr[2][1]);
-        R qxxg = ugf * txxg + vgf * txyg + wgf * txzg + akg * gr[3][0];
-        R qyyg = ugf * txyg + vgf * tyyg + wgf * tyzg + akg * gr[3][1];
-        R qzzg = ugf * txzg + vgf * tyzg + wgf * tzzg + akg * gr[3][2];
-        R delvp = gr[4][0] + gr[5][1] + gr[6][2];
-        R txxp = amup * (R(2) * gr[4][0] - c23 * delvp);
-        R tyyp = amup * (R(2) * gr[5][1] - c23 * delvp);
-        R tzzp = amup * (R(2) * gr[6][2] - c23 * delvp);
-        R txyp = amup * (gr[5][0] + gr[4][1]);
-        R txzp = amup * (gr[6][0] + gr[4][2]);
-        R tyzp = amup * (gr[5][2] + gr[6][1]);
-        R qxxp = upf * txxp + vpf * txyp + wpf * txzp + akp * gr[7][0];
-        R qyyp = upf * txyp + vpf * tyyp + wpf * tyzp + akp * gr[7][1];
-        R qzzp = upf * txzp + vpf * tyzp + wpf * tzzp + akp * gr[7][2];
-        acc[0] = acc[0] + (double)(phigf * (txxg * scx + txyg * scy + txzg * scz));
-        acc[1] = acc[1] + (double)(phigf * (txyg * scx + tyyg * scy + tyzg * scz));
-        acc[2] = acc[2] + (double)(phigf * (txzg * scx + tyzg * scy + tzzg * scz));
-        acc[3] = acc[3] + (double)(phigf * (qxxg * scx + qyyg * scy + qzzg * scz));
-        acc[4] = acc[4] + (double)(phipf * (txxp * scx + txyp * scy + txzp * scz));
-        acc[5] = acc[5] + (double)(phipf * (txyp * scx + tyyp * scy + tyzp * scz));
-        acc[6] = acc[6] + (double)(phipf * (txzp * scx + tyzp * scy + tzzp * scz));
-        acc[7] = acc[7] + (double)(phipf * (qxxp * scx + qyyp * scy + qzzp * scz));
+        for (int k = 0; k < 8; k++) acc[k] = acc[k] + c[k];
     }
 #pragma unroll
     for (int k = 0; k < 8; k++) COL(s.vis, k)[i] = acc[k];
+}
+
+// ---------------------------------------------------------------------------
+// Four lanes per cell (lane q = thread & 3 owns face q / field group q).
+// Per-cell sums are re-assembled in face order 1..4 with warp shuffles, so
+// the result is identical to the one-thread-per-cell kernels.  All 32 lanes
+// of a warp reach every shuffle (out-of-range lanes replay the last cell and
+// do not write).
+
+__global__ void __launch_bounds__(128, 3) k_visc4(DevMesh m, DevState<R> s, DevParams P) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (int)(gt & 3);
+    int i = (int)(gt >> 2);
+    const bool valid = i < m.neles;
+    if (!valid) i = m.neles - 1;
+    const bool active = valid && ldg(m.iblank + i) == 1;
+    int nci[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) nci[f] = ldg(COL(m.nc, f) + i);
+    double c[8];
+    visc_face(m, s, P, i, q, nci, c);
+    double acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = 0.0;
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[k] = acc[k] + qshfl(c[k], f);
+    if (active) {
+        COL(s.vis, q)[i] = acc[q];
+        COL(s.vis, q + 4)[i] = acc[q + 4];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1153,7 +1550,12 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
         if (m.aliased) k_bc_serial<true><<<1, 1, 0, st>>>(m, s, P);
         else k_bc<true><<<gg, 256, 0, st>>>(m, s, P);
     }
-    if (!P.inviscid) { MARK(KK_VISC); k_visc<<<gf, b, 0, st>>>(m, s, P); }
+    const unsigned g4 = grid_for(4ll * m.neles, 128);
+    if (!P.inviscid) {
+        MARK(KK_VISC);
+        if (m.aliased) k_visc<<<gf, b, 0, st>>>(m, s, P);
+        else k_visc4<<<g4, 128, 0, st>>>(m, s, P);
+    }
     for (int stage = 1; stage <= P.nstage; stage++) {
         // src/sr_hllcbatten.F90:29-33: primitiveplusbc, derivative, limiter
         MARK(KK_PRIM_STAGE);
@@ -1165,7 +1567,8 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
         }
         if (P.myorder == 2) {
             MARK(KK_GRAD);
-            k_grad<<<gf, b, 0, st>>>(m, s, P);
+            if (m.aliased) k_grad<<<gf, b, 0, st>>>(m, s, P);
+            else k_grad4<<<g4, 128, 0, st>>>(m, s, P);
             if (m.aliased) { MARK(KK_SERIAL); k_phi_copy_serial<<<1, 1, 0, st>>>(m, s); }
         }
         MARK(KK_FLUX);
@@ -1174,7 +1577,7 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             MARK(KK_SERIAL);
             k_flux_carry<<<1, 1, 0, st>>>(m, s, P);
         } else {
-            k_flux<false><<<gf, b, 0, st>>>(m, s, P, stage);
+            k_flux4<<<g4, 128, 0, st>>>(m, s, P, stage);
         }
     }
     // src/main.F90:595-641: primitive, residual norms, cu = cn
