@@ -142,7 +142,7 @@ def read_grid(path: str):
     with open(path) as f:
         nodes, neles = (int(t) for t in f.readline().split()[:2])
     nd = pd.read_csv(path, sep=r"\s+", header=None, skiprows=1, nrows=nodes,
-                     usecols=[0, 1, 2, 3, 4], engine="c").to_numpy()
+                     usecols=[0, 1, 2, 3, 4], engine="c", float_precision="round_trip").to_numpy()
     el = pd.read_csv(path, sep=r"\s+", header=None, skiprows=1 + nodes, nrows=neles,
                      usecols=list(range(10)), engine="c").to_numpy(dtype=np.int64)
     order = nd[:, 0].astype(np.int64) - 1

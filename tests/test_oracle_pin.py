@@ -6,17 +6,18 @@ reference wrote Velocity.dat (time and |u_g| of cell 1 per step) and
 restart_files/restart0000.in (full conserved state).  Fixtures extracted by
 tests/golden/make_golden.py.
 
-What is pinned, and how tightly:
-  * step 1 (time and |u_g(1)|) bit-exact: cell 1 borders a corrupted overset
-    cell, so this pins the NaN semantics of the HLLC wave-speed MIN/MAX and
-    the reuse of the previous face flux when no wave branch is taken;
-  * dt of steps 2-3 bit-exact (NaN-skipping MIN in the dt reduction);
-  * the 10-step trajectory to 1e-12 relative;
-  * the set of NaN cells of the final state exactly;
-  * air-phase conserved variables (1, 2, 5) of cells more than 20 layers from
-    the corrupted block to 1e-11 relative, median over all finite cells 1e-12.
-The water phase (vars 6-10) at alpha_w = 2e-8 is recovered as 1 - alpha_g,
-which amplifies 1e-14 air-state differences by ~5e7; it is checked at 2e-3.
+Everything is pinned bit for bit:
+  * all 10 (time, |u_g(1)|) records; cell 1 borders a corrupted overset cell
+    (ghost ids of the merged mesh alias element ids, inputfiles/mergefiles.f90
+    :100-110), so this pins the NaN semantics of the HLLC wave-speed MIN/MAX,
+    the reuse of the previous face flux when no wave branch is taken and the
+    NaN-skipping MIN of the dt reduction;
+  * the set of NaN cells of the final state;
+  * every finite conserved value of a 3000-cell sample and the per-variable
+    sums over all finite cells;
+  * a 1000-ghost sample of the ghost primitives written after the state.
+Coordinates must be parsed with correct rounding (as the reference's
+list-directed READ does); a 1-ulp parser breaks the match from step 2 on.
 """
 import os
 
@@ -39,34 +40,14 @@ def shipped_run(reference_dir):
     return flow, mesh, t, v, cu, gp
 
 
-def _layers_from(mesh, seed_mask):
-    ne = mesh.neles
-    nc = mesh.elem[:, 4:8].astype(np.int64) - 1
-    INF = 1 << 30
-    layer = np.full(ne, INF)
-    front = np.where(seed_mask)[0]
-    layer[front] = 0
-    lv = 0
-    while front.size:
-        lv += 1
-        nb = nc[front].ravel()
-        nb = np.unique(nb[nb < ne])
-        nb = nb[layer[nb] == INF]
-        layer[nb] = lv
-        front = nb
-    return layer
-
-
 @pytest.mark.slow
 def test_velocity_trajectory(shipped_run):
     g = np.load(os.path.join(GOLDEN_DIR, "shipped_case.npz"))
     _, _, t, v, _, _ = shipped_run
     vel = g["velocity"]
-    assert t[0] == vel[0, 0] and v[0] == vel[0, 1]          # step 1 bit-exact
-    assert t[1] == vel[1, 0] and t[2] == vel[2, 0]          # dt of steps 2, 3
-    np.testing.assert_allclose(t, vel[:, 0], rtol=1e-12, atol=0)
-    np.testing.assert_allclose(v, vel[:, 1], rtol=1e-12, atol=0)
-    assert t[-1] == pytest.approx(float(g["restart_time"]), rel=1e-12)
+    np.testing.assert_array_equal(t, vel[:, 0])
+    np.testing.assert_array_equal(v, vel[:, 1])
+    assert t[-1] == float(g["restart_time"])
 
 
 @pytest.mark.slow
@@ -76,20 +57,9 @@ def test_restart_state(shipped_run):
     nan_cells = np.where(np.isnan(cu).any(axis=0))[0] + 1
     np.testing.assert_array_equal(nan_cells, g["nan_cells"])
     ids = g["sample_ids"] - 1
-    mine = cu[:, ids].T
-    gold = g["sample_cu"]
-    rel = np.abs(mine - gold) / np.abs(gold)
-    nc = mesh.elem[:, 4:8]
-    alias = np.isin(nc, g["nan_cells"]).any(axis=1)
-    layer = _layers_from(mesh, alias)
-    far = layer[ids] > 20
-    for k in (0, 1, 4):
-        assert np.median(rel[:, k]) < 1e-12
-        assert rel[far, k].max() < 1e-11
-    for k in (5, 6, 9):
-        assert np.median(rel[:, k]) < 2e-3
-    assert rel[:, 0].max() < 1e-5
+    np.testing.assert_array_equal(cu[:, ids].T, g["sample_cu"])
+    sums = np.nansum(np.where(np.isnan(cu), 0.0, cu), axis=1)
+    np.testing.assert_array_equal(sums, g["var_sums"])
     # ghost primitives written after the state (main.F90:819-824)
     gi = g["ghost_ids"]
-    grel = np.abs(gp[:, gi].T - g["ghost_prims"]) / np.maximum(np.abs(g["ghost_prims"]), 1e-30)
-    assert np.median(grel) < 1e-12
+    np.testing.assert_array_equal(gp[:, gi].T, g["ghost_prims"])
