@@ -37,10 +37,29 @@ def _rel_l2(a, b):
     return np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-300)
 
 
+def _aliased(spec, shift=3, dup=(10, 11)):
+    """Ghost ids shifted down by `shift`, so the first ones collide with
+    element ids, plus one repeated ghost id: the indexing of the merged overset
+    case that inputfiles/mergefiles.f90:100-110 writes (background ghosts
+    without offsets).  The parents' neighbour entries follow the ghosts."""
+    m = spec.mesh
+    el, gh = m.elem.copy(), m.ghost.copy()
+    new = gh[:, 1] - shift
+    new[dup[0]] = new[dup[1]]
+    for g in range(gh.shape[0]):
+        p, side = gh[g, 0] - 1, gh[g, 3] - 1
+        assert el[p, 4 + side] == gh[g, 1]
+        el[p, 4 + side] = new[g]
+    gh[:, 1] = new
+    spec.mesh = MeshArrays(m.x, m.y, m.z, el, gh)
+    return spec
+
+
 SPECS = {
     "shock_bubble_ref": lambda: cases.shock_bubble(n=5, alpha_min=0.1, reference_scheme=True),
     "shock_bubble_ext": lambda: cases.shock_bubble(n=5, alpha_min=0.1, reference_scheme=False),
     "cylinder": lambda: cases.cylinder(nr=6, nt=16, nz=2),
+    "aliased_ghosts": lambda: _aliased(cases.shock_bubble(n=5, alpha_min=0.1, reference_scheme=True), shift=3),
 }
 
 
