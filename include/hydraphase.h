@@ -146,6 +146,29 @@ int hp_device_state(hp_handle *h, double **cu_dev, int64_t *ld);
 int hp_info(const hp_handle *h, int64_t *kernels_per_step, int64_t *device_bytes,
             int64_t *aliased);
 
+/* --- allocation-free time step ------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a Fortran/OpenACC host whose device arrays and memory budget belong
+ * to its compiler runtime, or a framework whose pool allocator owns the whole
+ * GPU): the time step dt = cfl * min(dl / (max(ag,ap) + max(|ug|,|up|)))
+ * of a conserved state, as hp_step computes it at the start of a step
+ * (primitive recovery + reduction of src/main.F90:529-556), from buffers the
+ * caller owns.  Inputs: cn_dev, 10 columns of leading dimension ld
+ * (column-major cn(1:ncells,1:10), any cell order), dl_dev[ncells] (minimum
+ * edge length per cell, as src/sr_geometry.F90:210-217 defines it); output:
+ * dt_dev[0].  Device pointers; the work is queued on `stream` (a
+ * cudaStream_t, NULL for the default stream) and the call returns without
+ * waiting.  The call allocates nothing: its only scratch, one partial minimum
+ * per 256 cells, is a static device array sized for HP_NOALLOC_MAX_CELLS
+ * cells that each GPU using the library keeps until exit; larger ncells is
+ * rejected with HP_E_ARG.  All calls share that array, so calls that overlap
+ * on the GPU race.  The first call on each device looks up the array's device
+ * address; make it before any stream capture. */
+#define HP_NOALLOC_MAX_CELLS (1 << 24)
+int hp_dt_noalloc(const double *cn_dev, int64_t ld, const double *dl_dev,
+                  int32_t ncells, const hp_params *params, double *dt_dev,
+                  void *stream);
+
 /* --- reference file formats (drop-in inputs/outputs) -------------------- */
 /* flow.in parser, src/sr_Read_flow.F90:19-268. */
 int hp_read_flow(const char *path, hp_params *out);
