@@ -65,6 +65,9 @@ struct hp_handle {
     long long ld = 0;
     std::vector<int> perm;      // reference element (0-based) -> internal id
     std::vector<int> ghost_id;  // ghost-list position -> internal slot id
+    int* d_perm = nullptr;      // the two maps above, on the device
+    int* d_gid = nullptr;
+    double* d_gstage = nullptr; // 6 x nghosts staging of ghost primitives
     bool started = false, have_state = false;
     int aliased = 0;
     int max_diag = 4096;
@@ -408,6 +411,9 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
         s.s = (DevScalars*)a.take(sizeof(DevScalars));
         s.diag = (double*)a.take((size_t)h->max_diag * 8 * D);
         s.max_diag = h->max_diag;
+        h->d_perm = (int*)a.take((neles + 1) * (size_t)I);
+        h->d_gid = (int*)a.take((nghosts + 1) * (size_t)I);
+        h->d_gstage = (double*)a.take(6 * (nghosts + 1) * D);
     };
     Arena probe;
     plan(probe);
@@ -456,6 +462,8 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     if (e == cudaSuccess && nghosts) e = up(m.g_par, hgpar.data(), nghosts * (size_t)I);
     if (e == cudaSuccess && nghosts) e = up(m.g_id, hgid.data(), nghosts * (size_t)I);
     if (e == cudaSuccess && nghosts) e = up(m.g_type, hgtyp.data(), nghosts * (size_t)I);
+    if (e == cudaSuccess) e = up(h->d_perm, h->perm.data(), neles * (size_t)I);
+    if (e == cudaSuccess && nghosts) e = up(h->d_gid, h->ghost_id.data(), nghosts * (size_t)I);
     if (e == cudaSuccess) {
         DevScalars s0{};
         s0.dtmin_bits = 0;
@@ -489,24 +497,81 @@ extern "C" int hp_destroy(hp_handle* h) {
 }
 
 // Upload cu (elements, reference order, column-major) and set cn = cu.
+// --- state transfer ----------------------------------------------------------
+// Caller arrays are in reference order (10 x neles, column-major); the device
+// keeps internal (renumbered) order with leading dimension ld.  Transfers go
+// straight between the caller's buffer and a device staging area (cn1, which
+// holds no live data between steps: every step writes it before reading it),
+// and the permutation runs on the device.
+namespace {
+struct Cols6 { int c[6]; };
+
+// dst[k*ld + idx[i]] = src[k*n + i], k < ncol
+__global__ void k_scatter_cols(const double* __restrict__ src, int n, int ncol, const int* __restrict__ idx,
+                               double* __restrict__ dst, long long ld) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * ncol) return;
+    int k = (int)(t / n), i = (int)(t - (long long)k * n);
+    dst[(size_t)k * ld + idx[i]] = src[(size_t)k * n + i];
+}
+// dst[k*n + i] = src[(col0 + k)*ld + idx[i]], k < ncol
+__global__ void k_gather_cols(const double* __restrict__ src, long long ld, int col0, int n, int ncol,
+                              const int* __restrict__ idx, double* __restrict__ dst) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * ncol) return;
+    int k = (int)(t / n), i = (int)(t - (long long)k * n);
+    dst[(size_t)k * n + i] = src[(size_t)(col0 + k) * ld + idx[i]];
+}
+// ghost primitives into their columns of pr.  One thread per column walks
+// the ghost list in order, so repeated ghost ids keep the last value, as the
+// reference's sequential restart read does (src/main.F90:433-438).
+__global__ void k_scatter_ghost_prims(const double* __restrict__ src, int ng, Cols6 cols, const int* __restrict__ gid,
+                                      double* __restrict__ pr, long long ld, int ordered) {
+    if (ordered) {
+        int v = threadIdx.x;
+        if (blockIdx.x != 0 || v >= 6) return;
+        for (int g = 0; g < ng; g++) pr[(size_t)cols.c[v] * ld + gid[g]] = src[(size_t)v * ng + g];
+        return;
+    }
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6LL * ng) return;
+    int v = (int)(t / ng), g = (int)(t - (long long)v * ng);
+    pr[(size_t)cols.c[v] * ld + gid[g]] = src[(size_t)v * ng + g];
+}
+__global__ void k_gather_ghost_prims(const double* __restrict__ pr, long long ld, Cols6 cols, int ng,
+                                     const int* __restrict__ gid, double* __restrict__ dst) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6LL * ng) return;
+    int v = (int)(t / ng), g = (int)(t - (long long)v * ng);
+    dst[(size_t)v * ng + g] = pr[(size_t)cols.c[v] * ld + gid[g]];
+}
+inline unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+const Cols6 GHOST_COLS = {{P_UG, P_VG, P_WG, P_PG, P_TG, P_ROG}};
+}  // namespace
+
 static int upload_state(hp_handle* h, double time, const double* cu_elem, const double* ghost_prims) {
     const long long ld = h->ld;
     const int ne = h->neles, ng = h->nghosts;
-    std::vector<double> cu(10 * ld, 0.0);
-    for (int k = 0; k < 10; k++)
-        for (int i = 0; i < ne; i++) cu[k * ld + h->perm[i]] = cu_elem[(size_t)k * ne + i];
     cudaStream_t st = h->stream;
     CUDA_OK(h, cudaStreamSynchronize(st));
-    CUDA_OK(h, cudaMemcpyAsync(h->ds.cu, cu.data(), 10 * ld * sizeof(double), cudaMemcpyHostToDevice, st));
-    CUDA_OK(h, cudaMemcpyAsync(h->ds.cn, cu.data(), 10 * ld * sizeof(double), cudaMemcpyHostToDevice, st));
+    // conserved state: ghost slots zero, elements scattered to internal order
+    CUDA_OK(h, cudaMemcpyAsync(h->ds.cn1, cu_elem, 10 * (size_t)ne * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(h, cudaMemsetAsync(h->ds.cu, 0, 10 * ld * sizeof(double), st));
+    k_scatter_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cn1, ne, 10, h->d_perm, h->ds.cu, ld);
+    CUDA_OK(h, cudaGetLastError());
+    CUDA_OK(h, cudaMemcpyAsync(h->ds.cn, h->ds.cu, 10 * ld * sizeof(double), cudaMemcpyDeviceToDevice, st));
     // primitives: zero, then the restart's ghost values (src/main.F90:433-438)
-    std::vector<double> pr(NPR * ld, 0.0);
-    if (ghost_prims) {
-        const int cols[6] = {P_UG, P_VG, P_WG, P_PG, P_TG, P_ROG};
-        for (int v = 0; v < 6; v++)
-            for (int g = 0; g < ng; g++) pr[cols[v] * ld + h->ghost_id[g]] = ghost_prims[(size_t)v * ng + g];
+    CUDA_OK(h, cudaMemsetAsync(h->ds.pr, 0, NPR * ld * sizeof(double), st));
+    if (ghost_prims && ng) {
+        CUDA_OK(h, cudaMemcpyAsync(h->d_gstage, ghost_prims, 6 * (size_t)ng * sizeof(double),
+                                   cudaMemcpyHostToDevice, st));
+        if (h->aliased)
+            k_scatter_ghost_prims<<<1, 32, 0, st>>>(h->d_gstage, ng, GHOST_COLS, h->d_gid, h->ds.pr, ld, 1);
+        else
+            k_scatter_ghost_prims<<<blocks_for(6LL * ng, 256), 256, 0, st>>>(h->d_gstage, ng, GHOST_COLS, h->d_gid,
+                                                                             h->ds.pr, ld, 0);
+        CUDA_OK(h, cudaGetLastError());
     }
-    CUDA_OK(h, cudaMemcpyAsync(h->ds.pr, pr.data(), NPR * ld * sizeof(double), cudaMemcpyHostToDevice, st));
     DevScalars s0{};
     double v = 1.0e8;
     std::memcpy(&s0.dtmin_bits, &v, 8);
@@ -678,25 +743,20 @@ extern "C" int hp_get_state(hp_handle* h, double* time, double* cu_elem, double*
     if (time) {
         CUDA_OK(h, cudaMemcpyAsync(h->h_scal, h->ds.s, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
     }
-    std::vector<double> cu, pr;
     if (cu_elem) {
-        cu.resize(10 * ld);
-        CUDA_OK(h, cudaMemcpyAsync(cu.data(), h->ds.cu, 10 * ld * sizeof(double), cudaMemcpyDeviceToHost, st));
+        k_gather_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cu, ld, 0, ne, 10, h->d_perm, h->ds.cn1);
+        CUDA_OK(h, cudaGetLastError());
+        CUDA_OK(h, cudaMemcpyAsync(cu_elem, h->ds.cn1, 10 * (size_t)ne * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
-    if (ghost_prims) {
-        pr.resize(NPR * ld);
-        CUDA_OK(h, cudaMemcpyAsync(pr.data(), h->ds.pr, NPR * ld * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (ghost_prims && ng) {
+        k_gather_ghost_prims<<<blocks_for(6LL * ng, 256), 256, 0, st>>>(h->ds.pr, ld, GHOST_COLS, ng, h->d_gid,
+                                                                        h->d_gstage);
+        CUDA_OK(h, cudaGetLastError());
+        CUDA_OK(h, cudaMemcpyAsync(ghost_prims, h->d_gstage, 6 * (size_t)ng * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
     }
     CUDA_OK(h, cudaStreamSynchronize(st));
     if (time) *time = h->h_scal->time;
-    if (cu_elem)
-        for (int k = 0; k < 10; k++)
-            for (int i = 0; i < ne; i++) cu_elem[(size_t)k * ne + i] = cu[k * ld + h->perm[i]];
-    if (ghost_prims) {
-        const int cols[6] = {P_UG, P_VG, P_WG, P_PG, P_TG, P_ROG};
-        for (int v = 0; v < 6; v++)
-            for (int g = 0; g < ng; g++) ghost_prims[(size_t)v * ng + g] = pr[cols[v] * ld + h->ghost_id[g]];
-    }
     return HP_OK;
 }
 
@@ -704,11 +764,17 @@ extern "C" int hp_get_prims(hp_handle* h, double* prims) {
     if (!h || !prims) return HP_E_ARG;
     const long long ld = h->ld;
     const int ne = h->neles;
-    std::vector<double> pr(NPR * ld);
-    CUDA_OK(h, cudaMemcpyAsync(pr.data(), h->ds.pr, NPR * ld * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CUDA_OK(h, cudaStreamSynchronize(h->stream));
-    for (int v = 0; v < NPR; v++)
-        for (int i = 0; i < ne; i++) prims[(size_t)v * ne + i] = pr[v * ld + h->perm[i]];
+    cudaStream_t st = h->stream;
+    // cn1 stages at most 10 columns at a time
+    for (int c0 = 0; c0 < NPR; c0 += 10) {
+        const int nc = NPR - c0 < 10 ? NPR - c0 : 10;
+        k_gather_cols<<<blocks_for((long long)nc * ne, 256), 256, 0, st>>>(h->ds.pr, ld, c0, ne, nc, h->d_perm,
+                                                                          h->ds.cn1);
+        CUDA_OK(h, cudaGetLastError());
+        CUDA_OK(h, cudaMemcpyAsync(prims + (size_t)c0 * ne, h->ds.cn1, (size_t)nc * ne * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+        CUDA_OK(h, cudaStreamSynchronize(st));
+    }
     return HP_OK;
 }
 

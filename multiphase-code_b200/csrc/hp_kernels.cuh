@@ -53,42 +53,76 @@ __device__ __forceinline__ float cube_rn(float a) { return (float)cube_rn((doubl
 
 template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 
-// a / b when RN(1/b) = rb is already known (divisors reused within a cell):
-// two FMA correction steps after q0 = RN(a * rb) give the IEEE
-// round-to-nearest quotient (Markstein's theorem: rb correctly rounded and q1
-// within one ulp make RN(q1 + (a - b q1) rb) = RN(a / b)).  Operands near the
-// overflow / underflow range take the hardware division.  The XU pipe that
-// IEEE division uses for its reciprocal seed is the bottleneck of these
-// kernels; this form runs on the FP64 pipe only.
-__device__ __noinline__ double div_slow(double a, double b) { return a / b; }
-#ifndef HP_DIV_MARKSTEIN
-#define HP_DIV_MARKSTEIN 0
+// Minimum resident 128-thread blocks per SM of the 4-lanes-per-cell kernels
+// (sets their register cap: 65536 / (128 * minb)).
+#ifndef HP_GRAD4_MINB
+#define HP_GRAD4_MINB 4
 #endif
-__device__ __forceinline__ double div_rn(double a, double b, double rb) {
-#if HP_DIV_MARKSTEIN
-    double q0 = a * rb;
-    double r0 = fma(-b, q0, a);
-    double q1 = fma(r0, rb, q0);
-    double r1 = fma(-b, q1, a);
-    double q2 = fma(r1, rb, q1);
-    // results outside [2^-960, 2^960) (zero, denormal, inf, NaN, or operands
-    // near the range limits) take the hardware division
-    const unsigned eq = (unsigned)(__double2hiint(q2) >> 20) & 0x7ffu;
-    if (__builtin_expect(eq - 63u > 1919u, 0)) q2 = div_slow(a, b);
-    return q2;
-#else
-    (void)rb;
-    return a / b;
+#ifndef HP_FLUX4_MINB
+#define HP_FLUX4_MINB 4
 #endif
+#ifndef HP_VISC4_MINB
+#define HP_VISC4_MINB 3
+#endif
+
+// ---------------------------------------------------------------------------
+// Division.  The parity path must return the IEEE round-to-nearest quotient
+// of every division the reference performs.  Where several quotients share a
+// divisor b, the fast form (F = 1) takes rb = RN(1/b) once and each a / b as
+//     q0 = RN(a rb),  q1 = RN(q0 + RN(a - b q0) rb),  q2 = RN(q1 + (a - b q1) rb)
+// with fused multiply-adds.  Markstein's theorem (rb within half an ulp of
+// 1/b and q1 within one ulp of a/b make a - b q1 exact and q2 = RN(a/b),
+// barring underflow and overflow) gives the IEEE quotient whenever |b| lies
+// in [2^-100, 2^101) and |q2| in [2^-800, 2^801); a == 0 returns RN(a rb),
+// the correctly signed zero.  Any other operand (out of range, Inf, NaN)
+// sets `bad` instead, and the kernel whose warp saw it redoes its work with
+// hardware division (F = 0), so every stored quotient is the IEEE one.  The
+// fast form is straight-line FMA code that the compiler interleaves across
+// independent divisions.
+#ifndef HP_DIV_FAST
+#define HP_DIV_FAST 0
+#endif
+// kernels that take the fast form when HP_DIV_FAST is set: 1 gradients,
+// 2 fluxes, 4 viscous fluxes, 8 JST smoothing
+#ifndef HP_FAST_MASK
+#define HP_FAST_MASK 15
+#endif
+#define HP_FAST(bit) (HP_DIV_FAST && (HP_FAST_MASK & (bit)) && sizeof(R) == 8)
+template <int F>
+__device__ __forceinline__ double mdiv(double a, double b, double rb, unsigned& bad) {
+    if constexpr (F == 0) {
+        (void)rb; (void)bad;
+        return a / b;
+    } else {
+        const double q0 = a * rb;
+        const double q1 = fma(fma(-b, q0, a), rb, q0);
+        const double q2 = fma(fma(-b, q1, a), rb, q1);
+        const unsigned eq = ((unsigned)__double2hiint(q2) >> 20) & 0x7ffu;
+        const bool z = a == 0.0;
+        bad |= (unsigned)(!z && eq - 223u > 1600u);
+        return z ? q0 : q2;
+    }
+}
+template <int F>
+__device__ __forceinline__ double mrcp(double b, unsigned& bad) {
+    if constexpr (F == 0) {
+        (void)b; (void)bad;
+        return 0.0;
+    } else {
+        const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
+        bad |= (unsigned)(eb - 923u > 200u);
+        return 1.0 / b;
+    }
 }
 // the mixed variant divides approximately
+template <int F> __device__ __forceinline__ float mdiv(float a, float b, float rb, unsigned&) { return a * rb; }
+template <int F> __device__ __forceinline__ float mrcp(float b, unsigned&) { return 1.0f / b; }
+
+// Exact division at sites that are not on the fast path.
+__device__ __forceinline__ double div_rn(double a, double b, double) { return a / b; }
 __device__ __forceinline__ float div_rn(float a, float b, float rb) { return a * rb; }
-#if HP_DIV_MARKSTEIN
-template <class T> __device__ __forceinline__ T rcp(T b) { return T(1) / b; }
-#else
 __device__ __forceinline__ double rcp(double) { return 0.0; }
 __device__ __forceinline__ float rcp(float b) { return 1.0f / b; }
-#endif
 
 // Value of lane q of this thread's group of four consecutive lanes.
 template <class T>
@@ -497,52 +531,50 @@ __global__ void __launch_bounds__(256) k_smooth1(DevMesh m, DevState<R> s) {
     const double* pg = COL(s.pr, P_PG);
     const double* pp = COL(s.pr, P_PP);
     const double e6 = (double)1.0e-6f;
+    // the switch sums of variables 1, 5, 6, 10 (sw[0..3]) and the Laplacian
+    // d2q of every variable, one variable at a time
+    double swn[4], swd[4];
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+        const double* col = COL(s.cn, k);
+        const double v0 = col[i], v1 = col[a], v2 = col[b], v3 = col[c], v4 = col[d];
+        const int slot = k == 0 ? 0 : k == 4 ? 1 : k == 5 ? 2 : k == 9 ? 3 : -1;
+        if (slot >= 0) {
+            swn[slot] = fabs(v1 - v0) + fabs(v2 - v0) + fabs(v3 - v0) + fabs(v4 - v0);
+            swd[slot] = fabs(v1 + v0) + fabs(v2 + v0) + fabs(v3 + v0) + fabs(v4 + v0);
+        }
+        COL(s.d2q, k)[i] = v1 - v0 + v2 - v0 + v3 - v0 + v4 - v0;
+    }
     double pgi = pg[i];
     double anun = fabs(pg[a] - pgi) + fabs(pg[b] - pgi) + fabs(pg[c] - pgi) + fabs(pg[d] - pgi);
     double anud = fabs(pg[a] + pgi) + fabs(pg[b] + pgi) + fabs(pg[c] + pgi) + fabs(pg[d] + pgi);
     double anupg = anun / anud;
-    double cv[10][5];
-#pragma unroll
-    for (int k = 0; k < 10; k++) {
-        const double* col = COL(s.cn, k);
-        cv[k][0] = col[i]; cv[k][1] = col[a]; cv[k][2] = col[b]; cv[k][3] = col[c]; cv[k][4] = col[d];
-    }
-#define SW(K)                                                                                    \
-    anun = fabs(cv[K][1] - cv[K][0]) + fabs(cv[K][2] - cv[K][0]) + fabs(cv[K][3] - cv[K][0]) +   \
-           fabs(cv[K][4] - cv[K][0]);                                                            \
-    anud = fabs(cv[K][1] + cv[K][0]) + fabs(cv[K][2] + cv[K][0]) + fabs(cv[K][3] + cv[K][0]) +   \
-           fabs(cv[K][4] + cv[K][0]);
-    SW(4);
-    double anu1 = anupg + anun / (anud + e6);
-    SW(0);
-    anu1 = anu1 + anun / (anud + e6);
+    double anu1 = anupg + swn[1] / (swd[1] + e6);
+    anu1 = anu1 + swn[0] / (swd[0] + e6);
     double ppi = pp[i];
     anun = fabs(pp[a] - ppi) + fabs(pp[b] - ppi) + fabs(pp[c] - ppi) + fabs(pp[d] - ppi);
     anud = fabs(pp[a] + ppi) + fabs(pp[b] + ppi) + fabs(pp[c] + ppi) + fabs(pp[d] + ppi);
     double anupp = anun / anud;
-    SW(5);
-    double anu2 = anupp + anun / (anud + e6);
-    SW(9);
-    anu2 = anu2 + anun / (anud + e6);
-#undef SW
+    double anu2 = anupp + swn[2] / (swd[2] + e6);
+    anu2 = anu2 + swn[3] / (swd[3] + e6);
     COL(s.anu, 0)[i] = anu1;
     COL(s.anu, 1)[i] = anu2;
-#pragma unroll
-    for (int k = 0; k < 10; k++)
-        COL(s.d2q, k)[i] = cv[k][1] - cv[k][0] + cv[k][2] - cv[k][0] + cv[k][3] - cv[k][0] +
-                           cv[k][4] - cv[k][0];
 }
 
-// src/sr_smooth.F90:200-374: blended 2nd/4th difference d24.
-__global__ void __launch_bounds__(256) k_smooth2(DevMesh m, DevState<R> s, DevParams P) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.neles) return;
+// src/sr_smooth.F90:200-374: blended 2nd/4th difference d24.  F selects the
+// division form (see mdiv); returns the fast form's out-of-range flag.
+template <int F>
+__device__ __forceinline__ unsigned smooth2_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int i) {
+    unsigned bad = 0;
     const double dt = s.s->dt;
-    const double rdt = rcp(dt);
+    const double rdt = mrcp<F>(dt, bad);
     int nb[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) nb[f] = ldg(COL(m.snb, f) + i);
-    const double voli = ldg(m.vol + i);
+    const double vi = mdiv<F>(ldg(m.vol + i), dt, rdt, bad);
+    double d24nc[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) d24nc[f] = 0.5 * (vi + mdiv<F>(ldg(m.vol + nb[f]), dt, rdt, bad));
 #pragma unroll
     for (int set = 0; set < 2; set++) {
         const double* anu = COL(s.anu, set);
@@ -552,9 +584,8 @@ __global__ void __launch_bounds__(256) k_smooth2(DevMesh m, DevState<R> s, DevPa
         for (int f = 0; f < 4; f++) {
             double e2 = P.co2 * mx2(ai, anu[nb[f]]);
             double e4 = mx2(0.0, P.co4 - e2);
-            double d24nc = 0.5 * (div_rn(voli, dt, rdt) + div_rn(ldg(m.vol + nb[f]), dt, rdt));
-            d2c[f] = e2 * d24nc;
-            d4c[f] = e4 * d24nc;
+            d2c[f] = e2 * d24nc[f];
+            d4c[f] = e4 * d24nc[f];
         }
 #pragma unroll
         for (int k = 5 * set; k < 5 * set + 5; k++) {
@@ -567,6 +598,20 @@ __global__ void __launch_bounds__(256) k_smooth2(DevMesh m, DevState<R> s, DevPa
                         d4c[2] * (dq[nb[2]] - qi) + d4c[3] * (dq[nb[3]] - qi);
             COL(s.d24, k)[i] = d2 - d4;
         }
+    }
+    return bad;
+}
+
+__global__ void __launch_bounds__(256) k_smooth2(DevMesh m, DevState<R> s, DevParams P) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < m.neles;
+    if (!valid) i = m.neles - 1;      // keep the warp whole for the vote below
+    if constexpr (HP_FAST(8)) {
+        unsigned bad = 0;
+        if (valid) bad = smooth2_body<1>(m, s, P, i);
+        if (__any_sync(0xffffffffu, bad) && valid) smooth2_body<0>(m, s, P, i);
+    } else {
+        if (valid) smooth2_body<0>(m, s, P, i);
     }
 }
 
@@ -676,9 +721,10 @@ struct FaceOut {
     bool wall, takeg, takep;
 };
 
+template <int F>
 __device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& phip, R& ug, R& vg,
                                                R& wg, R& tg, R& pg, R& up, R& vp, R& wp, R& tp,
-                                               R& pp) {
+                                               R& pp, unsigned& bad) {
     const R emin = (R)P.emin, emax = (R)P.emax;
     if (phig < emin) {
         phig = emin; phip = R(1) - phig;
@@ -689,14 +735,14 @@ __device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& p
         up = ug; vp = vg; wp = wg; tp = tg; pp = pg;
     }
     if (phig >= emin && phig <= emax) {
-        R psig = div_rn(phig - emin, emax - emin, (R)P.r_emm);
+        R psig = mdiv<F>(phig - emin, emax - emin, (R)P.r_emm, bad);
         R f = -(psig * psig * (R(2) * psig - R(3)));
         ug = f * ug + (R(1) - f) * up; vg = f * vg + (R(1) - f) * vp;
         wg = f * wg + (R(1) - f) * wp; tg = f * tg + (R(1) - f) * tp;
         pg = f * pg + (R(1) - f) * pp;
     }
     if (phip >= emin && phip <= emax) {
-        R psig = div_rn(phip - emin, emax - emin, (R)P.r_emm);
+        R psig = mdiv<F>(phip - emin, emax - emin, (R)P.r_emm, bad);
         R f = -(psig * psig * (R(2) * psig - R(3)));
         up = f * up + (R(1) - f) * ug; vp = f * vp + (R(1) - f) * vg;
         wp = f * wp + (R(1) - f) * wg; tp = f * tp + (R(1) - f) * tg;
@@ -704,16 +750,18 @@ __device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& p
     }
 }
 
+// F selects the division form (see mdiv); bad collects its out-of-range flag.
+template <int F>
 __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s, const DevParams& P,
-                                          int i, int f, FaceOut& o) {
+                                          int i, int f, FaceOut& o, unsigned& bad) {
     const int neigh = ldg(COL(m.nc, f) + i);
     const unsigned kind = (ldg(m.fk + i) >> (4 * f)) & 0xFu;
     const double scxd = ldg(COL(m.sc, 3 * f) + i), scyd = ldg(COL(m.sc, 3 * f + 1) + i),
                  sczd = ldg(COL(m.sc, 3 * f + 2) + i);
     const R scx = (R)scxd, scy = (R)scyd, scz = (R)sczd;
     const R area = sqrt(scx * scx + scy * scy + scz * scz);
-    const R rarea = rcp(area);
-    const R enx = div_rn(scx, area, rarea), eny = div_rn(scy, area, rarea), enz = div_rn(scz, area, rarea);
+    const R rarea = mrcp<F>(area, bad);
+    const R enx = mdiv<F>(scx, area, rarea, bad), eny = mdiv<F>(scy, area, rarea, bad), enz = mdiv<F>(scz, area, rarea, bad);
     const double* pr = s.pr;
     R ugL = (R)COL(pr, P_UG)[i], vgL = (R)COL(pr, P_VG)[i], wgL = (R)COL(pr, P_WG)[i];
     R tgL = (R)COL(pr, P_TG)[i], phigL = (R)COL(pr, P_PHIG)[i];
@@ -749,10 +797,10 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     }
     const R rrg = (R)P.rrg, gamag = (R)P.gamag, gamap = (R)P.gamap, pinf = (R)P.pinf, cpp = (R)P.cpp;
     R phipL = R(1) - phigL, phipR = R(1) - phigR;
-    blend_phases_r(P, phigL, phipL, ugL, vgL, wgL, tgL, pgL, upL, vpL, wpL, tpL, ppL);
+    blend_phases_r<F>(P, phigL, phipL, ugL, vgL, wgL, tgL, pgL, upL, vpL, wpL, tpL, ppL, bad);
     R rogL = pgL / (rrg * tgL);
     R ropL = gamap * (ppL + pinf) / ((gamap - R(1)) * cpp * tpL);
-    blend_phases_r(P, phigR, phipR, ugR, vgR, wgR, tgR, pgR, upR, vpR, wpR, tpR, ppR);
+    blend_phases_r<F>(P, phigR, phipR, ugR, vgR, wgR, tgR, pgR, upR, vpR, wpR, tpR, ppR, bad);
     R rogR = pgR / (rrg * tgR);
     R ropR = gamap * (ppR + pinf) / ((gamap - R(1)) * cpp * tpR);
     o.wall = (kind & FK_WALL) != 0;
@@ -768,25 +816,26 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     }
     const R eps8 = (R)(double)1.0e-8f, eps6 = (R)(double)1.0e-6f;
     const R rgm1 = (R)P.r_gm1, rgamap = (R)P.r_gamap;
-    const R rropL = rcp(ropL), rropR = rcp(ropR);
-    R egL = div_rn(rrg * tgL, gamag - R(1), rgm1) + R(0.5) * (ugL * ugL + vgL * vgL + wgL * wgL);
-    R hgL = egL + pgL / rogL;
+    const R rropL = mrcp<F>(ropL, bad), rropR = mrcp<F>(ropR, bad);
+    R egL = mdiv<F>(rrg * tgL, gamag - R(1), rgm1, bad) + R(0.5) * (ugL * ugL + vgL * vgL + wgL * wgL);
+    const R rrogL = mrcp<F>(rogL, bad), rrogR = mrcp<F>(rogR, bad);
+    R hgL = egL + mdiv<F>(pgL, rogL, rrogL, bad);
     R qgL = ugL * enx + vgL * eny + wgL * enz;
-    R agL = sqrt(gamag * pgL / rogL);
-    R egR = div_rn(rrg * tgR, gamag - R(1), rgm1) + R(0.5) * (ugR * ugR + vgR * vgR + wgR * wgR);
-    R hgR = egR + pgR / rogR;
+    R agL = sqrt(mdiv<F>(gamag * pgL, rogL, rrogL, bad));
+    R egR = mdiv<F>(rrg * tgR, gamag - R(1), rgm1, bad) + R(0.5) * (ugR * ugR + vgR * vgR + wgR * wgR);
+    R hgR = egR + mdiv<F>(pgR, rogR, rrogR, bad);
     R qgR = ugR * enx + vgR * eny + wgR * enz;
-    R agR = sqrt(gamag * pgR / rogR);
-    R epL = div_rn(cpp * tpL, gamap, rgamap) + div_rn(pinf, ropL, rropL) +
+    R agR = sqrt(mdiv<F>(gamag * pgR, rogR, rrogR, bad));
+    R epL = mdiv<F>(cpp * tpL, gamap, rgamap, bad) + mdiv<F>(pinf, ropL, rropL, bad) +
             R(0.5) * (upL * upL + vpL * vpL + wpL * wpL);
-    R hpL = epL + div_rn(ppL, ropL, rropL);
+    R hpL = epL + mdiv<F>(ppL, ropL, rropL, bad);
     R qpL = upL * enx + vpL * eny + wpL * enz;
-    R apL = sqrt(div_rn(gamap * (ppL + pinf), ropL, rropL));
-    R epR = div_rn(cpp * tpR, gamap, rgamap) + div_rn(pinf, ropR, rropR) +
+    R apL = sqrt(mdiv<F>(gamap * (ppL + pinf), ropL, rropL, bad));
+    R epR = mdiv<F>(cpp * tpR, gamap, rgamap, bad) + mdiv<F>(pinf, ropR, rropR, bad) +
             R(0.5) * (upR * upR + vpR * vpR + wpR * wpR);
-    R hpR = epR + div_rn(ppR, ropR, rropR);
+    R hpR = epR + mdiv<F>(ppR, ropR, rropR, bad);
     R qpR = upR * enx + vpR * eny + wpR * enz;
-    R apR = sqrt(div_rn(gamap * (ppR + pinf), ropR, rropR));
+    R apR = sqrt(mdiv<F>(gamap * (ppR + pinf), ropR, rropR, bad));
     R sgl = mn2(mn2(qgL - agL, qgR - agR), eps8);
     R spl = mn2(mn2(qpL - apL, qpR - apR), eps8);
     R sgr = mx2(mx2(qgL + agL, qgR + agR), eps8);
@@ -815,12 +864,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 o.F[3] = fl3 * area; o.F[4] = fl4 * area;
             } else {
                 R dnrg = (sgstar - sgl) + eps6;
-                const R rd = rcp(dnrg);
-                R cs0 = div_rn((qgL - sgl) * cn0, dnrg, rd);
-                R cs1 = div_rn((qgL - sgl) * cn1 + phigL * (pgL * enx - pgstar * enx), dnrg, rd);
-                R cs2 = div_rn((qgL - sgl) * cn2 + phigL * (pgL * eny - pgstar * eny), dnrg, rd);
-                R cs3 = div_rn((qgL - sgl) * cn3 + phigL * (pgL * enz - pgstar * enz), dnrg, rd);
-                R cs4 = div_rn((qgL - sgl) * cn4 + phigL * (pgL * qgL - pgstar * sgstar), dnrg, rd);
+                const R rd = mrcp<F>(dnrg, bad);
+                R cs0 = mdiv<F>((qgL - sgl) * cn0, dnrg, rd, bad);
+                R cs1 = mdiv<F>((qgL - sgl) * cn1 + phigL * (pgL * enx - pgstar * enx), dnrg, rd, bad);
+                R cs2 = mdiv<F>((qgL - sgl) * cn2 + phigL * (pgL * eny - pgstar * eny), dnrg, rd, bad);
+                R cs3 = mdiv<F>((qgL - sgl) * cn3 + phigL * (pgL * enz - pgstar * enz), dnrg, rd, bad);
+                R cs4 = mdiv<F>((qgL - sgl) * cn4 + phigL * (pgL * qgL - pgstar * sgstar), dnrg, rd, bad);
                 o.F[0] = (fl0 + sgl * (cs0 - cn0)) * area;
                 o.F[1] = (fl1 + sgl * (cs1 - cn1)) * area;
                 o.F[2] = (fl2 + sgl * (cs2 - cn2)) * area;
@@ -840,12 +889,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 o.F[3] = fr3 * area; o.F[4] = fr4 * area;
             } else {
                 R dnrg = (sgstar - sgr) + eps6;
-                const R rd = rcp(dnrg);
-                R cs0 = div_rn((qgR - sgr) * cn0, dnrg, rd);
-                R cs1 = div_rn((qgR - sgr) * cn1 + phigR * (pgR * enx - pgstar * enx), dnrg, rd);
-                R cs2 = div_rn((qgR - sgr) * cn2 + phigR * (pgR * eny - pgstar * eny), dnrg, rd);
-                R cs3 = div_rn((qgR - sgr) * cn3 + phigR * (pgR * enz - pgstar * enz), dnrg, rd);
-                R cs4 = div_rn((qgR - sgr) * cn4 + phigR * (pgR * qgR - pgstar * sgstar), dnrg, rd);
+                const R rd = mrcp<F>(dnrg, bad);
+                R cs0 = mdiv<F>((qgR - sgr) * cn0, dnrg, rd, bad);
+                R cs1 = mdiv<F>((qgR - sgr) * cn1 + phigR * (pgR * enx - pgstar * enx), dnrg, rd, bad);
+                R cs2 = mdiv<F>((qgR - sgr) * cn2 + phigR * (pgR * eny - pgstar * eny), dnrg, rd, bad);
+                R cs3 = mdiv<F>((qgR - sgr) * cn3 + phigR * (pgR * enz - pgstar * enz), dnrg, rd, bad);
+                R cs4 = mdiv<F>((qgR - sgr) * cn4 + phigR * (pgR * qgR - pgstar * sgstar), dnrg, rd, bad);
                 o.F[0] = (fr0 + sgr * (cs0 - cn0)) * area;
                 o.F[1] = (fr1 + sgr * (cs1 - cn1)) * area;
                 o.F[2] = (fr2 + sgr * (cs2 - cn2)) * area;
@@ -872,12 +921,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 o.F[8] = fl3 * area; o.F[9] = fl4 * area;
             } else {
                 R dnrp = (spstar - spl) + eps6;
-                const R rd = rcp(dnrp);
-                R cs0 = div_rn((qpL - spl) * cn0, dnrp, rd);
-                R cs1 = div_rn((qpL - spl) * cn1 + phipL * (ppL * enx - ppstar * enx), dnrp, rd);
-                R cs2 = div_rn((qpL - spl) * cn2 + phipL * (ppL * eny - ppstar * eny), dnrp, rd);
-                R cs3 = div_rn((qpL - spl) * cn3 + phipL * (ppL * enz - ppstar * enz), dnrp, rd);
-                R cs4 = div_rn((qpL - spl) * cn4 + phipL * (ppL * qpL - ppstar * spstar), dnrp, rd);
+                const R rd = mrcp<F>(dnrp, bad);
+                R cs0 = mdiv<F>((qpL - spl) * cn0, dnrp, rd, bad);
+                R cs1 = mdiv<F>((qpL - spl) * cn1 + phipL * (ppL * enx - ppstar * enx), dnrp, rd, bad);
+                R cs2 = mdiv<F>((qpL - spl) * cn2 + phipL * (ppL * eny - ppstar * eny), dnrp, rd, bad);
+                R cs3 = mdiv<F>((qpL - spl) * cn3 + phipL * (ppL * enz - ppstar * enz), dnrp, rd, bad);
+                R cs4 = mdiv<F>((qpL - spl) * cn4 + phipL * (ppL * qpL - ppstar * spstar), dnrp, rd, bad);
                 o.F[5] = (fl0 + spl * (cs0 - cn0)) * area;
                 o.F[6] = (fl1 + spl * (cs1 - cn1)) * area;
                 o.F[7] = (fl2 + spl * (cs2 - cn2)) * area;
@@ -897,12 +946,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 o.F[8] = fr3 * area; o.F[9] = fr4 * area;
             } else {
                 R dnrp = (spstar - spr) + eps6;
-                const R rd = rcp(dnrp);
-                R cs0 = div_rn((qpR - spr) * cn0, dnrp, rd);
-                R cs1 = div_rn((qpR - spr) * cn1 + phipR * (ppR * enx - ppstar * enx), dnrp, rd);
-                R cs2 = div_rn((qpR - spr) * cn2 + phipR * (ppR * eny - ppstar * eny), dnrp, rd);
-                R cs3 = div_rn((qpR - spr) * cn3 + phipR * (ppR * enz - ppstar * enz), dnrp, rd);
-                R cs4 = div_rn((qpR - spr) * cn4 + phipR * (ppR * qpR - ppstar * spstar), dnrp, rd);
+                const R rd = mrcp<F>(dnrp, bad);
+                R cs0 = mdiv<F>((qpR - spr) * cn0, dnrp, rd, bad);
+                R cs1 = mdiv<F>((qpR - spr) * cn1 + phipR * (ppR * enx - ppstar * enx), dnrp, rd, bad);
+                R cs2 = mdiv<F>((qpR - spr) * cn2 + phipR * (ppR * eny - ppstar * eny), dnrp, rd, bad);
+                R cs3 = mdiv<F>((qpR - spr) * cn3 + phipR * (ppR * enz - ppstar * enz), dnrp, rd, bad);
+                R cs4 = mdiv<F>((qpR - spr) * cn4 + phipR * (ppR * qpR - ppstar * spstar), dnrp, rd, bad);
                 o.F[5] = (fr0 + spr * (cs0 - cn0)) * area;
                 o.F[6] = (fr1 + spr * (cs1 - cn1)) * area;
                 o.F[7] = (fr2 + spr * (cs2 - cn2)) * area;
@@ -928,7 +977,8 @@ __device__ __noinline__ void stale_flux(const DevMesh& m, const DevState<R>& s, 
             face = 3;
         }
         FaceOut o;
-        face_eval(m, s, P, cell, face, o);
+        unsigned bad_ = 0;
+        face_eval<0>(m, s, P, cell, face, o, bad_);
         if (!o.wall && (gas ? o.takeg : o.takep)) {
             for (int k = 0; k < 5; k++) out[k] = o.F[(gas ? 0 : 5) + k];
             return;
@@ -966,7 +1016,8 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
 #pragma unroll 1
     for (int f = 0; f < 4; f++) {
         FaceOut o;
-        face_eval(m, s, P, i, f, o);
+        unsigned bad_ = 0;
+        face_eval<0>(m, s, P, i, f, o, bad_);
         if (o.wall) {
             rhs[1] = rhs[1] + (double)o.w[0]; rhs[2] = rhs[2] + (double)o.w[1];
             rhs[3] = rhs[3] + (double)o.w[2]; rhs[6] = rhs[6] + (double)o.w[3];
@@ -1098,14 +1149,12 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
 // k_grad with four lanes per cell: lane q computes the LSQ gradients of
 // fields q, q+4, q+8, q+12 and the limiter of one of pg, pp, rog, rop; phi is
 // the in-order minimum over the lanes (equal to the reference's chain when no
-// value is NaN).
-__global__ void __launch_bounds__(128, 4) k_grad4(DevMesh m, DevState<R> s, DevParams P) {
-    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int q = (int)(gt & 3);
-    int i = (int)(gt >> 2);
-    const bool valid = i < m.neles;
-    if (!valid) i = m.neles - 1;
-    const bool active = valid && ldg(m.iblank + i) == 1;
+// value is NaN).  F selects the division form (see mdiv); the return value is
+// the fast form's out-of-range flag.
+template <int F>
+__device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int i,
+                                               int q, bool active) {
+    unsigned bad = 0;
     int n[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
@@ -1120,16 +1169,17 @@ __global__ void __launch_bounds__(128, 4) k_grad4(DevMesh m, DevState<R> s, DevP
     // geometry-only terms (wt, a1..b3, dnr of src/sr_derivative.F90:163-176,
     // 255), evaluated once at set-up with the same expressions
     R wt[4], rw[4];
-#define DW(x, f) div_rn((x), wt[f], rw[f])
+#undef DW
+#define DW(x, f) mdiv<F>((x), wt[f], rw[f], bad)
 #if HP_LSQ_TABLE
 #pragma unroll
-    for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqa, f) + i); rw[f] = rcp(wt[f]); }
+    for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqa, f) + i); rw[f] = mrcp<F>(wt[f], bad); }
     const R a1 = (R)ldg(COL(m.lsqa, 4) + i), a2 = (R)ldg(COL(m.lsqa, 5) + i), a3 = (R)ldg(COL(m.lsqa, 6) + i);
     const R b1 = (R)ldg(COL(m.lsqa, 7) + i), b2 = (R)ldg(COL(m.lsqa, 8) + i), b3 = (R)ldg(COL(m.lsqa, 9) + i);
     const R dnr = (R)ldg(COL(m.lsqa, 10) + i);
 #else
 #pragma unroll
-    for (int f = 0; f < 4; f++) { wt[f] = xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]; rw[f] = rcp(wt[f]); }
+    for (int f = 0; f < 4; f++) { wt[f] = xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]; rw[f] = mrcp<F>(wt[f], bad); }
     const R a1 = DW(xa[0] * xa[0], 0) + DW(xa[1] * xa[1], 1) + DW(xa[2] * xa[2], 2) + DW(xa[3] * xa[3], 3);
     const R a2 = DW(ya[0] * ya[0], 0) + DW(ya[1] * ya[1], 1) + DW(ya[2] * ya[2], 2) + DW(ya[3] * ya[3], 3);
     const R a3 = DW(za[0] * za[0], 0) + DW(za[1] * za[1], 1) + DW(za[2] * za[2], 2) + DW(za[3] * za[3], 3);
@@ -1138,7 +1188,7 @@ __global__ void __launch_bounds__(128, 4) k_grad4(DevMesh m, DevState<R> s, DevP
     const R b3 = DW(za[0] * ya[0], 0) + DW(za[1] * ya[1], 1) + DW(za[2] * ya[2], 2) + DW(za[3] * ya[3], 3);
     const R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
 #endif
-    const R rdnr = rcp(dnr);
+    const R rdnr = mrcp<F>(dnr, bad);
     const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
     // limiter field of this lane: pg (grad field 8), pp (9), rog (11), rop (12)
     R lg[3] = {R(0), R(0), R(0)};     // gradient of the lane's limiter field
@@ -1157,9 +1207,9 @@ __global__ void __launch_bounds__(128, 4) k_grad4(DevMesh m, DevState<R> s, DevP
         else
             c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + DW(qd * ya[3], 3);
         R c3 = DW(qa * za[0], 0) + DW(qb * za[1], 1) + DW(qc * za[2], 2) + DW(qd * za[3], 3);
-        R gx = div_rn(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr);
-        R gy = div_rn(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr);
-        R gz = div_rn(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr);
+        R gx = mdiv<F>(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr, bad);
+        R gy = mdiv<F>(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr, bad);
+        R gz = mdiv<F>(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr, bad);
         if (v < 11 && active) {
             COL(s.gr, 3 * v + 0)[i] = gx;
             COL(s.gr, 3 * v + 1)[i] = gy;
@@ -1168,6 +1218,8 @@ __global__ void __launch_bounds__(128, 4) k_grad4(DevMesh m, DevState<R> s, DevP
         if (v == 8 || v == 9) { lg[0] = gx; lg[1] = gy; lg[2] = gz; }          // lanes 0, 1
         if (v == 11 || v == 12) { sg[0] = gx; sg[1] = gy; sg[2] = gz; }        // lanes 3, 0
     }
+#undef DW
+#define DW(x, f) div_rn((x), wt[f], rw[f])
     // lane 2 takes rog from lane 3, lane 3 takes rop from lane 0
     const int src = q == 2 ? 3 : (q == 3 ? 0 : q);
     R fx0 = qshfl(sg[0], src), fy0 = qshfl(sg[1], src), fz0 = qshfl(sg[2], src);
@@ -1194,25 +1246,43 @@ __global__ void __launch_bounds__(128, 4) k_grad4(DevMesh m, DevState<R> s, DevP
     }
     R p0 = qshfl(phl, 0), p1 = qshfl(phl, 1), p2 = qshfl(phl, 2), p3 = qshfl(phl, 3);
     if (q == 0 && active) s.phi[i] = (double)mn2(mn2(mn2(p0, p1), p2), p3);
+    return bad;
 }
 
-// Residual + sources + RK update with four lanes per cell: lane q evaluates
-// face q; every lane re-assembles the residual in face order and computes
-// the sources; lane q writes variables q, q+4, q+8.
-__global__ void __launch_bounds__(128, 4) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
+__global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevState<R> s, DevParams P) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
     int i = (int)(gt >> 2);
     const bool valid = i < m.neles;
     if (!valid) i = m.neles - 1;
     const bool active = valid && ldg(m.iblank + i) == 1;
+    if constexpr (HP_FAST(1)) {
+        // the outputs are not inputs of this kernel, so a warp that flagged
+        // an operand simply recomputes and overwrites them
+        const unsigned bad = grad4_body<1>(m, s, P, i, q, active);
+        if (__any_sync(0xffffffffu, bad)) grad4_body<0>(m, s, P, i, q, active);
+    } else {
+        grad4_body<0>(m, s, P, i, q, active);
+    }
+}
+
+// Residual + sources + RK update with four lanes per cell: lane q evaluates
+// face q; every lane re-assembles the residual in face order and computes
+// the sources; lane q writes variables q, q+4, q+8.  F selects the division
+// form (see mdiv).  The fast form returns false, before any store, when a lane
+// of the warp flagged an operand (cn is read and written here, so the stores
+// must wait for that vote).
+template <int F>
+__device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int stage,
+                                           int i, int q, bool active) {
+    unsigned bad = 0;
     const double* pr = s.pr;
     // this lane's face
     R eff[10];
     int flags;
     {
         FaceOut o;
-        face_eval(m, s, P, i, q, o);
+        face_eval<F>(m, s, P, i, q, o, bad);
         if (o.wall) {
 #pragma unroll
             for (int k = 0; k < 10; k++) eff[k] = R(0);
@@ -1290,14 +1360,16 @@ __global__ void __launch_bounds__(128, 4) k_flux4(DevMesh m, DevState<R> s, DevP
         const R uint_ = qshfl(vq_int, 0), vint = qshfl(vq_int, 1), wint = qshfl(vq_int, 2);
         // geometry-only terms (src/sr_source.F90:100-117), evaluated at set-up
         R wt[4], rw[4];
+#undef DW
+#define DW(x, f) mdiv<F>((x), wt[f], rw[f], bad)
 #if HP_LSQ_TABLE
 #pragma unroll
-        for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqb, f) + i); rw[f] = rcp(wt[f]); }
+        for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqb, f) + i); rw[f] = mrcp<F>(wt[f], bad); }
         const R a1 = (R)ldg(COL(m.lsqb, 4) + i), a2 = (R)ldg(COL(m.lsqb, 5) + i), a3 = (R)ldg(COL(m.lsqb, 6) + i);
         const R b1 = (R)ldg(COL(m.lsqb, 7) + i), b2 = (R)ldg(COL(m.lsqb, 8) + i), b3 = (R)ldg(COL(m.lsqb, 9) + i);
 #else
 #pragma unroll
-        for (int f = 0; f < 4; f++) { wt[f] = sqrt(xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]); rw[f] = rcp(wt[f]); }
+        for (int f = 0; f < 4; f++) { wt[f] = sqrt(xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]); rw[f] = mrcp<F>(wt[f], bad); }
         const R a1 = DW(xa[0] * xa[0], 0) + DW(xa[1] * xa[1], 1) + DW(xa[2] * xa[2], 2) + DW(xa[3] * xa[3], 3);
         const R a2 = DW(ya[0] * ya[0], 0) + DW(ya[1] * ya[1], 1) + DW(ya[2] * ya[2], 2) + DW(ya[3] * ya[3], 3);
         const R a3 = DW(za[0] * za[0], 0) + DW(za[1] * za[1], 1) + DW(za[2] * za[2], 2) + DW(za[3] * za[3], 3);
@@ -1322,6 +1394,8 @@ __global__ void __launch_bounds__(128, 4) k_flux4(DevMesh m, DevState<R> s, DevP
         const R A13 = q >= 2 ? c1 : b2, A23 = q >= 2 ? c2 : b3, A33 = q >= 2 ? c3 : a3;
         const R dq = det3(A11, A21, A31, A12, A22, A32, A13, A23, A33) / dnr;
         const R dpx = qshfl(dq, 0), dpy = qshfl(dq, 1), dpz = qshfl(dq, 2);
+#undef DW
+#define DW(x, f) div_rn((x), wt[f], rw[f])
         const R g = R(0);
         R en = pint * (uint_ * dpx + vint * dpy + wint * dpz) + uint_ * fdgx + vint * fdgy + wint * fdgz + qsource;
         const double* vis = s.vis;
@@ -1334,7 +1408,10 @@ __global__ void __launch_bounds__(128, 4) k_flux4(DevMesh m, DevState<R> s, DevP
         rhs[8] = rhs[8] + (double)((fdgz + pint * dpz) * voli) - COL(vis, 6)[i];
         rhs[9] = rhs[9] + (double)(en * voli) - COL(vis, 7)[i];
     }
-    if (!active) return;
+    if constexpr (F == 1) {
+        if (__any_sync(0xffffffffu, bad)) return false;
+    }
+    if (!active) return true;
     const double dtbyvol = s.s->dt / ldg(m.vol + i);
 #pragma unroll
     for (int r = 0; r < 3; r++) {
@@ -1363,6 +1440,21 @@ __global__ void __launch_bounds__(128, 4) k_flux4(DevMesh m, DevState<R> s, DevP
             }
         }
     }
+    return true;
+}
+
+__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (int)(gt & 3);
+    int i = (int)(gt >> 2);
+    const bool valid = i < m.neles;
+    if (!valid) i = m.neles - 1;
+    const bool active = valid && ldg(m.iblank + i) == 1;
+    if constexpr (HP_FAST(2)) {
+        if (!flux4_body<1>(m, s, P, stage, i, q, active)) flux4_body<0>(m, s, P, stage, i, q, active);
+    } else {
+        flux4_body<0>(m, s, P, stage, i, q, active);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1370,8 +1462,9 @@ __global__ void __launch_bounds__(128, 4) k_flux4(DevMesh m, DevState<R> s, DevP
 // One face f of cell i: face-centred LSQ over 5 (boundary) or 8 (interior)
 // cell centres, Newtonian stresses and heat flux; c[8] = the face's
 // contribution to visug..vistp.
+template <int F>
 __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s, const DevParams& P,
-                                          int i, int f, const int nci[4], double c[8]) {
+                                          int i, int f, const int nci[4], double c[8], unsigned& bad) {
     const double* pr = s.pr;
     const int fcol[8] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP};
     const R c23 = (R)P.c23;
@@ -1387,9 +1480,9 @@ __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s
     const R phipf = (R)((COL(pr, P_PHIP)[i] + COL(pr, P_PHIP)[neigh]) * 0.5);
     const R tgf = ff[3];
     const R amug = (R)P.as * sqrt(tgf) / (R(1) + (R)P.ts / tgf);
-    const R akg = div_rn(amug * (R)P.cpg, (R)P.prg, (R)P.r_prg);
+    const R akg = mdiv<F>(amug * (R)P.cpg, (R)P.prg, (R)P.r_prg, bad);
     const R amup = (R)P.amup;
-    const R akp = div_rn(amup * (R)P.cpp, (R)P.prp, (R)P.r_prp);
+    const R akp = mdiv<F>(amup * (R)P.cpp, (R)P.prp, (R)P.r_prp, bad);
     int mm[8];
     int nm;
     mm[0] = nci[0]; mm[1] = nci[1]; mm[2] = nci[2]; mm[3] = nci[3];
@@ -1413,7 +1506,7 @@ __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s
         a12 = a12 + dx[k] * dy[k]; a13 = a13 + dx[k] * dz[k]; a23 = a23 + dy[k] * dz[k];
     }
     const R dnr = det3(a11, a12, a13, a12, a22, a23, a13, a23, a33);
-    const R rdnr = rcp(dnr);
+    const R rdnr = mrcp<F>(dnr, bad);
     R gr[8][3];
 #pragma unroll
     for (int v = 0; v < 8; v++) {
@@ -1424,9 +1517,9 @@ __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s
             R dk = (R)q[mm[k]] - ff[v];
             b1 = b1 + dk * dx[k]; b2 = b2 + dk * dy[k]; b3 = b3 + dk * dz[k];
         }
-        gr[v][0] = div_rn(det3(b1, b2, b3, a12, a22, a23, a13, a23, a33), dnr, rdnr);
-        gr[v][1] = div_rn(det3(a11, a12, a13, b1, b2, b3, a13, a23, a33), dnr, rdnr);
-        gr[v][2] = div_rn(det3(a11, a12, a13, a12, a22, a23, b1, b2, b3), dnr, rdnr);
+        gr[v][0] = mdiv<F>(det3(b1, b2, b3, a12, a22, a23, a13, a23, a33), dnr, rdnr, bad);
+        gr[v][1] = mdiv<F>(det3(a11, a12, a13, b1, b2, b3, a13, a23, a33), dnr, rdnr, bad);
+        gr[v][2] = mdiv<F>(det3(a11, a12, a13, a12, a22, a23, b1, b2, b3), dnr, rdnr, bad);
     }
     const R ugf = ff[0], vgf = ff[1], wgf = ff[2], upf = ff[4], vpf = ff[5], wpf = ff[6];
     R delvg = gr[0][0] + gr[1][1] + gr[2][2];
@@ -1473,7 +1566,8 @@ __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParam
 #pragma unroll 1
     for (int f = 0; f < 4; f++) {
         double c[8];
-        visc_face(m, s, P, i, f, nci, c);
+        unsigned bad_ = 0;
+        visc_face<0>(m, s, P, i, f, nci, c, bad_);
 #pragma unroll
         for (int k = 0; k < 8; k++) acc[k] = acc[k] + c[k];
     }
@@ -1488,7 +1582,7 @@ __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParam
 // of a warp reach every shuffle (out-of-range lanes replay the last cell and
 // do not write).
 
-__global__ void __launch_bounds__(128, 3) k_visc4(DevMesh m, DevState<R> s, DevParams P) {
+__global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevState<R> s, DevParams P) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
     int i = (int)(gt >> 2);
@@ -1498,18 +1592,25 @@ __global__ void __launch_bounds__(128, 3) k_visc4(DevMesh m, DevState<R> s, DevP
     int nci[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) nci[f] = ldg(COL(m.nc, f) + i);
-    double c[8];
-    visc_face(m, s, P, i, q, nci, c);
-    double acc[8];
+    // vis is not an input of this kernel: a warp whose fast pass flagged an
+    // operand recomputes and overwrites its sums
+    for (int pass = HP_FAST(4) ? 1 : 0; pass >= 0; pass--) {
+        double c[8];
+        unsigned bad = 0;
+        if (pass) visc_face<1>(m, s, P, i, q, nci, c, bad);
+        else visc_face<0>(m, s, P, i, q, nci, c, bad);
+        double acc[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) acc[k] = 0.0;
+        for (int k = 0; k < 8; k++) acc[k] = 0.0;
 #pragma unroll
-    for (int f = 0; f < 4; f++)
+        for (int f = 0; f < 4; f++)
 #pragma unroll
-        for (int k = 0; k < 8; k++) acc[k] = acc[k] + qshfl(c[k], f);
-    if (active) {
-        COL(s.vis, q)[i] = acc[q];
-        COL(s.vis, q + 4)[i] = acc[q + 4];
+            for (int k = 0; k < 8; k++) acc[k] = acc[k] + qshfl(c[k], f);
+        if (active) {
+            COL(s.vis, q)[i] = acc[q];
+            COL(s.vis, q + 4)[i] = acc[q + 4];
+        }
+        if (!__any_sync(0xffffffffu, bad)) break;
     }
 }
 

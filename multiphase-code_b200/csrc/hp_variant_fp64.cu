@@ -3,6 +3,24 @@
 #define HP_R double
 // geometry-only least-squares terms: loaded from the set-up tables
 #define HP_LSQ_TABLE 1
+// division form and blocks per SM of the 4-lane kernels (measured per variant)
+#ifndef HP_DIV_FAST
+#define HP_DIV_FAST 1
+#endif
+// fast division in gradients, fluxes and JST; the viscous kernel spills with
+// its second (fallback) body and is faster with hardware division
+#ifndef HP_FAST_MASK
+#define HP_FAST_MASK 11
+#endif
+#ifndef HP_GRAD4_MINB
+#define HP_GRAD4_MINB 6
+#endif
+#ifndef HP_FLUX4_MINB
+#define HP_FLUX4_MINB 4
+#endif
+#ifndef HP_VISC4_MINB
+#define HP_VISC4_MINB 3
+#endif
 #include "hp_kernels.cuh"
 
 namespace hp {

@@ -3,6 +3,19 @@
 #define HP_R float
 // geometry-only least-squares terms: recomputed in FP32
 #define HP_LSQ_TABLE 0
+// division form and blocks per SM of the 4-lane kernels (measured per variant)
+#ifndef HP_DIV_FAST
+#define HP_DIV_FAST 0
+#endif
+#ifndef HP_GRAD4_MINB
+#define HP_GRAD4_MINB 6
+#endif
+#ifndef HP_FLUX4_MINB
+#define HP_FLUX4_MINB 5
+#endif
+#ifndef HP_VISC4_MINB
+#define HP_VISC4_MINB 4
+#endif
 #include "hp_kernels.cuh"
 
 namespace hp {
