@@ -146,6 +146,16 @@ int hp_device_state(hp_handle *h, double **cu_dev, int64_t *ld);
 int hp_info(const hp_handle *h, int64_t *kernels_per_step, int64_t *device_bytes,
             int64_t *aliased);
 
+/* --- serving many cases ---------------------------------------------------- */
+/* No counterpart in the reference, which runs one case per process.  Device
+ * bytes hp_create would allocate for this mesh and precision (admission
+ * against an HBM budget before creating). */
+int hp_estimate_bytes(const hp_mesh *mesh, const hp_params *params, int64_t *bytes);
+/* *busy = 1 while steps queued on the handle's stream are still running,
+ * 0 once they are done; never blocks.  Lets one host thread drive many
+ * handles whose streams overlap on the device. */
+int hp_poll(hp_handle *h, int32_t *busy);
+
 /* --- allocation-free time step ------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory (a Fortran/OpenACC host whose device arrays and memory budget belong

@@ -104,6 +104,36 @@ extern "C" const char* hp_create_error(void) { return g_create_error.c_str(); }
 
 extern "C" const char* hp_last_error(const hp_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
+// Carves every device array of a handle out of one arena (a probe arena
+// with no base only measures).  The same plan sizes hp_estimate_bytes.
+static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long ld, size_t gb) {
+    const size_t D = sizeof(double), I = sizeof(int);
+    DevMesh& m = h->dm;
+    m.nc = (int*)a.take(4 * ld * I); m.snb = (int*)a.take(4 * ld * I);
+    m.fk = (unsigned*)a.take(ld * sizeof(unsigned)); m.iblank = (int*)a.take(ld * I);
+    m.xc = (double*)a.take(ld * D); m.yc = (double*)a.take(ld * D); m.zc = (double*)a.take(ld * D);
+    m.vol = (double*)a.take(ld * D); m.dl = (double*)a.take(ld * D); m.dd = (double*)a.take(ld * D);
+    m.sc = (double*)a.take(12 * ld * D); m.fch = (double*)a.take(12 * ld * D);
+    m.fcv = (double*)a.take(12 * ld * D);
+    m.lsqa = (double*)a.take(11 * ld * D);
+    m.lsqb = (double*)a.take(11 * ld * D);
+    m.g_par = (int*)a.take((nghosts + 1) * (size_t)I); m.g_id = (int*)a.take((nghosts + 1) * (size_t)I);
+    m.g_type = (int*)a.take((nghosts + 1) * (size_t)I);
+    DevState<double>& s = h->ds;
+    s.cn = (double*)a.take(10 * ld * D); s.cu = (double*)a.take(10 * ld * D);
+    s.cn1 = (double*)a.take(10 * ld * D); s.pr = (double*)a.take(NPR * ld * D);
+    s.gr = (double*)a.take(NGR * ld * gb); s.phi = (double*)a.take(ld * D);
+    s.anu = (double*)a.take(2 * ld * D); s.d2q = (double*)a.take(10 * ld * D);
+    s.d24 = (double*)a.take(10 * ld * D); s.vis = (double*)a.take(8 * ld * D);
+    s.egt = (double*)a.take(2 * ld * D);
+    s.s = (DevScalars*)a.take(sizeof(DevScalars));
+    s.diag = (double*)a.take((size_t)h->max_diag * 8 * D);
+    s.max_diag = h->max_diag;
+    h->d_perm = (int*)a.take((neles + 1) * (size_t)I);
+    h->d_gid = (int*)a.take((nghosts + 1) * (size_t)I);
+    h->d_gstage = (double*)a.take(6 * (nghosts + 1) * D);
+}
+
 extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle** out) {
     g_create_error.clear();
     if (!mesh || !params || !out) return fail(nullptr, HP_E_ARG, "null argument");
@@ -162,6 +192,9 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     auto SC = [&](int k, int i) -> double& { return sc[(size_t)k * (ntot + 1) + i]; };
     auto FCH = [&](int k, int i) -> double& { return fch[(size_t)k * (ntot + 1) + i]; };
     auto FCV = [&](int k, int i) -> double& { return fcv[(size_t)k * (ntot + 1) + i]; };
+    // per-cell loops below are independent across cells (each writes only
+    // its own slots), so they run on all host cores with identical results
+#pragma omp parallel for schedule(static)
     for (int i = 1; i <= neles; i++) {
         for (int f = 0; f < 4; f++) {
             int n1 = nod[GEO_FACE[f][0] - 1][i], n2 = nod[GEO_FACE[f][1] - 1][i], n3 = nod[GEO_FACE[f][2] - 1][i];
@@ -240,6 +273,7 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     std::vector<double> lsqa(11 * (size_t)(neles + 1), 0.0), lsqb(11 * (size_t)(neles + 1), 0.0);
     auto LA = [&](int k, int i) -> double& { return lsqa[(size_t)k * (neles + 1) + i]; };
     auto LB = [&](int k, int i) -> double& { return lsqb[(size_t)k * (neles + 1) + i]; };
+#pragma omp parallel for schedule(static)
     for (int i = 1; i <= neles; i++) {
         double xa[4], ya[4], za[4], wa[4], wb[4];
         for (int f = 0; f < 4; f++) {
@@ -297,6 +331,7 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
             for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], p[d]); hi[d] = std::max(hi[d], p[d]); }
         }
         std::vector<std::pair<uint32_t, int>> key(neles);
+#pragma omp parallel for schedule(static)
         for (int i = 1; i <= neles; i++) {
             double p[3] = {xcel[i], ycel[i], zcel[i]};
             uint32_t q[3];
@@ -325,6 +360,9 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     std::vector<double> hla(11 * ld, 0.0), hlb(11 * ld, 0.0);
     std::vector<int> slot_parent(ntot + 1, 0);
     for (int g = 0; g < nghosts; g++) slot_parent[gid[g]] = gpar[g];
+    // slots t = map(i) are distinct for distinct i on meshes without aliased
+    // ghost ids; aliased meshes keep the sequential order
+#pragma omp parallel for schedule(static) if (!h->aliased)
     for (int i = 1; i <= ntot; i++) {
         int t = map(i);
         hx[t] = xcel[i]; hy[t] = ycel[i]; hz[t] = zcel[i]; hvol[t] = vol[i]; hdd[t] = dd[i];
@@ -389,32 +427,7 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     h->device = dev;
     const size_t D = sizeof(double), I = sizeof(int), gb = h->var->grad_bytes;
     Arena& A = h->arena;
-    auto plan = [&](Arena& a) {
-        DevMesh& m = h->dm;
-        m.nc = (int*)a.take(4 * ld * I); m.snb = (int*)a.take(4 * ld * I);
-        m.fk = (unsigned*)a.take(ld * sizeof(unsigned)); m.iblank = (int*)a.take(ld * I);
-        m.xc = (double*)a.take(ld * D); m.yc = (double*)a.take(ld * D); m.zc = (double*)a.take(ld * D);
-        m.vol = (double*)a.take(ld * D); m.dl = (double*)a.take(ld * D); m.dd = (double*)a.take(ld * D);
-        m.sc = (double*)a.take(12 * ld * D); m.fch = (double*)a.take(12 * ld * D);
-        m.fcv = (double*)a.take(12 * ld * D);
-        m.lsqa = (double*)a.take(11 * ld * D);
-        m.lsqb = (double*)a.take(11 * ld * D);
-        m.g_par = (int*)a.take((nghosts + 1) * (size_t)I); m.g_id = (int*)a.take((nghosts + 1) * (size_t)I);
-        m.g_type = (int*)a.take((nghosts + 1) * (size_t)I);
-        DevState<double>& s = h->ds;
-        s.cn = (double*)a.take(10 * ld * D); s.cu = (double*)a.take(10 * ld * D);
-        s.cn1 = (double*)a.take(10 * ld * D); s.pr = (double*)a.take(NPR * ld * D);
-        s.gr = (double*)a.take(NGR * ld * gb); s.phi = (double*)a.take(ld * D);
-        s.anu = (double*)a.take(2 * ld * D); s.d2q = (double*)a.take(10 * ld * D);
-        s.d24 = (double*)a.take(10 * ld * D); s.vis = (double*)a.take(8 * ld * D);
-        s.egt = (double*)a.take(2 * ld * D);
-        s.s = (DevScalars*)a.take(sizeof(DevScalars));
-        s.diag = (double*)a.take((size_t)h->max_diag * 8 * D);
-        s.max_diag = h->max_diag;
-        h->d_perm = (int*)a.take((neles + 1) * (size_t)I);
-        h->d_gid = (int*)a.take((nghosts + 1) * (size_t)I);
-        h->d_gstage = (double*)a.take(6 * (nghosts + 1) * D);
-    };
+    auto plan = [&](Arena& a) { plan_arena(h, a, neles, nghosts, ld, gb); };
     Arena probe;
     plan(probe);
     A.size = probe.used + 256;
@@ -425,21 +438,24 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
         return fail(nullptr, HP_E_NOMEM, "case needs " + std::to_string(A.size >> 20) + " MiB, " +
                                              std::to_string(freeb >> 20) + " MiB free");
     }
-    if (cudaMalloc((void**)&A.base, A.size) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
-        return fail(nullptr, HP_E_NOMEM, "cudaMalloc of the case arena failed");
+        return fail(nullptr, HP_E_CUDA, "stream creation failed");
+    }
+    cudaStream_t st = h->stream;
+    // stream-ordered allocation: creating or destroying a case does not
+    // synchronise the device under the other cases' work
+    if (cudaMallocAsync((void**)&A.base, A.size, st) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(st);
+        delete h;
+        return fail(nullptr, HP_E_NOMEM, "allocation of the case arena failed");
     }
     A.used = 0;
     plan(A);
     DevMesh& m = h->dm;
     m.neles = neles; m.nghosts = nghosts; m.ntot = ntot; m.aliased = h->aliased; m.ld = ld;
     m.cell1 = perm[1];
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        cudaFree(A.base);
-        delete h;
-        return fail(nullptr, HP_E_CUDA, "stream creation failed");
-    }
-    cudaStream_t st = h->stream;
     auto up = [&](const void* dst, const void* src, size_t bytes) {
         return cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, st);
     };
@@ -469,7 +485,7 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
         s0.dtmin_bits = 0;
         double v = 1.0e8;
         std::memcpy(&s0.dtmin_bits, &v, 8);
-        e = cudaMemcpy(h->ds.s, &s0, sizeof s0, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(h->ds.s, &s0, sizeof s0, cudaMemcpyHostToDevice, st);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_diag, (size_t)h->max_diag * 8 * D);
@@ -488,7 +504,10 @@ extern "C" int hp_destroy(hp_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
-    if (h->arena.base) cudaFree(h->arena.base);
+    if (h->arena.base) {
+        cudaFreeAsync(h->arena.base, h->stream);
+        cudaStreamSynchronize(h->stream);
+    }
     if (h->h_diag) cudaFreeHost(h->h_diag);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -726,6 +745,26 @@ extern "C" int hp_profile_steps(hp_handle* h, int32_t nsteps, double* ms_per_kin
         launches_per_kind[kd] += 1;
     }
     for (auto e : ctx.ev) cudaEventDestroy(e);
+    return HP_OK;
+}
+
+extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, int64_t* bytes) {
+    if (!mesh || !params || !bytes || mesh->neles <= 0 || mesh->nghosts < 0) return HP_E_ARG;
+    hp_handle probe_h;
+    const long long ld = ((long long)mesh->neles + mesh->nghosts + 63) / 64 * 64;
+    const size_t gb = params->precision == HP_PREC_MIXED ? sizeof(float) : sizeof(double);
+    Arena probe;
+    plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb);
+    *bytes = (int64_t)(probe.used + 256);
+    return HP_OK;
+}
+
+extern "C" int hp_poll(hp_handle* h, int32_t* busy) {
+    if (!h || !busy) return HP_E_ARG;
+    cudaError_t e = cudaStreamQuery(h->stream);
+    if (e == cudaErrorNotReady) { *busy = 1; return HP_OK; }
+    *busy = 0;
+    CUDA_OK(h, e);
     return HP_OK;
 }
 

@@ -243,9 +243,16 @@ __global__ void __launch_bounds__(256) k_prim(DevMesh m, DevState<R> s, DevParam
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long kmin = ~0ull, kd[4] = {0, 0, 0, 0}, nanc = 0;
     if (i < m.neles) {
-        double c[10];
+        double c[10], u[10];
 #pragma unroll
         for (int k = 0; k < 10; k++) c[k] = COL(s.cn, k)[i];
+        // cu is read before any store of this thread: the compiler cannot
+        // prove cn, cu and the primitive columns disjoint, so a load after a
+        // store would wait for it
+        if (MODE == PM_END) {
+#pragma unroll
+            for (int k = 0; k < 10; k++) u[k] = COL(s.cu, k)[i];
+        }
         PrimV q;
         prim_full(c, q, P);
 #pragma unroll
@@ -263,9 +270,8 @@ __global__ void __launch_bounds__(256) k_prim(DevMesh m, DevState<R> s, DevParam
             bool bad = false;
 #pragma unroll
             for (int k = 0; k < 10; k++) {
-                double u = COL(s.cu, k)[i];
                 if (k < 4) {
-                    double d = fabs(c[k] - u);
+                    double d = fabs(c[k] - u[k]);
                     if (d == d) kd[k] = (unsigned long long)__double_as_longlong(d);
                 }
                 bad |= (c[k] != c[k]);
@@ -533,7 +539,7 @@ __global__ void __launch_bounds__(256) k_smooth1(DevMesh m, DevState<R> s) {
     const double e6 = (double)1.0e-6f;
     // the switch sums of variables 1, 5, 6, 10 (sw[0..3]) and the Laplacian
     // d2q of every variable, one variable at a time
-    double swn[4], swd[4];
+    double swn[4], swd[4], lap[10];
 #pragma unroll
     for (int k = 0; k < 10; k++) {
         const double* col = COL(s.cn, k);
@@ -543,7 +549,7 @@ __global__ void __launch_bounds__(256) k_smooth1(DevMesh m, DevState<R> s) {
             swn[slot] = fabs(v1 - v0) + fabs(v2 - v0) + fabs(v3 - v0) + fabs(v4 - v0);
             swd[slot] = fabs(v1 + v0) + fabs(v2 + v0) + fabs(v3 + v0) + fabs(v4 + v0);
         }
-        COL(s.d2q, k)[i] = v1 - v0 + v2 - v0 + v3 - v0 + v4 - v0;
+        lap[k] = v1 - v0 + v2 - v0 + v3 - v0 + v4 - v0;
     }
     double pgi = pg[i];
     double anun = fabs(pg[a] - pgi) + fabs(pg[b] - pgi) + fabs(pg[c] - pgi) + fabs(pg[d] - pgi);
@@ -557,6 +563,10 @@ __global__ void __launch_bounds__(256) k_smooth1(DevMesh m, DevState<R> s) {
     double anupp = anun / anud;
     double anu2 = anupp + swn[2] / (swd[2] + e6);
     anu2 = anu2 + swn[3] / (swd[3] + e6);
+    // all stores after all loads (the output columns may alias the inputs
+    // as far as the compiler can tell)
+#pragma unroll
+    for (int k = 0; k < 10; k++) COL(s.d2q, k)[i] = lap[k];
     COL(s.anu, 0)[i] = anu1;
     COL(s.anu, 1)[i] = anu2;
 }
@@ -572,7 +582,7 @@ __device__ __forceinline__ unsigned smooth2_body(const DevMesh& m, const DevStat
 #pragma unroll
     for (int f = 0; f < 4; f++) nb[f] = ldg(COL(m.snb, f) + i);
     const double vi = mdiv<F>(ldg(m.vol + i), dt, rdt, bad);
-    double d24nc[4];
+    double d24nc[4], out[10];
 #pragma unroll
     for (int f = 0; f < 4; f++) d24nc[f] = 0.5 * (vi + mdiv<F>(ldg(m.vol + nb[f]), dt, rdt, bad));
 #pragma unroll
@@ -596,9 +606,12 @@ __device__ __forceinline__ unsigned smooth2_body(const DevMesh& m, const DevStat
                         d2c[2] * (cn[nb[2]] - ci) + d2c[3] * (cn[nb[3]] - ci);
             double d4 = d4c[0] * (dq[nb[0]] - qi) + d4c[1] * (dq[nb[1]] - qi) +
                         d4c[2] * (dq[nb[2]] - qi) + d4c[3] * (dq[nb[3]] - qi);
-            COL(s.d24, k)[i] = d2 - d4;
+            out[k] = d2 - d4;
         }
     }
+    // all stores after all loads (see k_smooth1)
+#pragma unroll
+    for (int k = 0; k < 10; k++) COL(s.d24, k)[i] = out[k];
     return bad;
 }
 

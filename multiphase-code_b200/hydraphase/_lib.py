@@ -81,6 +81,8 @@ def lib():
     L.hp_device_state.argtypes = [vp, ctypes.POINTER(_DP), ctypes.POINTER(ctypes.c_int64)]
     L.hp_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                           ctypes.POINTER(ctypes.c_int64)]
+    L.hp_estimate_bytes.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(HpParams), ctypes.POINTER(ctypes.c_int64)]
+    L.hp_poll.argtypes = [vp, ctypes.POINTER(_I)]
     L.hp_dt_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _I,
                                 ctypes.POINTER(HpParams), ctypes.c_void_p, ctypes.c_void_p]
     L.hp_read_flow.argtypes = [ctypes.c_char_p, ctypes.POINTER(HpParams)]
@@ -89,7 +91,7 @@ def lib():
     L.hp_read_restart.argtypes = [ctypes.c_char_p, _I, _I, _DP, _DP, _DP]
     L.hp_write_restart.argtypes = [ctypes.c_char_p, _I, _I, _D, _DP, _DP]
     for fn in ("hp_create", "hp_destroy", "hp_init_uniform", "hp_set_state", "hp_step", "hp_sync",
-               "hp_step_timed", "hp_profile_steps", "hp_dt_noalloc",
+               "hp_step_timed", "hp_profile_steps", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll",
                "hp_get_state", "hp_get_prims", "hp_device_state", "hp_info", "hp_read_flow",
                "hp_read_mesh", "hp_read_restart", "hp_write_restart"):
         getattr(L, fn).restype = ctypes.c_int
@@ -104,6 +106,6 @@ EXPORTED_SYMBOLS = (
     "hp_create", "hp_destroy", "hp_last_error", "hp_create_error", "hp_init_uniform",
     "hp_set_state", "hp_step", "hp_sync", "hp_step_timed", "hp_profile_steps", "hp_get_state", "hp_get_prims", "hp_device_state",
     "hp_info", "hp_read_flow", "hp_read_mesh", "hp_free_mesh", "hp_read_restart",
-    "hp_write_restart", "hp_dt_noalloc",
+    "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll",
 )
 NOALLOC_MAX_CELLS = 1 << 24

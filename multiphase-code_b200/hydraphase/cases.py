@@ -239,6 +239,16 @@ def shock_bubble(n=20, jitter=0.1, seed=0, radius=0.2, p_post=1.0e9, rho_post=12
     elsewhere.  The post-shock water moves with the Rankine-Hugoniot velocity
     of that jump unless post_velocity is given."""
     b = box_mesh(n, n, n, jitter=jitter, seed=seed, bc_type=5)
+    return shock_bubble_on(b, radius=radius, p_post=p_post, rho_post=rho_post, center=center, shock_x=shock_x,
+                           pinf=pinf, gamap=gamap, cpp=cpp, post_velocity=post_velocity,
+                           reference_scheme=reference_scheme, alpha_min=alpha_min)
+
+
+def shock_bubble_on(b: Built, radius=0.2, p_post=1.0e9, rho_post=1230.0, center=(0.5, 0.5, 0.5), shock_x=0.2,
+                    pinf=6.0e8, gamap=4.4, cpp=4186.0, post_velocity=None, reference_scheme=False,
+                    alpha_min=1e-6) -> CaseSpec:
+    """The shock-bubble state of shock_bubble() on an already built unit-box
+    mesh (several cases may share one mesh)."""
     gamag = 1.4
     p0, rho0 = 1.0e5, 1000.0
     if post_velocity is None:
@@ -365,3 +375,43 @@ def write_case_dir(spec: CaseSpec, path: str) -> None:
     with open(os.path.join(path, "geometry_files", "proc_bc0000.in"), "w") as f:
         f.write("           0           0\n")
     write_restart(os.path.join(path, "restart_files", "restart0000.in"), 0.0, spec.cu, spec.ghost_prims)
+
+
+@dataclass
+class StreamCase:
+    """One request of a serving stream: arrival time (s from the stream's
+    start), number of steps, and the case itself."""
+    rid: int
+    arrival: float
+    steps: int
+    spec: CaseSpec
+
+
+def serving_stream(n_cases=256, rate=40.0, steps=500, cells=(6000, 400000), seed=2, alpha_min=0.1,
+                   jitter=0.1, cfl=0.1):
+    """A stream of shock-bubble cases: mesh sizes log-uniform in `cells`
+    (box grids of n^3 hexes split into 6 tets, n = round((cells/6)^(1/3)),
+    jittered by +-jitter*h), bubble radius U[0.1, 0.3], post-shock water
+    pressure log-U[1e8, 2e9] Pa, Poisson arrivals at `rate` per second, all
+    drawn from `seed`.  Cases of the same n share one mesh (its generation is
+    the client's cost, not the server's); each carries its own state.  The
+    explicit scheme keeps these cases finite over 500 SSP-RK3 steps at CFL
+    0.1 with an air volume fraction of 1 - alpha_min / alpha_min (at CFL 0.4
+    they blow up within 25-100 steps, at alpha_min = 1e-6 at any CFL)."""
+    rng = np.random.default_rng(seed)
+    target = np.exp(rng.uniform(np.log(cells[0]), np.log(cells[1]), n_cases))
+    nside = np.maximum(np.rint(np.cbrt(target / 6.0)).astype(int), 2)
+    radius = rng.uniform(0.1, 0.3, n_cases)
+    p_post = np.exp(rng.uniform(np.log(1.0e8), np.log(2.0e9), n_cases))
+    gaps = rng.exponential(1.0 / rate, n_cases)
+    arrival = np.cumsum(gaps) - gaps[0]
+    meshes = {}
+    out = []
+    for k in range(n_cases):
+        n = int(nside[k])
+        if n not in meshes:
+            meshes[n] = box_mesh(n, n, n, jitter=jitter, seed=1000 * seed + n, bc_type=5)
+        spec = shock_bubble_on(meshes[n], radius=float(radius[k]), p_post=float(p_post[k]), alpha_min=alpha_min)
+        spec.flow["cfl"] = cfl
+        out.append(StreamCase(k, float(arrival[k]), int(steps), spec))
+    return out

@@ -78,6 +78,14 @@ class MeshArrays:
         return int(self.ghost.shape[0])
 
 
+def estimate_bytes(mesh: MeshArrays, params: HpParams) -> int:
+    """Device bytes a Case of this mesh and precision would hold."""
+    hm = HpMesh(mesh.nodes, mesh.neles, mesh.nghosts, 0, None, None, None, None, None)
+    b = ctypes.c_int64()
+    _check(lib().hp_estimate_bytes(ctypes.byref(hm), ctypes.byref(params), ctypes.byref(b)))
+    return int(b.value)
+
+
 class Case:
     """One mesh + solution resident on the current CUDA device."""
 
@@ -136,6 +144,12 @@ class Case:
 
     def sync(self):
         _check(self.L.hp_sync(self.h), self.h)
+
+    def poll(self) -> bool:
+        """True while steps queued on this case's stream are still running."""
+        busy = ctypes.c_int32()
+        _check(self.L.hp_poll(self.h, ctypes.byref(busy)), self.h)
+        return bool(busy.value)
 
     def step_timed(self, nsteps: int) -> float:
         """Run nsteps; device milliseconds from CUDA events on the case's stream."""
