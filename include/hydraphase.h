@@ -102,6 +102,15 @@ typedef struct hp_handle hp_handle;
  * src/sr_geometry.F90:147-347 (bit-identical to the reference), builds the
  * device layout, and allocates all device memory on the current device. */
 int hp_create(const hp_mesh *mesh, const hp_params *params, hp_handle **out);
+/* A batch: ncase meshes (same parameters) in one handle.  No counterpart in
+ * the reference.  Their cell and ghost lists are concatenated on the device,
+ * so every kernel of a step sweeps all cases in one launch; each case keeps
+ * its own dt, time, residuals and diagnostics, and its results are those
+ * it would have alone.  Meshes whose ghost ids alias element ids
+ * (HP_E_UNSUPPORTED) and partition ghosts cannot be batched.  hp_create is
+ * hp_create_batch with ncase = 1. */
+int hp_create_batch(const hp_mesh *meshes, int32_t ncase, const hp_params *params, hp_handle **out);
+int hp_case_count(const hp_handle *h, int32_t *ncase);
 int hp_destroy(hp_handle *h);
 const char *hp_last_error(const hp_handle *h);
 /* Message of the last failed hp_create (no handle exists then). */
@@ -114,8 +123,13 @@ int hp_init_uniform(hp_handle *h);
  * ids in ghost-list order (6 x nghosts).  Host pointers. */
 int hp_set_state(hp_handle *h, double time, const double *cu_elem,
                  const double *ghost_prims);
+/* The same for case c of a batch (hp_set_state is case 0).  Every case of a
+ * batch is set before its first step (HP_E_STATE afterwards). */
+int hp_set_state_case(hp_handle *h, int32_t c, double time, const double *cu_elem,
+                      const double *ghost_prims);
 
-/* nsteps of src/main.F90:515-654.  diag may be NULL or hold nsteps entries.
+/* nsteps of src/main.F90:515-654 for every case of the handle.  diag may be
+ * NULL or hold ncase * nsteps entries (case c's steps at c * nsteps).
  * Asynchronous with respect to the host unless diag != NULL. */
 int hp_step(hp_handle *h, int32_t nsteps, hp_diag *diag);
 /* Blocks until the handle's stream is idle. */
@@ -133,8 +147,10 @@ int hp_profile_steps(hp_handle *h, int32_t nsteps, double *ms_per_kind,
 /* State read-back in the restart layout (src/main.F90:817-824). */
 int hp_get_state(hp_handle *h, double *time, double *cu_elem,
                  double *ghost_prims);
+int hp_get_state_case(hp_handle *h, int32_t c, double *time, double *cu_elem,
+                      double *ghost_prims);
 /* Cell primitives after the last step (ug,vg,wg,tg,pg,pp,phig,phip,up,vp,wp,
- * tp,rog,rop; 14 x neles, reference cell order). */
+ * tp,rog,rop; 14 x neles, reference cell order) of case 0. */
 int hp_get_prims(hp_handle *h, double *prims);
 
 /* --- device-resident access (for callers that keep data in HBM) --------- */
@@ -151,6 +167,8 @@ int hp_info(const hp_handle *h, int64_t *kernels_per_step, int64_t *device_bytes
  * bytes hp_create would allocate for this mesh and precision (admission
  * against an HBM budget before creating). */
 int hp_estimate_bytes(const hp_mesh *mesh, const hp_params *params, int64_t *bytes);
+int hp_estimate_batch_bytes(const hp_mesh *meshes, int32_t ncase, const hp_params *params,
+                            int64_t *bytes);
 /* *busy = 1 while steps queued on the handle's stream are still running,
  * 0 once they are done; never blocks.  Lets one host thread drive many
  * handles whose streams overlap on the device. */

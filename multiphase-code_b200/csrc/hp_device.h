@@ -38,10 +38,16 @@ struct DevParams {
     int rk_scheme, inviscid, myorder, nstage;
 };
 
+// A handle holds one case or a batch of cases whose meshes are concatenated:
+// the elements of case c occupy [elem_base_c, elem_base_c + neles_c) and its
+// ghosts a range of [neles, neles + nghosts); neighbour ids point into the
+// same case only, so every kernel sweeps all cases in one launch.  `cid`
+// maps an element to its case (null for a single case: case 0).
 struct DevMesh {
     int neles, nghosts, ntot, aliased;
     long long ld;
-    int cell1;              // internal id of the reference's cell 1
+    int ncase;
+    const int* cid;         // [neles] case of each element, or null
     const int* nc;          // [4][ld] face neighbours
     const int* snb;         // [4][ld] neighbours as smoothing sees them
     const unsigned* fk;     // [ld] face kind nibbles
@@ -60,6 +66,7 @@ struct DevMesh {
     const int *g_par, *g_id, *g_type;   // [nghosts] ghost list (reference order)
 };
 
+// Per-case scalars (one entry per case of the handle).
 struct DevScalars {
     unsigned long long dtmin_bits;    // running min of dl/(a+|u|), skips NaN
     unsigned long long diff_bits[4];  // running max |cn - cu|, skips NaN
@@ -69,6 +76,7 @@ struct DevScalars {
     int step_in_call;
     double fcarry[10];                // stale-flux carry (aliased meshes)
     int err_flags;
+    int cell1;                        // internal id of the case's cell 1
 };
 
 template <class R>

@@ -50,6 +50,14 @@ const int VIS_FACE[4][3] = {{2, 3, 4}, {1, 3, 4}, {1, 2, 4}, {1, 2, 3}};
 
 }  // namespace
 
+// Element and ghost ranges of one case of a handle (see DevMesh).
+struct CaseRange {
+    int e0 = 0, ne = 0;     // elements [e0, e0 + ne)
+    int g0 = 0, ng = 0;     // ghost list entries [g0, g0 + ng), slots neles + g0 ...
+    int cell1 = 0;          // slot of the case's reference cell 1
+    int aliased = 0;
+};
+
 struct hp_handle {
     hp_params prm{};
     DevParams dp{};
@@ -63,12 +71,15 @@ struct hp_handle {
     int device = 0;
     int neles = 0, nghosts = 0, ntot = 0;
     long long ld = 0;
-    std::vector<int> perm;      // reference element (0-based) -> internal id
-    std::vector<int> ghost_id;  // ghost-list position -> internal slot id
+    int ncase = 1;
+    std::vector<CaseRange> cases;
+    std::vector<int> perm;      // [neles] case c's reference element i -> slot, at cases[c].e0 + i
+    std::vector<int> ghost_id;  // [nghosts] case c's ghost g -> slot, at cases[c].g0 + g
     int* d_perm = nullptr;      // the two maps above, on the device
     int* d_gid = nullptr;
     double* d_gstage = nullptr; // 6 x nghosts staging of ghost primitives
     bool started = false, have_state = false;
+    std::vector<char> state_set;   // per case: state uploaded
     int aliased = 0;
     int max_diag = 4096;
     std::string err;
@@ -106,7 +117,7 @@ extern "C" const char* hp_last_error(const hp_handle* h) { return h ? h->err.c_s
 
 // Carves every device array of a handle out of one arena (a probe arena
 // with no base only measures).  The same plan sizes hp_estimate_bytes.
-static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long ld, size_t gb) {
+static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long ld, size_t gb, int ncase) {
     const size_t D = sizeof(double), I = sizeof(int);
     DevMesh& m = h->dm;
     m.nc = (int*)a.take(4 * ld * I); m.snb = (int*)a.take(4 * ld * I);
@@ -126,48 +137,58 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     s.anu = (double*)a.take(2 * ld * D); s.d2q = (double*)a.take(10 * ld * D);
     s.d24 = (double*)a.take(10 * ld * D); s.vis = (double*)a.take(8 * ld * D);
     s.egt = (double*)a.take(2 * ld * D);
-    s.s = (DevScalars*)a.take(sizeof(DevScalars));
-    s.diag = (double*)a.take((size_t)h->max_diag * 8 * D);
+    s.s = (DevScalars*)a.take(ncase * sizeof(DevScalars));
+    s.diag = (double*)a.take((size_t)ncase * h->max_diag * 8 * D);
     s.max_diag = h->max_diag;
+    m.cid = ncase > 1 ? (const int*)a.take((size_t)neles * I) : nullptr;
     h->d_perm = (int*)a.take((neles + 1) * (size_t)I);
     h->d_gid = (int*)a.take((nghosts + 1) * (size_t)I);
     h->d_gstage = (double*)a.take(6 * (nghosts + 1) * D);
 }
 
-extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle** out) {
-    g_create_error.clear();
-    if (!mesh || !params || !out) return fail(nullptr, HP_E_ARG, "null argument");
-    *out = nullptr;
+// Host staging of a handle's device layout (columns of leading dimension ld)
+// and ghost lists, filled case by case by fill_case.
+struct Layout {
+    int neles = 0, nghosts = 0;
+    long long ld = 0;
+    std::vector<int> nc, snb, ib, gpar, gid, gtyp, perm, ghost_id;
+    std::vector<unsigned> fk;
+    std::vector<double> x, y, z, vol, dl, dd, sc, fch, fcv, la, lb;
+    Layout(int ne, int ng) : neles(ne), nghosts(ng), ld(((long long)ne + ng + 63) / 64 * 64) {
+        nc.assign(4 * ld, 0); snb.assign(4 * ld, 0); ib.assign(ld, 0); fk.assign(ld, 0u);
+        gpar.assign(ng, 0); gid.assign(ng, 0); gtyp.assign(ng, 0); perm.assign(ne, 0); ghost_id.assign(ng, 0);
+        for (auto* v : {&x, &y, &z, &vol, &dl, &dd}) v->assign(ld, 0.0);
+        for (auto* v : {&sc, &fch, &fcv}) v->assign(12 * ld, 0.0);
+        la.assign(11 * ld, 0.0); lb.assign(11 * ld, 0.0);
+    }
+};
+
+// One case of a handle: validates its connectivity, computes its geometry
+// and static least-squares terms, picks its internal cell order and writes
+// everything into the handle's staging layout at the case's offsets
+// (elements from cr.e0, ghosts from L.neles + cr.g0).  On error returns an
+// HP_E_* code with the message in err.
+static int fill_case(const hp_mesh* mesh, const hp_params* params, Layout& L, CaseRange& cr, std::string& err) {
     const int nodes = mesh->nodes, neles = mesh->neles, nghosts = mesh->nghosts;
-    if (mesh->pghosts != 0)
-        return fail(nullptr, HP_E_UNSUPPORTED, "partition ghosts: one partition per GPU only");
-    if (nodes <= 0 || neles <= 0 || nghosts < 0 || !mesh->x || !mesh->y || !mesh->z || !mesh->elem ||
-        (nghosts > 0 && !mesh->ghost))
-        return fail(nullptr, HP_E_ARG, "empty or incomplete mesh");
-    if (params->myflux != 2)
-        return fail(nullptr, HP_E_UNSUPPORTED, "myflux must be 2 (HLLC-Batten)");
-    if (params->myorder != 1 && params->myorder != 2)
-        return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
     const int ntot = neles + nghosts;
+    const int E0 = cr.e0, G0 = cr.g0, Etot = L.neles;
+    const long long ld = L.ld;
+    auto bad = [&](int code, const std::string& m) { err = m; return code; };
     // --- validate connectivity (1-based as read) ---
     for (long long e = 0; e < neles; e++) {
         const int32_t* r = mesh->elem + 9 * e;
         for (int k = 0; k < 4; k++)
             if (r[k] < 1 || r[k] > nodes)
-                return fail(nullptr, HP_E_ARG, "element " + std::to_string(e + 1) + ": node id out of range");
+                return bad(HP_E_ARG, "element " + std::to_string(e + 1) + ": node id out of range");
         for (int k = 4; k < 8; k++)
             if (r[k] < 1 || r[k] > ntot)
-                return fail(nullptr, HP_E_ARG, "element " + std::to_string(e + 1) + ": neighbour id out of range");
+                return bad(HP_E_ARG, "element " + std::to_string(e + 1) + ": neighbour id out of range");
     }
     for (long long g = 0; g < nghosts; g++) {
         const int32_t* r = mesh->ghost + 4 * g;
         if (r[0] < 1 || r[0] > ntot || r[1] < 1 || r[1] > ntot || r[3] < 1 || r[3] > 4)
-            return fail(nullptr, HP_E_ARG, "ghost " + std::to_string(g + 1) + ": bad parent/id/side");
+            return bad(HP_E_ARG, "ghost " + std::to_string(g + 1) + ": bad parent/id/side");
     }
-
-    auto* h = new hp_handle();
-    h->prm = *params;
-    h->neles = neles; h->nghosts = nghosts; h->ntot = ntot;
 
     // --- geometry, src/sr_geometry.F90:112-347 (1-based work arrays) ---
     std::vector<double> x(nodes + 1), y(nodes + 1), z(nodes + 1);
@@ -319,12 +340,12 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
         for (int e = 1; e <= neles && !al; e++)
             for (int k = 0; k < 4; k++)
                 if (nc[k][e] > neles && !seen[nc[k][e]]) { al = 1; break; }
-        h->aliased = al;
+        cr.aliased = al;
     }
     // --- internal order: space-filling curve over element centroids ---
     std::vector<int> perm(neles + 1);   // 1-based reference id -> 0-based internal
     std::iota(perm.begin(), perm.end(), -1);
-    if (params->renumber && !h->aliased) {
+    if (params->renumber && !cr.aliased) {
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
         for (int i = 1; i <= neles; i++) {
             double p[3] = {xcel[i], ycel[i], zcel[i]};
@@ -344,25 +365,27 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
         std::stable_sort(key.begin(), key.end());
         for (int r = 0; r < neles; r++) perm[key[r].second] = r;
     }
-    auto map = [&](int id1) -> int { return id1 <= neles ? perm[id1] : id1 - 1; };
-    h->perm.assign(neles, 0);
-    for (int i = 1; i <= neles; i++) h->perm[i - 1] = perm[i];
-    h->ghost_id.resize(nghosts);
-    for (int g = 0; g < nghosts; g++) h->ghost_id[g] = map(gid[g]);
+    // reference id (1-based, this case) -> slot of the handle: elements
+    // after the earlier cases' elements, ghosts after all elements and the
+    // earlier cases' ghosts (a single case keeps ghost g at neles + g; the
+    // aliased ids of a merged mesh are element ids and map as such)
+    auto map = [&](int id1) -> int { return id1 <= neles ? E0 + perm[id1] : Etot + G0 + (id1 - neles - 1); };
+    for (int i = 1; i <= neles; i++) L.perm[E0 + i - 1] = E0 + perm[i];
+    for (int g = 0; g < nghosts; g++) L.ghost_id[G0 + g] = map(gid[g]);
+    cr.cell1 = E0 + perm[1];
 
     // --- device layout ---
-    const long long ld = ((long long)ntot + 63) / 64 * 64;
-    h->ld = ld;
-    std::vector<int> hnc(4 * ld, 0), hsnb(4 * ld, 0), hib(ld, 0), hgpar(nghosts), hgid(nghosts), hgtyp(nghosts);
-    std::vector<unsigned> hfk(ld, 0u);
-    std::vector<double> hx(ld, 0.0), hy(ld, 0.0), hz(ld, 0.0), hvol(ld, 0.0), hdl(ld, 0.0), hdd(ld, 0.0);
-    std::vector<double> hsc(12 * ld, 0.0), hfch(12 * ld, 0.0), hfcv(12 * ld, 0.0);
-    std::vector<double> hla(11 * ld, 0.0), hlb(11 * ld, 0.0);
+    std::vector<int>& hnc = L.nc; std::vector<int>& hsnb = L.snb; std::vector<int>& hib = L.ib;
+    std::vector<unsigned>& hfk = L.fk;
+    std::vector<double>& hx = L.x; std::vector<double>& hy = L.y; std::vector<double>& hz = L.z;
+    std::vector<double>& hvol = L.vol; std::vector<double>& hdl = L.dl; std::vector<double>& hdd = L.dd;
+    std::vector<double>& hsc = L.sc; std::vector<double>& hfch = L.fch; std::vector<double>& hfcv = L.fcv;
+    std::vector<double>& hla = L.la; std::vector<double>& hlb = L.lb;
     std::vector<int> slot_parent(ntot + 1, 0);
     for (int g = 0; g < nghosts; g++) slot_parent[gid[g]] = gpar[g];
     // slots t = map(i) are distinct for distinct i on meshes without aliased
     // ghost ids; aliased meshes keep the sequential order
-#pragma omp parallel for schedule(static) if (!h->aliased)
+#pragma omp parallel for schedule(static) if (!cr.aliased)
     for (int i = 1; i <= ntot; i++) {
         int t = map(i);
         hx[t] = xcel[i]; hy[t] = ycel[i]; hz[t] = zcel[i]; hvol[t] = vol[i]; hdd[t] = dd[i];
@@ -374,8 +397,8 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
                 int nb = nc[k][i];
                 hnc[k * ld + t] = map(nb);
                 int snb = nb;
-                if (!h->aliased && nb > neles) snb = slot_parent[nb];
-                hsnb[k * ld + t] = h->aliased ? map(nb) : map(snb);
+                if (!cr.aliased && nb > neles) snb = slot_parent[nb];
+                hsnb[k * ld + t] = cr.aliased ? map(nb) : map(snb);
                 int nt = 0;
                 if (nb > neles && nb <= neles + nghosts) nt = gtyp[nb - neles - 1];
                 unsigned kind = 0;
@@ -392,10 +415,66 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
             for (int k = 0; k < 4; k++) { hnc[k * ld + t] = map(nc[k][i]); hsnb[k * ld + t] = map(nc[k][i]); }
         }
     }
-    for (int g = 0; g < nghosts; g++) { hgpar[g] = map(gpar[g]); hgid[g] = map(gid[g]); hgtyp[g] = gtyp[g]; }
+    for (int g = 0; g < nghosts; g++) {
+        L.gpar[G0 + g] = map(gpar[g]); L.gid[G0 + g] = map(gid[g]); L.gtyp[G0 + g] = gtyp[g];
+    }
+    return HP_OK;
+}
+
+
+extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_params* params, hp_handle** out) {
+    g_create_error.clear();
+    if (!meshes || !params || !out || ncase < 1) return fail(nullptr, HP_E_ARG, "null argument or no case");
+    *out = nullptr;
+    if (params->myflux != 2)
+        return fail(nullptr, HP_E_UNSUPPORTED, "myflux must be 2 (HLLC-Batten)");
+    if (params->myorder != 1 && params->myorder != 2)
+        return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
+    long long etot = 0, gtot = 0;
+    for (int c = 0; c < ncase; c++) {
+        const hp_mesh* mesh = meshes + c;
+        const std::string tag = ncase > 1 ? "case " + std::to_string(c) + ": " : "";
+        if (mesh->pghosts != 0)
+            return fail(nullptr, HP_E_UNSUPPORTED, tag + "partition ghosts: one partition per GPU only");
+        if (mesh->nodes <= 0 || mesh->neles <= 0 || mesh->nghosts < 0 || !mesh->x || !mesh->y || !mesh->z ||
+            !mesh->elem || (mesh->nghosts > 0 && !mesh->ghost))
+            return fail(nullptr, HP_E_ARG, tag + "empty or incomplete mesh");
+        etot += mesh->neles;
+        gtot += mesh->nghosts;
+    }
+    if (etot + gtot > 2000000000LL) return fail(nullptr, HP_E_ARG, "more than 2e9 cells in one handle");
+    auto* h = new hp_handle();
+    h->prm = *params;
+    h->ncase = ncase;
+    Layout L((int)etot, (int)gtot);
+    int e0 = 0, g0 = 0;
+    for (int c = 0; c < ncase; c++) {
+        CaseRange cr;
+        cr.e0 = e0; cr.ne = meshes[c].neles; cr.g0 = g0; cr.ng = meshes[c].nghosts;
+        std::string err;
+        int rc = fill_case(meshes + c, params, L, cr, err);
+        if (rc != HP_OK) {
+            delete h;
+            return fail(nullptr, rc, (ncase > 1 ? "case " + std::to_string(c) + ": " : "") + err);
+        }
+        if (cr.aliased && ncase > 1) {
+            delete h;
+            return fail(nullptr, HP_E_UNSUPPORTED, "case " + std::to_string(c) +
+                                                       ": aliased ghost ids cannot share a batch");
+        }
+        h->cases.push_back(cr);
+        e0 += cr.ne;
+        g0 += cr.ng;
+    }
+    h->aliased = h->cases[0].aliased;
+    h->neles = L.neles; h->nghosts = L.nghosts; h->ntot = L.neles + L.nghosts; h->ld = L.ld;
+    h->perm = std::move(L.perm);
+    h->ghost_id = std::move(L.ghost_id);
 
     // --- parameters ---
     const hp_params& p = h->prm;
+    const int neles = L.neles, nghosts = L.nghosts, ntot = neles + nghosts;
+    const long long ld = L.ld;
     DevParams& P = h->dp;
     P.gamag = p.gamag; P.gamap = p.gamap; P.pinf = p.pinf; P.cpp = p.cpp; P.cpg = p.cpg; P.prg = p.prg;
     P.rrg = 287.0; P.prp = 10.0;
@@ -427,7 +506,7 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     h->device = dev;
     const size_t D = sizeof(double), I = sizeof(int), gb = h->var->grad_bytes;
     Arena& A = h->arena;
-    auto plan = [&](Arena& a) { plan_arena(h, a, neles, nghosts, ld, gb); };
+    auto plan = [&](Arena& a) { plan_arena(h, a, neles, nghosts, ld, gb, ncase); };
     Arena probe;
     plan(probe);
     A.size = probe.used + 256;
@@ -455,41 +534,50 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     plan(A);
     DevMesh& m = h->dm;
     m.neles = neles; m.nghosts = nghosts; m.ntot = ntot; m.aliased = h->aliased; m.ld = ld;
-    m.cell1 = perm[1];
+    m.ncase = ncase;
+    if (ncase == 1) m.cid = nullptr;
     auto up = [&](const void* dst, const void* src, size_t bytes) {
         return cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, st);
     };
     cudaError_t e = cudaMemsetAsync(A.base, 0, A.size, st);
-    if (e == cudaSuccess) e = up(m.nc, hnc.data(), 4 * ld * I);
-    if (e == cudaSuccess) e = up(m.snb, hsnb.data(), 4 * ld * I);
-    if (e == cudaSuccess) e = up(m.fk, hfk.data(), ld * sizeof(unsigned));
-    if (e == cudaSuccess) e = up(m.iblank, hib.data(), ld * I);
-    if (e == cudaSuccess) e = up(m.xc, hx.data(), ld * D);
-    if (e == cudaSuccess) e = up(m.yc, hy.data(), ld * D);
-    if (e == cudaSuccess) e = up(m.zc, hz.data(), ld * D);
-    if (e == cudaSuccess) e = up(m.vol, hvol.data(), ld * D);
-    if (e == cudaSuccess) e = up(m.dl, hdl.data(), ld * D);
-    if (e == cudaSuccess) e = up(m.dd, hdd.data(), ld * D);
-    if (e == cudaSuccess) e = up(m.sc, hsc.data(), 12 * ld * D);
-    if (e == cudaSuccess) e = up(m.fch, hfch.data(), 12 * ld * D);
-    if (e == cudaSuccess) e = up(m.fcv, hfcv.data(), 12 * ld * D);
-    if (e == cudaSuccess) e = up(m.lsqa, hla.data(), 11 * ld * D);
-    if (e == cudaSuccess) e = up(m.lsqb, hlb.data(), 11 * ld * D);
-    if (e == cudaSuccess && nghosts) e = up(m.g_par, hgpar.data(), nghosts * (size_t)I);
-    if (e == cudaSuccess && nghosts) e = up(m.g_id, hgid.data(), nghosts * (size_t)I);
-    if (e == cudaSuccess && nghosts) e = up(m.g_type, hgtyp.data(), nghosts * (size_t)I);
+    if (e == cudaSuccess) e = up(m.nc, L.nc.data(), 4 * ld * I);
+    if (e == cudaSuccess) e = up(m.snb, L.snb.data(), 4 * ld * I);
+    if (e == cudaSuccess) e = up(m.fk, L.fk.data(), ld * sizeof(unsigned));
+    if (e == cudaSuccess) e = up(m.iblank, L.ib.data(), ld * I);
+    if (e == cudaSuccess) e = up(m.xc, L.x.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.yc, L.y.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.zc, L.z.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.vol, L.vol.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.dl, L.dl.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.dd, L.dd.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.sc, L.sc.data(), 12 * ld * D);
+    if (e == cudaSuccess) e = up(m.fch, L.fch.data(), 12 * ld * D);
+    if (e == cudaSuccess) e = up(m.fcv, L.fcv.data(), 12 * ld * D);
+    if (e == cudaSuccess) e = up(m.lsqa, L.la.data(), 11 * ld * D);
+    if (e == cudaSuccess) e = up(m.lsqb, L.lb.data(), 11 * ld * D);
+    if (e == cudaSuccess && nghosts) e = up(m.g_par, L.gpar.data(), nghosts * (size_t)I);
+    if (e == cudaSuccess && nghosts) e = up(m.g_id, L.gid.data(), nghosts * (size_t)I);
+    if (e == cudaSuccess && nghosts) e = up(m.g_type, L.gtyp.data(), nghosts * (size_t)I);
     if (e == cudaSuccess) e = up(h->d_perm, h->perm.data(), neles * (size_t)I);
     if (e == cudaSuccess && nghosts) e = up(h->d_gid, h->ghost_id.data(), nghosts * (size_t)I);
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && ncase > 1) {
+        std::vector<int> cid(neles);
+        for (int c = 0; c < ncase; c++)
+            for (int i = 0; i < h->cases[c].ne; i++) cid[h->cases[c].e0 + i] = c;
+        e = up(m.cid, cid.data(), neles * (size_t)I);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // cid is a local vector
+    }
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_diag, (size_t)h->max_diag * 8 * D * ncase);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_scal, sizeof(DevScalars));
+    for (int c = 0; c < ncase && e == cudaSuccess; c++) {
         DevScalars s0{};
-        s0.dtmin_bits = 0;
         double v = 1.0e8;
         std::memcpy(&s0.dtmin_bits, &v, 8);
-        e = cudaMemcpyAsync(h->ds.s, &s0, sizeof s0, cudaMemcpyHostToDevice, st);
+        s0.cell1 = h->cases[c].cell1;
+        *h->h_scal = s0;
+        e = cudaMemcpyAsync(h->ds.s + c, h->h_scal, sizeof s0, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_diag, (size_t)h->max_diag * 8 * D);
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_scal, sizeof(DevScalars));
     if (e != cudaSuccess) {
         std::string msg = std::string("device upload failed: ") + cudaGetErrorString(e);
         hp_destroy(h);
@@ -497,6 +585,11 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     }
     *out = h;
     return HP_OK;
+}
+
+
+extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle** out) {
+    return hp_create_batch(mesh, 1, params, out);
 }
 
 extern "C" int hp_destroy(hp_handle* h) {
@@ -564,42 +657,74 @@ __global__ void k_gather_ghost_prims(const double* __restrict__ pr, long long ld
     int v = (int)(t / ng), g = (int)(t - (long long)v * ng);
     dst[(size_t)v * ng + g] = pr[(size_t)cols.c[v] * ld + gid[g]];
 }
+// p[k*ld + start + i] = v and dst[k*ld + start + i] = src[k*ld + start + i],
+// k < ncol, i < count (one case's element or ghost range)
+__global__ void k_fill_cols(double* __restrict__ p, long long ld, int ncol, int start, int count, double v) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)count * ncol) return;
+    int k = (int)(t / count), i = (int)(t - (long long)k * count);
+    p[(size_t)k * ld + start + i] = v;
+}
+__global__ void k_copy_cols(double* __restrict__ dst, const double* __restrict__ src, long long ld, int ncol, int start,
+                            int count) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)count * ncol) return;
+    int k = (int)(t / count), i = (int)(t - (long long)k * count);
+    dst[(size_t)k * ld + start + i] = src[(size_t)k * ld + start + i];
+}
 inline unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 const Cols6 GHOST_COLS = {{P_UG, P_VG, P_WG, P_PG, P_TG, P_ROG}};
 }  // namespace
 
-static int upload_state(hp_handle* h, double time, const double* cu_elem, const double* ghost_prims) {
+// One case's state: its element slots get the caller's cu in internal order,
+// its ghost slots zero; cn = cu on both ranges; its primitive slots zero
+// except the restart's ghost values; its scalars restart at `time`.
+static int upload_state(hp_handle* h, int c, double time, const double* cu_elem, const double* ghost_prims) {
+    const CaseRange& cr = h->cases[c];
     const long long ld = h->ld;
-    const int ne = h->neles, ng = h->nghosts;
+    const int ne = cr.ne, ng = cr.ng, gs = h->neles + cr.g0;
     cudaStream_t st = h->stream;
     CUDA_OK(h, cudaStreamSynchronize(st));
-    // conserved state: ghost slots zero, elements scattered to internal order
     CUDA_OK(h, cudaMemcpyAsync(h->ds.cn1, cu_elem, 10 * (size_t)ne * sizeof(double), cudaMemcpyHostToDevice, st));
-    CUDA_OK(h, cudaMemsetAsync(h->ds.cu, 0, 10 * ld * sizeof(double), st));
-    k_scatter_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cn1, ne, 10, h->d_perm, h->ds.cu, ld);
-    CUDA_OK(h, cudaGetLastError());
-    CUDA_OK(h, cudaMemcpyAsync(h->ds.cn, h->ds.cu, 10 * ld * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (ng) k_fill_cols<<<blocks_for(10LL * ng, 256), 256, 0, st>>>(h->ds.cu, ld, 10, gs, ng, 0.0);
+    k_scatter_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cn1, ne, 10, h->d_perm + cr.e0, h->ds.cu, ld);
+    k_copy_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cn, h->ds.cu, ld, 10, cr.e0, ne);
+    if (ng) k_copy_cols<<<blocks_for(10LL * ng, 256), 256, 0, st>>>(h->ds.cn, h->ds.cu, ld, 10, gs, ng);
     // primitives: zero, then the restart's ghost values (src/main.F90:433-438)
-    CUDA_OK(h, cudaMemsetAsync(h->ds.pr, 0, NPR * ld * sizeof(double), st));
+    k_fill_cols<<<blocks_for((long long)NPR * ne, 256), 256, 0, st>>>(h->ds.pr, ld, NPR, cr.e0, ne, 0.0);
+    if (ng) k_fill_cols<<<blocks_for((long long)NPR * ng, 256), 256, 0, st>>>(h->ds.pr, ld, NPR, gs, ng, 0.0);
+    CUDA_OK(h, cudaGetLastError());
     if (ghost_prims && ng) {
         CUDA_OK(h, cudaMemcpyAsync(h->d_gstage, ghost_prims, 6 * (size_t)ng * sizeof(double),
                                    cudaMemcpyHostToDevice, st));
         if (h->aliased)
-            k_scatter_ghost_prims<<<1, 32, 0, st>>>(h->d_gstage, ng, GHOST_COLS, h->d_gid, h->ds.pr, ld, 1);
+            k_scatter_ghost_prims<<<1, 32, 0, st>>>(h->d_gstage, ng, GHOST_COLS, h->d_gid + cr.g0, h->ds.pr, ld, 1);
         else
-            k_scatter_ghost_prims<<<blocks_for(6LL * ng, 256), 256, 0, st>>>(h->d_gstage, ng, GHOST_COLS, h->d_gid,
-                                                                             h->ds.pr, ld, 0);
+            k_scatter_ghost_prims<<<blocks_for(6LL * ng, 256), 256, 0, st>>>(h->d_gstage, ng, GHOST_COLS,
+                                                                             h->d_gid + cr.g0, h->ds.pr, ld, 0);
         CUDA_OK(h, cudaGetLastError());
     }
     DevScalars s0{};
     double v = 1.0e8;
     std::memcpy(&s0.dtmin_bits, &v, 8);
     s0.time = time;
+    s0.cell1 = cr.cell1;
     *h->h_scal = s0;
-    CUDA_OK(h, cudaMemcpyAsync(h->ds.s, h->h_scal, sizeof s0, cudaMemcpyHostToDevice, st));
+    CUDA_OK(h, cudaMemcpyAsync(h->ds.s + c, h->h_scal, sizeof s0, cudaMemcpyHostToDevice, st));
     CUDA_OK(h, cudaStreamSynchronize(st));
     h->started = false;
-    h->have_state = true;
+    if (h->state_set.size() != (size_t)h->ncase) h->state_set.assign(h->ncase, 0);
+    h->state_set[c] = 1;
+    h->have_state = std::all_of(h->state_set.begin(), h->state_set.end(), [](char x) { return x != 0; });
+    return HP_OK;
+}
+
+// A batch's cases step together from their first step on; a case's state can
+// be replaced only before that (a single case can be reset at any time).
+static int check_settable(hp_handle* h, int c) {
+    if (c < 0 || c >= h->ncase) return fail(h, HP_E_ARG, "case index out of range");
+    if (h->ncase > 1 && h->started)
+        return fail(h, HP_E_STATE, "the cases of a batch are set before its first step");
     return HP_OK;
 }
 
@@ -612,20 +737,39 @@ extern "C" int hp_init_uniform(hp_handle* h) {
     double ropmin = (p.pmin + p.pinf) * p.gamap / ((p.gamap - 1.0) * p.cpp * p.tpmin);
     double egtmin = rrg * p.tgmin / (p.gamag - 1.0) + 0.5 * (sq(p.ugmin) + sq(p.vgmin) + sq(p.wgmin));
     double eptmin = (p.cpp * p.tpmin) / p.gamap + p.pinf / ropmin + 0.5 * (sq(p.upmin) + sq(p.vpmin) + sq(p.wpmin));
-    const int ne = h->neles;
-    std::vector<double> cu(10 * (size_t)ne);
+    int rc = check_settable(h, 0);
+    if (rc) return rc;
+    std::vector<double> cu;
     double phip = p.epslninf, phig = 1 - p.epslninf;
     double v[10] = {phig * rogmin, phig * rogmin * p.ugmin, phig * rogmin * p.vgmin, phig * rogmin * p.wgmin,
                     phig * rogmin * egtmin, phip * ropmin, phip * ropmin * p.upmin, phip * ropmin * p.vpmin,
                     phip * ropmin * p.wpmin, phip * ropmin * eptmin};
-    for (int k = 0; k < 10; k++)
-        for (int i = 0; i < ne; i++) cu[(size_t)k * ne + i] = v[k];
-    return upload_state(h, 0.0, cu.data(), nullptr);
+    for (int c = 0; c < h->ncase; c++) {
+        const int ne = h->cases[c].ne;
+        cu.assign(10 * (size_t)ne, 0.0);
+        for (int k = 0; k < 10; k++)
+            for (int i = 0; i < ne; i++) cu[(size_t)k * ne + i] = v[k];
+        rc = upload_state(h, c, 0.0, cu.data(), nullptr);
+        if (rc) return rc;
+    }
+    return HP_OK;
 }
 
 extern "C" int hp_set_state(hp_handle* h, double time, const double* cu_elem, const double* ghost_prims) {
+    return hp_set_state_case(h, 0, time, cu_elem, ghost_prims);
+}
+
+extern "C" int hp_set_state_case(hp_handle* h, int32_t c, double time, const double* cu_elem,
+                                 const double* ghost_prims) {
     if (!h || !cu_elem) return HP_E_ARG;
-    return upload_state(h, time, cu_elem, ghost_prims);
+    int rc = check_settable(h, c);
+    if (rc) return rc;
+    return upload_state(h, c, time, cu_elem, ghost_prims);
+}
+
+// zero every case's per-call step counter (the row index of its diagnostics)
+static cudaError_t reset_step_counters(hp_handle* h) {
+    return cudaMemset2DAsync(&h->ds.s->step_in_call, sizeof(DevScalars), 0, sizeof(int), h->ncase, h->stream);
 }
 
 static int run_steps(hp_handle* h, int n) {
@@ -656,20 +800,25 @@ extern "C" int hp_step(hp_handle* h, int32_t nsteps, hp_diag* diag) {
     int done = 0;
     while (done < nsteps) {
         int chunk = std::min(nsteps - done, h->max_diag);
-        CUDA_OK(h, cudaMemsetAsync(&h->ds.s->step_in_call, 0, sizeof(int), h->stream));
+        CUDA_OK(h, reset_step_counters(h));
         int rc = run_steps(h, chunk);
         if (rc) return rc;
         if (diag) {
-            CUDA_OK(h, cudaMemcpyAsync(h->h_diag, h->ds.diag, (size_t)chunk * 8 * sizeof(double),
-                                       cudaMemcpyDeviceToHost, h->stream));
+            // rows of case c start at c * max_diag on the device, at
+            // c * nsteps in the caller's array
+            for (int c = 0; c < h->ncase; c++)
+                CUDA_OK(h, cudaMemcpyAsync(h->h_diag + (size_t)c * h->max_diag * 8,
+                                           h->ds.diag + (size_t)c * h->max_diag * 8,
+                                           (size_t)chunk * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CUDA_OK(h, cudaStreamSynchronize(h->stream));
-            for (int k = 0; k < chunk; k++) {
-                const double* d = h->h_diag + 8 * (size_t)k;
-                hp_diag& o = diag[done + k];
-                o.time = d[0]; o.dt = d[1]; o.velmag = d[2];
-                for (int j = 0; j < 4; j++) o.diff[j] = d[3 + j];
-                o.nan_cells = d[7];
-            }
+            for (int c = 0; c < h->ncase; c++)
+                for (int k = 0; k < chunk; k++) {
+                    const double* d = h->h_diag + ((size_t)c * h->max_diag + k) * 8;
+                    hp_diag& o = diag[(size_t)c * nsteps + done + k];
+                    o.time = d[0]; o.dt = d[1]; o.velmag = d[2];
+                    for (int j = 0; j < 4; j++) o.diff[j] = d[3 + j];
+                    o.nan_cells = d[7];
+                }
         }
         done += chunk;
     }
@@ -686,7 +835,7 @@ extern "C" int hp_step_timed(hp_handle* h, int32_t nsteps, double* device_ms) {
         h->var->enqueue_start(h->dm, &h->ds, h->dp, h->stream, h->prm.block_size, nullptr);
         h->started = true;
     }
-    CUDA_OK(h, cudaMemsetAsync(&h->ds.s->step_in_call, 0, sizeof(int), h->stream));
+    CUDA_OK(h, reset_step_counters(h));
     CUDA_OK(h, cudaEventRecord(a, h->stream));
     int rc = run_steps(h, nsteps);
     CUDA_OK(h, cudaEventRecord(b, h->stream));
@@ -729,7 +878,7 @@ extern "C" int hp_profile_steps(hp_handle* h, int32_t nsteps, double* ms_per_kin
         h->var->enqueue_start(h->dm, &h->ds, h->dp, h->stream, h->prm.block_size, nullptr);
         h->started = true;
     }
-    CUDA_OK(h, cudaMemsetAsync(&h->ds.s->step_in_call, 0, sizeof(int), h->stream));
+    CUDA_OK(h, reset_step_counters(h));
     for (int k = 0; k < nsteps; k++) {
         h->var->enqueue_step(h->dm, &h->ds, h->dp, h->stream, h->prm.block_size, &hook);
         if (ctx.err != cudaSuccess) break;
@@ -754,8 +903,32 @@ extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, i
     const long long ld = ((long long)mesh->neles + mesh->nghosts + 63) / 64 * 64;
     const size_t gb = params->precision == HP_PREC_MIXED ? sizeof(float) : sizeof(double);
     Arena probe;
-    plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb);
+    plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb, 1);
     *bytes = (int64_t)(probe.used + 256);
+    return HP_OK;
+}
+
+extern "C" int hp_estimate_batch_bytes(const hp_mesh* meshes, int32_t ncase, const hp_params* params,
+                                       int64_t* bytes) {
+    if (!meshes || !params || !bytes || ncase < 1) return HP_E_ARG;
+    long long ne = 0, ng = 0;
+    for (int c = 0; c < ncase; c++) {
+        if (meshes[c].neles <= 0 || meshes[c].nghosts < 0) return HP_E_ARG;
+        ne += meshes[c].neles;
+        ng += meshes[c].nghosts;
+    }
+    hp_handle probe_h;
+    const long long ld = (ne + ng + 63) / 64 * 64;
+    const size_t gb = params->precision == HP_PREC_MIXED ? sizeof(float) : sizeof(double);
+    Arena probe;
+    plan_arena(&probe_h, probe, (int)ne, (int)ng, ld, gb, ncase);
+    *bytes = (int64_t)(probe.used + 256);
+    return HP_OK;
+}
+
+extern "C" int hp_case_count(const hp_handle* h, int32_t* ncase) {
+    if (!h || !ncase) return HP_E_ARG;
+    *ncase = h->ncase;
     return HP_OK;
 }
 
@@ -775,21 +948,28 @@ extern "C" int hp_sync(hp_handle* h) {
 }
 
 extern "C" int hp_get_state(hp_handle* h, double* time, double* cu_elem, double* ghost_prims) {
+    return hp_get_state_case(h, 0, time, cu_elem, ghost_prims);
+}
+
+extern "C" int hp_get_state_case(hp_handle* h, int32_t c, double* time, double* cu_elem, double* ghost_prims) {
     if (!h) return HP_E_ARG;
+    if (c < 0 || c >= h->ncase) return fail(h, HP_E_ARG, "case index out of range");
+    const CaseRange& cr = h->cases[c];
     const long long ld = h->ld;
-    const int ne = h->neles, ng = h->nghosts;
+    const int ne = cr.ne, ng = cr.ng;
     cudaStream_t st = h->stream;
     if (time) {
-        CUDA_OK(h, cudaMemcpyAsync(h->h_scal, h->ds.s, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(h, cudaMemcpyAsync(h->h_scal, h->ds.s + c, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
     }
     if (cu_elem) {
-        k_gather_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cu, ld, 0, ne, 10, h->d_perm, h->ds.cn1);
+        k_gather_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cu, ld, 0, ne, 10, h->d_perm + cr.e0,
+                                                                  h->ds.cn1);
         CUDA_OK(h, cudaGetLastError());
         CUDA_OK(h, cudaMemcpyAsync(cu_elem, h->ds.cn1, 10 * (size_t)ne * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
     if (ghost_prims && ng) {
-        k_gather_ghost_prims<<<blocks_for(6LL * ng, 256), 256, 0, st>>>(h->ds.pr, ld, GHOST_COLS, ng, h->d_gid,
-                                                                        h->d_gstage);
+        k_gather_ghost_prims<<<blocks_for(6LL * ng, 256), 256, 0, st>>>(h->ds.pr, ld, GHOST_COLS, ng,
+                                                                        h->d_gid + cr.g0, h->d_gstage);
         CUDA_OK(h, cudaGetLastError());
         CUDA_OK(h, cudaMemcpyAsync(ghost_prims, h->d_gstage, 6 * (size_t)ng * sizeof(double),
                                    cudaMemcpyDeviceToHost, st));
@@ -802,12 +982,12 @@ extern "C" int hp_get_state(hp_handle* h, double* time, double* cu_elem, double*
 extern "C" int hp_get_prims(hp_handle* h, double* prims) {
     if (!h || !prims) return HP_E_ARG;
     const long long ld = h->ld;
-    const int ne = h->neles;
+    const int ne = h->cases[0].ne;   // case 0 (the only one of a single-case handle)
     cudaStream_t st = h->stream;
     // cn1 stages at most 10 columns at a time
     for (int c0 = 0; c0 < NPR; c0 += 10) {
         const int nc = NPR - c0 < 10 ? NPR - c0 : 10;
-        k_gather_cols<<<blocks_for((long long)nc * ne, 256), 256, 0, st>>>(h->ds.pr, ld, c0, ne, nc, h->d_perm,
+        k_gather_cols<<<blocks_for((long long)nc * ne, 256), 256, 0, st>>>(h->ds.pr, ld, c0, ne, nc, h->d_perm + h->cases[0].e0,
                                                                           h->ds.cn1);
         CUDA_OK(h, cudaGetLastError());
         CUDA_OK(h, cudaMemcpyAsync(prims + (size_t)c0 * ne, h->ds.cn1, (size_t)nc * ne * sizeof(double),

@@ -132,6 +132,9 @@ __device__ __forceinline__ T qshfl(T v, int q) {
 
 #define COL(ptr, k) ((ptr) + (size_t)(k) * (size_t)m.ld)
 
+// case of element i (0 for a single-case handle)
+__device__ __forceinline__ int case_of(const DevMesh& m, int i) { return m.cid ? ldg(m.cid + i) : 0; }
+
 // ---------------------------------------------------------------------------
 // Primitive recovery, src/sr_primitive.F90:23-161 (== the element loop of
 // src/sr_primitiveplusbc.F90:36-172 without ag/ap).  c[] is renormalised.
@@ -278,10 +281,29 @@ __global__ void __launch_bounds__(256) k_prim(DevMesh m, DevState<R> s, DevParam
                 COL(s.cu, k)[i] = c[k];
             }
             nanc = bad ? 1 : 0;
-            if (i == m.cell1) s.s->velmag = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+            DevScalars& S = s.s[case_of(m, i)];
+            if (i == S.cell1) S.velmag = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
         }
     }
     if (MODE == PM_STAGE) return;
+    // a block whose cells belong to two cases of a batch reduces per thread
+    // (block-uniform branch: cases occupy contiguous element ranges)
+    const int b0 = blockIdx.x * blockDim.x;
+    const int c0 = case_of(m, b0), c1 = case_of(m, min(b0 + (int)blockDim.x, m.neles) - 1);
+    if (c0 != c1) {
+        if (i < m.neles) {
+            DevScalars& S = s.s[case_of(m, i)];
+            if (MODE == PM_START) {
+                if (kmin != ~0ull) atomicMin(&S.dtmin_bits, kmin);
+            } else {
+                for (int k = 0; k < 4; k++)
+                    if (kd[k]) atomicMax(&S.diff_bits[k], kd[k]);
+                if (nanc) atomicAdd(&S.nan_count, nanc);
+            }
+        }
+        return;
+    }
+    DevScalars* const S0 = s.s + c0;
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (MODE == PM_START) {
         kmin = warp_min_u64(kmin);
@@ -290,7 +312,7 @@ __global__ void __launch_bounds__(256) k_prim(DevMesh m, DevState<R> s, DevParam
         if (wid == 0) {
             unsigned long long v = lane < (int)(blockDim.x >> 5) ? red[0][lane] : ~0ull;
             v = warp_min_u64(v);
-            if (lane == 0 && v != ~0ull) atomicMin(&s.s->dtmin_bits, v);
+            if (lane == 0 && v != ~0ull) atomicMin(&S0->dtmin_bits, v);
         }
     } else {
 #pragma unroll
@@ -307,18 +329,20 @@ __global__ void __launch_bounds__(256) k_prim(DevMesh m, DevState<R> s, DevParam
             for (int k = 0; k < 4; k++) {
                 unsigned long long v = lane < nw ? red[k][lane] : 0ull;
                 v = warp_max_u64(v);
-                if (lane == 0 && v) atomicMax(&s.s->diff_bits[k], v);
+                if (lane == 0 && v) atomicMax(&S0->diff_bits[k], v);
             }
             unsigned long long c = lane < nw ? nred[lane] : 0ull;
             for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-            if (lane == 0 && c) atomicAdd(&s.s->nan_count, c);
+            if (lane == 0 && c) atomicAdd(&S0->nan_count, c);
         }
     }
 }
 
-// dt = cfl * dtmin, time += dt (src/main.F90:521-556); one thread.
-__global__ void k_step_begin(DevState<R> s, DevParams P) {
-    DevScalars* S = s.s;
+// dt = cfl * dtmin, time += dt (src/main.F90:521-556); one thread per case.
+__global__ void k_step_begin(DevState<R> s, DevParams P, int ncase) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncase) return;
+    DevScalars* S = s.s + c;
     double dtmin = __longlong_as_double((long long)S->dtmin_bits);
     S->dt = dtmin * P.cfl;
     S->time = S->time + S->dt;
@@ -326,12 +350,15 @@ __global__ void k_step_begin(DevState<R> s, DevParams P) {
     S->dtmin_bits = (unsigned long long)__double_as_longlong(1.0e8);
 }
 
-// per-step diagnostics and reset of the residual accumulators; one thread.
-__global__ void k_step_end(DevState<R> s) {
-    DevScalars* S = s.s;
+// per-step diagnostics and reset of the residual accumulators; one thread
+// per case (diag rows of case c start at c * max_diag).
+__global__ void k_step_end(DevState<R> s, int ncase) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncase) return;
+    DevScalars* S = s.s + c;
     int k = S->step_in_call;
     if (k < s.max_diag) {
-        double* d = s.diag + 8 * (size_t)k;
+        double* d = s.diag + 8 * ((size_t)c * s.max_diag + k);
         d[0] = S->time; d[1] = S->dt; d[2] = S->velmag;
         for (int j = 0; j < 4; j++) d[3 + j] = __longlong_as_double((long long)S->diff_bits[j]);
         d[7] = (double)S->nan_count;
@@ -487,7 +514,8 @@ template <bool VISC>
 __global__ void __launch_bounds__(256) k_bc(DevMesh m, DevState<R> s, DevParams P) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= m.nghosts) return;
-    bc_one<VISC>(m, s.pr, nullptr, P, g, s.s->dt, s.s->total);
+    const DevScalars& S = s.s[case_of(m, m.g_par[g])];
+    bc_one<VISC>(m, s.pr, nullptr, P, g, S.dt, S.total);
 }
 
 // Sequential ghost fill in the reference's exact order (type lists 2, 3, 5,
@@ -576,7 +604,7 @@ __global__ void __launch_bounds__(256) k_smooth1(DevMesh m, DevState<R> s) {
 template <int F>
 __device__ __forceinline__ unsigned smooth2_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int i) {
     unsigned bad = 0;
-    const double dt = s.s->dt;
+    const double dt = s.s[case_of(m, i)].dt;
     const double rdt = mrcp<F>(dt, bad);
     int nb[4];
 #pragma unroll
@@ -1130,7 +1158,7 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
         rhs[9] = rhs[9] + (double)(en * voli) - COL(vis, 7)[i];
     }
     // RK stage update (FP64)
-    const double dtbyvol = s.s->dt / ldg(m.vol + i);
+    const double dtbyvol = s.s[case_of(m, i)].dt / ldg(m.vol + i);
 #pragma unroll
     for (int j = 0; j < 10; j++) {
         const double r = rhs[j] - COL(s.d24, j)[i];
@@ -1425,7 +1453,7 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         if (__any_sync(0xffffffffu, bad)) return false;
     }
     if (!active) return true;
-    const double dtbyvol = s.s->dt / ldg(m.vol + i);
+    const double dtbyvol = s.s[case_of(m, i)].dt / ldg(m.vol + i);
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         const int j = q + 4 * r;
@@ -1650,7 +1678,7 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     const unsigned ge = grid_for(m.neles, 256), gf = grid_for(m.neles, b);
     const unsigned gg = grid_for(m.nghosts > 0 ? m.nghosts : 1, 256);
     MARK(KK_STEP_BEGIN);
-    k_step_begin<<<1, 1, 0, st>>>(s, P);
+    k_step_begin<<<grid_for(m.ncase, 128), 128, 0, st>>>(s, P, m.ncase);
     // JST dissipation, src/sr_smooth.F90 (once per step)
     if (m.aliased) { MARK(KK_SERIAL); k_smooth_copy_serial<<<1, 1, 0, st>>>(m, s, 0); }
     MARK(KK_SMOOTH1);
@@ -1698,7 +1726,7 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     MARK(KK_PRIM_END);
     k_prim<PM_END><<<ge, 256, 0, st>>>(m, s, P);
     MARK(KK_STEP_END);
-    k_step_end<<<1, 1, 0, st>>>(s);
+    k_step_end<<<grid_for(m.ncase, 128), 128, 0, st>>>(s, m.ncase);
     // start of the next step: primitive + dt contributions
     MARK(KK_PRIM_START);
     k_prim<PM_START><<<ge, 256, 0, st>>>(m, s, P);

@@ -81,6 +81,12 @@ def lib():
     L.hp_device_state.argtypes = [vp, ctypes.POINTER(_DP), ctypes.POINTER(ctypes.c_int64)]
     L.hp_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                           ctypes.POINTER(ctypes.c_int64)]
+    L.hp_create_batch.argtypes = [ctypes.POINTER(HpMesh), _I, ctypes.POINTER(HpParams), ctypes.POINTER(vp)]
+    L.hp_case_count.argtypes = [vp, ctypes.POINTER(_I)]
+    L.hp_set_state_case.argtypes = [vp, _I, _D, _DP, _DP]
+    L.hp_get_state_case.argtypes = [vp, _I, _DP, _DP, _DP]
+    L.hp_estimate_batch_bytes.argtypes = [ctypes.POINTER(HpMesh), _I, ctypes.POINTER(HpParams),
+                                          ctypes.POINTER(ctypes.c_int64)]
     L.hp_estimate_bytes.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(HpParams), ctypes.POINTER(ctypes.c_int64)]
     L.hp_poll.argtypes = [vp, ctypes.POINTER(_I)]
     L.hp_dt_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _I,
@@ -92,6 +98,8 @@ def lib():
     L.hp_write_restart.argtypes = [ctypes.c_char_p, _I, _I, _D, _DP, _DP]
     for fn in ("hp_create", "hp_destroy", "hp_init_uniform", "hp_set_state", "hp_step", "hp_sync",
                "hp_step_timed", "hp_profile_steps", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll",
+               "hp_create_batch", "hp_case_count", "hp_set_state_case", "hp_get_state_case",
+               "hp_estimate_batch_bytes",
                "hp_get_state", "hp_get_prims", "hp_device_state", "hp_info", "hp_read_flow",
                "hp_read_mesh", "hp_read_restart", "hp_write_restart"):
         getattr(L, fn).restype = ctypes.c_int
@@ -106,6 +114,7 @@ EXPORTED_SYMBOLS = (
     "hp_create", "hp_destroy", "hp_last_error", "hp_create_error", "hp_init_uniform",
     "hp_set_state", "hp_step", "hp_sync", "hp_step_timed", "hp_profile_steps", "hp_get_state", "hp_get_prims", "hp_device_state",
     "hp_info", "hp_read_flow", "hp_read_mesh", "hp_free_mesh", "hp_read_restart",
-    "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll",
+    "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll", "hp_create_batch", "hp_case_count",
+    "hp_set_state_case", "hp_get_state_case", "hp_estimate_batch_bytes",
 )
 NOALLOC_MAX_CELLS = 1 << 24

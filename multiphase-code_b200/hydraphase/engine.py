@@ -78,6 +78,24 @@ class MeshArrays:
         return int(self.ghost.shape[0])
 
 
+def _hp_mesh(mesh: MeshArrays, keep: list) -> HpMesh:
+    arrs = [np.ascontiguousarray(mesh.x, np.float64), np.ascontiguousarray(mesh.y, np.float64),
+            np.ascontiguousarray(mesh.z, np.float64), np.ascontiguousarray(mesh.elem, np.int32),
+            np.ascontiguousarray(mesh.ghost, np.int32)]
+    keep.extend(arrs)
+    x, y, z, el, gh = arrs
+    return HpMesh(mesh.nodes, mesh.neles, mesh.nghosts, 0, _dp(x), _dp(y), _dp(z), _ip(el), _ip(gh))
+
+
+def estimate_batch_bytes(meshes, params: HpParams) -> int:
+    """Device bytes a Batch of these meshes would hold."""
+    arr = (HpMesh * len(meshes))(*[HpMesh(m.nodes, m.neles, m.nghosts, 0, None, None, None, None, None)
+                                   for m in meshes])
+    b = ctypes.c_int64()
+    _check(lib().hp_estimate_batch_bytes(arr, len(meshes), ctypes.byref(params), ctypes.byref(b)))
+    return int(b.value)
+
+
 def estimate_bytes(mesh: MeshArrays, params: HpParams) -> int:
     """Device bytes a Case of this mesh and precision would hold."""
     hm = HpMesh(mesh.nodes, mesh.neles, mesh.nghosts, 0, None, None, None, None, None)
@@ -223,3 +241,81 @@ def write_restart(path: str, time: float, cu: np.ndarray, ghost_prims: np.ndarra
     neles = cu.size // 10
     nghosts = gp.size // 6
     _check(lib().hp_write_restart(path.encode(), neles, nghosts, float(time), _dp(cu), _dp(gp)))
+
+
+class Batch:
+    """Several cases (same parameters) in one handle: their cell and ghost
+    lists are concatenated on the device and every kernel of a step sweeps
+    all of them in one launch (hp_create_batch).  Each case keeps its own
+    dt, time and diagnostics; its results are those it would have alone."""
+
+    def __init__(self, meshes, params: HpParams):
+        self.L = lib()
+        self.params = params
+        self._keep = []
+        arr = (HpMesh * len(meshes))(*[_hp_mesh(m, self._keep) for m in meshes])
+        h = ctypes.c_void_p()
+        _check(self.L.hp_create_batch(arr, len(meshes), ctypes.byref(params), ctypes.byref(h)))
+        self.h = h
+        self.neles = [m.neles for m in meshes]
+        self.nghosts = [m.nghosts for m in meshes]
+
+    @property
+    def ncase(self) -> int:
+        return len(self.neles)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_state(self, c: int, time: float, cu: np.ndarray, ghost_prims: np.ndarray | None = None):
+        cu = np.ascontiguousarray(cu, np.float64).reshape(-1)
+        if cu.size != 10 * self.neles[c]:
+            raise ValueError("cu must hold 10 x neles values of case %d" % c)
+        gp = None if ghost_prims is None else np.ascontiguousarray(ghost_prims, np.float64).reshape(-1)
+        _check(self.L.hp_set_state_case(self.h, int(c), float(time), _dp(cu), _dp(gp)), self.h)
+
+    def step(self, nsteps: int, diagnostics: bool = True):
+        """Run nsteps on every case; per-case lists of per-step arrays."""
+        if not diagnostics:
+            _check(self.L.hp_step(self.h, int(nsteps), None), self.h)
+            return None
+        d = (HpDiag * max(int(nsteps) * self.ncase, 1))()
+        _check(self.L.hp_step(self.h, int(nsteps), d), self.h)
+        arr = np.frombuffer(d, dtype=np.float64).reshape(-1, 8)[:nsteps * self.ncase].reshape(self.ncase, nsteps, 8)
+        return [{"time": a[:, 0].copy(), "dt": a[:, 1].copy(), "velmag": a[:, 2].copy(),
+                 "diff": a[:, 3:7].copy(), "nan_cells": a[:, 7].copy()} for a in arr]
+
+    def sync(self):
+        _check(self.L.hp_sync(self.h), self.h)
+
+    def poll(self) -> bool:
+        busy = ctypes.c_int32()
+        _check(self.L.hp_poll(self.h, ctypes.byref(busy)), self.h)
+        return bool(busy.value)
+
+    def step_timed(self, nsteps: int) -> float:
+        ms = ctypes.c_double()
+        _check(self.L.hp_step_timed(self.h, int(nsteps), ctypes.byref(ms)), self.h)
+        return ms.value
+
+    def state(self, c: int):
+        t = ctypes.c_double()
+        ne, ng = self.neles[c], self.nghosts[c]
+        cu = np.zeros(10 * ne)
+        gp = np.zeros(6 * max(ng, 1))
+        _check(self.L.hp_get_state_case(self.h, int(c), ctypes.byref(t), _dp(cu), _dp(gp)), self.h)
+        return t.value, cu.reshape(10, ne), gp[:6 * ng].reshape(6, ng)
