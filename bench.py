@@ -34,7 +34,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import numpy as np  # noqa: E402
 
-METRIC = "cell-RK-stage updates/s"
+METRIC = "cell-RK-stage updates/s, mixed vs FP64 CUDA at stated L2 err; p50/p99 case latency"
 UNIT = "cell-stage/s"
 
 # Compulsory bytes per cell and RK stage (each array crossing HBM once):
@@ -220,6 +220,32 @@ def cpu_oracle_sample(name: str, threads: int, seconds_target: float = 15.0):
             "sample": f"{m.neles} cells (O-grid 40x64x8, same physics), {steps} steps, {t_used:.1f} s"}
 
 
+def serving_measure(n_cases: int, steps: int):
+    """The batched serving stream (shock-bubble cases of log-uniform size
+    6k-400k cells, Poisson arrivals at 40/s, SSP-RK3) served in real time in
+    the mixed and the plain FP64 variant, after tuning the per-cell kernel
+    block size for each mesh-size class present."""
+    from hydraphase import PREC_FP64_PARITY, PREC_MIXED, cases, tune
+    from hydraphase.serve import Server
+    t0 = time.perf_counter()
+    reqs = cases.serving_stream(n_cases=n_cases, steps=steps)
+    gen_s = time.perf_counter() - t0
+    out = {"workload": f"shock-bubble stream: {n_cases} cases, cells log-U[6000, 400000], Poisson 40/s, "
+                       f"{steps} SSP-RK3 steps each, CFL 0.1, HBM budget 150 GiB",
+           "cells_total": int(sum(r.spec.mesh.neles for r in reqs)), "generation_s": round(gen_s, 2)}
+    for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64_PARITY)):
+        blocks = {}
+        for r in reqs:
+            cls = tune.size_class(r.spec.mesh.neles)
+            if cls not in blocks:
+                blocks[cls] = tune.tune_block_size(r.spec, precision=prec, steps=4)[0]
+        rep_ = Server(150 << 30, precision=prec, max_active=16, chunk=25, batch_cells=200000,
+                      block_size=blocks, keep_state=False).run(reqs)
+        out[name] = {**rep_.summary(), "block_size": blocks}
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["updates_per_s"] / out["fp64"]["updates_per_s"]
+    return out
+
+
 def run_reference_arm(args, world, rank, pg):
     if rank != 0:
         return 0
@@ -345,6 +371,10 @@ def run_ours(args, world, rank, local, pg):
     }
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_oracle_sample(args.workload, os.cpu_count() or 1)
+    if world == 1 and rank == 0 and args.serving_cases > 0:
+        sv = serving_measure(args.serving_cases, args.serving_steps)
+        sv["mixed_served_vs_plain_fp64_value"] = sv["mixed"]["updates_per_s"] / value
+        line["serving"] = sv
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -358,6 +388,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cylinder")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving-cases", type=int, default=48,
+                    help="cases of the serving stream measured after the step benchmark (0: skip)")
+    ap.add_argument("--serving-steps", type=int, default=500)
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     try:

@@ -69,7 +69,9 @@ typedef struct hp_params {
     double twall;            /* isothermal wall temperature (BC type 6) */
     int32_t precision;       /* HP_PREC_* */
     int32_t renumber;        /* 1: space-filling-curve cell order on device */
-    int32_t block_size;      /* 0: autotuned */
+    int32_t block_size;      /* threads per block of the one-thread-per-cell
+                                kernels: 0 (= 256) or a multiple of 32 in
+                                [64, 512]; hydraphase.tune picks it */
     int32_t use_graph;       /* 1: capture each step in a CUDA graph */
     double pad_[4];
 } hp_params;

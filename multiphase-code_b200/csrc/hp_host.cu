@@ -430,6 +430,8 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
         return fail(nullptr, HP_E_UNSUPPORTED, "myflux must be 2 (HLLC-Batten)");
     if (params->myorder != 1 && params->myorder != 2)
         return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
+    if (params->block_size != 0 && (params->block_size < 64 || params->block_size > 512 || params->block_size % 32))
+        return fail(nullptr, HP_E_ARG, "block_size must be 0 or a multiple of 32 in [64, 512]");
     long long etot = 0, gtot = 0;
     for (int c = 0; c < ncase; c++) {
         const hp_mesh* mesh = meshes + c;

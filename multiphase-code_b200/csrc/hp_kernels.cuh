@@ -241,8 +241,8 @@ enum { PM_STAGE = 0, PM_START = 1, PM_END = 2 };
 // src/main.F90:529-546; PM_END adds the max-norm residual of :605-611, the
 // cu = cn copy of :619-625 and |u_g(1)| of :641.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_prim(DevMesh m, DevState<R> s, DevParams P) {
-    __shared__ unsigned long long red[4][8];
+__global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParams P) {
+    __shared__ unsigned long long red[4][16];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long kmin = ~0ull, kd[4] = {0, 0, 0, 0}, nanc = 0;
     if (i < m.neles) {
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(256) k_prim(DevMesh m, DevState<R> s, DevParam
         if (lane == 0) {
             for (int k = 0; k < 4; k++) red[k][wid] = kd[k];
         }
-        __shared__ unsigned long long nred[8];
+        __shared__ unsigned long long nred[16];
         if (lane == 0) nred[wid] = nanc;
         __syncthreads();
         if (wid == 0) {
@@ -511,7 +511,7 @@ __device__ __forceinline__ void ghost_cn_one(const DevMesh& m, double* pr, doubl
 // Parallel ghost fill: valid when every ghost id is its own slot and every
 // parent is an element (no aliasing), so ghost entries are independent.
 template <bool VISC>
-__global__ void __launch_bounds__(256) k_bc(DevMesh m, DevState<R> s, DevParams P) {
+__global__ void __launch_bounds__(512) k_bc(DevMesh m, DevState<R> s, DevParams P) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= m.nghosts) return;
     const DevScalars& S = s.s[case_of(m, m.g_par[g])];
@@ -557,7 +557,7 @@ __global__ void k_phi_copy_serial(DevMesh m, DevState<R> s) {
 
 // ---------------------------------------------------------------------------
 // JST dissipation, src/sr_smooth.F90:52-154: switches anu and Laplacian d2q.
-__global__ void __launch_bounds__(256) k_smooth1(DevMesh m, DevState<R> s) {
+__global__ void __launch_bounds__(512) k_smooth1(DevMesh m, DevState<R> s) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     const int a = ldg(COL(m.snb, 0) + i), b = ldg(COL(m.snb, 1) + i);
@@ -643,7 +643,7 @@ __device__ __forceinline__ unsigned smooth2_body(const DevMesh& m, const DevStat
     return bad;
 }
 
-__global__ void __launch_bounds__(256) k_smooth2(DevMesh m, DevState<R> s, DevParams P) {
+__global__ void __launch_bounds__(512) k_smooth2(DevMesh m, DevState<R> s, DevParams P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < m.neles;
     if (!valid) i = m.neles - 1;      // keep the warp whole for the vote below
@@ -1666,7 +1666,8 @@ static void enqueue_start(const DevMesh& m, const void* stp, const DevParams& P,
                           int block, const StepHook* hook) {
     const DevState<R>& s = *static_cast<const DevState<R>*>(stp);
     MARK(KK_PRIM_START);
-    k_prim<PM_START><<<grid_for(m.neles, 256), 256, 0, st>>>(m, s, P);
+    const int cb = block > 0 ? block : 256;
+    k_prim<PM_START><<<grid_for(m.neles, cb), cb, 0, st>>>(m, s, P);
     MARK(KK_COUNT);
 }
 
@@ -1674,23 +1675,26 @@ static void enqueue_start(const DevMesh& m, const void* stp, const DevParams& P,
 static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, cudaStream_t st,
                          int block, const StepHook* hook) {
     const DevState<R>& s = *static_cast<const DevState<R>*>(stp);
-    const int b = block > 0 ? block : 128;
-    const unsigned ge = grid_for(m.neles, 256), gf = grid_for(m.neles, b);
-    const unsigned gg = grid_for(m.nghosts > 0 ? m.nghosts : 1, 256);
+    // one-thread-per-cell kernels: `block` threads per block (64..512,
+    // 0 = 256); four-lane kernels and the one-thread kernels of aliased
+    // meshes: 128 (their launch bounds)
+    const int cb = block > 0 ? block : 256, b = 128;
+    const unsigned ge = grid_for(m.neles, cb), gf = grid_for(m.neles, b);
+    const unsigned gg = grid_for(m.nghosts > 0 ? m.nghosts : 1, cb);
     MARK(KK_STEP_BEGIN);
     k_step_begin<<<grid_for(m.ncase, 128), 128, 0, st>>>(s, P, m.ncase);
     // JST dissipation, src/sr_smooth.F90 (once per step)
     if (m.aliased) { MARK(KK_SERIAL); k_smooth_copy_serial<<<1, 1, 0, st>>>(m, s, 0); }
     MARK(KK_SMOOTH1);
-    k_smooth1<<<ge, 256, 0, st>>>(m, s);
+    k_smooth1<<<ge, cb, 0, st>>>(m, s);
     if (m.aliased) { MARK(KK_SERIAL); k_smooth_copy_serial<<<1, 1, 0, st>>>(m, s, 1); }
     MARK(KK_SMOOTH2);
-    k_smooth2<<<ge, 256, 0, st>>>(m, s, P);
+    k_smooth2<<<ge, cb, 0, st>>>(m, s, P);
     // viscous fluxes, src/sr_viscousgp.F90 (stage 1 of each step)
     if (m.nghosts > 0) {
         MARK(KK_BC_VISC);
         if (m.aliased) k_bc_serial<true><<<1, 1, 0, st>>>(m, s, P);
-        else k_bc<true><<<gg, 256, 0, st>>>(m, s, P);
+        else k_bc<true><<<gg, cb, 0, st>>>(m, s, P);
     }
     const unsigned g4 = grid_for(4ll * m.neles, 128);
     if (!P.inviscid) {
@@ -1701,11 +1705,11 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     for (int stage = 1; stage <= P.nstage; stage++) {
         // src/sr_hllcbatten.F90:29-33: primitiveplusbc, derivative, limiter
         MARK(KK_PRIM_STAGE);
-        k_prim<PM_STAGE><<<ge, 256, 0, st>>>(m, s, P);
+        k_prim<PM_STAGE><<<ge, cb, 0, st>>>(m, s, P);
         if (m.nghosts > 0) {
             MARK(KK_BC);
             if (m.aliased) k_bc_serial<false><<<1, 1, 0, st>>>(m, s, P);
-            else k_bc<false><<<gg, 256, 0, st>>>(m, s, P);
+            else k_bc<false><<<gg, cb, 0, st>>>(m, s, P);
         }
         if (P.myorder == 2) {
             MARK(KK_GRAD);
@@ -1724,12 +1728,12 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     }
     // src/main.F90:595-641: primitive, residual norms, cu = cn
     MARK(KK_PRIM_END);
-    k_prim<PM_END><<<ge, 256, 0, st>>>(m, s, P);
+    k_prim<PM_END><<<ge, cb, 0, st>>>(m, s, P);
     MARK(KK_STEP_END);
     k_step_end<<<grid_for(m.ncase, 128), 128, 0, st>>>(s, m.ncase);
     // start of the next step: primitive + dt contributions
     MARK(KK_PRIM_START);
-    k_prim<PM_START><<<ge, 256, 0, st>>>(m, s, P);
+    k_prim<PM_START><<<ge, cb, 0, st>>>(m, s, P);
     MARK(KK_COUNT);
 }
 #undef MARK

@@ -5,26 +5,32 @@ The reference runs one case per process. Here a request loop takes cases
 and solution resident on the device, and advances all admitted cases
 together:
 
-* **Admission.** It is FIFO. A case is admitted as soon as a slot is free
-  (at most `max_active` cases in flight) and its device bytes
-  (`hp_estimate_bytes`) fit in what is left of `hbm_budget`.
+* **Admission.** It is FIFO. A unit (one case or a batch of them) is
+  admitted as soon as a slot is free (at most `max_active` units in flight)
+  and its device bytes (`hp_estimate_bytes` / `hp_estimate_batch_bytes`) fit
+  in what is left of `hbm_budget`.
+* **Batching.** With `batch_cells` set, consecutive queued cases smaller than
+  that, with equal parameters and step counts, are set up together as one
+  multi-mesh batch (`hp_create_batch`) of at most `batch_cells` cells. Each
+  kernel launch of a step then sweeps all of them.
 * **Set-up.** Host-side geometry, layout and upload (`hp_create` +
   `hp_set_state`) run on a pool of worker threads. They overlap with the
-  device work of the cases already running.
-* **Overlap.** Every case owns a CUDA stream and replays its step as a CUDA
-  graph. The loop enqueues `chunk` steps on a case whenever its previous
-  chunk is done (`hp_poll`, non-blocking). So the kernels of different cases
+  device work of the units already running.
+* **Overlap.** Every unit owns a CUDA stream and replays its step as a CUDA
+  graph. The loop enqueues `chunk` steps on a unit whenever its previous
+  chunk is done (`hp_poll`, non-blocking). So the kernels of different units
   overlap on the device, and a case that arrives later joins at the next
   chunk boundary without waiting for the others.
-* **Completion.** When a case has run all its steps, its state is copied back
-  to the host, its device memory is released (stream-ordered, with no
+* **Completion.** When a unit has run all its steps, its states are copied
+  back to the host, its device memory is released (stream-ordered, with no
   device-wide synchronisation), and its slot and bytes are freed for the
   queue.
 
 Time-to-solution is measured from arrival to the result on the host,
 queueing included. A case's result does not depend on what else runs: each
-case has its own buffers, stream and reductions, and the kernels are
-deterministic. tests/test_serving.py checks this bit for bit.
+unit has its own buffers, stream and reductions, the members of a batch keep
+their own scalars, and the kernels are deterministic. tests/test_serving.py
+checks this bit for bit.
 """
 from __future__ import annotations
 
@@ -35,7 +41,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._lib import PREC_MIXED, HydraError
-from .engine import Case, estimate_bytes
+from .engine import Batch, Case, estimate_batch_bytes, estimate_bytes
 
 
 @dataclass
@@ -47,7 +53,7 @@ class CaseResult:
     admitted: float         # admission decision (set-up starts)
     started: float          # first chunk enqueued
     finished: float         # state back on the host
-    device_bytes: int
+    device_bytes: int       # of its unit, shared evenly by a batch's members
     time: float = 0.0       # simulation time reached
     cu: np.ndarray | None = None
     ghost_prims: np.ndarray | None = None
@@ -60,8 +66,8 @@ class CaseResult:
 
 @dataclass
 class _Active:
-    req: object
-    case: Case
+    reqs: list             # the requests of this unit (one case or a batch)
+    handle: object         # Case or Batch
     bytes: int
     admitted: float
     started: float
@@ -74,30 +80,42 @@ class ServeReport:
     makespan: float = 0.0
     peak_bytes: int = 0
     peak_active: int = 0
+    units: int = 0
 
     def summary(self) -> dict:
         ok = [r for r in self.results if r.error is None]
         lat = np.array([r.latency for r in ok]) if ok else np.zeros(1)
         upd = sum(r.cells * 3 * r.steps for r in ok)
-        return {"cases": len(ok), "failed": len(self.results) - len(ok), "p50_s": float(np.percentile(lat, 50)),
-                "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
-                "makespan_s": self.makespan, "updates_per_s": upd / self.makespan if self.makespan else 0.0,
+        return {"cases": len(ok), "failed": len(self.results) - len(ok), "units": self.units,
+                "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                "mean_s": float(lat.mean()), "makespan_s": self.makespan,
+                "updates_per_s": upd / self.makespan if self.makespan else 0.0,
                 "peak_device_bytes": self.peak_bytes, "peak_active": self.peak_active}
 
 
+def _same_setup(a, b) -> bool:
+    return a.steps == b.steps and a.spec.flow == b.spec.flow and a.spec.extra == b.spec.extra
+
+
 class Server:
-    """Continuous-batching request loop over per-case handles.
+    """Continuous-batching request loop over per-unit handles.
 
     requests: objects with .rid, .arrival (s), .steps, .spec (a CaseSpec)
     precision: HP_PREC_* of every case
-    hbm_budget: device bytes the admitted cases may hold together
-    max_active: cases in flight (set up or running)
-    chunk: steps enqueued per case per turn of the loop
+    hbm_budget: device bytes the admitted units may hold together
+    max_active: units in flight (set up or running)
+    chunk: steps enqueued per unit per turn of the loop
     keep_state: copy each final state back (False keeps only the timing)
+    batch_cells: cases below this size are grouped into multi-mesh batches of
+        at most this many cells (0: every case on its own handle)
+    max_batch: cases per batch at most
+    block_size: threads per block of the per-cell kernels: an int, a dict
+        from hydraphase.tune.size_class() to an int, or None (256)
     """
 
     def __init__(self, hbm_budget: int, precision: int = PREC_MIXED, max_active: int = 12, chunk: int = 25,
-                 setup_workers: int = 4, keep_state: bool = True, param_overrides: dict | None = None):
+                 setup_workers: int = 4, keep_state: bool = True, param_overrides: dict | None = None,
+                 batch_cells: int = 0, max_batch: int = 64, block_size=None):
         self.budget = int(hbm_budget)
         self.precision = precision
         self.max_active = max_active
@@ -105,21 +123,53 @@ class Server:
         self.workers = setup_workers
         self.keep_state = keep_state
         self.over = dict(param_overrides or {})
+        self.batch_cells = int(batch_cells)
+        self.max_batch = int(max_batch)
+        self.block_size = block_size
 
-    def _params(self, spec):
-        return spec.params(precision=self.precision, **self.over)
+    def _params(self, spec, cells: int):
+        over = dict(self.over)
+        b = self.block_size
+        if isinstance(b, dict):
+            from .tune import size_class
+            b = b.get(size_class(cells))
+        if b and "block_size" not in over:
+            over["block_size"] = int(b)
+        return spec.params(precision=self.precision, **over)
 
     @staticmethod
-    def _setup(spec, params):
-        c = Case(spec.mesh, params)
-        c.set_state(0.0, spec.cu, spec.ghost_prims)
-        return c
+    def _setup(unit, params):
+        if len(unit) == 1:
+            spec = unit[0].spec
+            c = Case(spec.mesh, params)
+            c.set_state(0.0, spec.cu, spec.ghost_prims)
+            return c
+        b = Batch([r.spec.mesh for r in unit], params)
+        for k, r in enumerate(unit):
+            b.set_state(k, 0.0, r.spec.cu, r.spec.ghost_prims)
+        return b
+
+    def _take_unit(self, queue):
+        """The next unit from the head of the queue: one case, or the longest
+        run of small compatible cases that fits in batch_cells."""
+        head = queue[0]
+        cells = head.spec.mesh.neles
+        if not self.batch_cells or cells >= self.batch_cells:
+            return [head]
+        unit = [head]
+        for r in queue[1:]:
+            n = r.spec.mesh.neles
+            if len(unit) >= self.max_batch or cells + n > self.batch_cells or not _same_setup(head, r):
+                break
+            unit.append(r)
+            cells += n
+        return unit
 
     def run(self, requests, realtime: bool = True) -> ServeReport:
         """Serve `requests`; with realtime=False every case arrives at t=0."""
         pending = sorted(requests, key=lambda r: r.arrival)
         queue: list = []
-        setting_up: list = []      # (future, req, bytes, t_admit)
+        setting_up: list = []      # (future, unit, bytes, t_admit)
         active: list[_Active] = []
         rep = ServeReport()
         used = 0
@@ -134,54 +184,62 @@ class Server:
                     progressed = True
                 # FIFO admission against slots and bytes
                 while queue and len(setting_up) + len(active) < self.max_active:
-                    req = queue[0]
-                    p = self._params(req.spec)
-                    b = estimate_bytes(req.spec.mesh, p)
+                    unit = self._take_unit(queue)
+                    cells = sum(r.spec.mesh.neles for r in unit)
+                    p = self._params(unit[0].spec, cells)
+                    b = estimate_bytes(unit[0].spec.mesh, p) if len(unit) == 1 else \
+                        estimate_batch_bytes([r.spec.mesh for r in unit], p)
                     if used + b > self.budget and (setting_up or active):
                         break
-                    queue.pop(0)
+                    del queue[:len(unit)]
                     used += b
                     rep.peak_bytes = max(rep.peak_bytes, used)
-                    setting_up.append((pool.submit(self._setup, req.spec, p), req, b, now()))
+                    rep.units += 1
+                    setting_up.append((pool.submit(self._setup, unit, p), unit, b, now()))
                     progressed = True
-                # cases whose set-up finished start stepping
+                # units whose set-up finished start stepping
                 still = []
-                for fut, req, b, ta in setting_up:
-                    if fut.done():
-                        try:
-                            case = fut.result()
-                        except HydraError as e:
-                            used -= b
-                            rep.results.append(CaseResult(req.rid, req.spec.mesh.neles, req.steps, req.arrival,
-                                                          ta, ta, now(), b, error=str(e)))
-                            progressed = True
-                            continue
-                        n = min(self.chunk, req.steps)
-                        case.step(n, diagnostics=False)
-                        active.append(_Active(req, case, b, ta, now(), req.steps - n))
-                        progressed = True
-                    else:
-                        still.append((fut, req, b, ta))
+                for fut, unit, b, ta in setting_up:
+                    if not fut.done():
+                        still.append((fut, unit, b, ta))
+                        continue
+                    progressed = True
+                    try:
+                        handle = fut.result()
+                    except HydraError as e:
+                        used -= b
+                        for r in unit:
+                            rep.results.append(CaseResult(r.rid, r.spec.mesh.neles, r.steps, r.arrival, ta, ta,
+                                                          now(), b // len(unit), error=str(e)))
+                        continue
+                    n = min(self.chunk, unit[0].steps)
+                    handle.step(n, diagnostics=False)
+                    active.append(_Active(unit, handle, b, ta, now(), unit[0].steps - n))
                 setting_up = still
                 rep.peak_active = max(rep.peak_active, len(active) + len(setting_up))
-                # next chunk for every case whose previous chunk is done
+                # next chunk for every unit whose previous chunk is done
                 keep = []
                 for a in active:
-                    if a.case.poll():
+                    if a.handle.poll():
                         keep.append(a)
                         continue
                     progressed = True
                     if a.remaining > 0:
                         n = min(self.chunk, a.remaining)
-                        a.case.step(n, diagnostics=False)
+                        a.handle.step(n, diagnostics=False)
                         a.remaining -= n
                         keep.append(a)
                         continue
-                    tm, cu, gp = a.case.state() if self.keep_state else (0.0, None, None)
-                    a.case.close()
+                    batch = isinstance(a.handle, Batch)
+                    for k, r in enumerate(a.reqs):
+                        if self.keep_state:
+                            tm, cu, gp = a.handle.state(k) if batch else a.handle.state()
+                        else:
+                            tm, cu, gp = 0.0, None, None
+                        rep.results.append(CaseResult(r.rid, r.spec.mesh.neles, r.steps, r.arrival, a.admitted,
+                                                      a.started, now(), a.bytes // len(a.reqs), tm, cu, gp))
+                    a.handle.close()
                     used -= a.bytes
-                    rep.results.append(CaseResult(a.req.rid, a.req.spec.mesh.neles, a.req.steps, a.req.arrival,
-                                                  a.admitted, a.started, now(), a.bytes, tm, cu, gp))
                 active = keep
                 if not progressed:
                     time.sleep(0.0002)

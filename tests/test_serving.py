@@ -50,3 +50,48 @@ def test_admission_respects_the_budget():
     assert rep.peak_bytes <= budget
     s = rep.summary()
     assert s["p99_s"] >= s["p50_s"] > 0 and s["updates_per_s"] > 0
+
+
+def test_size_classes_and_tune_cache(tmp_path, monkeypatch):
+    from hydraphase import tune
+    assert [tune.size_class(n) for n in (6000, 50000, 200000, 5000000)] == ["xs", "s", "m", "l"]
+    monkeypatch.setenv("HYDRAPHASE_TUNE_CACHE", str(tmp_path / "t.json"))
+    tune._store({"k": {"best": 128}})
+    assert tune._load() == {"k": {"best": 128}}
+
+
+def test_server_groups_small_compatible_cases():
+    from hydraphase.serve import Server
+    reqs = cases.serving_stream(n_cases=10, steps=5, cells=(6000, 60000), seed=9)
+    s = Server(hbm_budget=1 << 40, batch_cells=100000, max_batch=4)
+    unit = s._take_unit(list(reqs))
+    assert 1 <= len(unit) <= 4
+    assert sum(r.spec.mesh.neles for r in unit) <= 100000 or len(unit) == 1
+    assert [r.rid for r in unit] == [r.rid for r in reqs[:len(unit)]]
+    assert Server(hbm_budget=1 << 40)._take_unit(list(reqs)) == [reqs[0]]
+
+
+@pytest.mark.gpu
+def test_batched_serving_equals_alone():
+    from hydraphase.serve import Server, run_alone
+    reqs = cases.serving_stream(n_cases=7, rate=1000.0, steps=9, cells=(6000, 30000), seed=11)
+    rep = Server(hbm_budget=8 << 30, precision=PREC_MIXED, max_active=3, chunk=4, batch_cells=60000,
+                 block_size=128).run(reqs, realtime=False)
+    assert len(rep.results) == 7 and all(r.error is None for r in rep.results)
+    assert rep.units < 7                 # some cases did share a batch
+    for r, q in zip(rep.results, reqs):
+        t, cu, gp = run_alone(q.spec, q.steps, precision=PREC_MIXED)
+        assert t == r.time
+        np.testing.assert_array_equal(r.cu, cu)
+        np.testing.assert_array_equal(r.ghost_prims, gp)
+
+
+@pytest.mark.gpu
+def test_block_size_tuner_measures_and_caches(tmp_path, monkeypatch):
+    from hydraphase import tune
+    monkeypatch.setenv("HYDRAPHASE_TUNE_CACHE", str(tmp_path / "t.json"))
+    spec = cases.shock_bubble(n=8, alpha_min=0.1)
+    best, ms = tune.tune_block_size(spec, candidates=(128, 256), steps=2)
+    assert best in (128, 256) and set(ms) == {128, 256}
+    best2, ms2 = tune.tune_block_size(spec, candidates=(128, 256), steps=2)
+    assert best2 == best and ms2 == ms
