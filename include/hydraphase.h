@@ -140,9 +140,9 @@ int hp_sync(hp_handle *h);
  * measured with CUDA events on the handle's stream. */
 int hp_step_timed(hp_handle *h, int32_t nsteps, double *device_ms);
 /* nsteps launched eagerly with a CUDA event between every two kernels;
- * accumulates device time and launch counts per kernel kind (nkinds >= 13:
+ * accumulates device time and launch counts per kernel kind (nkinds >= 14:
  * prim_start, step_begin, smooth1, smooth2, bc_visc, visc, prim_stage, bc,
- * grad, flux, prim_end, step_end, serial). */
+ * grad, flux, prim_end, step_end, serial, overset). */
 int hp_profile_steps(hp_handle *h, int32_t nsteps, double *ms_per_kind,
                      int64_t *launches_per_kind, int32_t nkinds);
 
@@ -163,6 +163,31 @@ int hp_device_state(hp_handle *h, double **cu_dev, int64_t *ld);
  * holds. */
 int hp_info(const hp_handle *h, int64_t *kernels_per_step, int64_t *device_bytes,
             int64_t *aliased);
+
+/* --- overset meshes -------------------------------------------------------- */
+/* New work: the reference only freezes cells with iblank != 1
+ * (src/sr_RK.F90:31); its hole cut and donor search come from TIOGA, outside
+ * the solver.  An overset mesh here is one element list of two blocks
+ * (block[e] = 0 background, 1 component), with the caller's hole cut as
+ * iblank = 0 on background cells.  hp_overset_build marks the fringe
+ * (background field cells next to holes, component field cells next to
+ * ghosts of type outer_type, `layers` layers deep; iblank_out = -1 there,
+ * the input iblank elsewhere) and finds, for each fringe cell, four donor
+ * cells of the other block and barycentric weights.  Create the handle with
+ * iblank_out in the mesh, then hp_set_overset: after every RK stage each
+ * fringe cell's state becomes sum_k weight_k * state(donor_k). */
+typedef struct hp_overset {
+    int32_t nfringe;
+    int32_t *fringe;    /* [nfringe] element ids (1-based), ascending */
+    int32_t *donor;     /* [4 * nfringe] element ids (1-based), row-major */
+    double *weight;     /* [4 * nfringe] */
+    int32_t nfallback;  /* fringe cells inside no donor-block cell (nearest used) */
+} hp_overset;
+int hp_overset_build(const hp_mesh *mesh, const int32_t *block, int32_t layers, int32_t outer_type,
+                     int32_t *iblank_out, hp_overset *out);
+void hp_free_overset(hp_overset *ov);
+/* Single-case handles only; replaces any earlier table. */
+int hp_set_overset(hp_handle *h, const hp_overset *ov);
 
 /* --- serving many cases ---------------------------------------------------- */
 /* No counterpart in the reference, which runs one case per process.  Device

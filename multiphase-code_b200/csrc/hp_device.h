@@ -64,6 +64,12 @@ struct DevMesh {
     const double* lsqa;     // [11][ld]
     const double* lsqb;     // [11][ld]
     const int *g_par, *g_id, *g_type;   // [nghosts] ghost list (reference order)
+    // overset fringe (nfringe = 0: none): cells, 4 donor cells each and
+    // barycentric weights, [4][nfringe] column-major
+    int nfringe;
+    const int* fr;
+    const int* fdon;
+    const double* fw;
 };
 
 // Per-case scalars (one entry per case of the handle).
@@ -97,7 +103,7 @@ struct DevState {
 enum KernelKind {
     KK_PRIM_START = 0, KK_STEP_BEGIN, KK_SMOOTH1, KK_SMOOTH2, KK_BC_VISC, KK_VISC,
     KK_PRIM_STAGE, KK_BC, KK_GRAD, KK_FLUX, KK_PRIM_END, KK_STEP_END, KK_SERIAL,
-    KK_COUNT
+    KK_OVERSET, KK_COUNT
 };
 
 // Optional hook called before every launch (and with KK_COUNT after the

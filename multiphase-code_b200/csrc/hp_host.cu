@@ -75,6 +75,7 @@ struct hp_handle {
     std::vector<CaseRange> cases;
     std::vector<int> perm;      // [neles] case c's reference element i -> slot, at cases[c].e0 + i
     std::vector<int> ghost_id;  // [nghosts] case c's ghost g -> slot, at cases[c].g0 + g
+    void* d_overset = nullptr;  // overset fringe table (hp_set_overset)
     int* d_perm = nullptr;      // the two maps above, on the device
     int* d_gid = nullptr;
     double* d_gstage = nullptr; // 6 x nghosts staging of ghost primitives
@@ -599,6 +600,7 @@ extern "C" int hp_destroy(hp_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->d_overset) cudaFreeAsync(h->d_overset, h->stream);
     if (h->arena.base) {
         cudaFreeAsync(h->arena.base, h->stream);
         cudaStreamSynchronize(h->stream);
@@ -899,6 +901,51 @@ extern "C" int hp_profile_steps(hp_handle* h, int32_t nsteps, double* ms_per_kin
     return HP_OK;
 }
 
+extern "C" int hp_set_overset(hp_handle* h, const hp_overset* ov) {
+    if (!h || !ov) return HP_E_ARG;
+    if (h->ncase != 1) return fail(h, HP_E_UNSUPPORTED, "overset tables: single-case handles only");
+    const int nf = ov->nfringe, ne = h->neles;
+    if (nf < 0 || (nf > 0 && (!ov->fringe || !ov->donor || !ov->weight)))
+        return fail(h, HP_E_ARG, "overset table: missing arrays");
+    // [fringe | donor column-major 4 x nf] ints, then [weight 4 x nf] doubles
+    std::vector<int> iv(5 * (size_t)nf);
+    std::vector<double> wv(4 * (size_t)nf);
+    for (int f = 0; f < nf; f++) {
+        const int e = ov->fringe[f];
+        if (e < 1 || e > ne) return fail(h, HP_E_ARG, "overset table: fringe id out of range");
+        iv[f] = h->perm[e - 1];
+        for (int k = 0; k < 4; k++) {
+            const int d = ov->donor[4 * (size_t)f + k];
+            if (d < 1 || d > ne) return fail(h, HP_E_ARG, "overset table: donor id out of range");
+            iv[(size_t)(1 + k) * nf + f] = h->perm[d - 1];
+            wv[(size_t)k * nf + f] = ov->weight[4 * (size_t)f + k];
+        }
+    }
+    cudaStream_t st = h->stream;
+    if (h->d_overset) {
+        CUDA_OK(h, cudaFreeAsync(h->d_overset, st));
+        h->d_overset = nullptr;
+    }
+    h->dm.nfringe = 0;
+    h->dm.fr = nullptr; h->dm.fdon = nullptr; h->dm.fw = nullptr;
+    if (nf > 0) {
+        const size_t ib = ((5 * (size_t)nf * sizeof(int)) + 255) & ~size_t(255);
+        CUDA_OK(h, cudaMallocAsync(&h->d_overset, ib + 4 * (size_t)nf * sizeof(double), st));
+        char* base = static_cast<char*>(h->d_overset);
+        CUDA_OK(h, cudaMemcpyAsync(base, iv.data(), iv.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        CUDA_OK(h, cudaMemcpyAsync(base + ib, wv.data(), wv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        h->dm.nfringe = nf;
+        h->dm.fr = reinterpret_cast<const int*>(base);
+        h->dm.fdon = reinterpret_cast<const int*>(base) + nf;
+        h->dm.fw = reinterpret_cast<const double*>(base + ib);
+    }
+    CUDA_OK(h, cudaStreamSynchronize(st));
+    // a captured step holds the mesh description it was launched with
+    if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    return HP_OK;
+}
+
 extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, int64_t* bytes) {
     if (!mesh || !params || !bytes || mesh->neles <= 0 || mesh->nghosts < 0) return HP_E_ARG;
     hp_handle probe_h;
@@ -1014,6 +1061,7 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
         int64_t n = 1 + 2 + (h->nghosts ? 1 : 0) + (h->prm.inviscid ? 0 : 1);
         int64_t per_stage = 1 + (h->nghosts ? 1 : 0) + (h->prm.myorder == 2 ? 1 : 0) + 1;
         if (h->aliased) per_stage += (h->prm.myorder == 2 ? 1 : 0) + 1;
+        if (h->dm.nfringe > 0) per_stage += 1;
         n += (int64_t)h->dp.nstage * per_stage + 3;
         if (h->aliased) n += 2;
         *kernels_per_step = n;

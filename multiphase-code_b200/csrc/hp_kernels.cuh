@@ -1656,6 +1656,27 @@ __global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevStat
 }
 
 // ---------------------------------------------------------------------------
+// Overset fringe cells take the barycentric combination of their four donor
+// cells' conserved state after every RK stage (table from hp_overset_build).
+// Donors are field cells, never fringe cells, so the updates are independent.
+__global__ void __launch_bounds__(256) k_overset(DevMesh m, DevState<R> s) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.nfringe) return;
+    const int n = m.nfringe;
+    const int i = ldg(m.fr + t);
+    const int d0 = ldg(m.fdon + t), d1 = ldg(m.fdon + n + t), d2 = ldg(m.fdon + 2 * n + t),
+              d3 = ldg(m.fdon + 3 * n + t);
+    const double w0 = ldg(m.fw + t), w1 = ldg(m.fw + n + t), w2 = ldg(m.fw + 2 * n + t), w3 = ldg(m.fw + 3 * n + t);
+    double v[10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+        const double* c = COL(s.cn, k);
+        v[k] = w0 * c[d0] + w1 * c[d1] + w2 * c[d2] + w3 * c[d3];
+    }
+#pragma unroll
+    for (int k = 0; k < 10; k++) COL(s.cn, k)[i] = v[k];
+}
+
 static inline unsigned grid_for(long long n, int block) {
     return (unsigned)((n + block - 1) / block);
 }
@@ -1724,6 +1745,10 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             k_flux_carry<<<1, 1, 0, st>>>(m, s, P);
         } else {
             k_flux4<<<g4, 128, 0, st>>>(m, s, P, stage);
+        }
+        if (m.nfringe > 0) {
+            MARK(KK_OVERSET);
+            k_overset<<<grid_for(m.nfringe, 256), 256, 0, st>>>(m, s);
         }
     }
     // src/main.F90:595-641: primitive, residual norms, cu = cn

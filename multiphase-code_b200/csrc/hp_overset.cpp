@@ -1,0 +1,285 @@
+// hp_overset.cpp -- overset fringe cells and donor tables of a two-block mesh.
+//
+// New work: the reference only freezes cells with iblank != 1
+// (src/sr_RK.F90:31); its hole cutting and donor search come from the TIOGA
+// library outside the solver.  Here the two blocks of an overset mesh
+// (block 0 background, block 1 component) are one element list, the caller's
+// hole cut marks background cells inside the component's body with
+// iblank = 0, and this file builds, once per mesh:
+//
+//   fringe  background field cells next to a hole cell and component field
+//           cells next to a ghost of the component's outer boundary type,
+//           plus layers - 1 further layers inward; they get iblank = -1 (no
+//           RK update of their own);
+//   donors  for each fringe cell with centroid x, the lowest-id field cell D
+//           of the other block whose tet contains x (barycentric coordinates
+//           >= -1e-10), or, if none does, the field cell of that block with
+//           the nearest centroid;
+//   weights the barycentric coordinates of x in a tet of four centroids
+//           among D, its field neighbours and theirs (two rings, face
+//           order): of the tets containing x, the one whose vertices are
+//           closest to x (least sum of squared distances); if none contains
+//           x, the one whose smallest coordinate is largest; or D alone.
+//
+// Every RK stage then sets a fringe cell's conserved state to
+// sum_k w_k cn(donor_k) (k_overset in hp_kernels.cuh).  A uniform grid over
+// the donor block's field tets limits the containment tests; it does not
+// change the result (every tet containing x is registered in x's grid cell,
+// and the lowest id among them is taken).  The arithmetic is the oracle's
+// (oracle/hydra_oracle.c), so the tables agree bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/hydraphase.h"
+
+namespace {
+
+inline double det3(double A11, double A21, double A31, double A12, double A22, double A32, double A13,
+                   double A23, double A33) {
+    return A11 * (A22 * A33 - A23 * A32) - A21 * (A12 * A33 - A13 * A32) + A31 * (A12 * A23 - A13 * A22);
+}
+// Fortran MIN of finite values
+inline double mn2(double a, double b) { return (b < a || a != a) ? b : a; }
+
+double bary(const double p0[3], const double p1[3], const double p2[3], const double p3[3], const double x[3],
+            double lam[4]) {
+    double a[3], b[3], c[3], d[3];
+    for (int k = 0; k < 3; k++) {
+        a[k] = p1[k] - p0[k]; b[k] = p2[k] - p0[k]; c[k] = p3[k] - p0[k]; d[k] = x[k] - p0[k];
+    }
+    double v = det3(a[0], a[1], a[2], b[0], b[1], b[2], c[0], c[1], c[2]);
+    if (v == 0.0) return 0.0;
+    double l1 = det3(d[0], d[1], d[2], b[0], b[1], b[2], c[0], c[1], c[2]) / v;
+    double l2 = det3(a[0], a[1], a[2], d[0], d[1], d[2], c[0], c[1], c[2]) / v;
+    double l3 = det3(a[0], a[1], a[2], b[0], b[1], b[2], d[0], d[1], d[2]) / v;
+    lam[0] = 1.0 - l1 - l2 - l3; lam[1] = l1; lam[2] = l2; lam[3] = l3;
+    return v;
+}
+
+struct Mesh {
+    const hp_mesh* m;
+    const int32_t* row(int e) const { return m->elem + 9 * (size_t)(e - 1); }
+    void node(int n, double p[3]) const { p[0] = m->x[n - 1]; p[1] = m->y[n - 1]; p[2] = m->z[n - 1]; }
+    void centroid(int e, double c[3]) const {
+        const int32_t* r = row(e);
+        const double* x = m->x; const double* y = m->y; const double* z = m->z;
+        c[0] = 0.25 * (x[r[0] - 1] + x[r[1] - 1] + x[r[2] - 1] + x[r[3] - 1]);
+        c[1] = 0.25 * (y[r[0] - 1] + y[r[1] - 1] + y[r[2] - 1] + y[r[3] - 1]);
+        c[2] = 0.25 * (z[r[0] - 1] + z[r[1] - 1] + z[r[2] - 1] + z[r[3] - 1]);
+    }
+};
+
+// Field tets of one block binned by bounding box (CSR lists, ascending ids).
+struct Grid {
+    double lo[3] = {0, 0, 0}, h = 1.0;
+    int n[3] = {1, 1, 1};
+    std::vector<int> start, items;
+    int idx(int d, double v) const {
+        double t = std::floor((v - lo[d]) / h);
+        if (!(t >= 0.0)) return 0;
+        return t >= n[d] - 1 ? n[d] - 1 : (int)t;
+    }
+    size_t cell(int i, int j, int k) const { return ((size_t)i * n[1] + j) * n[2] + k; }
+};
+
+void build_grid(const Mesh& M, const std::vector<int>& field, Grid& G) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int t : field)
+        for (int q = 0; q < 4; q++) {
+            double p[3];
+            M.node(M.row(t)[q], p);
+            for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], p[d]); hi[d] = std::max(hi[d], p[d]); }
+        }
+    double ext[3], vol = 1.0;
+    for (int d = 0; d < 3; d++) { ext[d] = std::max(hi[d] - lo[d], 1e-300); vol *= ext[d]; G.lo[d] = lo[d]; }
+    G.h = std::cbrt(vol / std::max<size_t>(field.size(), 1)) * 1.5;
+    if (!(G.h > 0.0)) G.h = 1.0;
+    for (int d = 0; d < 3; d++) G.n[d] = std::max(1, std::min(512, (int)(ext[d] / G.h) + 1));
+    const size_t ncell = (size_t)G.n[0] * G.n[1] * G.n[2];
+    std::vector<int> cnt(ncell + 1, 0);
+    auto span = [&](int t, int a[3], int b[3]) {
+        double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
+        for (int q = 0; q < 4; q++) {
+            double p[3];
+            M.node(M.row(t)[q], p);
+            for (int d = 0; d < 3; d++) { bl[d] = std::min(bl[d], p[d]); bh[d] = std::max(bh[d], p[d]); }
+        }
+        for (int d = 0; d < 3; d++) { a[d] = G.idx(d, bl[d]); b[d] = G.idx(d, bh[d]); }
+    };
+    for (int t : field) {
+        int a[3], b[3];
+        span(t, a, b);
+        for (int i = a[0]; i <= b[0]; i++)
+            for (int j = a[1]; j <= b[1]; j++)
+                for (int k = a[2]; k <= b[2]; k++) cnt[G.cell(i, j, k) + 1]++;
+    }
+    for (size_t c = 0; c < ncell; c++) cnt[c + 1] += cnt[c];
+    G.start = cnt;
+    G.items.assign(cnt[ncell], 0);
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int t : field) {
+        int a[3], b[3];
+        span(t, a, b);
+        for (int i = a[0]; i <= b[0]; i++)
+            for (int j = a[1]; j <= b[1]; j++)
+                for (int k = a[2]; k <= b[2]; k++) G.items[fill[G.cell(i, j, k)]++] = t;
+    }
+}
+
+}  // namespace
+
+// See include/hydraphase.h.
+extern "C" int hp_overset_build(const hp_mesh* mesh, const int32_t* block, int32_t layers, int32_t outer_type,
+                                int32_t* iblank_out, hp_overset* out) {
+    if (!mesh || !block || !iblank_out || !out || layers < 1 || mesh->neles <= 0 || mesh->nghosts < 0 ||
+        !mesh->elem || (mesh->nghosts && !mesh->ghost) || !mesh->x || !mesh->y || !mesh->z)
+        return HP_E_ARG;
+    std::memset(out, 0, sizeof *out);
+    const int neles = mesh->neles, nghosts = mesh->nghosts, ntot = neles + nghosts;
+    Mesh M{mesh};
+    for (int e = 1; e <= neles; e++) {
+        const int32_t* r = M.row(e);
+        for (int k = 0; k < 4; k++)
+            if (r[k] < 1 || r[k] > mesh->nodes || r[4 + k] < 1 || r[4 + k] > ntot) return HP_E_ARG;
+        if (block[e - 1] != 0 && block[e - 1] != 1) return HP_E_ARG;
+    }
+    std::vector<int> gtype(ntot + 2, 0), mark(neles + 1, 0);
+    for (int g = 0; g < nghosts; g++) {
+        int id = mesh->ghost[4 * g + 1];
+        if (id >= 1 && id <= ntot) gtype[id] = mesh->ghost[4 * g + 2];
+    }
+    for (int e = 1; e <= neles; e++) {
+        const int32_t* r = M.row(e);
+        if (r[8] != 1) continue;
+        for (int k = 0; k < 4; k++) {
+            int n = r[4 + k];
+            if ((block[e - 1] == 0 && n <= neles && M.row(n)[8] == 0) ||
+                (block[e - 1] == 1 && n > neles && gtype[n] == outer_type)) { mark[e] = 1; break; }
+        }
+    }
+    for (int l = 2; l <= layers; l++)
+        for (int e = 1; e <= neles; e++) {
+            const int32_t* r = M.row(e);
+            if (r[8] != 1 || mark[e]) continue;
+            for (int k = 0; k < 4; k++) {
+                int n = r[4 + k];
+                if (n <= neles && mark[n] == l - 1 && block[n - 1] == block[e - 1]) { mark[e] = l; break; }
+            }
+        }
+    std::vector<int> fr;
+    for (int e = 1; e <= neles; e++) {
+        iblank_out[e - 1] = mark[e] ? -1 : M.row(e)[8];
+        if (mark[e]) fr.push_back(e);
+    }
+    const int nf = (int)fr.size();
+    std::vector<int> field[2];
+    for (int e = 1; e <= neles; e++)
+        if (iblank_out[e - 1] == 1) field[block[e - 1]].push_back(e);
+    Grid G[2];
+    for (int b = 0; b < 2; b++)
+        if (!field[b].empty()) build_grid(M, field[b], G[b]);
+    out->nfringe = nf;
+    out->fringe = (int32_t*)std::malloc(sizeof(int32_t) * (size_t)(nf + 1));
+    out->donor = (int32_t*)std::malloc(sizeof(int32_t) * 4 * (size_t)(nf + 1));
+    out->weight = (double*)std::malloc(sizeof(double) * 4 * (size_t)(nf + 1));
+    if (!out->fringe || !out->donor || !out->weight) { hp_free_overset(out); return HP_E_NOMEM; }
+    std::vector<char> fell(nf, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int f = 0; f < nf; f++) {
+        const int e = fr[f], B = 1 - block[e - 1];
+        int32_t* dn = out->donor + 4 * (size_t)f;
+        double* w = out->weight + 4 * (size_t)f;
+        out->fringe[f] = e;
+        double xp[3];
+        M.centroid(e, xp);
+        int D = 0;
+        if (!field[B].empty()) {
+            const Grid& g = G[B];
+            const size_t c = g.cell(g.idx(0, xp[0]), g.idx(1, xp[1]), g.idx(2, xp[2]));
+            for (int it = g.start[c]; it < g.start[c + 1]; it++) {
+                const int t = g.items[it];
+                if (D && t > D) break;                 // lists are ascending
+                const int32_t* r = M.row(t);
+                double p[4][3], lam[4];
+                for (int q = 0; q < 4; q++) M.node(r[q], p[q]);
+                if (bary(p[0], p[1], p[2], p[3], xp, lam) == 0.0) continue;
+                if (lam[0] >= -1e-10 && lam[1] >= -1e-10 && lam[2] >= -1e-10 && lam[3] >= -1e-10) D = t;
+            }
+            if (!D) {   // nearest field centroid of the donor block
+                double best = 0.0;
+                for (int t : field[B]) {
+                    double cc[3];
+                    M.centroid(t, cc);
+                    double d2 = (cc[0] - xp[0]) * (cc[0] - xp[0]) + (cc[1] - xp[1]) * (cc[1] - xp[1]) +
+                                (cc[2] - xp[2]) * (cc[2] - xp[2]);
+                    if (!D || d2 < best) { best = d2; D = t; }
+                }
+                fell[f] = 1;
+            }
+        }
+        if (!D) {   // the other block has no field cell at all
+            dn[0] = dn[1] = dn[2] = dn[3] = e;
+            w[0] = 1.0; w[1] = w[2] = w[3] = 0.0;
+            fell[f] = 1;
+            continue;
+        }
+        dn[0] = dn[1] = dn[2] = dn[3] = D;
+        w[0] = 1.0; w[1] = w[2] = w[3] = 0.0;
+        int cand[17], m = 0;
+        cand[m++] = D;
+        for (int ring = 0, lo = 0; ring < 2; ring++) {
+            int hi = m;
+            for (int a = lo; a < hi; a++)
+                for (int k = 0; k < 4 && m < 17; k++) {
+                    int n = M.row(cand[a])[4 + k];
+                    if (n > neles || iblank_out[n - 1] != 1 || block[n - 1] != B) continue;
+                    bool seen = false;
+                    for (int q = 0; q < m; q++) seen |= (cand[q] == n);
+                    if (!seen) cand[m++] = n;
+                }
+            lo = hi;
+        }
+        double cc[17][3];
+        for (int a = 0; a < m; a++) M.centroid(cand[a], cc[a]);
+        double best_in = 0.0, best_out = -1.0e300;
+        bool have_in = false;
+        for (int i = 0; i < m; i++)
+            for (int j = i + 1; j < m; j++)
+                for (int k = j + 1; k < m; k++)
+                    for (int l = k + 1; l < m; l++) {
+                        double lam[4];
+                        if (bary(cc[i], cc[j], cc[k], cc[l], xp, lam) == 0.0) continue;
+                        const double sc = mn2(mn2(mn2(lam[0], lam[1]), lam[2]), lam[3]);
+                        const int id[4] = {i, j, k, l};
+                        if (sc >= -1e-12) {
+                            double s2 = 0.0;
+                            for (int q = 0; q < 4; q++)
+                                s2 = s2 + ((cc[id[q]][0] - xp[0]) * (cc[id[q]][0] - xp[0]) +
+                                           (cc[id[q]][1] - xp[1]) * (cc[id[q]][1] - xp[1]) +
+                                           (cc[id[q]][2] - xp[2]) * (cc[id[q]][2] - xp[2]));
+                            if (!have_in || s2 < best_in) {
+                                have_in = true; best_in = s2;
+                                for (int q = 0; q < 4; q++) { dn[q] = cand[id[q]]; w[q] = lam[q]; }
+                            }
+                        } else if (!have_in && sc > best_out) {
+                            best_out = sc;
+                            for (int q = 0; q < 4; q++) { dn[q] = cand[id[q]]; w[q] = lam[q]; }
+                        }
+                    }
+    }
+    out->nfallback = 0;
+    for (int f = 0; f < nf; f++) out->nfallback += fell[f];
+    return HP_OK;
+}
+
+extern "C" void hp_free_overset(hp_overset* ov) {
+    if (!ov) return;
+    std::free(ov->fringe);
+    std::free(ov->donor);
+    std::free(ov->weight);
+    ov->fringe = nullptr; ov->donor = nullptr; ov->weight = nullptr;
+    ov->nfringe = 0;
+}

@@ -47,6 +47,11 @@ class HpDiag(ctypes.Structure):
     _fields_ = [("time", _D), ("dt", _D), ("velmag", _D), ("diff", _D * 4), ("nan_cells", _D)]
 
 
+class HpOverset(ctypes.Structure):
+    _fields_ = [("nfringe", _I), ("fringe", ctypes.POINTER(_I)), ("donor", ctypes.POINTER(_I)),
+                ("weight", _DP), ("nfallback", _I)]
+
+
 class HydraError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
@@ -87,6 +92,11 @@ def lib():
     L.hp_get_state_case.argtypes = [vp, _I, _DP, _DP, _DP]
     L.hp_estimate_batch_bytes.argtypes = [ctypes.POINTER(HpMesh), _I, ctypes.POINTER(HpParams),
                                           ctypes.POINTER(ctypes.c_int64)]
+    L.hp_overset_build.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(_I), _I, _I, ctypes.POINTER(_I),
+                                   ctypes.POINTER(HpOverset)]
+    L.hp_free_overset.argtypes = [ctypes.POINTER(HpOverset)]
+    L.hp_free_overset.restype = None
+    L.hp_set_overset.argtypes = [vp, ctypes.POINTER(HpOverset)]
     L.hp_estimate_bytes.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(HpParams), ctypes.POINTER(ctypes.c_int64)]
     L.hp_poll.argtypes = [vp, ctypes.POINTER(_I)]
     L.hp_dt_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _I,
@@ -99,7 +109,7 @@ def lib():
     for fn in ("hp_create", "hp_destroy", "hp_init_uniform", "hp_set_state", "hp_step", "hp_sync",
                "hp_step_timed", "hp_profile_steps", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll",
                "hp_create_batch", "hp_case_count", "hp_set_state_case", "hp_get_state_case",
-               "hp_estimate_batch_bytes",
+               "hp_estimate_batch_bytes", "hp_overset_build", "hp_set_overset",
                "hp_get_state", "hp_get_prims", "hp_device_state", "hp_info", "hp_read_flow",
                "hp_read_mesh", "hp_read_restart", "hp_write_restart"):
         getattr(L, fn).restype = ctypes.c_int
@@ -108,13 +118,14 @@ def lib():
 
 
 KERNEL_KINDS = ("prim_start", "step_begin", "smooth1", "smooth2", "bc_visc", "visc", "prim_stage",
-                "bc", "grad", "flux", "prim_end", "step_end", "serial")
+                "bc", "grad", "flux", "prim_end", "step_end", "serial", "overset")
 
 EXPORTED_SYMBOLS = (
     "hp_create", "hp_destroy", "hp_last_error", "hp_create_error", "hp_init_uniform",
     "hp_set_state", "hp_step", "hp_sync", "hp_step_timed", "hp_profile_steps", "hp_get_state", "hp_get_prims", "hp_device_state",
     "hp_info", "hp_read_flow", "hp_read_mesh", "hp_free_mesh", "hp_read_restart",
     "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll", "hp_create_batch", "hp_case_count",
-    "hp_set_state_case", "hp_get_state_case", "hp_estimate_batch_bytes",
+    "hp_set_state_case", "hp_get_state_case", "hp_estimate_batch_bytes", "hp_overset_build", "hp_free_overset",
+    "hp_set_overset",
 )
 NOALLOC_MAX_CELLS = 1 << 24

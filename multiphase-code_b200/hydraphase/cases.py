@@ -288,6 +288,15 @@ def cylinder(nr=160, nt=256, nz=20, ndrop=32, seed=1, mach=0.3, re_d=150.0, t_in
     Re_D through the Sutherland constant, isothermal no-slip wall at the
     free-stream temperature, far field outside."""
     b = ogrid_mesh(nr, nt, nz, seed=seed)
+    return _cylinder_flow(b, "cylinder", ndrop=ndrop, seed=seed, mach=mach, re_d=re_d, t_inf=t_inf, p_inf=p_inf,
+                          pinf=pinf, gamap=gamap, cpp=cpp, drop_r=drop_r, alpha_w_drop=alpha_w_drop,
+                          alpha_w_bg=alpha_w_bg)
+
+
+def _cylinder_flow(b: Built, name, ndrop=32, seed=1, mach=0.3, re_d=150.0, t_inf=288.15, p_inf=101325.0,
+                   pinf=6.0e8, gamap=4.4, cpp=4186.0, drop_r=0.1, alpha_w_drop=1.0 - 1e-6,
+                   alpha_w_bg=1e-6) -> CaseSpec:
+    """Initial state and parameters of the cylinder flow on mesh b."""
     gamag = 1.4
     a_inf = np.sqrt(gamag * R_GAS * t_inf)
     U = mach * a_inf
@@ -318,7 +327,73 @@ def cylinder(nr=160, nt=256, nz=20, ndrop=32, seed=1, mach=0.3, re_d=150.0, t_in
                 cfl=0.5, niter=1, itersub=1000, istart=1, diap=1.0e-4, surfacetension=0.0, myflux=2,
                 myorder=2, as_=as_, ts=ts)
     extra = dict(venkat_k=5.0, rk_scheme=1, inviscid=0, twall=t_inf)
-    return CaseSpec("cylinder", b.mesh, flow, cu, gp, 1000, extra)
+    return CaseSpec(name, b.mesh, flow, cu, gp, 1000, extra)
+
+
+def union_mesh(a: Built, b: Built) -> tuple[Built, np.ndarray]:
+    """One element list of two meshes: a's elements, then b's; ghosts of a,
+    then of b, all after the elements (so no ghost id aliases an element id,
+    unlike meshes merged without ghost offsets).  Returns the union and the
+    block of each element (0 for a, 1 for b)."""
+    ma, mb = a.mesh, b.mesh
+    ea, eb, ga = ma.neles, mb.neles, ma.nghosts
+    E = ea + eb
+
+    def remap(nc, ne_own, eoff, goff):
+        out = nc.astype(np.int64).copy()
+        el = nc <= ne_own
+        out[el] = nc[el] + eoff
+        out[~el] = E + goff + (nc[~el] - ne_own)
+        return out
+
+    el_a, el_b = ma.elem.copy(), mb.elem.copy()
+    el_b[:, 0:4] += ma.nodes
+    el_a[:, 4:8] = remap(ma.elem[:, 4:8], ea, 0, 0)
+    el_b[:, 4:8] = remap(mb.elem[:, 4:8], eb, ea, ga)
+    gh_a, gh_b = ma.ghost.copy(), mb.ghost.copy()
+    gh_a[:, 1] = E + (ma.ghost[:, 1] - ea)
+    gh_b[:, 0] += ea
+    gh_b[:, 1] = E + ga + (mb.ghost[:, 1] - eb)
+    mesh = MeshArrays(np.concatenate([ma.x, mb.x]), np.concatenate([ma.y, mb.y]), np.concatenate([ma.z, mb.z]),
+                      np.concatenate([el_a, el_b]).astype(np.int32), np.concatenate([gh_a, gh_b]).astype(np.int32))
+    block = np.concatenate([np.zeros(ea, np.int32), np.ones(eb, np.int32)])
+    return Built(mesh, np.concatenate([a.xc, b.xc]), np.concatenate([a.vol, b.vol])), block
+
+
+@dataclass
+class OversetSpec:
+    """An overset case: the union mesh with the hole cut as iblank 0, the
+    block of each element and the component's outer boundary type."""
+    spec: CaseSpec
+    block: np.ndarray
+    outer_type: int
+    layers: int
+
+
+def overset_cylinder(bg=(200, 120, 20), comp=(96, 256, 20), hole_r=1.2, comp_r_out=3.0, layers=2, seed=1,
+                     box=((-10.0, -12.0, 0.0), (30.0, 12.0, 4.0)), **flow_kw) -> OversetSpec:
+    """Overset cylinder: a background box of bg hexes on [-10,30]x[-12,12]x[0,4]
+    (6 tets each; far field on its x/y faces, symmetry 53 on z; `box` moves
+    its corners, the span must stay [0, 4]) and an O-grid
+    component of comp = (radial, azimuthal, spanwise) hexes around the
+    cylinder (D = 1) out to comp_r_out; background cells whose centroid lies
+    within hole_r of the cylinder axis are holes (iblank 0).  Flow as in
+    cylinder() (Mach 0.3, Re_D 150, droplets)."""
+    nx, ny, nz = bg
+
+    def bg_types(fc):
+        t = np.full(fc.shape[0], 7)
+        t[(fc[:, 2] < 1e-9) | (fc[:, 2] > 4.0 - 1e-9)] = 53
+        return t
+
+    a = box_mesh(nx, ny, nz, lo=box[0], hi=box[1], seed=seed, bc_type=bg_types)
+    nr, nt, nzc = comp
+    b = ogrid_mesh(nr, nt, nzc, r_in=0.5, r_out=comp_r_out, dr0=0.005, seed=seed + 1)
+    u, block = union_mesh(a, b)
+    hole = (block == 0) & (np.hypot(u.xc[:, 0], u.xc[:, 1]) < hole_r)
+    u.mesh.elem[hole, 8] = 0
+    spec = _cylinder_flow(u, "overset_cylinder", seed=seed, **flow_kw)
+    return OversetSpec(spec, block, 7, layers)
 
 
 # ---------------------------------------------------------------------------

@@ -14,7 +14,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import (KERNEL_KINDS, HpDiag, HpMesh, HpParams, HydraError, PREC_FP64_PARITY, lib)
+from ._lib import (KERNEL_KINDS, HpDiag, HpMesh, HpOverset, HpParams, HydraError, PREC_FP64_PARITY, lib)
 
 FLOW_FIELDS = (
     "pmax", "pmin", "tgmax", "tgmin", "ugmax", "ugmin", "vgmax", "vgmin", "wgmax", "wgmin",
@@ -85,6 +85,37 @@ def _hp_mesh(mesh: MeshArrays, keep: list) -> HpMesh:
     keep.extend(arrs)
     x, y, z, el, gh = arrs
     return HpMesh(mesh.nodes, mesh.neles, mesh.nghosts, 0, _dp(x), _dp(y), _dp(z), _ip(el), _ip(gh))
+
+
+@dataclass
+class OversetTable:
+    """Fringe cells (1-based element ids), their four donors and barycentric
+    weights, as hp_overset_build returns them."""
+    fringe: np.ndarray      # (nf,) int32
+    donor: np.ndarray       # (nf, 4) int32
+    weight: np.ndarray      # (nf, 4) float64
+    nfallback: int
+
+
+def overset_build(mesh: MeshArrays, block, layers: int = 2, outer_type: int = 7):
+    """Fringe and donor tables of a two-block overset mesh (block[e] = 0
+    background, 1 component; holes as iblank 0).  Returns (iblank, table):
+    iblank marks the fringe with -1 and goes into the mesh given to Case."""
+    keep = []
+    hm = _hp_mesh(mesh, keep)
+    bl = np.ascontiguousarray(block, np.int32)
+    ib = np.zeros(mesh.neles, np.int32)
+    ov = HpOverset()
+    _check(lib().hp_overset_build(ctypes.byref(hm), _ip(bl), int(layers), int(outer_type), _ip(ib),
+                                  ctypes.byref(ov)))
+    try:
+        n = ov.nfringe
+        fr = np.ctypeslib.as_array(ov.fringe, (n,)).copy() if n else np.zeros(0, np.int32)
+        dn = np.ctypeslib.as_array(ov.donor, (n * 4,)).reshape(n, 4).copy() if n else np.zeros((0, 4), np.int32)
+        w = np.ctypeslib.as_array(ov.weight, (n * 4,)).reshape(n, 4).copy() if n else np.zeros((0, 4))
+        return ib, OversetTable(fr, dn, w, int(ov.nfallback))
+    finally:
+        lib().hp_free_overset(ctypes.byref(ov))
 
 
 def estimate_batch_bytes(meshes, params: HpParams) -> int:
@@ -162,6 +193,14 @@ class Case:
 
     def sync(self):
         _check(self.L.hp_sync(self.h), self.h)
+
+    def set_overset(self, table: "OversetTable"):
+        """Interpolate the fringe cells from their donors after every RK stage."""
+        fr = np.ascontiguousarray(table.fringe, np.int32)
+        dn = np.ascontiguousarray(table.donor, np.int32).reshape(-1)
+        w = np.ascontiguousarray(table.weight, np.float64).reshape(-1)
+        ov = HpOverset(int(fr.size), _ip(fr), _ip(dn), _dp(w), int(table.nfallback))
+        _check(self.L.hp_set_overset(self.h, ctypes.byref(ov)), self.h)
 
     def poll(self) -> bool:
         """True while steps queued on this case's stream are still running."""

@@ -49,6 +49,9 @@ struct or_case {
     int total;
     double fstar[10];                        /* stale HLLC flux carry */
     int aliased;                             /* ghost ids alias elements/each other */
+    int nfringe;                             /* overset fringe cells (0: none) */
+    int *ofr, *odon;                         /* [nfringe], [4*nfringe] 1-based */
+    double *ow;                              /* [4*nfringe] */
 };
 
 /* Cell loops run in parallel only when the result cannot depend on the
@@ -296,6 +299,7 @@ void or_destroy(or_case *S) {
     free(S->rhs); free(S->d24);
     for (int k = 0; k < 8; k++) free(S->vis[k]);
     for (int k = 0; k < NGRAD; k++) free(S->g[k]);
+    free(S->ofr); free(S->odon); free(S->ow);
     free(S);
 }
 
@@ -1186,12 +1190,15 @@ static void stage(or_case *S, int st) {
     }
 }
 
+static void overset_apply(or_case *S);
+
 static void rk(or_case *S) {
     or_viscous(S);
     int nst = S->p.rk_scheme == 0 ? 4 : 3;
     for (int st = 1; st <= nst; st++) {
         or_flux(S);
         stage(S, st);
+        if (S->nfringe) overset_apply(S);
     }
 }
 
@@ -1297,4 +1304,184 @@ void or_get_grad(const or_case *S, double *out) {
     for (int v = 0; v < NGRAD; v++)
         memcpy(out + (size_t)v * S->ntot, S->g[v] + 1, sizeof(double) * S->ntot);
     memcpy(out + (size_t)NGRAD * S->ntot, S->phi + 1, sizeof(double) * S->ntot);
+}
+
+/* ------------------------------------------------------------------ */
+/* Overset fringe interpolation.  New work: the reference only freezes
+ * cells with iblank != 1 (src/sr_RK.F90:31; its hole cutting comes from
+ * TIOGA, outside the path).  Test infrastructure: the library's own
+ * hp_overset_build (csrc/hp_overset.cpp) and the device interpolation are
+ * checked against this restatement of the same rules.
+ *
+ * Fringe: background (block 0) field cells next to a hole cell (iblank 0),
+ * component (block 1) field cells next to a ghost of type outer_type, then
+ * `layers - 1` further layers of field cells of the same block next to the
+ * previous layer; fringe cells get iblank -1.
+ * Donor cell D of a fringe cell with centroid x: the lowest-id field cell of
+ * the other block whose tet contains x (barycentric coordinates >= -1e-10);
+ * if none does, the field cell of that block with the nearest centroid.
+ * Weights: barycentric coordinates of x in a tet spanned by four centroids
+ * among D, its field neighbours and theirs (two rings, face order): of the
+ * tets that contain x (coordinates >= -1e-12), the one whose vertices are
+ * closest to x (least sum of squared distances); if none contains x, the one
+ * whose smallest coordinate is largest; D alone (weight 1) without any tet.
+ * Every RK stage then sets cn of each fringe cell to sum_k w_k cn(donor_k). */
+static double ov_bary(const double p0[3], const double p1[3], const double p2[3], const double p3[3],
+                      const double x[3], double lam[4]) {
+    double a[3], b[3], c[3], d[3];
+    for (int k = 0; k < 3; k++) {
+        a[k] = p1[k] - p0[k]; b[k] = p2[k] - p0[k]; c[k] = p3[k] - p0[k]; d[k] = x[k] - p0[k];
+    }
+    double v = det(a[0], a[1], a[2], b[0], b[1], b[2], c[0], c[1], c[2]);
+    if (v == 0.0) return 0.0;
+    double l1 = det(d[0], d[1], d[2], b[0], b[1], b[2], c[0], c[1], c[2]) / v;
+    double l2 = det(a[0], a[1], a[2], d[0], d[1], d[2], c[0], c[1], c[2]) / v;
+    double l3 = det(a[0], a[1], a[2], b[0], b[1], b[2], d[0], d[1], d[2]) / v;
+    lam[0] = 1.0 - l1 - l2 - l3; lam[1] = l1; lam[2] = l2; lam[3] = l3;
+    return v;
+}
+
+static void ov_centroid(const double *x, const double *y, const double *z, const int32_t *r, double c[3]) {
+    c[0] = 0.25 * (x[r[0] - 1] + x[r[1] - 1] + x[r[2] - 1] + x[r[3] - 1]);
+    c[1] = 0.25 * (y[r[0] - 1] + y[r[1] - 1] + y[r[2] - 1] + y[r[3] - 1]);
+    c[2] = 0.25 * (z[r[0] - 1] + z[r[1] - 1] + z[r[2] - 1] + z[r[3] - 1]);
+}
+
+int or_overset_build(int32_t nodes, int32_t neles, int32_t nghosts, const double *x, const double *y,
+                     const double *z, const int32_t *elem, const int32_t *ghost, const int32_t *block,
+                     int32_t layers, int32_t outer_type, int32_t *iblank_out, int32_t *nfringe,
+                     int32_t *fringe, int32_t *donor, double *weight, int32_t *nfallback) {
+    (void)nodes;
+    const int ntot = neles + nghosts;
+    int *gtype = ialloc(ntot + 2), *mark = ialloc(neles + 1);
+    for (int g = 0; g < nghosts; g++) {
+        int id = ghost[4 * g + 1];
+        if (id >= 1 && id <= ntot) gtype[id] = ghost[4 * g + 2];
+    }
+#define ROW(e) (elem + 9 * (size_t)((e) - 1))
+    for (int e = 1; e <= neles; e++) {
+        const int32_t *r = ROW(e);
+        if (r[8] != 1) continue;
+        for (int k = 0; k < 4; k++) {
+            int n = r[4 + k];
+            if ((block[e - 1] == 0 && n <= neles && ROW(n)[8] == 0) ||
+                (block[e - 1] == 1 && n > neles && gtype[n] == outer_type)) { mark[e] = 1; break; }
+        }
+    }
+    for (int l = 2; l <= layers; l++)
+        for (int e = 1; e <= neles; e++) {
+            const int32_t *r = ROW(e);
+            if (r[8] != 1 || mark[e]) continue;
+            for (int k = 0; k < 4; k++) {
+                int n = r[4 + k];
+                if (n <= neles && mark[n] == l - 1 && block[n - 1] == block[e - 1]) { mark[e] = l; break; }
+            }
+        }
+    int nf = 0, nfb = 0;
+    for (int e = 1; e <= neles; e++) {
+        iblank_out[e - 1] = mark[e] ? -1 : ROW(e)[8];
+        if (mark[e]) fringe[nf++] = e;
+    }
+    for (int f = 0; f < nf; f++) {
+        const int e = fringe[f], B = 1 - block[e - 1];
+        double xp[3];
+        ov_centroid(x, y, z, ROW(e), xp);
+        int D = 0;
+        for (int t = 1; t <= neles && !D; t++) {
+            if (iblank_out[t - 1] != 1 || block[t - 1] != B) continue;
+            const int32_t *r = ROW(t);
+            double p[4][3], lam[4];
+            for (int k = 0; k < 4; k++) { p[k][0] = x[r[k] - 1]; p[k][1] = y[r[k] - 1]; p[k][2] = z[r[k] - 1]; }
+            if (ov_bary(p[0], p[1], p[2], p[3], xp, lam) == 0.0) continue;
+            if (lam[0] >= -1e-10 && lam[1] >= -1e-10 && lam[2] >= -1e-10 && lam[3] >= -1e-10) D = t;
+        }
+        if (!D) {
+            double best = 0.0;
+            for (int t = 1; t <= neles; t++) {
+                if (iblank_out[t - 1] != 1 || block[t - 1] != B) continue;
+                double c[3];
+                ov_centroid(x, y, z, ROW(t), c);
+                double d2 = (c[0] - xp[0]) * (c[0] - xp[0]) + (c[1] - xp[1]) * (c[1] - xp[1]) +
+                            (c[2] - xp[2]) * (c[2] - xp[2]);
+                if (!D || d2 < best) { best = d2; D = t; }
+            }
+            nfb++;
+        }
+        int *dn = donor + 4 * (size_t)f;
+        double *w = weight + 4 * (size_t)f;
+        dn[0] = dn[1] = dn[2] = dn[3] = D;
+        w[0] = 1.0; w[1] = w[2] = w[3] = 0.0;
+        if (!D) { dn[0] = dn[1] = dn[2] = dn[3] = e; continue; }   /* no field cell at all */
+        /* candidates: D, its field neighbours, theirs (two rings, face order) */
+        int cand[17], m = 0;
+        cand[m++] = D;
+        for (int ring = 0, lo = 0; ring < 2; ring++) {
+            int hi = m;
+            for (int a = lo; a < hi; a++)
+                for (int k = 0; k < 4 && m < 17; k++) {
+                    int n = ROW(cand[a])[4 + k];
+                    if (n > neles || iblank_out[n - 1] != 1 || block[n - 1] != B) continue;
+                    int seen = 0;
+                    for (int q = 0; q < m; q++) seen |= (cand[q] == n);
+                    if (!seen) cand[m++] = n;
+                }
+            lo = hi;
+        }
+        double cc[17][3];
+        for (int a = 0; a < m; a++) ov_centroid(x, y, z, ROW(cand[a]), cc[a]);
+        /* the containing tet (coordinates >= -1e-12) whose vertices are
+         * closest to x (sum of squared distances); none containing x: the
+         * tet whose smallest coordinate is largest */
+        double best_in = 0.0, best_out = -1.0e300;
+        int have_in = 0;
+        for (int i = 0; i < m; i++)
+            for (int j = i + 1; j < m; j++)
+                for (int k = j + 1; k < m; k++)
+                    for (int l = k + 1; l < m; l++) {
+                        double lam[4];
+                        if (ov_bary(cc[i], cc[j], cc[k], cc[l], xp, lam) == 0.0) continue;
+                        double sc = mn4(lam[0], lam[1], lam[2], lam[3]);
+                        const int id[4] = {i, j, k, l};
+                        if (sc >= -1e-12) {
+                            double s2 = 0.0;
+                            for (int q = 0; q < 4; q++)
+                                s2 = s2 + ((cc[id[q]][0] - xp[0]) * (cc[id[q]][0] - xp[0]) +
+                                           (cc[id[q]][1] - xp[1]) * (cc[id[q]][1] - xp[1]) +
+                                           (cc[id[q]][2] - xp[2]) * (cc[id[q]][2] - xp[2]));
+                            if (!have_in || s2 < best_in) {
+                                have_in = 1; best_in = s2;
+                                for (int q = 0; q < 4; q++) { dn[q] = cand[id[q]]; w[q] = lam[q]; }
+                            }
+                        } else if (!have_in && sc > best_out) {
+                            best_out = sc;
+                            for (int q = 0; q < 4; q++) { dn[q] = cand[id[q]]; w[q] = lam[q]; }
+                        }
+                    }
+    }
+#undef ROW
+    *nfringe = nf;
+    if (nfallback) *nfallback = nfb;
+    free(gtype); free(mark);
+    return 0;
+}
+
+void or_set_overset(or_case *S, int32_t nfringe, const int32_t *fringe, const int32_t *donor,
+                    const double *weight) {
+    free(S->ofr); free(S->odon); free(S->ow);
+    S->nfringe = nfringe;
+    S->ofr = ialloc(nfringe + 1); S->odon = ialloc(4 * (size_t)nfringe + 1);
+    S->ow = dalloc(4 * (size_t)nfringe + 1);
+    memcpy(S->ofr, fringe, sizeof(int) * (size_t)nfringe);
+    memcpy(S->odon, donor, sizeof(int) * 4 * (size_t)nfringe);
+    memcpy(S->ow, weight, sizeof(double) * 4 * (size_t)nfringe);
+}
+
+static void overset_apply(or_case *S) {
+    for (int f = 0; f < S->nfringe; f++) {
+        const int i = S->ofr[f];
+        const int *d = S->odon + 4 * (size_t)f;
+        const double *w = S->ow + 4 * (size_t)f;
+        for (int j = 1; j <= NEQ; j++)
+            CN(i, j) = w[0] * CN(d[0], j) + w[1] * CN(d[1], j) + w[2] * CN(d[2], j) + w[3] * CN(d[3], j);
+    }
 }

@@ -104,6 +104,15 @@ void or_viscous(or_case *c);
 void or_flux(or_case *c);
 void or_set_dt(or_case *c, double dt);
 
+/* Overset fringe tables (rules in hydra_oracle.c); output arrays hold neles
+ * entries (fringe), 4*neles (donor, weight) and neles (iblank_out). */
+int or_overset_build(int32_t nodes, int32_t neles, int32_t nghosts, const double *x, const double *y,
+                     const double *z, const int32_t *elem, const int32_t *ghost, const int32_t *block,
+                     int32_t layers, int32_t outer_type, int32_t *iblank_out, int32_t *nfringe,
+                     int32_t *fringe, int32_t *donor, double *weight, int32_t *nfallback);
+void or_set_overset(or_case *c, int32_t nfringe, const int32_t *fringe, const int32_t *donor,
+                    const double *weight);
+
 #ifdef __cplusplus
 }
 #endif

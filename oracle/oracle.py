@@ -233,6 +233,11 @@ def lib():
             getattr(L, fn).argtypes = [ctypes.c_void_p]
         L.or_set_dt.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.or_set_threads.argtypes = [ctypes.c_int]
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        L.or_overset_build.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, dp, dp, dp, ip, ip, ip,
+                                       ctypes.c_int32, ctypes.c_int32, ip, i32p, ip, ip, dp, i32p]
+        L.or_overset_build.restype = ctypes.c_int
+        L.or_set_overset.argtypes = [ctypes.c_void_p, ctypes.c_int32, ip, ip, dp]
     return _lib
 
 
@@ -247,6 +252,27 @@ def _dp(a):
 
 def _ip(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def overset_build(mesh: Mesh, block, layers: int, outer_type: int):
+    """Fringe cells, donors and weights of a two-block overset mesh, by the
+    oracle's restatement of the rules; returns (iblank, fringe (1-based),
+    donor (nf, 4), weight (nf, 4), nfallback)."""
+    ne = mesh.neles
+    keep = [np.ascontiguousarray(mesh.x, np.float64), np.ascontiguousarray(mesh.y, np.float64),
+            np.ascontiguousarray(mesh.z, np.float64), np.ascontiguousarray(mesh.elem, np.int32),
+            np.ascontiguousarray(mesh.ghost, np.int32), np.ascontiguousarray(block, np.int32)]
+    ib = np.zeros(ne, np.int32)
+    fr = np.zeros(ne, np.int32)
+    dn = np.zeros(4 * ne, np.int32)
+    w = np.zeros(4 * ne, np.float64)
+    nf, nfb = ctypes.c_int32(), ctypes.c_int32()
+    x, y, z, el, gh, bl = keep
+    lib().or_overset_build(mesh.nodes, ne, mesh.nghosts, _dp(x), _dp(y), _dp(z), _ip(el), _ip(gh), _ip(bl),
+                           int(layers), int(outer_type), _ip(ib), ctypes.byref(nf), _ip(fr), _ip(dn), _dp(w),
+                           ctypes.byref(nfb))
+    n = nf.value
+    return ib, fr[:n].copy(), dn[:4 * n].reshape(n, 4).copy(), w[:4 * n].reshape(n, 4).copy(), nfb.value
 
 
 class Oracle:
@@ -338,3 +364,10 @@ class Oracle:
 
     def set_dt(self, dt: float):
         self.L.or_set_dt(self.h, float(dt))
+
+    def set_overset(self, fringe, donor, weight):
+        """Fringe table applied after every RK stage (see overset_build)."""
+        self._ov = [np.ascontiguousarray(fringe, np.int32), np.ascontiguousarray(donor, np.int32).ravel(),
+                    np.ascontiguousarray(weight, np.float64).ravel()]
+        f, d, w = self._ov
+        self.L.or_set_overset(self.h, f.size, _ip(f), _ip(d), _dp(w))
