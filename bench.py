@@ -231,7 +231,8 @@ def serving_measure(n_cases: int, steps: int):
     reqs = cases.serving_stream(n_cases=n_cases, steps=steps)
     gen_s = time.perf_counter() - t0
     out = {"workload": f"shock-bubble stream: {n_cases} cases, cells log-U[6000, 400000], Poisson 40/s, "
-                       f"{steps} SSP-RK3 steps each, CFL 0.1, HBM budget 150 GiB",
+                       f"{steps} SSP-RK3 steps each, CFL 0.05, HBM budget 150 GiB; time-to-solution "
+                       f"from arrival to the final state on the host",
            "cells_total": int(sum(r.spec.mesh.neles for r in reqs)), "generation_s": round(gen_s, 2)}
     for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64_PARITY)):
         blocks = {}
@@ -240,9 +241,47 @@ def serving_measure(n_cases: int, steps: int):
             if cls not in blocks:
                 blocks[cls] = tune.tune_block_size(r.spec, precision=prec, steps=4)[0]
         rep_ = Server(150 << 30, precision=prec, max_active=16, chunk=25, batch_cells=200000,
-                      block_size=blocks, keep_state=False).run(reqs)
+                      block_size=blocks, keep_state=True).run(reqs)
         out[name] = {**rep_.summary(), "block_size": blocks}
     out["speedup_mixed_vs_fp64"] = out["mixed"]["updates_per_s"] / out["fp64"]["updates_per_s"]
+    return out
+
+
+def overset_measure(steps: int):
+    """The overset cylinder (background 200x120x20 hexes on [-10,30]x[-12,12]
+    x[0,4], O-grid component 96x256x20 to r = 3D, hole r < 1.2D, two fringe
+    layers): device-timed steps of the FP64 parity and the mixed variant with
+    the fringe interpolated from its donors after every RK stage."""
+    from hydraphase import PREC_FP64_PARITY, PREC_MIXED, Case, cases
+    from hydraphase.engine import MeshArrays, overset_build
+    t0 = time.perf_counter()
+    ov = cases.overset_cylinder(alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+    m = ov.spec.mesh
+    t1 = time.perf_counter()
+    ib, tab = overset_build(m, ov.block, ov.layers, ov.outer_type)
+    t2 = time.perf_counter()
+    el = m.elem.copy()
+    el[:, 8] = ib
+    mesh = MeshArrays(m.x, m.y, m.z, el, m.ghost)
+    out = {"workload": "overset cylinder: background 200x120x20 + O-grid 96x256x20 hexes (6 tets each), "
+                       "hole r < 1.2D, 2 fringe layers, SSP-RK3, viscous",
+           "cells": m.neles, "holes": int((m.elem[:, 8] == 0).sum()), "fringe": int(tab.fringe.size),
+           "donor_fallbacks": int(tab.nfallback), "table_build_s": round(t2 - t1, 2),
+           "mesh_generation_s": round(t1 - t0, 2)}
+    states = {}
+    for name, prec in (("fp64", PREC_FP64_PARITY), ("mixed", PREC_MIXED)):
+        with Case(mesh, ov.spec.params(precision=prec)) as c:
+            c.set_state(0.0, ov.spec.cu, ov.spec.ghost_prims)
+            c.set_overset(tab)
+            c.step(3, diagnostics=False)
+            ms = c.step_timed(steps)
+            pr = c.profile(1)
+            share = pr["ms"][pr["kinds"].index("overset")] / sum(pr["ms"])
+            _, states[name], _ = c.state()
+        out[name] = {"value": m.neles * 3 * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                     "overset_kernel_share": share}
+    out["mixed_rel_l2_vs_fp64"] = accuracy(states["mixed"], states["fp64"], ov.spec.flow)
+    out["unit"] = UNIT
     return out
 
 
@@ -371,6 +410,8 @@ def run_ours(args, world, rank, local, pg):
     }
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_oracle_sample(args.workload, os.cpu_count() or 1)
+    if world == 1 and rank == 0 and not args.no_overset:
+        line["overset"] = overset_measure(max(args.steps // 2, 5))
     if world == 1 and rank == 0 and args.serving_cases > 0:
         sv = serving_measure(args.serving_cases, args.serving_steps)
         sv["mixed_served_vs_plain_fp64_value"] = sv["mixed"]["updates_per_s"] / value
@@ -391,6 +432,7 @@ def main():
     ap.add_argument("--serving-cases", type=int, default=48,
                     help="cases of the serving stream measured after the step benchmark (0: skip)")
     ap.add_argument("--serving-steps", type=int, default=500)
+    ap.add_argument("--no-overset", action="store_true", help="skip the overset cylinder measurement")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     try:

@@ -60,6 +60,11 @@ class CaseResult:
     error: str | None = None  # set-up failure (e.g. HP_E_NOMEM), no result
 
     @property
+    def nan_cells(self) -> int:
+        """Cells whose final state holds a NaN (-1 without a kept state)."""
+        return -1 if self.cu is None else int(np.isnan(self.cu).any(axis=0).sum())
+
+    @property
     def latency(self) -> float:
         return self.finished - self.arrival
 
@@ -87,6 +92,7 @@ class ServeReport:
         lat = np.array([r.latency for r in ok]) if ok else np.zeros(1)
         upd = sum(r.cells * 3 * r.steps for r in ok)
         return {"cases": len(ok), "failed": len(self.results) - len(ok), "units": self.units,
+                "cases_with_nan": sum(1 for r in ok if r.nan_cells > 0),
                 "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                 "mean_s": float(lat.mean()), "makespan_s": self.makespan,
                 "updates_per_s": upd / self.makespan if self.makespan else 0.0,
