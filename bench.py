@@ -127,7 +127,10 @@ def workload_config(spec, name):
             "l2_policy": "state larger than L2 (about 10 GB resident per replica)"}
 
 
-def dist_setup():
+def dist_setup(backend: str):
+    """Process group of a torchrun launch (None for one process).  The
+    reference arm uses gloo (no device data crosses ranks); the CUDA arm
+    uses nccl unless BENCH_BACKEND says otherwise."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -136,8 +139,7 @@ def dist_setup():
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group(backend="nccl" if os.environ.get("BENCH_BACKEND", "nccl") == "nccl" else "gloo",
-                                timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
 
@@ -434,7 +436,8 @@ def main():
     ap.add_argument("--serving-steps", type=int, default=500)
     ap.add_argument("--no-overset", action="store_true", help="skip the overset cylinder measurement")
     args = ap.parse_args()
-    world, rank, local, pg = dist_setup()
+    backend = "gloo" if args.impl == "reference" else os.environ.get("BENCH_BACKEND", "nccl")
+    world, rank, local, pg = dist_setup(backend)
     try:
         if args.impl == "reference":
             rc = run_reference_arm(args, world, rank, pg)
