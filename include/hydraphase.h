@@ -40,8 +40,11 @@ enum {
 enum {
     HP_PREC_FP64_PARITY = 0, /* FP64, no FMA contraction: bit-parity path */
     HP_PREC_FP64 = 1,        /* FP64 with FMA */
-    HP_PREC_MIXED = 2        /* FP32 gradients/limiter/fluxes, FP64 state,
+    HP_PREC_MIXED = 2,       /* FP32 gradients/limiter/fluxes, FP64 state,
                                 EOS recovery and reductions */
+    HP_PREC_FP32 = 3         /* everything FP32, state path included: the
+                                precision-stress reference (ghost fill and
+                                diagnostics stay FP64) */
 };
 
 /* flow.in in file order (src/sr_Read_flow.F90:19-268) plus the switches of

@@ -129,5 +129,6 @@ struct Variant {
 extern const Variant variant_fp64_parity;
 extern const Variant variant_fp64;
 extern const Variant variant_mixed;
+extern const Variant variant_fp32;
 
 }  // namespace hp

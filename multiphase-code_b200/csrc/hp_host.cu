@@ -500,6 +500,10 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
         case HP_PREC_FP64_PARITY: h->var = &variant_fp64_parity; break;
         case HP_PREC_FP64: h->var = &variant_fp64; break;
         case HP_PREC_MIXED: h->var = &variant_mixed; break;
+        case HP_PREC_FP32:
+            if (h->aliased) { delete h; return fail(nullptr, HP_E_UNSUPPORTED, "fp32 variant: aliased ghost ids"); }
+            h->var = &variant_fp32;
+            break;
         default: delete h; return fail(nullptr, HP_E_ARG, "unknown precision mode");
     }
 
@@ -950,7 +954,8 @@ extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, i
     if (!mesh || !params || !bytes || mesh->neles <= 0 || mesh->nghosts < 0) return HP_E_ARG;
     hp_handle probe_h;
     const long long ld = ((long long)mesh->neles + mesh->nghosts + 63) / 64 * 64;
-    const size_t gb = params->precision == HP_PREC_MIXED ? sizeof(float) : sizeof(double);
+    const size_t gb = (params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32) ? sizeof(float)
+                                                                                                : sizeof(double);
     Arena probe;
     plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb, 1);
     *bytes = (int64_t)(probe.used + 256);
@@ -968,7 +973,8 @@ extern "C" int hp_estimate_batch_bytes(const hp_mesh* meshes, int32_t ncase, con
     }
     hp_handle probe_h;
     const long long ld = (ne + ng + 63) / 64 * 64;
-    const size_t gb = params->precision == HP_PREC_MIXED ? sizeof(float) : sizeof(double);
+    const size_t gb = (params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32) ? sizeof(float)
+                                                                                                : sizeof(double);
     Arena probe;
     plan_arena(&probe_h, probe, (int)ne, (int)ng, ld, gb, ncase);
     *bytes = (int64_t)(probe.used + 256);

@@ -82,6 +82,9 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 #ifndef HP_DIV_FAST
 #define HP_DIV_FAST 0
 #endif
+#ifndef HP_S
+#define HP_S double
+#endif
 // kernels that take the fast form when HP_DIV_FAST is set: 1 gradients,
 // 2 fluxes, 4 viscous fluxes, 8 JST smoothing
 #ifndef HP_FAST_MASK
@@ -138,77 +141,83 @@ __device__ __forceinline__ int case_of(const DevMesh& m, int i) { return m.cid ?
 // ---------------------------------------------------------------------------
 // Primitive recovery, src/sr_primitive.F90:23-161 (== the element loop of
 // src/sr_primitiveplusbc.F90:36-172 without ag/ap).  c[] is renormalised.
+// S is the arithmetic of the state path (EOS recovery, RK update, JST, dt):
+// double in every variant except the all-FP32 one.
+using S = HP_S;
+
 struct PrimV {
-    double ug, vg, wg, tg, pg, pp, phig, phip, up, vp, wp, tp, rog, rop;
+    S ug, vg, wg, tg, pg, pp, phig, phip, up, vp, wp, tp, rog, rop;
 };
 
-__device__ __forceinline__ void blend_phases(const DevParams& P, double& phig, double& phip,
-                                             double& ug, double& vg, double& wg, double& tg,
-                                             double& pg, double& up, double& vp, double& wp,
-                                             double& tp, double& pp) {
-    const double emin = P.emin, emax = P.emax;
+__device__ __forceinline__ void blend_phases(const DevParams& P, S& phig, S& phip, S& ug, S& vg, S& wg, S& tg,
+                                             S& pg, S& up, S& vp, S& wp, S& tp, S& pp) {
+    const S emin = (S)P.emin, emax = (S)P.emax;
     if (phig < emin) {
-        phig = emin; phip = 1.0 - phig;
+        phig = emin; phip = S(1.0) - phig;
         ug = up; vg = vp; wg = wp; tg = tp; pg = pp;
     }
     if (phip < emin) {
-        phip = emin; phig = 1.0 - phip;
+        phip = emin; phig = S(1.0) - phip;
         up = ug; vp = vg; wp = wg; tp = tg; pp = pg;
     }
     if (phig >= emin && phig <= emax) {
-        double psig = div_rn(phig - emin, emax - emin, P.r_emm);
-        double f = -(psig * psig * (2.0 * psig - 3.0));
-        ug = f * ug + (1.0 - f) * up;
-        vg = f * vg + (1.0 - f) * vp;
-        wg = f * wg + (1.0 - f) * wp;
-        tg = f * tg + (1.0 - f) * tp;
-        pg = f * pg + (1.0 - f) * pp;
+        S psig = div_rn(phig - emin, emax - emin, (S)P.r_emm);
+        S f = -(psig * psig * (S(2.0) * psig - S(3.0)));
+        ug = f * ug + (S(1.0) - f) * up;
+        vg = f * vg + (S(1.0) - f) * vp;
+        wg = f * wg + (S(1.0) - f) * wp;
+        tg = f * tg + (S(1.0) - f) * tp;
+        pg = f * pg + (S(1.0) - f) * pp;
     }
     if (phip >= emin && phip <= emax) {
-        double psig = div_rn(phip - emin, emax - emin, P.r_emm);
-        double f = -(psig * psig * (2.0 * psig - 3.0));
-        up = f * up + (1.0 - f) * ug;
-        vp = f * vp + (1.0 - f) * vg;
-        wp = f * wp + (1.0 - f) * wg;
-        tp = f * tp + (1.0 - f) * tg;
-        pp = f * pp + (1.0 - f) * pg;
+        S psig = div_rn(phip - emin, emax - emin, (S)P.r_emm);
+        S f = -(psig * psig * (S(2.0) * psig - S(3.0)));
+        up = f * up + (S(1.0) - f) * ug;
+        vp = f * vp + (S(1.0) - f) * vg;
+        wp = f * wp + (S(1.0) - f) * wg;
+        tp = f * tp + (S(1.0) - f) * tg;
+        pp = f * pp + (S(1.0) - f) * pg;
     }
 }
 
-__device__ __forceinline__ void prim_full(double c[10], PrimV& q, const DevParams& P) {
-    const double gamag = P.gamag, gamap = P.gamap, pinf = P.pinf;
-    const double r0 = rcp(c[0]), r5 = rcp(c[5]);
+__device__ __forceinline__ void prim_full(double cd[10], PrimV& q, const DevParams& P) {
+    S c[10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) c[k] = (S)cd[k];
+    const S gamag = (S)P.gamag, gamap = (S)P.gamap, pinf = (S)P.pinf, fsd = (S)P.fsd;
+    const S rrg = (S)P.rrg, cpp = (S)P.cpp;
+    const S r0 = rcp(c[0]), r5 = rcp(c[5]);
     q.ug = div_rn(c[1], c[0], r0); q.vg = div_rn(c[2], c[0], r0); q.wg = div_rn(c[3], c[0], r0);
     q.up = div_rn(c[6], c[5], r5); q.vp = div_rn(c[7], c[5], r5); q.wp = div_rn(c[8], c[5], r5);
-    double eg = div_rn(c[4], c[0], r0) - 0.5 * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
-    double ep = div_rn(c[9], c[5], r5) - 0.5 * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
-    double bbb = (P.fsd + pinf * gamap) - (c[0] * (gamag - 1.0) * eg) - (c[5] * (gamap - 1.0) * ep);
-    double ccc = c[0] * (gamag - 1.0) * eg * (P.fsd + pinf * gamap);
-    q.pg = (-bbb + sqrt(bbb * bbb + 4.0 * ccc)) * 0.5;
-    q.pp = q.pg + P.fsd;
-    q.phig = (c[0] * (gamag - 1.0) * eg) / q.pg;
-    q.phip = 1.0 - q.phig;
+    S eg = div_rn(c[4], c[0], r0) - S(0.5) * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+    S ep = div_rn(c[9], c[5], r5) - S(0.5) * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
+    S bbb = (fsd + pinf * gamap) - (c[0] * (gamag - S(1.0)) * eg) - (c[5] * (gamap - S(1.0)) * ep);
+    S ccc = c[0] * (gamag - S(1.0)) * eg * (fsd + pinf * gamap);
+    q.pg = (-bbb + sqrt(bbb * bbb + S(4.0) * ccc)) * S(0.5);
+    q.pp = q.pg + fsd;
+    q.phig = (c[0] * (gamag - S(1.0)) * eg) / q.pg;
+    q.phip = S(1.0) - q.phig;
     q.rog = c[0] / q.phig;
     q.rop = c[5] / q.phip;
-    q.tg = q.pg / (q.rog * P.rrg);
-    q.tp = ((q.pp + pinf) * gamap) / ((gamap - 1.0) * q.rop * P.cpp);
+    q.tg = q.pg / (q.rog * rrg);
+    q.tp = ((q.pp + pinf) * gamap) / ((gamap - S(1.0)) * q.rop * cpp);
     blend_phases(P, q.phig, q.phip, q.ug, q.vg, q.wg, q.tg, q.pg, q.up, q.vp, q.wp, q.tp, q.pp);
-    q.rog = q.pg / (P.rrg * q.tg);
-    q.rop = (q.pp + pinf) * gamap / ((gamap - 1.0) * P.cpp * q.tp);
-    double eg2 = q.pg / ((gamag - 1.0) * q.rog);
-    double ep2 = (q.pp + gamap * pinf) / ((gamap - 1.0) * q.rop);
-    double egt = eg2 + 0.5 * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
-    double ept = ep2 + 0.5 * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
-    c[0] = q.phig * q.rog;
-    c[1] = q.phig * q.rog * q.ug;
-    c[2] = q.phig * q.rog * q.vg;
-    c[3] = q.phig * q.rog * q.wg;
-    c[4] = q.phig * q.rog * egt;
-    c[5] = q.phip * q.rop;
-    c[6] = q.phip * q.rop * q.up;
-    c[7] = q.phip * q.rop * q.vp;
-    c[8] = q.phip * q.rop * q.wp;
-    c[9] = q.phip * q.rop * ept;
+    q.rog = q.pg / (rrg * q.tg);
+    q.rop = (q.pp + pinf) * gamap / ((gamap - S(1.0)) * cpp * q.tp);
+    S eg2 = q.pg / ((gamag - S(1.0)) * q.rog);
+    S ep2 = (q.pp + gamap * pinf) / ((gamap - S(1.0)) * q.rop);
+    S egt = eg2 + S(0.5) * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+    S ept = ep2 + S(0.5) * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
+    cd[0] = q.phig * q.rog;
+    cd[1] = q.phig * q.rog * q.ug;
+    cd[2] = q.phig * q.rog * q.vg;
+    cd[3] = q.phig * q.rog * q.wg;
+    cd[4] = q.phig * q.rog * egt;
+    cd[5] = q.phip * q.rop;
+    cd[6] = q.phip * q.rop * q.up;
+    cd[7] = q.phip * q.rop * q.vp;
+    cd[8] = q.phip * q.rop * q.wp;
+    cd[9] = q.phip * q.rop * ept;
 }
 
 __device__ __forceinline__ void store_prims(const DevMesh& m, double* pr, int i, const PrimV& q) {
@@ -262,12 +271,12 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
         for (int k = 0; k < 10; k++) COL(s.cn, k)[i] = c[k];
         store_prims(m, s.pr, i, q);
         if (MODE == PM_START) {
-            double ag = sqrt((P.gamag * q.pg) / q.rog);
-            double ap = sqrt((P.gamap * (q.pp + P.pinf)) / q.rop);
-            double qg = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
-            double qp = sqrt(q.up * q.up + q.vp * q.vp + q.wp * q.wp);
-            double x = ldg(m.dl + i) / (mx2(ag, ap) + mx2(qg, qp));
-            if (x == x) kmin = (unsigned long long)__double_as_longlong(x);
+            S ag = sqrt(((S)P.gamag * q.pg) / q.rog);
+            S ap = sqrt(((S)P.gamap * (q.pp + (S)P.pinf)) / q.rop);
+            S qg = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+            S qp = sqrt(q.up * q.up + q.vp * q.vp + q.wp * q.wp);
+            S x = (S)ldg(m.dl + i) / (mx2(ag, ap) + mx2(qg, qp));
+            if (x == x) kmin = (unsigned long long)__double_as_longlong((double)x);
         }
         if (MODE == PM_END) {
             bool bad = false;
@@ -281,8 +290,8 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
                 COL(s.cu, k)[i] = c[k];
             }
             nanc = bad ? 1 : 0;
-            DevScalars& S = s.s[case_of(m, i)];
-            if (i == S.cell1) S.velmag = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
+            DevScalars& sc = s.s[case_of(m, i)];
+            if (i == sc.cell1) sc.velmag = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
         }
     }
     if (MODE == PM_STAGE) return;
@@ -292,13 +301,13 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
     const int c0 = case_of(m, b0), c1 = case_of(m, min(b0 + (int)blockDim.x, m.neles) - 1);
     if (c0 != c1) {
         if (i < m.neles) {
-            DevScalars& S = s.s[case_of(m, i)];
+            DevScalars& sc = s.s[case_of(m, i)];
             if (MODE == PM_START) {
-                if (kmin != ~0ull) atomicMin(&S.dtmin_bits, kmin);
+                if (kmin != ~0ull) atomicMin(&sc.dtmin_bits, kmin);
             } else {
                 for (int k = 0; k < 4; k++)
-                    if (kd[k]) atomicMax(&S.diff_bits[k], kd[k]);
-                if (nanc) atomicAdd(&S.nan_count, nanc);
+                    if (kd[k]) atomicMax(&sc.diff_bits[k], kd[k]);
+                if (nanc) atomicAdd(&sc.nan_count, nanc);
             }
         }
         return;
@@ -342,12 +351,12 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
 __global__ void k_step_begin(DevState<R> s, DevParams P, int ncase) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncase) return;
-    DevScalars* S = s.s + c;
-    double dtmin = __longlong_as_double((long long)S->dtmin_bits);
-    S->dt = dtmin * P.cfl;
-    S->time = S->time + S->dt;
-    S->total = S->total + 1;
-    S->dtmin_bits = (unsigned long long)__double_as_longlong(1.0e8);
+    DevScalars* sc = s.s + c;
+    double dtmin = __longlong_as_double((long long)sc->dtmin_bits);
+    sc->dt = dtmin * P.cfl;
+    sc->time = sc->time + sc->dt;
+    sc->total = sc->total + 1;
+    sc->dtmin_bits = (unsigned long long)__double_as_longlong(1.0e8);
 }
 
 // per-step diagnostics and reset of the residual accumulators; one thread
@@ -355,17 +364,17 @@ __global__ void k_step_begin(DevState<R> s, DevParams P, int ncase) {
 __global__ void k_step_end(DevState<R> s, int ncase) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncase) return;
-    DevScalars* S = s.s + c;
-    int k = S->step_in_call;
+    DevScalars* sc = s.s + c;
+    int k = sc->step_in_call;
     if (k < s.max_diag) {
         double* d = s.diag + 8 * ((size_t)c * s.max_diag + k);
-        d[0] = S->time; d[1] = S->dt; d[2] = S->velmag;
-        for (int j = 0; j < 4; j++) d[3 + j] = __longlong_as_double((long long)S->diff_bits[j]);
-        d[7] = (double)S->nan_count;
+        d[0] = sc->time; d[1] = sc->dt; d[2] = sc->velmag;
+        for (int j = 0; j < 4; j++) d[3 + j] = __longlong_as_double((long long)sc->diff_bits[j]);
+        d[7] = (double)sc->nan_count;
     }
-    S->step_in_call = k + 1;
-    for (int j = 0; j < 4; j++) S->diff_bits[j] = 0ull;
-    S->nan_count = 0ull;
+    sc->step_in_call = k + 1;
+    for (int j = 0; j < 4; j++) sc->diff_bits[j] = 0ull;
+    sc->nan_count = 0ull;
 }
 
 // ---------------------------------------------------------------------------
@@ -514,8 +523,8 @@ template <bool VISC>
 __global__ void __launch_bounds__(512) k_bc(DevMesh m, DevState<R> s, DevParams P) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= m.nghosts) return;
-    const DevScalars& S = s.s[case_of(m, m.g_par[g])];
-    bc_one<VISC>(m, s.pr, nullptr, P, g, S.dt, S.total);
+    const DevScalars& sc = s.s[case_of(m, m.g_par[g])];
+    bc_one<VISC>(m, s.pr, nullptr, P, g, sc.dt, sc.total);
 }
 
 // Sequential ghost fill in the reference's exact order (type lists 2, 3, 5,
@@ -564,14 +573,14 @@ __global__ void __launch_bounds__(512) k_smooth1(DevMesh m, DevState<R> s) {
     const int c = ldg(COL(m.snb, 2) + i), d = ldg(COL(m.snb, 3) + i);
     const double* pg = COL(s.pr, P_PG);
     const double* pp = COL(s.pr, P_PP);
-    const double e6 = (double)1.0e-6f;
+    const S e6 = (S)(double)1.0e-6f;
     // the switch sums of variables 1, 5, 6, 10 (sw[0..3]) and the Laplacian
     // d2q of every variable, one variable at a time
-    double swn[4], swd[4], lap[10];
+    S swn[4], swd[4], lap[10];
 #pragma unroll
     for (int k = 0; k < 10; k++) {
         const double* col = COL(s.cn, k);
-        const double v0 = col[i], v1 = col[a], v2 = col[b], v3 = col[c], v4 = col[d];
+        const S v0 = (S)col[i], v1 = (S)col[a], v2 = (S)col[b], v3 = (S)col[c], v4 = (S)col[d];
         const int slot = k == 0 ? 0 : k == 4 ? 1 : k == 5 ? 2 : k == 9 ? 3 : -1;
         if (slot >= 0) {
             swn[slot] = fabs(v1 - v0) + fabs(v2 - v0) + fabs(v3 - v0) + fabs(v4 - v0);
@@ -579,17 +588,17 @@ __global__ void __launch_bounds__(512) k_smooth1(DevMesh m, DevState<R> s) {
         }
         lap[k] = v1 - v0 + v2 - v0 + v3 - v0 + v4 - v0;
     }
-    double pgi = pg[i];
-    double anun = fabs(pg[a] - pgi) + fabs(pg[b] - pgi) + fabs(pg[c] - pgi) + fabs(pg[d] - pgi);
-    double anud = fabs(pg[a] + pgi) + fabs(pg[b] + pgi) + fabs(pg[c] + pgi) + fabs(pg[d] + pgi);
-    double anupg = anun / anud;
-    double anu1 = anupg + swn[1] / (swd[1] + e6);
+    const S pgi = (S)pg[i], pga = (S)pg[a], pgb = (S)pg[b], pgc = (S)pg[c], pgd = (S)pg[d];
+    S anun = fabs(pga - pgi) + fabs(pgb - pgi) + fabs(pgc - pgi) + fabs(pgd - pgi);
+    S anud = fabs(pga + pgi) + fabs(pgb + pgi) + fabs(pgc + pgi) + fabs(pgd + pgi);
+    S anupg = anun / anud;
+    S anu1 = anupg + swn[1] / (swd[1] + e6);
     anu1 = anu1 + swn[0] / (swd[0] + e6);
-    double ppi = pp[i];
-    anun = fabs(pp[a] - ppi) + fabs(pp[b] - ppi) + fabs(pp[c] - ppi) + fabs(pp[d] - ppi);
-    anud = fabs(pp[a] + ppi) + fabs(pp[b] + ppi) + fabs(pp[c] + ppi) + fabs(pp[d] + ppi);
-    double anupp = anun / anud;
-    double anu2 = anupp + swn[2] / (swd[2] + e6);
+    const S ppi = (S)pp[i], ppa = (S)pp[a], ppb = (S)pp[b], ppc = (S)pp[c], ppd = (S)pp[d];
+    anun = fabs(ppa - ppi) + fabs(ppb - ppi) + fabs(ppc - ppi) + fabs(ppd - ppi);
+    anud = fabs(ppa + ppi) + fabs(ppb + ppi) + fabs(ppc + ppi) + fabs(ppd + ppi);
+    S anupp = anun / anud;
+    S anu2 = anupp + swn[2] / (swd[2] + e6);
     anu2 = anu2 + swn[3] / (swd[3] + e6);
     // all stores after all loads (the output columns may alias the inputs
     // as far as the compiler can tell)
@@ -604,24 +613,24 @@ __global__ void __launch_bounds__(512) k_smooth1(DevMesh m, DevState<R> s) {
 template <int F>
 __device__ __forceinline__ unsigned smooth2_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int i) {
     unsigned bad = 0;
-    const double dt = s.s[case_of(m, i)].dt;
-    const double rdt = mrcp<F>(dt, bad);
+    const S dt = (S)s.s[case_of(m, i)].dt;
+    const S rdt = mrcp<F>(dt, bad);
     int nb[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) nb[f] = ldg(COL(m.snb, f) + i);
-    const double vi = mdiv<F>(ldg(m.vol + i), dt, rdt, bad);
-    double d24nc[4], out[10];
+    const S vi = mdiv<F>((S)ldg(m.vol + i), dt, rdt, bad);
+    S d24nc[4], out[10];
 #pragma unroll
-    for (int f = 0; f < 4; f++) d24nc[f] = 0.5 * (vi + mdiv<F>(ldg(m.vol + nb[f]), dt, rdt, bad));
+    for (int f = 0; f < 4; f++) d24nc[f] = S(0.5) * (vi + mdiv<F>((S)ldg(m.vol + nb[f]), dt, rdt, bad));
 #pragma unroll
     for (int set = 0; set < 2; set++) {
         const double* anu = COL(s.anu, set);
-        double ai = anu[i];
-        double d2c[4], d4c[4];
+        S ai = (S)anu[i];
+        S d2c[4], d4c[4];
 #pragma unroll
         for (int f = 0; f < 4; f++) {
-            double e2 = P.co2 * mx2(ai, anu[nb[f]]);
-            double e4 = mx2(0.0, P.co4 - e2);
+            S e2 = (S)P.co2 * mx2(ai, (S)anu[nb[f]]);
+            S e4 = mx2(S(0.0), (S)P.co4 - e2);
             d2c[f] = e2 * d24nc[f];
             d4c[f] = e4 * d24nc[f];
         }
@@ -629,11 +638,11 @@ __device__ __forceinline__ unsigned smooth2_body(const DevMesh& m, const DevStat
         for (int k = 5 * set; k < 5 * set + 5; k++) {
             const double* cn = COL(s.cn, k);
             const double* dq = COL(s.d2q, k);
-            double ci = cn[i], qi = dq[i];
-            double d2 = d2c[0] * (cn[nb[0]] - ci) + d2c[1] * (cn[nb[1]] - ci) +
-                        d2c[2] * (cn[nb[2]] - ci) + d2c[3] * (cn[nb[3]] - ci);
-            double d4 = d4c[0] * (dq[nb[0]] - qi) + d4c[1] * (dq[nb[1]] - qi) +
-                        d4c[2] * (dq[nb[2]] - qi) + d4c[3] * (dq[nb[3]] - qi);
+            S ci = (S)cn[i], qi = (S)dq[i];
+            S d2 = d2c[0] * ((S)cn[nb[0]] - ci) + d2c[1] * ((S)cn[nb[1]] - ci) +
+                   d2c[2] * ((S)cn[nb[2]] - ci) + d2c[3] * ((S)cn[nb[3]] - ci);
+            S d4 = d4c[0] * ((S)dq[nb[0]] - qi) + d4c[1] * ((S)dq[nb[1]] - qi) +
+                   d4c[2] * ((S)dq[nb[2]] - qi) + d4c[3] * ((S)dq[nb[3]] - qi);
             out[k] = d2 - d4;
         }
     }
@@ -1341,9 +1350,9 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     const R xq = (R)(ldg(m.xc + nq) - x0), yq = (R)(ldg(m.yc + nq) - y0), zq = (R)(ldg(m.zc + nq) - z0);
     const R pq = (R)(COL(pr, P_PHIG)[nq] - COL(pr, P_PHIG)[i]);
     // residual in face order 1..4 (src/sr_hllcbatten.F90:534-552)
-    double rhs[10];
+    S rhs[10];
 #pragma unroll
-    for (int k = 0; k < 10; k++) rhs[k] = 0.0;
+    for (int k = 0; k < 10; k++) rhs[k] = S(0.0);
     R Fg[5] = {R(0), R(0), R(0), R(0), R(0)}, Fp[5] = {R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll
     for (int f = 0; f < 4; f++) {
@@ -1352,8 +1361,8 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         for (int k = 0; k < 10; k++) e[k] = qshfl(eff[k], f);
         const int fl = qshfl(flags, f);
         if (fl & 1) {
-            rhs[1] = rhs[1] + (double)e[1]; rhs[2] = rhs[2] + (double)e[2]; rhs[3] = rhs[3] + (double)e[3];
-            rhs[6] = rhs[6] + (double)e[6]; rhs[7] = rhs[7] + (double)e[7]; rhs[8] = rhs[8] + (double)e[8];
+            rhs[1] = rhs[1] + (S)e[1]; rhs[2] = rhs[2] + (S)e[2]; rhs[3] = rhs[3] + (S)e[3];
+            rhs[6] = rhs[6] + (S)e[6]; rhs[7] = rhs[7] + (S)e[7]; rhs[8] = rhs[8] + (S)e[8];
         } else {
             if (fl & 2) {
 #pragma unroll
@@ -1365,8 +1374,8 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
             }
 #pragma unroll
             for (int k = 0; k < 5; k++) {
-                rhs[k] = rhs[k] + (double)Fg[k];
-                rhs[5 + k] = rhs[5 + k] + (double)Fp[k];
+                rhs[k] = rhs[k] + (S)Fg[k];
+                rhs[5 + k] = rhs[5 + k] + (S)Fp[k];
             }
         }
     }
@@ -1440,44 +1449,44 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         const R g = R(0);
         R en = pint * (uint_ * dpx + vint * dpy + wint * dpz) + uint_ * fdgx + vint * fdgy + wint * fdgz + qsource;
         const double* vis = s.vis;
-        rhs[1] = rhs[1] - (double)((fdgx + pint * dpx + phig * rog * g) * voli) - COL(vis, 0)[i];
-        rhs[2] = rhs[2] - (double)((fdgy + pint * dpy) * voli) - COL(vis, 1)[i];
-        rhs[3] = rhs[3] - (double)((fdgz + pint * dpz) * voli) - COL(vis, 2)[i];
-        rhs[4] = rhs[4] - (double)(en * voli) - COL(vis, 3)[i];
-        rhs[6] = rhs[6] + (double)((fdgx + pint * dpx - phip * rop * g) * voli) - COL(vis, 4)[i];
-        rhs[7] = rhs[7] + (double)((fdgy + pint * dpy) * voli) - COL(vis, 5)[i];
-        rhs[8] = rhs[8] + (double)((fdgz + pint * dpz) * voli) - COL(vis, 6)[i];
-        rhs[9] = rhs[9] + (double)(en * voli) - COL(vis, 7)[i];
+        rhs[1] = rhs[1] - (S)((fdgx + pint * dpx + phig * rog * g) * voli) - (S)COL(vis, 0)[i];
+        rhs[2] = rhs[2] - (S)((fdgy + pint * dpy) * voli) - (S)COL(vis, 1)[i];
+        rhs[3] = rhs[3] - (S)((fdgz + pint * dpz) * voli) - (S)COL(vis, 2)[i];
+        rhs[4] = rhs[4] - (S)(en * voli) - (S)COL(vis, 3)[i];
+        rhs[6] = rhs[6] + (S)((fdgx + pint * dpx - phip * rop * g) * voli) - (S)COL(vis, 4)[i];
+        rhs[7] = rhs[7] + (S)((fdgy + pint * dpy) * voli) - (S)COL(vis, 5)[i];
+        rhs[8] = rhs[8] + (S)((fdgz + pint * dpz) * voli) - (S)COL(vis, 6)[i];
+        rhs[9] = rhs[9] + (S)(en * voli) - (S)COL(vis, 7)[i];
     }
     if constexpr (F == 1) {
         if (__any_sync(0xffffffffu, bad)) return false;
     }
     if (!active) return true;
-    const double dtbyvol = s.s[case_of(m, i)].dt / ldg(m.vol + i);
+    const S dtbyvol = (S)s.s[case_of(m, i)].dt / (S)ldg(m.vol + i);
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         const int j = q + 4 * r;
         if (j >= 10) break;
-        const double rr = rhs[j] - COL(s.d24, j)[i];
-        const double cu = COL(s.cu, j)[i];
+        const S rr = rhs[j] - (S)COL(s.d24, j)[i];
+        const S cu = (S)COL(s.cu, j)[i];
         double* cnp = COL(s.cn, j) + i;
         if (P.rk_scheme == 0) {
             if (stage == 1) {
-                double v = cu - (11.0 / 20.0) * dtbyvol * rr;
+                S v = cu - S(11.0 / 20.0) * dtbyvol * rr;
                 *cnp = v;
                 COL(s.cn1, j)[i] = v;
             } else {
-                double upd = *cnp - (11.0 / 20.0) * dtbyvol * rr;
-                if (stage == 2) *cnp = (3.0 / 8.0) * cu + (5.0 / 8.0) * upd;
-                else if (stage == 3) *cnp = (4.0 / 9.0) * cu + (5.0 / 9.0) * upd;
-                else *cnp = (111.0 / 1331.0) * cu + (260.0 / 1331.0) * COL(s.cn1, j)[i] + (960.0 / 1331.0) * upd;
+                S upd = (S)*cnp - S(11.0 / 20.0) * dtbyvol * rr;
+                if (stage == 2) *cnp = S(3.0 / 8.0) * cu + S(5.0 / 8.0) * upd;
+                else if (stage == 3) *cnp = S(4.0 / 9.0) * cu + S(5.0 / 9.0) * upd;
+                else *cnp = S(111.0 / 1331.0) * cu + S(260.0 / 1331.0) * (S)COL(s.cn1, j)[i] + S(960.0 / 1331.0) * upd;
             }
         } else {
             if (stage == 1) *cnp = cu - dtbyvol * rr;
             else {
-                double upd = *cnp - dtbyvol * rr;
-                if (stage == 2) *cnp = 0.75 * cu + 0.25 * upd;
-                else *cnp = (1.0 / 3.0) * cu + (2.0 / 3.0) * upd;
+                S upd = (S)*cnp - dtbyvol * rr;
+                if (stage == 2) *cnp = S(0.75) * cu + S(0.25) * upd;
+                else *cnp = S(1.0 / 3.0) * cu + S(2.0 / 3.0) * upd;
             }
         }
     }

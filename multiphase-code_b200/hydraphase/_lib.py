@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("HYDRAPHASE_LIB", os.path.join(HERE, "libhydraphase.so"))
 
 HP_OK, HP_E_ARG, HP_E_CUDA, HP_E_NOMEM, HP_E_IO, HP_E_STATE, HP_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
-PREC_FP64_PARITY, PREC_FP64, PREC_MIXED = 0, 1, 2
+PREC_FP64_PARITY, PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2, 3
 
 ERROR_NAMES = {HP_E_ARG: "HP_E_ARG", HP_E_CUDA: "HP_E_CUDA", HP_E_NOMEM: "HP_E_NOMEM",
                HP_E_IO: "HP_E_IO", HP_E_STATE: "HP_E_STATE", HP_E_UNSUPPORTED: "HP_E_UNSUPPORTED"}

@@ -492,3 +492,44 @@ def serving_stream(n_cases=256, rate=40.0, steps=500, cells=(6000, 400000), seed
         spec.flow["cfl"] = cfl
         out.append(StreamCase(k, float(arrival[k]), int(steps), spec))
     return out
+
+
+def shock_lattice(nx=60, ny=60, nz=90, jitter=0.15, seed=3, p_post=5.0e9, lattice=5, radius=0.05,
+                  shock_z=0.2, bubble_z=0.5, alpha_min=0.1, cfl=0.05, pinf=6.0e8, gamap=4.4,
+                  cpp=4186.0) -> CaseSpec:
+    """Precision stress: a planar water shock (p_post behind it, 1e5 Pa ahead:
+    a pressure ratio of 5e4 at 5e9 Pa) travelling in +z through a box of
+    nx x ny x nz hexes (6 tets each) on [0,1] x [0,1] x [0, nz/nx], jittered
+    by +-jitter*h, towards a lattice x lattice grid of air bubbles of
+    `radius` in the plane z = bubble_z.  Slip walls; SSP-RK3, K = 5,
+    inviscid; air volume fraction 1 - alpha_min in the bubbles, alpha_min
+    outside (the stable contrast of this scheme, as in serving_stream)."""
+    b = box_mesh(nx, ny, nz, hi=(1.0, 1.0, nz / nx), jitter=jitter, seed=seed, bc_type=5)
+    gamag = 1.4
+    p0, rho0 = 1.0e5, 1000.0
+    rho_post = rho0 * (1.0 + (p_post - p0) / (gamap * (p0 + pinf)))   # weak-shock estimate of the
+    rho_post = min(rho_post, 1.8 * rho0)                              # jump, capped at 1.8x
+    m2 = (p_post - p0) / (1.0 / rho0 - 1.0 / rho_post)
+    post_velocity = np.sqrt(m2) / rho0 - np.sqrt(m2) / rho_post
+    xc = b.xc
+    cen = (np.arange(lattice) + 0.5) / lattice
+    inb = np.zeros(xc.shape[0], bool)
+    for cx in cen:
+        for cy in cen:
+            inb |= (xc[:, 0] - cx) ** 2 + (xc[:, 1] - cy) ** 2 + (xc[:, 2] - bubble_z) ** 2 < radius ** 2
+    post = xc[:, 2] < shock_z
+    ag = np.where(inb, 1.0 - alpha_min, alpha_min)
+    p = np.where(post, p_post, p0)
+    rho_p = np.where(post, rho_post, rho0)
+    t_air = p0 / (1.2 * R_GAS)
+    rho_g = p / (R_GAS * t_air)
+    u = np.zeros((xc.shape[0], 3))
+    u[post, 2] = post_velocity
+    cu = conserved(ag, p, rho_g, rho_p, u, gamag, gamap, pinf)
+    gp = ghost_prims_from_parents(b.mesh, cu, gamag, gamap, pinf)
+    spec = shock_bubble_on(b, alpha_min=alpha_min)      # parameters of the shock-bubble family
+    spec.name = "shock_lattice"
+    spec.cu, spec.ghost_prims = cu, gp
+    spec.flow["cfl"] = cfl
+    spec.steps = 2000
+    return spec

@@ -1,0 +1,104 @@
+"""Precision stress: the same case run with FP64 everywhere, with the mixed
+variant (FP32 gradients, limiter, reconstruction and fluxes; FP64 state, EOS
+and reductions) and with everything in FP32. Each result is compared with
+the FP64 one.
+
+The FP64 run uses the parity variant, which is bit-identical to the CPU
+oracle (tests/test_gpu_parity.py), so it stands in for the oracle at sizes
+and step counts the oracle cannot reach in reasonable time. Reported per
+variant:
+
+* relative L2 and max errors of mixture density, pressure and air volume
+  fraction, recovered from the conserved state with the reference's
+  pressure-equilibrium quadratic (src/sr_primitive.F90:53-91);
+* positivity violations: cells with a NaN, a non-positive phase density or
+  pressure, or a volume fraction outside [0, 1];
+* device time per step.
+
+Run as `python -m hydraphase.stress [--steps N] [--small]`; prints one JSON
+object.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+from ._lib import PREC_FP32, PREC_FP64_PARITY, PREC_MIXED
+from .engine import Case
+
+VARIANTS = (("fp64", PREC_FP64_PARITY), ("mixed", PREC_MIXED), ("fp32", PREC_FP32))
+
+
+def recover(cu: np.ndarray, flow: dict):
+    """Pressure and air volume fraction of a conserved state (10, n)."""
+    gg, gp, pinf = flow["gamag"], flow["gamap"], flow["pinf"]
+    with np.errstate(all="ignore"):
+        eg = cu[4] / cu[0] - 0.5 * (cu[1] ** 2 + cu[2] ** 2 + cu[3] ** 2) / cu[0] ** 2
+        ep = cu[9] / cu[5] - 0.5 * (cu[6] ** 2 + cu[7] ** 2 + cu[8] ** 2) / cu[5] ** 2
+        bbb = pinf * gp - cu[0] * (gg - 1) * eg - cu[5] * (gp - 1) * ep
+        ccc = cu[0] * (gg - 1) * eg * pinf * gp
+        pg = (-bbb + np.sqrt(bbb * bbb + 4 * ccc)) * 0.5
+        return pg, cu[0] * (gg - 1) * eg / pg
+
+
+def positivity(cu: np.ndarray, flow: dict) -> dict:
+    pg, ag = recover(cu, flow)
+    with np.errstate(invalid="ignore"):
+        return {"nan_cells": int(np.isnan(cu).any(axis=0).sum()),
+                "nonpositive_density": int(((cu[0] <= 0) | (cu[5] <= 0)).sum()),
+                "nonpositive_pressure": int((pg <= 0).sum()),
+                "alpha_out_of_range": int(((ag < 0) | (ag > 1)).sum())}
+
+
+def errors(cu: np.ndarray, ref: np.ndarray, flow: dict) -> dict:
+    p, a = recover(cu, flow)
+    p0, a0 = recover(ref, flow)
+    out = {}
+    for name, x, y in (("density", cu[0] + cu[5], ref[0] + ref[5]), ("pressure", p, p0), ("alpha_g", a, a0)):
+        d = x - y
+        with np.errstate(invalid="ignore"):
+            out[name] = {"rel_l2": float(np.linalg.norm(d) / max(np.linalg.norm(y), 1e-300)),
+                         "max_rel": float(np.nanmax(np.abs(d) / np.maximum(np.abs(y), 1e-300)))
+                         if np.isfinite(d).any() else float("nan")}
+    return out
+
+
+def run(spec, steps: int, chunk: int = 100, variants=VARIANTS) -> dict:
+    states, out = {}, {}
+    for name, prec in variants:
+        with Case(spec.mesh, spec.params(precision=prec)) as c:
+            c.set_state(0.0, spec.cu, spec.ghost_prims)
+            ms, done, first_nan = 0.0, 0, None
+            while done < steps:
+                n = min(chunk, steps - done)
+                ms += c.step_timed(n)
+                done += n
+                _, cu, _ = c.state()
+                if first_nan is None and np.isnan(cu).any():
+                    first_nan = done
+            states[name] = cu
+            out[name] = {"ms_per_step": ms / steps, "first_nan_by_step": first_nan,
+                         "positivity": positivity(cu, spec.flow)}
+    for name, _ in variants:
+        if name != "fp64":
+            out[name]["error_vs_fp64"] = errors(states[name], states["fp64"], spec.flow)
+    return out
+
+
+def main():
+    from . import cases
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--small", action="store_true", help="24 x 24 x 36 hexes instead of 60 x 60 x 90")
+    a = ap.parse_args()
+    spec = cases.shock_lattice(nx=24, ny=24, nz=36, radius=0.08) if a.small else cases.shock_lattice()
+    res = {"workload": f"shock lattice: {spec.mesh.neles} cells, 5e9 Pa water shock on a 5x5 air-bubble "
+                       f"lattice, SSP-RK3, CFL {spec.flow['cfl']}, {a.steps} steps",
+           "cells": spec.mesh.neles, "steps": a.steps, **run(spec, a.steps)}
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()
