@@ -15,7 +15,7 @@ variant:
   pressure, or a volume fraction outside [0, 1];
 * device time per step.
 
-Run as `python -m hydraphase.stress [--steps N] [--small]`; prints one JSON
+Run as `python -m hydraphase.stress [--steps N] [--size nx,ny,nz]`; prints one JSON
 object.
 """
 from __future__ import annotations
@@ -91,9 +91,10 @@ def main():
     from . import cases
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--small", action="store_true", help="24 x 24 x 36 hexes instead of 60 x 60 x 90")
+    ap.add_argument("--size", default="60,60,90", help="hexes nx,ny,nz of the box (6 tets each)")
     a = ap.parse_args()
-    spec = cases.shock_lattice(nx=24, ny=24, nz=36, radius=0.08) if a.small else cases.shock_lattice()
+    nx, ny, nz = (int(v) for v in a.size.split(","))
+    spec = cases.shock_lattice(nx=nx, ny=ny, nz=nz)
     res = {"workload": f"shock lattice: {spec.mesh.neles} cells, 5e9 Pa water shock on a 5x5 air-bubble "
                        f"lattice, SSP-RK3, CFL {spec.flow['cfl']}, {a.steps} steps",
            "cells": spec.mesh.neles, "steps": a.steps, **run(spec, a.steps)}
