@@ -66,6 +66,14 @@ struct DevMesh {
     const int *g_par, *g_id, *g_type;   // [nghosts] ghost list (reference order)
     // overset fringe (nfringe = 0: none): cells, 4 donor cells each and
     // barycentric weights, [4][nfringe] column-major
+    // unique faces (FP32-arithmetic variants; nface = 0: cell-centric
+    // fluxes): owner cell and local face of each, and per cell and local
+    // face the signed face id + 1 (negative when the cell is not the owner)
+    int nface;
+    long long fld;          // leading dimension of the face-flux columns
+    const int* f_i;
+    const int* f_code;      // local face of the owner (bits 0-1)
+    const int* cface;       // [4][ld]
     int nfringe;
     const int* fr;
     const int* fdon;
@@ -89,11 +97,15 @@ template <class R>
 struct DevState {
     double *cn, *cu, *cn1;   // [10][ld]
     double* pr;              // [14][ld]
+    R* prr;                  // [14][ld] primitives in R: pr itself when R is
+                             // double, a float copy otherwise
     R* gr;                   // [33][ld]
     double* phi;             // [ld]
     double *anu, *d2q;       // [2][ld], [10][ld]
     double *d24, *vis;       // [10][ld], [8][ld]
     double* egt;             // [2][ld] ghost egtotal/eptotal (aliased meshes)
+    R* ff;                   // [10][fld] face fluxes (face-based variants)
+    unsigned char* fflag;    // [fld] 1: wall face (pressure terms only)
     DevScalars* s;
     double* diag;            // [max_steps][8]
     int max_diag;

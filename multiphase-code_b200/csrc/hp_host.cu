@@ -118,7 +118,8 @@ extern "C" const char* hp_last_error(const hp_handle* h) { return h ? h->err.c_s
 
 // Carves every device array of a handle out of one arena (a probe arena
 // with no base only measures).  The same plan sizes hp_estimate_bytes.
-static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long ld, size_t gb, int ncase) {
+static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long ld, size_t gb, int ncase,
+                       int nface) {
     const size_t D = sizeof(double), I = sizeof(int);
     DevMesh& m = h->dm;
     m.nc = (int*)a.take(4 * ld * I); m.snb = (int*)a.take(4 * ld * I);
@@ -134,6 +135,9 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     DevState<double>& s = h->ds;
     s.cn = (double*)a.take(10 * ld * D); s.cu = (double*)a.take(10 * ld * D);
     s.cn1 = (double*)a.take(10 * ld * D); s.pr = (double*)a.take(NPR * ld * D);
+    // primitives in the arithmetic of the gradients and fluxes: a float copy
+    // for the FP32-arithmetic variants, the FP64 columns themselves otherwise
+    s.prr = gb == D ? s.pr : (double*)a.take(NPR * ld * gb);
     s.gr = (double*)a.take(NGR * ld * gb); s.phi = (double*)a.take(ld * D);
     s.anu = (double*)a.take(2 * ld * D); s.d2q = (double*)a.take(10 * ld * D);
     s.d24 = (double*)a.take(10 * ld * D); s.vis = (double*)a.take(8 * ld * D);
@@ -142,6 +146,19 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     s.diag = (double*)a.take((size_t)ncase * h->max_diag * 8 * D);
     s.max_diag = h->max_diag;
     m.cid = ncase > 1 ? (const int*)a.take((size_t)neles * I) : nullptr;
+    m.nface = nface;
+    m.fld = ((long long)nface + 63) / 64 * 64;
+    if (nface > 0) {
+        m.f_i = (const int*)a.take((size_t)nface * I);
+        m.f_code = (const int*)a.take((size_t)nface * I);
+        m.cface = (const int*)a.take(4 * (size_t)ld * I);
+        s.ff = (double*)a.take(10 * (size_t)m.fld * gb);
+        s.fflag = (unsigned char*)a.take((size_t)m.fld);
+    } else {
+        m.f_i = m.f_code = m.cface = nullptr;
+        s.ff = nullptr;
+        s.fflag = nullptr;
+    }
     h->d_perm = (int*)a.take((neles + 1) * (size_t)I);
     h->d_gid = (int*)a.take((nghosts + 1) * (size_t)I);
     h->d_gstage = (double*)a.take(6 * (nghosts + 1) * D);
@@ -512,8 +529,34 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     if (cudaGetDevice(&dev) != cudaSuccess) { delete h; return fail(nullptr, HP_E_CUDA, "no CUDA device"); }
     h->device = dev;
     const size_t D = sizeof(double), I = sizeof(int), gb = h->var->grad_bytes;
+    // --- unique faces for the face-based fluxes of the FP32-arithmetic
+    // variants: a face belongs to its lower-id element (or to its element
+    // when the other side is a ghost); meshes whose neighbour lists are not
+    // mutual, and aliased meshes, keep the cell-centric fluxes ---
+    std::vector<int> hf_i, hf_code, hcface;
+    if (gb != D && !h->aliased) {
+        hcface.assign(4 * (size_t)ld, 0);
+        bool mutual = true;
+        for (int t = 0; t < neles && mutual; t++)
+            for (int f = 0; f < 4; f++) {
+                const int j = L.nc[(size_t)f * ld + t];
+                if (j < neles && j < t) continue;
+                int fj = -1;
+                if (j < neles)
+                    for (int k = 0; k < 4; k++)
+                        if (L.nc[(size_t)k * ld + j] == t) { fj = k; break; }
+                if (j < neles && fj < 0) { mutual = false; break; }
+                const int id = (int)hf_i.size();
+                hf_i.push_back(t);
+                hf_code.push_back(f);
+                hcface[(size_t)f * ld + t] = id + 1;
+                if (j < neles) hcface[(size_t)fj * ld + j] = -(id + 1);
+            }
+        if (!mutual) { hf_i.clear(); hf_code.clear(); hcface.clear(); }
+    }
+    const int nface = (int)hf_i.size();
     Arena& A = h->arena;
-    auto plan = [&](Arena& a) { plan_arena(h, a, neles, nghosts, ld, gb, ncase); };
+    auto plan = [&](Arena& a) { plan_arena(h, a, neles, nghosts, ld, gb, ncase, nface); };
     Arena probe;
     plan(probe);
     A.size = probe.used + 256;
@@ -567,6 +610,9 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     if (e == cudaSuccess && nghosts) e = up(m.g_type, L.gtyp.data(), nghosts * (size_t)I);
     if (e == cudaSuccess) e = up(h->d_perm, h->perm.data(), neles * (size_t)I);
     if (e == cudaSuccess && nghosts) e = up(h->d_gid, h->ghost_id.data(), nghosts * (size_t)I);
+    if (e == cudaSuccess && nface) e = up(m.f_i, hf_i.data(), nface * (size_t)I);
+    if (e == cudaSuccess && nface) e = up(m.f_code, hf_code.data(), nface * (size_t)I);
+    if (e == cudaSuccess && nface) e = up(m.cface, hcface.data(), 4 * (size_t)ld * I);
     if (e == cudaSuccess && ncase > 1) {
         std::vector<int> cid(neles);
         for (int c = 0; c < ncase; c++)
@@ -957,7 +1003,8 @@ extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, i
     const size_t gb = (params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32) ? sizeof(float)
                                                                                                 : sizeof(double);
     Arena probe;
-    plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb, 1);
+    const int nface = gb == sizeof(double) ? 0 : (int)((4LL * mesh->neles + mesh->nghosts) / 2);
+    plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb, 1, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
 }
@@ -976,7 +1023,8 @@ extern "C" int hp_estimate_batch_bytes(const hp_mesh* meshes, int32_t ncase, con
     const size_t gb = (params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32) ? sizeof(float)
                                                                                                 : sizeof(double);
     Arena probe;
-    plan_arena(&probe_h, probe, (int)ne, (int)ng, ld, gb, ncase);
+    const int nface = gb == sizeof(double) ? 0 : (int)((4 * ne + ng) / 2);
+    plan_arena(&probe_h, probe, (int)ne, (int)ng, ld, gb, ncase, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
 }
@@ -1068,6 +1116,7 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
         int64_t per_stage = 1 + (h->nghosts ? 1 : 0) + (h->prm.myorder == 2 ? 1 : 0) + 1;
         if (h->aliased) per_stage += (h->prm.myorder == 2 ? 1 : 0) + 1;
         if (h->dm.nfringe > 0) per_stage += 1;
+        if (h->dm.nface > 0) per_stage += 1;   // k_faceflux
         n += (int64_t)h->dp.nstage * per_stage + 3;
         if (h->aliased) n += 2;
         *kernels_per_step = n;

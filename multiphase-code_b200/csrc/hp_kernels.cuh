@@ -85,6 +85,11 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 #ifndef HP_S
 #define HP_S double
 #endif
+// face-based variants: one thread per cell (1) or four lanes per cell (0)
+// gather the face fluxes, add the sources and update the state
+#ifndef HP_FACE_CELL1
+#define HP_FACE_CELL1 1
+#endif
 // kernels that take the fast form when HP_DIV_FAST is set: 1 gradients,
 // 2 fluxes, 4 viscous fluxes, 8 JST smoothing
 #ifndef HP_FAST_MASK
@@ -220,12 +225,13 @@ __device__ __forceinline__ void prim_full(double cd[10], PrimV& q, const DevPara
     cd[9] = q.phip * q.rop * ept;
 }
 
-__device__ __forceinline__ void store_prims(const DevMesh& m, double* pr, int i, const PrimV& q) {
-    COL(pr, P_UG)[i] = q.ug; COL(pr, P_VG)[i] = q.vg; COL(pr, P_WG)[i] = q.wg;
-    COL(pr, P_TG)[i] = q.tg; COL(pr, P_PG)[i] = q.pg; COL(pr, P_PP)[i] = q.pp;
-    COL(pr, P_PHIG)[i] = q.phig; COL(pr, P_PHIP)[i] = q.phip;
-    COL(pr, P_UP)[i] = q.up; COL(pr, P_VP)[i] = q.vp; COL(pr, P_WP)[i] = q.wp;
-    COL(pr, P_TP)[i] = q.tp; COL(pr, P_ROG)[i] = q.rog; COL(pr, P_ROP)[i] = q.rop;
+template <class T>
+__device__ __forceinline__ void store_prims(const DevMesh& m, T* pr, int i, const PrimV& q) {
+    COL(pr, P_UG)[i] = (T)q.ug; COL(pr, P_VG)[i] = (T)q.vg; COL(pr, P_WG)[i] = (T)q.wg;
+    COL(pr, P_TG)[i] = (T)q.tg; COL(pr, P_PG)[i] = (T)q.pg; COL(pr, P_PP)[i] = (T)q.pp;
+    COL(pr, P_PHIG)[i] = (T)q.phig; COL(pr, P_PHIP)[i] = (T)q.phip;
+    COL(pr, P_UP)[i] = (T)q.up; COL(pr, P_VP)[i] = (T)q.vp; COL(pr, P_WP)[i] = (T)q.wp;
+    COL(pr, P_TP)[i] = (T)q.tp; COL(pr, P_ROG)[i] = (T)q.rog; COL(pr, P_ROP)[i] = (T)q.rop;
 }
 
 // Block-wide min / max of 64-bit keys, then one atomic per block.
@@ -270,6 +276,7 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
 #pragma unroll
         for (int k = 0; k < 10; k++) COL(s.cn, k)[i] = c[k];
         store_prims(m, s.pr, i, q);
+        if constexpr (sizeof(R) != sizeof(double)) store_prims(m, s.prr, i, q);
         if (MODE == PM_START) {
             S ag = sqrt(((S)P.gamag * q.pg) / q.rog);
             S ap = sqrt(((S)P.gamap * (q.pp + (S)P.pinf)) / q.rop);
@@ -525,6 +532,11 @@ __global__ void __launch_bounds__(512) k_bc(DevMesh m, DevState<R> s, DevParams 
     if (g >= m.nghosts) return;
     const DevScalars& sc = s.s[case_of(m, m.g_par[g])];
     bc_one<VISC>(m, s.pr, nullptr, P, g, sc.dt, sc.total);
+    if constexpr (sizeof(R) != sizeof(double)) {
+        const int ng = m.g_id[g];
+#pragma unroll
+        for (int k = 0; k < NPR; k++) COL(s.prr, k)[ng] = (R)COL(s.pr, k)[ng];
+    }
 }
 
 // Sequential ghost fill in the reference's exact order (type lists 2, 3, 5,
@@ -801,9 +813,9 @@ __device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& p
 }
 
 // F selects the division form (see mdiv); bad collects its out-of-range flag.
-template <int F>
+template <int F, class PT>
 __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s, const DevParams& P,
-                                          int i, int f, FaceOut& o, unsigned& bad) {
+                                          int i, int f, FaceOut& o, unsigned& bad, const PT* pr) {
     const int neigh = ldg(COL(m.nc, f) + i);
     const unsigned kind = (ldg(m.fk + i) >> (4 * f)) & 0xFu;
     const double scxd = ldg(COL(m.sc, 3 * f) + i), scyd = ldg(COL(m.sc, 3 * f + 1) + i),
@@ -812,7 +824,6 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     const R area = sqrt(scx * scx + scy * scy + scz * scz);
     const R rarea = mrcp<F>(area, bad);
     const R enx = mdiv<F>(scx, area, rarea, bad), eny = mdiv<F>(scy, area, rarea, bad), enz = mdiv<F>(scz, area, rarea, bad);
-    const double* pr = s.pr;
     R ugL = (R)COL(pr, P_UG)[i], vgL = (R)COL(pr, P_VG)[i], wgL = (R)COL(pr, P_WG)[i];
     R tgL = (R)COL(pr, P_TG)[i], phigL = (R)COL(pr, P_PHIG)[i];
     R upL = (R)COL(pr, P_UP)[i], vpL = (R)COL(pr, P_VP)[i], wpL = (R)COL(pr, P_WP)[i];
@@ -1028,7 +1039,7 @@ __device__ __noinline__ void stale_flux(const DevMesh& m, const DevState<R>& s, 
         }
         FaceOut o;
         unsigned bad_ = 0;
-        face_eval<0>(m, s, P, cell, face, o, bad_);
+        face_eval<0>(m, s, P, cell, face, o, bad_, s.pr);
         if (!o.wall && (gas ? o.takeg : o.takep)) {
             for (int k = 0; k < 5; k++) out[k] = o.F[(gas ? 0 : 5) + k];
             return;
@@ -1053,7 +1064,9 @@ __global__ void k_flux_carry(DevMesh m, DevState<R> s, DevParams P) {
 
 // Residual (4 faces + interphase sources, src/sr_source.F90:42-155) and the
 // RK stage update of src/sr_RK.F90 fused; iblank == 1 cells.
-template <bool ALIASED>
+// FACE: the four face fluxes are gathered from k_faceflux's output (face-
+// based variants) instead of evaluated here.
+template <bool ALIASED, bool FACE = false>
 __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParams P, int stage) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
@@ -1063,11 +1076,29 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
     for (int k = 0; k < 10; k++) rhs[k] = 0.0;
     R Fg[5] = {R(0), R(0), R(0), R(0), R(0)}, Fp[5] = {R(0), R(0), R(0), R(0), R(0)};
     bool haveg = false, havep = false;
+    if constexpr (FACE) {
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            const int code = ldg(COL(m.cface, f) + i);
+            const int fid = (code > 0 ? code : -code) - 1;
+            const R sg = code > 0 ? R(1) : R(-1);
+            R e[10];
+#pragma unroll
+            for (int k = 0; k < 10; k++) e[k] = sg * s.ff[(size_t)k * (size_t)m.fld + fid];
+            if (s.fflag[fid]) {
+                rhs[1] = rhs[1] + (double)e[1]; rhs[2] = rhs[2] + (double)e[2]; rhs[3] = rhs[3] + (double)e[3];
+                rhs[6] = rhs[6] + (double)e[6]; rhs[7] = rhs[7] + (double)e[7]; rhs[8] = rhs[8] + (double)e[8];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 10; k++) rhs[k] = rhs[k] + (double)e[k];
+            }
+        }
+    }
 #pragma unroll 1
-    for (int f = 0; f < 4; f++) {
+    for (int f = 0; f < 4 && !FACE; f++) {
         FaceOut o;
         unsigned bad_ = 0;
-        face_eval<0>(m, s, P, i, f, o, bad_);
+        face_eval<0>(m, s, P, i, f, o, bad_, s.pr);
         if (o.wall) {
             rhs[1] = rhs[1] + (double)o.w[0]; rhs[2] = rhs[2] + (double)o.w[1];
             rhs[3] = rhs[3] + (double)o.w[2]; rhs[6] = rhs[6] + (double)o.w[3];
@@ -1247,8 +1278,8 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
     for (int r = 0; r < 4; r++) {
         const int v = q + 4 * r;
         if (v >= 13) break;
-        const double* qq = COL(s.pr, pcol[v]);
-        double qi = qq[i];
+        const R* qq = COL(s.prr, pcol[v]);
+        R qi = qq[i];
         R qa = (R)(qq[n[0]] - qi), qb = (R)(qq[n[1]] - qi), qc = (R)(qq[n[2]] - qi), qd = (R)(qq[n[3]] - qi);
         R c1 = DW(qa * xa[0], 0) + DW(qb * xa[1], 1) + DW(qc * xa[2], 2) + DW(qd * xa[3], 3);
         R c2;
@@ -1276,10 +1307,10 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
     if (q >= 2) { lg[0] = fx0; lg[1] = fy0; lg[2] = fz0; }
     const int lcol = q == 0 ? P_PG : q == 1 ? P_PP : q == 2 ? P_ROG : P_ROP;
     const R epssq = (R)cube_rn((double)(P.venkat_k * ldg(m.dl + i)));
-    const double* qq = COL(s.pr, lcol);
-    double qi = qq[i];
-    double vmax = mx2(mx2(mx2(mx2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
-    double vmin = mn2(mn2(mn2(mn2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
+    const R* qq = COL(s.prr, lcol);
+    R qi = qq[i];
+    R vmax = mx2(mx2(mx2(mx2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
+    R vmin = mn2(mn2(mn2(mn2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
     R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
     R phl = R(0);
 #pragma unroll
@@ -1322,17 +1353,26 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
 // form (see mdiv).  The fast form returns false, before any store, when a lane
 // of the warp flagged an operand (cn is read and written here, so the stores
 // must wait for that vote).
-template <int F>
+template <int F, bool FACE>
 __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int stage,
                                            int i, int q, bool active) {
     unsigned bad = 0;
-    const double* pr = s.pr;
+    const R* pr = s.prr;
     // this lane's face
     R eff[10];
     int flags;
-    {
+    if constexpr (FACE) {
+        // the face's flux, evaluated once by k_faceflux in the owner's
+        // orientation: outgoing for the owner, incoming for the other cell
+        const int code = ldg(COL(m.cface, q) + i);
+        const int fid = (code > 0 ? code : -code) - 1;
+        const R sg = code > 0 ? R(1) : R(-1);
+#pragma unroll
+        for (int k = 0; k < 10; k++) eff[k] = sg * s.ff[(size_t)k * (size_t)m.fld + fid];
+        flags = s.fflag[fid] ? 1 : 6;
+    } else {
         FaceOut o;
-        face_eval<F>(m, s, P, i, q, o, bad);
+        face_eval<F>(m, s, P, i, q, o, bad, s.prr);
         if (o.wall) {
 #pragma unroll
             for (int k = 0; k < 10; k++) eff[k] = R(0);
@@ -1493,6 +1533,7 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     return true;
 }
 
+template <bool FACE>
 __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
@@ -1500,11 +1541,36 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevStat
     const bool valid = i < m.neles;
     if (!valid) i = m.neles - 1;
     const bool active = valid && ldg(m.iblank + i) == 1;
-    if constexpr (HP_FAST(2)) {
-        if (!flux4_body<1>(m, s, P, stage, i, q, active)) flux4_body<0>(m, s, P, stage, i, q, active);
+    if constexpr (HP_FAST(2) && !FACE) {
+        if (!flux4_body<1, false>(m, s, P, stage, i, q, active)) flux4_body<0, false>(m, s, P, stage, i, q, active);
     } else {
-        flux4_body<0>(m, s, P, stage, i, q, active);
+        flux4_body<0, FACE>(m, s, P, stage, i, q, active);
     }
+}
+
+// Face-based fluxes (FP32-arithmetic variants on meshes without aliased
+// ghosts): every face is evaluated once, in its owner cell's orientation,
+// instead of once from each side.  Phases with no HLLC branch taken (only
+// with NaN states) contribute zero here.
+__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_faceflux(DevMesh m, DevState<R> s, DevParams P) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.nface) return;
+    const int i = ldg(m.f_i + t), f = ldg(m.f_code + t) & 3;
+    FaceOut o{};
+    unsigned bad = 0;
+    face_eval<0>(m, s, P, i, f, o, bad, s.prr);
+    R* ff = s.ff;
+    const size_t ld = (size_t)m.fld;
+    if (o.wall) {
+#pragma unroll
+        for (int k = 0; k < 10; k++) ff[k * ld + t] = R(0);
+        ff[1 * ld + t] = o.w[0]; ff[2 * ld + t] = o.w[1]; ff[3 * ld + t] = o.w[2];
+        ff[6 * ld + t] = o.w[3]; ff[7 * ld + t] = o.w[4]; ff[8 * ld + t] = o.w[5];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 10; k++) ff[k * ld + t] = o.F[k];
+    }
+    s.fflag[t] = o.wall ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1512,10 +1578,10 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevStat
 // One face f of cell i: face-centred LSQ over 5 (boundary) or 8 (interior)
 // cell centres, Newtonian stresses and heat flux; c[8] = the face's
 // contribution to visug..vistp.
-template <int F>
+template <int F, class PT>
 __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s, const DevParams& P,
-                                          int i, int f, const int nci[4], double c[8], unsigned& bad) {
-    const double* pr = s.pr;
+                                          int i, int f, const int nci[4], double c[8], unsigned& bad,
+                                          const PT* pr) {
     const int fcol[8] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP};
     const R c23 = (R)P.c23;
     const R scx = (R)ldg(COL(m.sc, 3 * f) + i), scy = (R)ldg(COL(m.sc, 3 * f + 1) + i),
@@ -1560,7 +1626,7 @@ __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s
     R gr[8][3];
 #pragma unroll
     for (int v = 0; v < 8; v++) {
-        const double* q = COL(pr, fcol[v]);
+        const PT* q = COL(pr, fcol[v]);
         R d0 = (R)q[mm[0]] - ff[v];
         R b1 = d0 * dx[0], b2 = d0 * dy[0], b3 = d0 * dz[0];
         for (int k = 1; k < nm; k++) {
@@ -1617,7 +1683,7 @@ __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParam
     for (int f = 0; f < 4; f++) {
         double c[8];
         unsigned bad_ = 0;
-        visc_face<0>(m, s, P, i, f, nci, c, bad_);
+        visc_face<0>(m, s, P, i, f, nci, c, bad_, s.pr);
 #pragma unroll
         for (int k = 0; k < 8; k++) acc[k] = acc[k] + c[k];
     }
@@ -1647,8 +1713,8 @@ __global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevStat
     for (int pass = HP_FAST(4) ? 1 : 0; pass >= 0; pass--) {
         double c[8];
         unsigned bad = 0;
-        if (pass) visc_face<1>(m, s, P, i, q, nci, c, bad);
-        else visc_face<0>(m, s, P, i, q, nci, c, bad);
+        if (pass) visc_face<1>(m, s, P, i, q, nci, c, bad, s.prr);
+        else visc_face<0>(m, s, P, i, q, nci, c, bad, s.prr);
         double acc[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) acc[k] = 0.0;
@@ -1752,8 +1818,12 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             k_flux<true><<<gf, b, 0, st>>>(m, s, P, stage);
             MARK(KK_SERIAL);
             k_flux_carry<<<1, 1, 0, st>>>(m, s, P);
+        } else if (sizeof(R) != sizeof(double) && m.nface > 0) {
+            k_faceflux<<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
+            if (HP_FACE_CELL1) k_flux<false, true><<<gf, 128, 0, st>>>(m, s, P, stage);
+            else k_flux4<true><<<g4, 128, 0, st>>>(m, s, P, stage);
         } else {
-            k_flux4<<<g4, 128, 0, st>>>(m, s, P, stage);
+            k_flux4<false><<<g4, 128, 0, st>>>(m, s, P, stage);
         }
         if (m.nfringe > 0) {
             MARK(KK_OVERSET);
