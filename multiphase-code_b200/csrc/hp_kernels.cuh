@@ -13,6 +13,7 @@
 // bit for bit, and it needs no atomics.
 #include <cfloat>
 #include <cmath>
+#include <type_traits>
 
 #include "hp_device.h"
 
@@ -89,6 +90,16 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 // gather the face fluxes, add the sources and update the state
 #ifndef HP_FACE_CELL1
 #define HP_FACE_CELL1 1
+#endif
+// FP32-arithmetic variants: one-thread-per-cell gradients (1) or four lanes
+// per cell (0)
+#ifndef HP_GRAD_CELL1
+#define HP_GRAD_CELL1 1
+#endif
+// FP32-arithmetic variants: one-thread-per-cell viscous fluxes (1) or four
+// lanes per cell (0)
+#ifndef HP_VISC_CELL1
+#define HP_VISC_CELL1 0
 #endif
 // kernels that take the fast form when HP_DIV_FAST is set: 1 gradients,
 // 2 fluxes, 4 viscous fluxes, 8 JST smoothing
@@ -680,7 +691,12 @@ __global__ void __launch_bounds__(512) k_smooth2(DevMesh m, DevState<R> s, DevPa
 // ---------------------------------------------------------------------------
 // LSQ gradients (src/sr_derivative.F90:45-322) fused with the
 // Venkatakrishnan limiter (src/sr_VK.F90:32-272).  iblank == 1 cells.
+// FPR: read the primitives in R (the float copy of the FP32-arithmetic
+// variants) instead of the FP64 columns; false on aliased meshes.
+template <bool FPR>
 __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParams P) {
+    using PT = typename std::conditional<FPR, R, double>::type;
+    const PT* const prb = reinterpret_cast<const PT*>(FPR ? (const void*)s.prr : (const void*)s.pr);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     if (ldg(m.iblank + i) != 1) return;
@@ -722,8 +738,8 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParam
     R gv[13][3];
 #pragma unroll
     for (int v = 0; v < 13; v++) {
-        const double* q = COL(s.pr, pcol[v]);
-        double qi = q[i];
+        const PT* q = COL(prb, pcol[v]);
+        PT qi = q[i];
         R qa = (R)(q[n[0]] - qi), qb = (R)(q[n[1]] - qi), qc = (R)(q[n[2]] - qi), qd = (R)(q[n[3]] - qi);
         R c1 = DW(qa * xa[0], 0) + DW(qb * xa[1], 1) + DW(qc * xa[2], 2) + DW(qd * xa[3], 3);
         R c2;
@@ -755,10 +771,10 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParam
     R phi = R(0);
 #pragma unroll
     for (int t = 0; t < 4; t++) {
-        const double* q = COL(s.pr, pcol[lv[t]]);
-        double qi = q[i];
-        double vmax = mx2(mx2(mx2(mx2(qi, q[n[0]]), q[n[1]]), q[n[2]]), q[n[3]]);
-        double vmin = mn2(mn2(mn2(mn2(qi, q[n[0]]), q[n[1]]), q[n[2]]), q[n[3]]);
+        const PT* q = COL(prb, pcol[lv[t]]);
+        PT qi = q[i];
+        PT vmax = mx2(mx2(mx2(mx2(qi, q[n[0]]), q[n[1]]), q[n[2]]), q[n[3]]);
+        PT vmin = mn2(mn2(mn2(mn2(qi, q[n[0]]), q[n[1]]), q[n[2]]), q[n[3]]);
         R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
         R gx = gv[lv[t]][0], gy = gv[lv[t]][1], gz = gv[lv[t]][2];
 #pragma unroll
@@ -1669,6 +1685,7 @@ __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s
 }
 
 // one thread per cell (aliased meshes)
+template <bool FPR>
 __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParams P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
@@ -1683,7 +1700,8 @@ __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParam
     for (int f = 0; f < 4; f++) {
         double c[8];
         unsigned bad_ = 0;
-        visc_face<0>(m, s, P, i, f, nci, c, bad_, s.pr);
+        if constexpr (FPR) visc_face<0>(m, s, P, i, f, nci, c, bad_, s.prr);
+        else visc_face<0>(m, s, P, i, f, nci, c, bad_, s.pr);
 #pragma unroll
         for (int k = 0; k < 8; k++) acc[k] = acc[k] + c[k];
     }
@@ -1795,7 +1813,8 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     const unsigned g4 = grid_for(4ll * m.neles, 128);
     if (!P.inviscid) {
         MARK(KK_VISC);
-        if (m.aliased) k_visc<<<gf, b, 0, st>>>(m, s, P);
+        if (m.aliased) k_visc<false><<<gf, b, 0, st>>>(m, s, P);
+        else if (sizeof(R) != sizeof(double) && HP_VISC_CELL1) k_visc<true><<<gf, b, 0, st>>>(m, s, P);
         else k_visc4<<<g4, 128, 0, st>>>(m, s, P);
     }
     for (int stage = 1; stage <= P.nstage; stage++) {
@@ -1809,7 +1828,8 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
         }
         if (P.myorder == 2) {
             MARK(KK_GRAD);
-            if (m.aliased) k_grad<<<gf, b, 0, st>>>(m, s, P);
+            if (m.aliased) k_grad<false><<<gf, b, 0, st>>>(m, s, P);
+            else if (sizeof(R) != sizeof(double) && HP_GRAD_CELL1) k_grad<true><<<gf, b, 0, st>>>(m, s, P);
             else k_grad4<<<g4, 128, 0, st>>>(m, s, P);
             if (m.aliased) { MARK(KK_SERIAL); k_phi_copy_serial<<<1, 1, 0, st>>>(m, s); }
         }
