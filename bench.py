@@ -2,7 +2,7 @@
 """Throughput benchmark of the residual-and-update step (one JSON line).
 
 Metric: cell-RK-stage updates/s = active cells x RK stages x steps / device
-time of the step loop (SURVEY/BASELINE metric of the reference solver).
+time of the step loop, the reference solver's throughput measure.
 
 Workload (N=1): viscous air flow past a cylinder, O-grid 160 x 256 x 20 hexes
 split into 6 tets (4,915,200 cells), Mach 0.3, Re_D 150, SSP-RK3, CFL 0.5,
@@ -38,7 +38,7 @@ METRIC = "cell-RK-stage updates/s, mixed vs FP64 CUDA at stated L2 err; p50/p99 
 UNIT = "cell-stage/s"
 
 # Compulsory bytes per cell and RK stage (each array crossing HBM once):
-# SURVEY's figure for the whole step (FP64) and the flux kernel's own set.
+# the whole step in FP64 and in the mixed variant.
 STEP_BYTES_FP64 = 772
 STEP_BYTES_MIXED = 566
 
@@ -112,6 +112,8 @@ def make_workload(name: str, seed_offset: int = 0):
         return cases.cylinder(seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
     if name == "cylinder_small":
         return cases.cylinder(nr=40, nt=64, nz=16, seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+    if name == "cylinder_medium":
+        return cases.cylinder(nr=80, nt=128, nz=16, seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
     if name == "shock_bubble":
         return cases.shock_bubble(n=20, alpha_min=0.1, reference_scheme=True, seed=seed_offset)
     raise SystemExit(f"unknown workload {name}")
@@ -124,7 +126,14 @@ def workload_config(spec, name):
             "scheme": "SSP-RK3" if spec.extra.get("rk_scheme", 0) == 1 else "ESSPRK-4",
             "flux": "HLLC-Batten", "limiter_K": spec.extra.get("venkat_k", 0.3),
             "viscous": not spec.extra.get("inviscid", 0),
-            "l2_policy": "state larger than L2 (about 10 GB resident per replica)"}
+            "l2_policy": f"state larger than L2 ({resident_gb(spec):.1f} GB resident per replica, L2 126 MB)"}
+
+
+def resident_gb(spec) -> float:
+    """Device bytes of one Case of this workload (FP64 parity variant)."""
+    from hydraphase import PREC_FP64_PARITY
+    from hydraphase.engine import estimate_bytes
+    return estimate_bytes(spec.mesh, spec.params(precision=PREC_FP64_PARITY)) / 1e9
 
 
 def dist_setup(backend: str):

@@ -93,6 +93,10 @@ struct DevScalars {
     int cell1;                        // internal id of the case's cell 1
 };
 
+// R values per face record of the face-based variants: 48 bytes in FP32, read
+// as three 16-byte loads
+constexpr int FACE_REC = 12;
+
 template <class R>
 struct DevState {
     double *cn, *cu, *cn1;   // [10][ld]
@@ -104,8 +108,9 @@ struct DevState {
     double *anu, *d2q;       // [2][ld], [10][ld]
     double *d24, *vis;       // [10][ld], [8][ld]
     double* egt;             // [2][ld] ghost egtotal/eptotal (aliased meshes)
-    R* ff;                   // [10][fld] face fluxes (face-based variants)
-    unsigned char* fflag;    // [fld] 1: wall face (pressure terms only)
+    R* ff;                   // [nface][FACE_REC] face records (face-based
+                             // variants): 10 flux components, the wall flag
+                             // (1: pressure terms only), one pad
     DevScalars* s;
     double* diag;            // [max_steps][8]
     int max_diag;
@@ -135,7 +140,9 @@ struct Variant {
     // enqueue one full step (after enqueue_start of the same step)
     void (*enqueue_step)(const DevMesh&, const void* st, const DevParams&,
                          cudaStream_t, int block, const StepHook* hook);
-    int kernels_per_step;
+    // 1 when the viscous fluxes are evaluated once per face on meshes with a
+    // face list (k_facevisc + k_vis_gather instead of one kernel)
+    int face_visc;
 };
 
 extern const Variant variant_fp64_parity;

@@ -152,12 +152,10 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
         m.f_i = (const int*)a.take((size_t)nface * I);
         m.f_code = (const int*)a.take((size_t)nface * I);
         m.cface = (const int*)a.take(4 * (size_t)ld * I);
-        s.ff = (double*)a.take(10 * (size_t)m.fld * gb);
-        s.fflag = (unsigned char*)a.take((size_t)m.fld);
+        s.ff = (double*)a.take((size_t)FACE_REC * (size_t)m.fld * gb);
     } else {
         m.f_i = m.f_code = m.cface = nullptr;
         s.ff = nullptr;
-        s.fflag = nullptr;
     }
     h->d_perm = (int*)a.take((neles + 1) * (size_t)I);
     h->d_gid = (int*)a.take((nghosts + 1) * (size_t)I);
@@ -1117,6 +1115,7 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
         if (h->aliased) per_stage += (h->prm.myorder == 2 ? 1 : 0) + 1;
         if (h->dm.nfringe > 0) per_stage += 1;
         if (h->dm.nface > 0) per_stage += 1;   // k_faceflux
+        if (h->dm.nface > 0 && !h->prm.inviscid && h->var->face_visc) n += 1;   // k_vis_gather
         n += (int64_t)h->dp.nstage * per_stage + 3;
         if (h->aliased) n += 2;
         *kernels_per_step = n;

@@ -101,6 +101,11 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 #ifndef HP_VISC_CELL1
 #define HP_VISC_CELL1 0
 #endif
+// FP32-arithmetic variants with a face list: viscous fluxes evaluated once
+// per face (1) instead of once from each side (0)
+#ifndef HP_FACE_VISC
+#define HP_FACE_VISC 1
+#endif
 // kernels that take the fast form when HP_DIV_FAST is set: 1 gradients,
 // 2 fluxes, 4 viscous fluxes, 8 JST smoothing
 #ifndef HP_FAST_MASK
@@ -136,6 +141,30 @@ __device__ __forceinline__ double mrcp(double b, unsigned& bad) {
 // the mixed variant divides approximately
 template <int F> __device__ __forceinline__ float mdiv(float a, float b, float rb, unsigned&) { return a * rb; }
 template <int F> __device__ __forceinline__ float mrcp(float b, unsigned&) { return 1.0f / b; }
+
+// One face record (FACE_REC values of R) of the face-based variants; the
+// record of face t starts at FACE_REC * t, 16-byte aligned in FP32.
+__device__ __forceinline__ void load_frec(const float* p, float e[FACE_REC]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    e[0] = a.x; e[1] = a.y; e[2] = a.z; e[3] = a.w;
+    e[4] = b.x; e[5] = b.y; e[6] = b.z; e[7] = b.w;
+    e[8] = c.x; e[9] = c.y; e[10] = c.z; e[11] = c.w;
+}
+__device__ __forceinline__ void load_frec(const double* p, double e[FACE_REC]) {
+#pragma unroll
+    for (int k = 0; k < FACE_REC; k++) e[k] = __ldg(p + k);
+}
+__device__ __forceinline__ void store_frec(float* p, const float e[FACE_REC]) {
+    float4* q = reinterpret_cast<float4*>(p);
+    q[0] = make_float4(e[0], e[1], e[2], e[3]);
+    q[1] = make_float4(e[4], e[5], e[6], e[7]);
+    q[2] = make_float4(e[8], e[9], e[10], e[11]);
+}
+__device__ __forceinline__ void store_frec(double* p, const double e[FACE_REC]) {
+#pragma unroll
+    for (int k = 0; k < FACE_REC; k++) p[k] = e[k];
+}
 
 // Exact division at sites that are not on the fast path.
 __device__ __forceinline__ double div_rn(double a, double b, double) { return a / b; }
@@ -1098,10 +1127,11 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
             const int code = ldg(COL(m.cface, f) + i);
             const int fid = (code > 0 ? code : -code) - 1;
             const R sg = code > 0 ? R(1) : R(-1);
-            R e[10];
+            R e[FACE_REC];
+            load_frec(s.ff + (size_t)FACE_REC * (size_t)fid, e);
 #pragma unroll
-            for (int k = 0; k < 10; k++) e[k] = sg * s.ff[(size_t)k * (size_t)m.fld + fid];
-            if (s.fflag[fid]) {
+            for (int k = 0; k < 10; k++) e[k] = sg * e[k];
+            if (e[10] != R(0)) {
                 rhs[1] = rhs[1] + (double)e[1]; rhs[2] = rhs[2] + (double)e[2]; rhs[3] = rhs[3] + (double)e[3];
                 rhs[6] = rhs[6] + (double)e[6]; rhs[7] = rhs[7] + (double)e[7]; rhs[8] = rhs[8] + (double)e[8];
             } else {
@@ -1383,9 +1413,11 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         const int code = ldg(COL(m.cface, q) + i);
         const int fid = (code > 0 ? code : -code) - 1;
         const R sg = code > 0 ? R(1) : R(-1);
+        R rec[FACE_REC];
+        load_frec(s.ff + (size_t)FACE_REC * (size_t)fid, rec);
 #pragma unroll
-        for (int k = 0; k < 10; k++) eff[k] = sg * s.ff[(size_t)k * (size_t)m.fld + fid];
-        flags = s.fflag[fid] ? 1 : 6;
+        for (int k = 0; k < 10; k++) eff[k] = sg * rec[k];
+        flags = rec[10] != R(0) ? 1 : 6;
     } else {
         FaceOut o;
         face_eval<F>(m, s, P, i, q, o, bad, s.prr);
@@ -1575,18 +1607,19 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_faceflux(DevMesh m, DevS
     FaceOut o{};
     unsigned bad = 0;
     face_eval<0>(m, s, P, i, f, o, bad, s.prr);
-    R* ff = s.ff;
-    const size_t ld = (size_t)m.fld;
+    R rec[FACE_REC];
     if (o.wall) {
 #pragma unroll
-        for (int k = 0; k < 10; k++) ff[k * ld + t] = R(0);
-        ff[1 * ld + t] = o.w[0]; ff[2 * ld + t] = o.w[1]; ff[3 * ld + t] = o.w[2];
-        ff[6 * ld + t] = o.w[3]; ff[7 * ld + t] = o.w[4]; ff[8 * ld + t] = o.w[5];
+        for (int k = 0; k < 10; k++) rec[k] = R(0);
+        rec[1] = o.w[0]; rec[2] = o.w[1]; rec[3] = o.w[2];
+        rec[6] = o.w[3]; rec[7] = o.w[4]; rec[8] = o.w[5];
     } else {
 #pragma unroll
-        for (int k = 0; k < 10; k++) ff[k * ld + t] = o.F[k];
+        for (int k = 0; k < 10; k++) rec[k] = o.F[k];
     }
-    s.fflag[t] = o.wall ? 1 : 0;
+    rec[10] = o.wall ? R(1) : R(0);
+    rec[11] = R(0);
+    store_frec(s.ff + (size_t)FACE_REC * (size_t)t, rec);
 }
 
 // ---------------------------------------------------------------------------
@@ -1748,6 +1781,51 @@ __global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevStat
     }
 }
 
+// Viscous fluxes once per face (FP32-arithmetic variants with a face list):
+// the owner's contribution goes to the face record's first 8 values (the
+// records are free until the first stage's k_faceflux); the other cell of an interior face takes its negative,
+// since the face-centred stencil (both cells' neighbours), the face averages
+// and the face vector are the same from either side up to the vector's sign.
+__global__ void __launch_bounds__(128, HP_VISC4_MINB) k_facevisc(DevMesh m, DevState<R> s, DevParams P) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.nface) return;
+    const int i = ldg(m.f_i + t), f = ldg(m.f_code + t) & 3;
+    int nci[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) nci[k] = ldg(COL(m.nc, k) + i);
+    double c[8];
+    unsigned bad = 0;
+    visc_face<0>(m, s, P, i, f, nci, c, bad, s.prr);
+    R rec[FACE_REC];
+#pragma unroll
+    for (int k = 0; k < 8; k++) rec[k] = (R)c[k];
+#pragma unroll
+    for (int k = 8; k < FACE_REC; k++) rec[k] = R(0);
+    store_frec(s.ff + (size_t)FACE_REC * (size_t)t, rec);
+}
+
+// Per-cell viscous sums from k_facevisc's face values, in face order 1..4.
+__global__ void __launch_bounds__(256) k_vis_gather(DevMesh m, DevState<R> s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles) return;
+    if (ldg(m.iblank + i) != 1) return;
+    double acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = 0.0;
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        const int code = ldg(COL(m.cface, f) + i);
+        const size_t fid = (size_t)((code > 0 ? code : -code) - 1);
+        const double sg = code > 0 ? 1.0 : -1.0;
+        R rec[FACE_REC];
+        load_frec(s.ff + (size_t)FACE_REC * fid, rec);
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[k] = acc[k] + sg * (double)rec[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) COL(s.vis, k)[i] = acc[k];
+}
+
 // ---------------------------------------------------------------------------
 // Overset fringe cells take the barycentric combination of their four donor
 // cells' conserved state after every RK stage (table from hp_overset_build).
@@ -1813,9 +1891,16 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     const unsigned g4 = grid_for(4ll * m.neles, 128);
     if (!P.inviscid) {
         MARK(KK_VISC);
-        if (m.aliased) k_visc<false><<<gf, b, 0, st>>>(m, s, P);
-        else if (sizeof(R) != sizeof(double) && HP_VISC_CELL1) k_visc<true><<<gf, b, 0, st>>>(m, s, P);
-        else k_visc4<<<g4, 128, 0, st>>>(m, s, P);
+        if (m.aliased) {
+            k_visc<false><<<gf, b, 0, st>>>(m, s, P);
+        } else if (sizeof(R) != sizeof(double) && HP_FACE_VISC && m.nface > 0) {
+            k_facevisc<<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
+            k_vis_gather<<<grid_for(m.neles, 256), 256, 0, st>>>(m, s);
+        } else if (sizeof(R) != sizeof(double) && HP_VISC_CELL1) {
+            k_visc<true><<<gf, b, 0, st>>>(m, s, P);
+        } else {
+            k_visc4<<<g4, 128, 0, st>>>(m, s, P);
+        }
     }
     for (int stage = 1; stage <= P.nstage; stage++) {
         // src/sr_hllcbatten.F90:29-33: primitiveplusbc, derivative, limiter

@@ -24,5 +24,5 @@
 #include "hp_kernels.cuh"
 
 namespace hp {
-const Variant variant_fp64 = {"fp64", sizeof(double), &v_fp64::enqueue_start, &v_fp64::enqueue_step, 0};
+const Variant variant_fp64 = {"fp64", sizeof(double), &v_fp64::enqueue_start, &v_fp64::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0};
 }

@@ -24,5 +24,5 @@
 #include "hp_kernels.cuh"
 
 namespace hp {
-const Variant variant_fp64_parity = {"fp64_parity", sizeof(double), &v_fp64_parity::enqueue_start, &v_fp64_parity::enqueue_step, 0};
+const Variant variant_fp64_parity = {"fp64_parity", sizeof(double), &v_fp64_parity::enqueue_start, &v_fp64_parity::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0};
 }

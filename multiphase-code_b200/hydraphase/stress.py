@@ -15,8 +15,19 @@ variant:
   pressure, or a volume fraction outside [0, 1];
 * device time per step.
 
-Run as `python -m hydraphase.stress [--steps N] [--size nx,ny,nz]`; prints one JSON
-object.
+Two more runs measure the rounding floor, the distance to the FP64 parity
+result of a variant that differs from it only by rounding. The FP64 FMA
+variant ("fma") is that yardstick: it computes in FP64 throughout and differs
+from parity only where the compiler contracts a multiply and an add. Each run
+reports the errors of "fma", "mixed" and "fp32" against parity at several step
+counts:
+
+* `--stream`: cases of the serving stream (shock-bubble, CFL 0.05), run as one
+  batch per variant;
+* `--smooth`: the viscous cylinder (O-grid 80x128x16, 983,040 cells, CFL 0.5).
+
+Run as `python -m hydraphase.stress [--steps N] [--size nx,ny,nz] [--stream]
+[--smooth]`; prints one JSON object.
 """
 from __future__ import annotations
 
@@ -25,8 +36,8 @@ import json
 
 import numpy as np
 
-from ._lib import PREC_FP32, PREC_FP64_PARITY, PREC_MIXED
-from .engine import Case
+from ._lib import PREC_FP32, PREC_FP64, PREC_FP64_PARITY, PREC_MIXED
+from .engine import Batch, Case
 
 VARIANTS = (("fp64", PREC_FP64_PARITY), ("mixed", PREC_MIXED), ("fp32", PREC_FP32))
 
@@ -87,12 +98,62 @@ def run(spec, steps: int, chunk: int = 100, variants=VARIANTS) -> dict:
     return out
 
 
+FLOOR_VARIANTS = (("fma", PREC_FP64), ("mixed", PREC_MIXED), ("fp32", PREC_FP32))
+
+
+def _summarise(errs: list) -> dict:
+    """Median and maximum over cases of the density and alpha_g errors."""
+    out = {}
+    for q in ("density", "alpha_g"):
+        v = [e[q]["rel_l2"] for e in errs]
+        out[q] = {"median": float(np.median(v)), "max": float(np.max(v))}
+    return out
+
+
+def floor_batch(specs, checkpoints=(10, 100, 500, 1000), variants=FLOOR_VARIANTS) -> dict:
+    """Run every case of `specs` as one batch per variant, FP64 parity
+    first, and report each variant's errors against parity at every
+    checkpoint (median and maximum over the cases)."""
+    states = {}
+    for name, prec in (("fp64", PREC_FP64_PARITY),) + tuple(variants):
+        with Batch([sp.mesh for sp in specs], specs[0].params(precision=prec)) as b:
+            for k, sp in enumerate(specs):
+                b.set_state(k, 0.0, sp.cu, sp.ghost_prims)
+            done, snaps = 0, []
+            for c in checkpoints:
+                b.step(c - done, diagnostics=False)
+                done = c
+                snaps.append([b.state(k)[1] for k in range(len(specs))])
+            states[name] = snaps
+    out = {}
+    for name, _ in variants:
+        out[name] = {str(c): _summarise([errors(states[name][i][k], states["fp64"][i][k], specs[k].flow)
+                                         for k in range(len(specs))])
+                     for i, c in enumerate(checkpoints)}
+    return out
+
+
 def main():
     from . import cases
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--size", default="60,60,90", help="hexes nx,ny,nz of the box (6 tets each)")
+    ap.add_argument("--stream", action="store_true", help="rounding floor on 16 serving-stream cases")
+    ap.add_argument("--smooth", action="store_true", help="rounding floor on the viscous cylinder")
     a = ap.parse_args()
+    if a.stream or a.smooth:
+        res = {}
+        if a.stream:
+            reqs = cases.serving_stream(n_cases=16, steps=1000, cells=(6000, 100000), seed=5)
+            res["stream"] = {"workload": "16 serving-stream shock-bubble cases, 6k-100k cells, CFL 0.05, "
+                                         "SSP-RK3 (seed 5)",
+                             **floor_batch([r.spec for r in reqs])}
+        if a.smooth:
+            sp = cases.cylinder(nr=80, nt=128, nz=16, seed=1, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+            res["smooth"] = {"workload": f"viscous cylinder O-grid 80x128x16, {sp.mesh.neles} cells, CFL 0.5, "
+                                         "SSP-RK3", **floor_batch([sp])}
+        print(json.dumps(res))
+        return
     nx, ny, nz = (int(v) for v in a.size.split(","))
     spec = cases.shock_lattice(nx=nx, ny=ny, nz=nz)
     res = {"workload": f"shock lattice: {spec.mesh.neles} cells, 5e9 Pa water shock on a 5x5 air-bubble "

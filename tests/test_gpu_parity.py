@@ -3,7 +3,7 @@
 Bar: the FP64 parity variant (no FMA contraction) is bit-identical to the
 oracle on every conserved variable, every ghost primitive and every
 per-step diagnostic.  The FMA variant is held to a relative L2 error of
-1e-10 per conserved variable (the north-star bound for the plain FP64 path),
+1e-10 per conserved variable (the stated bound for a plain FP64 path),
 the mixed FP32/FP64 variant to 1e-4 after a few steps.
 """
 import numpy as np
