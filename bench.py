@@ -5,7 +5,7 @@ Metric: cell-RK-stage updates/s = active cells x RK stages x steps / device
 time of the step loop, the reference solver's throughput measure.
 
 Workload (N=1): viscous air flow past a cylinder, O-grid 160 x 256 x 20 hexes
-split into 6 tets (4,915,200 cells), Mach 0.3, Re_D 150, SSP-RK3, CFL 0.5,
+split into 6 tets (4,915,200 cells), Mach 0.3, Re_D 150, SSP-RK3, CFL 0.25,
 32 water-rich droplets; synthetic, generated in the reference's formats.
 Every rank runs its own replica (the path does not shard across GPUs here):
 value = cells x stages x steps summed over ranks / max-over-ranks time.
@@ -106,14 +106,24 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+# CFL of the cylinder workloads. The reference's time step is convective
+# only (src/main.F90:541-555), and with it the near-wall cells of this O-grid
+# (0.005D spacing, Re_D 150) go unstable at CFL 0.5 after 150-200 steps (NaN
+# from the wall outwards), while CFL 0.25 runs 1000 steps. The cost of a step
+# does not depend on the CFL.
+CYL_CFL = 0.25
+
+
 def make_workload(name: str, seed_offset: int = 0):
     from hydraphase import cases
-    if name == "cylinder":
-        return cases.cylinder(seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
-    if name == "cylinder_small":
-        return cases.cylinder(nr=40, nt=64, nz=16, seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
-    if name == "cylinder_medium":
-        return cases.cylinder(nr=80, nt=128, nz=16, seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+    if name.startswith("cylinder"):
+        nr, nt, nz = {"cylinder": (160, 256, 20), "cylinder_small": (40, 64, 16),
+                      "cylinder_medium": (80, 128, 16)}.get(name, (0, 0, 0))
+        if nr == 0:
+            raise SystemExit(f"unknown workload {name}")
+        spec = cases.cylinder(nr=nr, nt=nt, nz=nz, seed=1 + seed_offset, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+        spec.flow["cfl"] = CYL_CFL
+        return spec
     if name == "shock_bubble":
         return cases.shock_bubble(n=20, alpha_min=0.1, reference_scheme=True, seed=seed_offset)
     raise SystemExit(f"unknown workload {name}")
@@ -125,7 +135,7 @@ def workload_config(spec, name):
             "rk_stages_per_step": 3 if spec.extra.get("rk_scheme", 0) == 1 else 4,
             "scheme": "SSP-RK3" if spec.extra.get("rk_scheme", 0) == 1 else "ESSPRK-4",
             "flux": "HLLC-Batten", "limiter_K": spec.extra.get("venkat_k", 0.3),
-            "viscous": not spec.extra.get("inviscid", 0),
+            "viscous": not spec.extra.get("inviscid", 0), "cfl": spec.flow["cfl"],
             "l2_policy": f"state larger than L2 ({resident_gb(spec):.1f} GB resident per replica, L2 126 MB)"}
 
 
@@ -267,6 +277,7 @@ def overset_measure(steps: int):
     from hydraphase.engine import MeshArrays, overset_build
     t0 = time.perf_counter()
     ov = cases.overset_cylinder(alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+    ov.spec.flow["cfl"] = CYL_CFL
     m = ov.spec.mesh
     t1 = time.perf_counter()
     ib, tab = overset_build(m, ov.block, ov.layers, ov.outer_type)
@@ -294,6 +305,22 @@ def overset_measure(steps: int):
     out["mixed_rel_l2_vs_fp64"] = accuracy(states["mixed"], states["fp64"], ov.spec.flow)
     out["unit"] = UNIT
     return out
+
+
+def accuracy_run(spec, steps: int) -> dict:
+    """The mixed variant against the FP64 parity variant after `steps` steps
+    from the same initial state, on the timed workload (rel L2 of mixture
+    density, alpha_g and the conserved variables), with the NaN cells of
+    both final states."""
+    from hydraphase import PREC_FP64_PARITY, PREC_MIXED, Case
+    states = {}
+    for name, prec in (("fp64", PREC_FP64_PARITY), ("mixed", PREC_MIXED)):
+        with Case(spec.mesh, spec.params(precision=prec)) as c:
+            c.set_state(0.0, spec.cu, spec.ghost_prims)
+            c.step(steps, diagnostics=False)
+            _, states[name], _ = c.state()
+    return {"steps": steps, "rel_l2_vs_fp64": accuracy(states["mixed"], states["fp64"], spec.flow),
+            "nan_cells": {k: int((~np.isfinite(v)).any(axis=0).sum()) for k, v in states.items()}}
 
 
 def run_reference_arm(args, world, rank, pg):
@@ -421,6 +448,8 @@ def run_ours(args, world, rank, local, pg):
     }
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_oracle_sample(args.workload, os.cpu_count() or 1)
+    if world == 1 and rank == 0 and args.accuracy_steps > 0:
+        line["mixed"]["accuracy"] = accuracy_run(spec, args.accuracy_steps)
     if world == 1 and rank == 0 and not args.no_overset:
         line["overset"] = overset_measure(max(args.steps // 2, 5))
     if world == 1 and rank == 0 and args.serving_cases > 0:
@@ -444,6 +473,8 @@ def main():
                     help="cases of the serving stream measured after the step benchmark (0: skip)")
     ap.add_argument("--serving-steps", type=int, default=500)
     ap.add_argument("--no-overset", action="store_true", help="skip the overset cylinder measurement")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="steps of the mixed-vs-FP64 accuracy run on the timed workload (0: skip)")
     args = ap.parse_args()
     backend = "gloo" if args.impl == "reference" else os.environ.get("BENCH_BACKEND", "nccl")
     world, rank, local, pg = dist_setup(backend)

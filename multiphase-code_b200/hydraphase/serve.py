@@ -111,6 +111,9 @@ class Server:
     hbm_budget: device bytes the admitted units may hold together
     max_active: units in flight (set up or running)
     chunk: steps enqueued per unit per turn of the loop
+    setup_workers: host threads running hp_create + hp_set_state; with 4,
+        the 48-case stream of the benchmark queued for set-up (median wait
+        1.8 s), with 8 it did not (0.1 s)
     keep_state: copy each final state back (False keeps only the timing)
     batch_cells: cases below this size are grouped into multi-mesh batches of
         at most this many cells (0: every case on its own handle)
@@ -120,7 +123,7 @@ class Server:
     """
 
     def __init__(self, hbm_budget: int, precision: int = PREC_MIXED, max_active: int = 12, chunk: int = 25,
-                 setup_workers: int = 4, keep_state: bool = True, param_overrides: dict | None = None,
+                 setup_workers: int = 8, keep_state: bool = True, param_overrides: dict | None = None,
                  batch_cells: int = 0, max_batch: int = 64, block_size=None):
         self.budget = int(hbm_budget)
         self.precision = precision
