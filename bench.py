@@ -282,6 +282,10 @@ def overset_measure(steps: int):
     t1 = time.perf_counter()
     ib, tab = overset_build(m, ov.block, ov.layers, ov.outer_type)
     t2 = time.perf_counter()
+    ib_d, tab_d = overset_build(m, ov.block, ov.layers, ov.outer_type, device=True)
+    t3 = time.perf_counter()
+    same = bool(np.array_equal(ib, ib_d) and np.array_equal(tab.fringe, tab_d.fringe) and
+                np.array_equal(tab.donor, tab_d.donor) and np.array_equal(tab.weight, tab_d.weight))
     el = m.elem.copy()
     el[:, 8] = ib
     mesh = MeshArrays(m.x, m.y, m.z, el, m.ghost)
@@ -289,6 +293,7 @@ def overset_measure(steps: int):
                        "hole r < 1.2D, 2 fringe layers, SSP-RK3, viscous",
            "cells": m.neles, "holes": int((m.elem[:, 8] == 0).sum()), "fringe": int(tab.fringe.size),
            "donor_fallbacks": int(tab.nfallback), "table_build_s": round(t2 - t1, 2),
+           "table_build_gpu_s": round(t3 - t2, 3), "gpu_tables_equal_host": same,
            "mesh_generation_s": round(t1 - t0, 2)}
     states = {}
     for name, prec in (("fp64", PREC_FP64_PARITY), ("mixed", PREC_MIXED)):

@@ -188,6 +188,12 @@ typedef struct hp_overset {
 } hp_overset;
 int hp_overset_build(const hp_mesh *mesh, const int32_t *block, int32_t layers, int32_t outer_type,
                      int32_t *iblank_out, hp_overset *out);
+/* The same tables, bit for bit, with the donor search, the nearest-centroid
+ * fallback and the weights on the current CUDA device (the host marks the
+ * fringe and sizes the search grids).  Allocates temporary device memory;
+ * HP_E_CUDA if a device call fails. */
+int hp_overset_build_gpu(const hp_mesh *mesh, const int32_t *block, int32_t layers, int32_t outer_type,
+                         int32_t *iblank_out, hp_overset *out);
 void hp_free_overset(hp_overset *ov);
 /* Single-case handles only; replaces any earlier table. */
 int hp_set_overset(hp_handle *h, const hp_overset *ov);

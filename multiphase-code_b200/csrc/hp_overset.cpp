@@ -34,30 +34,12 @@
 #include <vector>
 
 #include "../../include/hydraphase.h"
+#include "hp_overset_common.h"
 
 namespace {
 
-inline double det3(double A11, double A21, double A31, double A12, double A22, double A32, double A13,
-                   double A23, double A33) {
-    return A11 * (A22 * A33 - A23 * A32) - A21 * (A12 * A33 - A13 * A32) + A31 * (A12 * A23 - A13 * A22);
-}
-// Fortran MIN of finite values
-inline double mn2(double a, double b) { return (b < a || a != a) ? b : a; }
-
-double bary(const double p0[3], const double p1[3], const double p2[3], const double p3[3], const double x[3],
-            double lam[4]) {
-    double a[3], b[3], c[3], d[3];
-    for (int k = 0; k < 3; k++) {
-        a[k] = p1[k] - p0[k]; b[k] = p2[k] - p0[k]; c[k] = p3[k] - p0[k]; d[k] = x[k] - p0[k];
-    }
-    double v = det3(a[0], a[1], a[2], b[0], b[1], b[2], c[0], c[1], c[2]);
-    if (v == 0.0) return 0.0;
-    double l1 = det3(d[0], d[1], d[2], b[0], b[1], b[2], c[0], c[1], c[2]) / v;
-    double l2 = det3(a[0], a[1], a[2], d[0], d[1], d[2], c[0], c[1], c[2]) / v;
-    double l3 = det3(a[0], a[1], a[2], b[0], b[1], b[2], d[0], d[1], d[2]) / v;
-    lam[0] = 1.0 - l1 - l2 - l3; lam[1] = l1; lam[2] = l2; lam[3] = l3;
-    return v;
-}
+using hp_ov::bary;
+using hp_ov::mn2;
 
 struct Mesh {
     const hp_mesh* m;
@@ -73,31 +55,14 @@ struct Mesh {
 };
 
 // Field tets of one block binned by bounding box (CSR lists, ascending ids).
-struct Grid {
-    double lo[3] = {0, 0, 0}, h = 1.0;
-    int n[3] = {1, 1, 1};
+struct Grid : hp_ov::GridParams {
     std::vector<int> start, items;
-    int idx(int d, double v) const {
-        double t = std::floor((v - lo[d]) / h);
-        if (!(t >= 0.0)) return 0;
-        return t >= n[d] - 1 ? n[d] - 1 : (int)t;
-    }
+    int idx(int d, double v) const { return hp_ov::grid_index(*this, d, v); }
     size_t cell(int i, int j, int k) const { return ((size_t)i * n[1] + j) * n[2] + k; }
 };
 
-void build_grid(const Mesh& M, const std::vector<int>& field, Grid& G) {
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int t : field)
-        for (int q = 0; q < 4; q++) {
-            double p[3];
-            M.node(M.row(t)[q], p);
-            for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], p[d]); hi[d] = std::max(hi[d], p[d]); }
-        }
-    double ext[3], vol = 1.0;
-    for (int d = 0; d < 3; d++) { ext[d] = std::max(hi[d] - lo[d], 1e-300); vol *= ext[d]; G.lo[d] = lo[d]; }
-    G.h = std::cbrt(vol / std::max<size_t>(field.size(), 1)) * 1.5;
-    if (!(G.h > 0.0)) G.h = 1.0;
-    for (int d = 0; d < 3; d++) G.n[d] = std::max(1, std::min(512, (int)(ext[d] / G.h) + 1));
+void build_grid(const Mesh& M, const std::vector<int>& field, const hp_ov::GridParams& gp, Grid& G) {
+    static_cast<hp_ov::GridParams&>(G) = gp;
     const size_t ncell = (size_t)G.n[0] * G.n[1] * G.n[2];
     std::vector<int> cnt(ncell + 1, 0);
     auto span = [&](int t, int a[3], int b[3]) {
@@ -131,13 +96,13 @@ void build_grid(const Mesh& M, const std::vector<int>& field, Grid& G) {
 
 }  // namespace
 
-// See include/hydraphase.h.
-extern "C" int hp_overset_build(const hp_mesh* mesh, const int32_t* block, int32_t layers, int32_t outer_type,
-                                int32_t* iblank_out, hp_overset* out) {
-    if (!mesh || !block || !iblank_out || !out || layers < 1 || mesh->neles <= 0 || mesh->nghosts < 0 ||
-        !mesh->elem || (mesh->nghosts && !mesh->ghost) || !mesh->x || !mesh->y || !mesh->z)
+namespace hp_ov {
+
+int prepare(const hp_mesh* mesh, const int32_t* block, int32_t layers, int32_t outer_type, int32_t* iblank_out,
+            Prep& P) {
+    if (!mesh || !block || !iblank_out || layers < 1 || mesh->neles <= 0 || mesh->nghosts < 0 || !mesh->elem ||
+        (mesh->nghosts && !mesh->ghost) || !mesh->x || !mesh->y || !mesh->z)
         return HP_E_ARG;
-    std::memset(out, 0, sizeof *out);
     const int neles = mesh->neles, nghosts = mesh->nghosts, ntot = neles + nghosts;
     Mesh M{mesh};
     for (int e = 1; e <= neles; e++) {
@@ -169,18 +134,54 @@ extern "C" int hp_overset_build(const hp_mesh* mesh, const int32_t* block, int32
                 if (n <= neles && mark[n] == l - 1 && block[n - 1] == block[e - 1]) { mark[e] = l; break; }
             }
         }
-    std::vector<int> fr;
+    P.fr.clear();
     for (int e = 1; e <= neles; e++) {
         iblank_out[e - 1] = mark[e] ? -1 : M.row(e)[8];
-        if (mark[e]) fr.push_back(e);
+        if (mark[e]) P.fr.push_back(e);
     }
-    const int nf = (int)fr.size();
-    std::vector<int> field[2];
+    for (int b = 0; b < 2; b++) P.field[b].clear();
     for (int e = 1; e <= neles; e++)
-        if (iblank_out[e - 1] == 1) field[block[e - 1]].push_back(e);
+        if (iblank_out[e - 1] == 1) P.field[block[e - 1]].push_back(e);
+    // grid over each block's field tets: bounding box, cell size 1.5x the
+    // mean tet size, at most 512 cells per axis
+    for (int b = 0; b < 2; b++) {
+        GridParams& G = P.grid[b];
+        G = GridParams{};
+        if (P.field[b].empty()) continue;
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int t : P.field[b])
+            for (int q = 0; q < 4; q++) {
+                double p[3];
+                M.node(M.row(t)[q], p);
+                for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], p[d]); hi[d] = std::max(hi[d], p[d]); }
+            }
+        double ext[3], vol = 1.0;
+        for (int d = 0; d < 3; d++) { ext[d] = std::max(hi[d] - lo[d], 1e-300); vol *= ext[d]; G.lo[d] = lo[d]; }
+        G.h = std::cbrt(vol / std::max<size_t>(P.field[b].size(), 1)) * 1.5;
+        if (!(G.h > 0.0)) G.h = 1.0;
+        for (int d = 0; d < 3; d++) G.n[d] = std::max(1, std::min(512, (int)(ext[d] / G.h) + 1));
+    }
+    return HP_OK;
+}
+
+}  // namespace hp_ov
+
+// See include/hydraphase.h.
+extern "C" int hp_overset_build(const hp_mesh* mesh, const int32_t* block, int32_t layers, int32_t outer_type,
+                                int32_t* iblank_out, hp_overset* out) {
+    if (!out) return HP_E_ARG;
+    std::memset(out, 0, sizeof *out);
+    hp_ov::Prep P;
+    const int rc = hp_ov::prepare(mesh, block, layers, outer_type, iblank_out, P);
+    if (rc != HP_OK) return rc;
+    const int neles = mesh->neles;
+    Mesh M{mesh};
+    const std::vector<int>& fr = P.fr;
+    const int nf = (int)fr.size();
+    const std::vector<int>* field = P.field;
     Grid G[2];
     for (int b = 0; b < 2; b++)
-        if (!field[b].empty()) build_grid(M, field[b], G[b]);
+        if (!field[b].empty()) build_grid(M, field[b], P.grid[b], G[b]);
     out->nfringe = nf;
     out->fringe = (int32_t*)std::malloc(sizeof(int32_t) * (size_t)(nf + 1));
     out->donor = (int32_t*)std::malloc(sizeof(int32_t) * 4 * (size_t)(nf + 1));

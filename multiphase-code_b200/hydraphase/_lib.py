@@ -94,6 +94,7 @@ def lib():
                                           ctypes.POINTER(ctypes.c_int64)]
     L.hp_overset_build.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(_I), _I, _I, ctypes.POINTER(_I),
                                    ctypes.POINTER(HpOverset)]
+    L.hp_overset_build_gpu.argtypes = L.hp_overset_build.argtypes
     L.hp_free_overset.argtypes = [ctypes.POINTER(HpOverset)]
     L.hp_free_overset.restype = None
     L.hp_set_overset.argtypes = [vp, ctypes.POINTER(HpOverset)]
@@ -109,7 +110,7 @@ def lib():
     for fn in ("hp_create", "hp_destroy", "hp_init_uniform", "hp_set_state", "hp_step", "hp_sync",
                "hp_step_timed", "hp_profile_steps", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll",
                "hp_create_batch", "hp_case_count", "hp_set_state_case", "hp_get_state_case",
-               "hp_estimate_batch_bytes", "hp_overset_build", "hp_set_overset",
+               "hp_estimate_batch_bytes", "hp_overset_build", "hp_overset_build_gpu", "hp_set_overset",
                "hp_get_state", "hp_get_prims", "hp_device_state", "hp_info", "hp_read_flow",
                "hp_read_mesh", "hp_read_restart", "hp_write_restart"):
         getattr(L, fn).restype = ctypes.c_int
@@ -126,6 +127,6 @@ EXPORTED_SYMBOLS = (
     "hp_info", "hp_read_flow", "hp_read_mesh", "hp_free_mesh", "hp_read_restart",
     "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll", "hp_create_batch", "hp_case_count",
     "hp_set_state_case", "hp_get_state_case", "hp_estimate_batch_bytes", "hp_overset_build", "hp_free_overset",
-    "hp_set_overset",
+    "hp_set_overset", "hp_overset_build_gpu",
 )
 NOALLOC_MAX_CELLS = 1 << 24

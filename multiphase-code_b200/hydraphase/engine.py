@@ -97,17 +97,19 @@ class OversetTable:
     nfallback: int
 
 
-def overset_build(mesh: MeshArrays, block, layers: int = 2, outer_type: int = 7):
+def overset_build(mesh: MeshArrays, block, layers: int = 2, outer_type: int = 7, device: bool = False):
     """Fringe and donor tables of a two-block overset mesh (block[e] = 0
     background, 1 component; holes as iblank 0).  Returns (iblank, table):
-    iblank marks the fringe with -1 and goes into the mesh given to Case."""
+    iblank marks the fringe with -1 and goes into the mesh given to Case.
+    device=True runs the donor search on the current CUDA device
+    (hp_overset_build_gpu); the tables are the same."""
     keep = []
     hm = _hp_mesh(mesh, keep)
     bl = np.ascontiguousarray(block, np.int32)
     ib = np.zeros(mesh.neles, np.int32)
     ov = HpOverset()
-    _check(lib().hp_overset_build(ctypes.byref(hm), _ip(bl), int(layers), int(outer_type), _ip(ib),
-                                  ctypes.byref(ov)))
+    build = lib().hp_overset_build_gpu if device else lib().hp_overset_build
+    _check(build(ctypes.byref(hm), _ip(bl), int(layers), int(outer_type), _ip(ib), ctypes.byref(ov)))
     try:
         n = ov.nfringe
         fr = np.ctypeslib.as_array(ov.fringe, (n,)).copy() if n else np.zeros(0, np.int32)

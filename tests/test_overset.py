@@ -7,7 +7,9 @@ holes / the component's outer boundary; donors are field cells of the other
 block; weights sum to one and reproduce linear fields.
 GPU: steps with the table attached (fringe cells interpolated after every RK
 stage) equal the oracle bit for bit in the FP64 parity variant, and the mixed
-variant stays within 1e-5 in mixture density and alpha_g.
+variant stays within 1e-5 in mixture density and alpha_g; the device builder
+(hp_overset_build_gpu) returns the host builder's tables bit for bit,
+nearest-centroid fallbacks included.
 """
 import numpy as np
 import pytest
@@ -120,3 +122,36 @@ def test_overset_table_rejected_on_batches():
                       dn.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                       w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0)
         assert lib().hp_set_overset(b.h, ctypes.byref(o)) == HP_E_UNSUPPORTED
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layers", [1, 2])
+def test_device_tables_equal_host(layers):
+    """hp_overset_build_gpu returns the host builder's tables bit for bit."""
+    ov = _small()
+    m = ov.spec.mesh
+    ib_h, th = overset_build(m, ov.block, layers, ov.outer_type)
+    ib_d, td = overset_build(m, ov.block, layers, ov.outer_type, device=True)
+    np.testing.assert_array_equal(ib_h, ib_d)
+    np.testing.assert_array_equal(th.fringe, td.fringe)
+    np.testing.assert_array_equal(th.donor, td.donor)
+    np.testing.assert_array_equal(th.weight, td.weight)
+    assert th.nfallback == td.nfallback
+
+
+@pytest.mark.gpu
+def test_device_tables_with_nearest_fallback():
+    """A component that reaches beyond the background: its outer fringe lies
+    in no background tet, so the nearest-centroid fallback runs; host and
+    device agree on it too."""
+    ov = cases.overset_cylinder(bg=(12, 12, 2), comp=(8, 32, 2), box=((-2.5, -2.5, 0.0), (2.5, 2.5, 4.0)),
+                                alpha_w_drop=1e-5, alpha_w_bg=1e-6)
+    m = ov.spec.mesh
+    ib_h, th = overset_build(m, ov.block, ov.layers, ov.outer_type)
+    ib_d, td = overset_build(m, ov.block, ov.layers, ov.outer_type, device=True)
+    assert th.nfallback > 0
+    np.testing.assert_array_equal(ib_h, ib_d)
+    np.testing.assert_array_equal(th.fringe, td.fringe)
+    np.testing.assert_array_equal(th.donor, td.donor)
+    np.testing.assert_array_equal(th.weight, td.weight)
+    assert th.nfallback == td.nfallback
