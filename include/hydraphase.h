@@ -198,6 +198,27 @@ void hp_free_overset(hp_overset *ov);
 /* Single-case handles only; replaces any earlier table. */
 int hp_set_overset(hp_handle *h, const hp_overset *ov);
 
+/* --- output ------------------------------------------------------------------ */
+/* The Tecplot file of src/main.F90:956-1268 (two-phase build): node
+ * coordinates, the 13 cell-centred fields (U V W PG PP TG UP VP WP PHIG TP
+ * ROG ROP, fields[13][neles], reference element order) and the
+ * connectivity; values as Fortran ES16.8.  Host only. */
+int hp_write_tecplot(const char *path, const hp_mesh *mesh, const double *fields);
+/* Asynchronous output of case c, with no counterpart in the reference (which
+ * stops its time loop to write): a snapshot of the state after the steps
+ * enqueued so far is taken on the device, copied to pinned memory on a side
+ * stream, and written by a host thread to restart_path (the restart format
+ * of hp_write_restart; may be NULL) and tecplot_path (hp_write_tecplot's
+ * file, fields computed on the device from cu; may be NULL), while later
+ * steps run.  For Tecplot, `mesh` is the case's mesh and must stay valid
+ * until hp_output_wait returns.  Two requests may be in flight; a third
+ * waits for the older one.  hp_output_wait blocks until the request's files
+ * are written and returns its status (HP_E_IO on a write failure); a ticket
+ * is valid until it is waited for or its slot is reused. */
+int hp_output_async(hp_handle *h, int32_t c, const hp_mesh *mesh, const char *restart_path,
+                    const char *tecplot_path, int32_t *ticket);
+int hp_output_wait(hp_handle *h, int32_t ticket);
+
 /* --- serving many cases ---------------------------------------------------- */
 /* No counterpart in the reference, which runs one case per process.  Device
  * bytes hp_create would allocate for this mesh and precision (admission

@@ -7,11 +7,13 @@
 // bit-identical.  The time step itself runs only on the device.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -58,6 +60,18 @@ struct CaseRange {
     int aliased = 0;
 };
 
+// One asynchronous output request (hp_output_async): the device staging of
+// the snapshot, its pinned host copy, and the thread that writes the files.
+struct OutSlot {
+    double* d_buf = nullptr;
+    double* h_buf = nullptr;
+    size_t cap = 0;            // doubles in each buffer
+    cudaEvent_t ready = nullptr, copied = nullptr;
+    std::thread writer;
+    int ticket = 0;            // 0: idle
+    int rc = HP_OK;
+};
+
 struct hp_handle {
     hp_params prm{};
     DevParams dp{};
@@ -86,6 +100,9 @@ struct hp_handle {
     std::string err;
     double* h_diag = nullptr;   // pinned
     DevScalars* h_scal = nullptr;
+    OutSlot out[2];             // asynchronous output, two requests in flight
+    cudaStream_t ostream = nullptr;
+    int next_ticket = 1;
 };
 
 static int fail(hp_handle* h, int code, const std::string& msg) {
@@ -643,8 +660,23 @@ extern "C" int hp_create(const hp_mesh* mesh, const hp_params* params, hp_handle
     return hp_create_batch(mesh, 1, params, out);
 }
 
+static int output_join(OutSlot& s) {
+    if (!s.ticket) return HP_OK;
+    if (s.writer.joinable()) s.writer.join();
+    s.ticket = 0;
+    return s.rc;
+}
+
 extern "C" int hp_destroy(hp_handle* h) {
     if (!h) return HP_OK;
+    for (OutSlot& o : h->out) {
+        output_join(o);
+        if (o.ready) cudaEventDestroy(o.ready);
+        if (o.copied) cudaEventDestroy(o.copied);
+        if (o.d_buf) cudaFree(o.d_buf);
+        if (o.h_buf) cudaFreeHost(o.h_buf);
+    }
+    if (h->ostream) cudaStreamDestroy(h->ostream);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
@@ -1078,6 +1110,86 @@ extern "C" int hp_get_state_case(hp_handle* h, int32_t c, double* time, double* 
     CUDA_OK(h, cudaStreamSynchronize(st));
     if (time) *time = h->h_scal->time;
     return HP_OK;
+}
+
+// --- asynchronous output -----------------------------------------------------
+// No counterpart in the reference, which stops its time loop to write.  The
+// snapshot (time, cu in reference order, ghost primitives and, for Tecplot,
+// the 13 cell-centred fields) is taken on the handle's stream, so it is the
+// state after the steps enqueued before the call; the device-to-host copy
+// runs on a second stream and the files are written by a host thread, both
+// overlapping the steps enqueued after it.
+namespace hp {
+cudaError_t launch_tecplot_fields(const double* cu, long long ld, int ne, const int* perm, const DevParams& P,
+                                  double* out, cudaStream_t st);
+}
+
+extern "C" int hp_output_async(hp_handle* h, int32_t c, const hp_mesh* mesh, const char* restart_path,
+                               const char* tecplot_path, int32_t* ticket) {
+    if (!h || !ticket || (!restart_path && !tecplot_path)) return HP_E_ARG;
+    if (c < 0 || c >= h->ncase) return fail(h, HP_E_ARG, "case index out of range");
+    const CaseRange& cr = h->cases[c];
+    if (tecplot_path && (!mesh || mesh->neles != cr.ne || !mesh->elem || !mesh->x || !mesh->y || !mesh->z))
+        return fail(h, HP_E_ARG, "Tecplot output needs the case's mesh");
+    const int ne = cr.ne, ng = cr.ng;
+    const long long ld = h->ld;
+    // an idle slot, else the older request, which is waited for first
+    OutSlot* o = !h->out[0].ticket ? &h->out[0]
+                 : !h->out[1].ticket ? &h->out[1]
+                 : (h->out[0].ticket < h->out[1].ticket ? &h->out[0] : &h->out[1]);
+    output_join(*o);
+    const size_t nstate = 1 + 10 * (size_t)ne + 6 * (size_t)ng;
+    const size_t need = nstate + (tecplot_path ? 13 * (size_t)ne : 0);
+    if (o->cap < need) {
+        if (o->d_buf) cudaFree(o->d_buf);
+        if (o->h_buf) cudaFreeHost(o->h_buf);
+        o->d_buf = nullptr; o->h_buf = nullptr; o->cap = 0;
+        CUDA_OK(h, cudaMalloc((void**)&o->d_buf, need * sizeof(double)));
+        CUDA_OK(h, cudaMallocHost((void**)&o->h_buf, need * sizeof(double)));
+        o->cap = need;
+    }
+    if (!o->ready) CUDA_OK(h, cudaEventCreateWithFlags(&o->ready, cudaEventDisableTiming));
+    if (!o->copied) CUDA_OK(h, cudaEventCreateWithFlags(&o->copied, cudaEventDisableTiming));
+    if (!h->ostream) CUDA_OK(h, cudaStreamCreateWithFlags(&h->ostream, cudaStreamNonBlocking));
+    cudaStream_t st = h->stream;
+    double* d = o->d_buf;
+    CUDA_OK(h, cudaMemcpyAsync(d, (const char*)(h->ds.s + c) + offsetof(DevScalars, time), sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
+    k_gather_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cu, ld, 0, ne, 10, h->d_perm + cr.e0, d + 1);
+    CUDA_OK(h, cudaGetLastError());
+    if (ng) {
+        k_gather_ghost_prims<<<blocks_for(6LL * ng, 256), 256, 0, st>>>(h->ds.pr, ld, GHOST_COLS, ng,
+                                                                        h->d_gid + cr.g0, d + 1 + 10 * (size_t)ne);
+        CUDA_OK(h, cudaGetLastError());
+    }
+    if (tecplot_path) CUDA_OK(h, hp::launch_tecplot_fields(h->ds.cu, ld, ne, h->d_perm + cr.e0, h->dp, d + nstate, st));
+    CUDA_OK(h, cudaEventRecord(o->ready, st));
+    CUDA_OK(h, cudaStreamWaitEvent(h->ostream, o->ready, 0));
+    CUDA_OK(h, cudaMemcpyAsync(o->h_buf, d, need * sizeof(double), cudaMemcpyDeviceToHost, h->ostream));
+    CUDA_OK(h, cudaEventRecord(o->copied, h->ostream));
+    o->ticket = h->next_ticket++;
+    o->rc = HP_OK;
+    const std::string rp = restart_path ? restart_path : "", tp = tecplot_path ? tecplot_path : "";
+    o->writer = std::thread([o, rp, tp, ne, ng, nstate, mesh]() {
+        if (cudaEventSynchronize(o->copied) != cudaSuccess) { o->rc = HP_E_CUDA; return; }
+        const double* b = o->h_buf;
+        int rc = HP_OK;
+        if (!rp.empty()) rc = hp_write_restart(rp.c_str(), ne, ng, b[0], b + 1, b + 1 + 10 * (size_t)ne);
+        if (rc == HP_OK && !tp.empty()) rc = hp_write_tecplot(tp.c_str(), mesh, b + nstate);
+        o->rc = rc;
+    });
+    *ticket = o->ticket;
+    return HP_OK;
+}
+
+extern "C" int hp_output_wait(hp_handle* h, int32_t ticket) {
+    if (!h) return HP_E_ARG;
+    for (OutSlot& o : h->out)
+        if (o.ticket && o.ticket == ticket) {
+            const int rc = output_join(o);
+            return rc == HP_OK ? HP_OK : fail(h, rc, "asynchronous output failed");
+        }
+    return fail(h, HP_E_ARG, "unknown or already collected output ticket");
 }
 
 extern "C" int hp_get_prims(hp_handle* h, double* prims) {

@@ -8,6 +8,7 @@
 // All reads are list-directed in the reference: one READ statement consumes
 // whole records (lines), values separated by blanks or commas, extra values
 // on a record ignored, 'd'/'D' accepted as exponent letters.
+#include <algorithm>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -313,4 +314,62 @@ extern "C" int hp_write_restart(const char* path, int32_t neles, int32_t nghosts
         std::fputc('\n', f);
     }
     return std::fclose(f) == 0 ? HP_OK : HP_E_IO;
+}
+
+// ---------------------------------------------------------------------------
+// Tecplot file of src/main.F90:956-1268 (two-phase build).  Values go out as
+// Fortran ES16.8: one significant digit before the point, eight after, a
+// two-digit exponent with its E, or a three-digit exponent without it, right
+// in a 16-character field.  Every value line is 17 bytes, so blocks of lines
+// are formatted in parallel into a buffer and written in order.
+namespace {
+void es16_8(double v, char* out) {
+    char b[40];
+    if (std::isnan(v)) {
+        std::snprintf(b, sizeof b, "NaN");
+    } else if (std::isinf(v)) {
+        std::snprintf(b, sizeof b, v > 0 ? "Infinity" : "-Infinity");
+    } else {
+        std::snprintf(b, sizeof b, "%.8E", v);
+        char* e = std::strchr(b, 'E');
+        if (e && std::strlen(e + 2) == 3) std::memmove(e, e + 1, std::strlen(e + 1) + 1);
+    }
+    const size_t n = std::strlen(b);
+    std::memset(out, ' ', 16);
+    std::memcpy(out + 16 - n, b, n);
+    out[16] = '\n';
+}
+
+bool put_column(FILE* f, const double* v, size_t n, std::vector<char>& buf) {
+    const size_t block = (size_t)1 << 20;
+    buf.resize(block * 17);
+    for (size_t s = 0; s < n; s += block) {
+        const long long m = (long long)std::min(block, n - s);
+#pragma omp parallel for schedule(static)
+        for (long long k = 0; k < m; k++) es16_8(v[s + k], buf.data() + 17 * k);
+        if (std::fwrite(buf.data(), 17, (size_t)m, f) != (size_t)m) return false;
+    }
+    return true;
+}
+}  // namespace
+
+extern "C" int hp_write_tecplot(const char* path, const hp_mesh* mesh, const double* fields) {
+    if (!path || !mesh || !fields || !mesh->x || !mesh->y || !mesh->z || !mesh->elem || mesh->neles <= 0 ||
+        mesh->nodes <= 0)
+        return HP_E_ARG;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return HP_E_IO;
+    const size_t ne = (size_t)mesh->neles, nn = (size_t)mesh->nodes;
+    std::fprintf(f, " VARIABLES = \"X\", \"Y\", \"Z\", \"U\",\"V\", \"W\", \"PG\", \"PP\", \"TG\", \"UP\", \"VP\", "
+                    "\"WP\", \"PHIG\", \"TP\", \"ROG\", \"ROP\"\n");
+    std::fprintf(f, "ZONE ZONETYPE=FETETRAHEDRON, NODES=%zu, ELEMENTS=%zu, DATAPACKING=BLOCK, "
+                    "VARLOCATION=([4-16]=CELLCENTERED)\n", nn, ne);
+    std::vector<char> buf;
+    bool ok = put_column(f, mesh->x, nn, buf) && put_column(f, mesh->y, nn, buf) && put_column(f, mesh->z, nn, buf);
+    for (int k = 0; k < 13 && ok; k++) ok = put_column(f, fields + (size_t)k * ne, ne, buf);
+    for (size_t e = 0; e < ne && ok; e++) {
+        const int32_t* r = mesh->elem + 9 * e;
+        ok = std::fprintf(f, "%12d%12d%12d%12d\n", r[0], r[1], r[2], r[3]) > 0;
+    }
+    return (std::fclose(f) == 0 && ok) ? HP_OK : HP_E_IO;
 }

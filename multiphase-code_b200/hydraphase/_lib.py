@@ -107,12 +107,17 @@ def lib():
     L.hp_free_mesh.argtypes = [ctypes.POINTER(HpMesh)]
     L.hp_read_restart.argtypes = [ctypes.c_char_p, _I, _I, _DP, _DP, _DP]
     L.hp_write_restart.argtypes = [ctypes.c_char_p, _I, _I, _D, _DP, _DP]
+    L.hp_write_tecplot.argtypes = [ctypes.c_char_p, ctypes.POINTER(HpMesh), _DP]
+    L.hp_output_async.argtypes = [vp, _I, ctypes.POINTER(HpMesh), ctypes.c_char_p, ctypes.c_char_p,
+                                  ctypes.POINTER(_I)]
+    L.hp_output_wait.argtypes = [vp, _I]
     for fn in ("hp_create", "hp_destroy", "hp_init_uniform", "hp_set_state", "hp_step", "hp_sync",
                "hp_step_timed", "hp_profile_steps", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll",
                "hp_create_batch", "hp_case_count", "hp_set_state_case", "hp_get_state_case",
                "hp_estimate_batch_bytes", "hp_overset_build", "hp_overset_build_gpu", "hp_set_overset",
                "hp_get_state", "hp_get_prims", "hp_device_state", "hp_info", "hp_read_flow",
-               "hp_read_mesh", "hp_read_restart", "hp_write_restart"):
+               "hp_read_mesh", "hp_read_restart", "hp_write_restart", "hp_write_tecplot", "hp_output_async",
+               "hp_output_wait"):
         getattr(L, fn).restype = ctypes.c_int
     _lib = L
     return L
@@ -127,6 +132,6 @@ EXPORTED_SYMBOLS = (
     "hp_info", "hp_read_flow", "hp_read_mesh", "hp_free_mesh", "hp_read_restart",
     "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll", "hp_create_batch", "hp_case_count",
     "hp_set_state_case", "hp_get_state_case", "hp_estimate_batch_bytes", "hp_overset_build", "hp_free_overset",
-    "hp_set_overset", "hp_overset_build_gpu",
+    "hp_set_overset", "hp_overset_build_gpu", "hp_write_tecplot", "hp_output_async", "hp_output_wait",
 )
 NOALLOC_MAX_CELLS = 1 << 24

@@ -120,6 +120,15 @@ def overset_build(mesh: MeshArrays, block, layers: int = 2, outer_type: int = 7,
         lib().hp_free_overset(ctypes.byref(ov))
 
 
+def write_tecplot(path: str, mesh: MeshArrays, fields: np.ndarray):
+    """The reference's Tecplot file (hp_write_tecplot) from the 13
+    cell-centred fields (13, neles)."""
+    keep = []
+    hm = _hp_mesh(mesh, keep)
+    f = np.ascontiguousarray(fields, np.float64)
+    _check(lib().hp_write_tecplot(path.encode(), ctypes.byref(hm), _dp(f)))
+
+
 def estimate_batch_bytes(meshes, params: HpParams) -> int:
     """Device bytes a Batch of these meshes would hold."""
     arr = (HpMesh * len(meshes))(*[HpMesh(m.nodes, m.neles, m.nghosts, 0, None, None, None, None, None)
@@ -231,6 +240,28 @@ class Case:
         gp = np.zeros(6 * max(self.nghosts, 1))
         _check(self.L.hp_get_state(self.h, ctypes.byref(t), _dp(cu), _dp(gp)), self.h)
         return t.value, cu.reshape(10, self.neles), gp[:6 * self.nghosts].reshape(6, self.nghosts)
+
+    def output_async(self, restart_path=None, tecplot_path=None, mesh: MeshArrays | None = None) -> int:
+        """Start writing the current state (after the steps enqueued so far)
+        to a restart file and/or a Tecplot file while later steps run
+        (hp_output_async); returns a ticket for output_wait.  Tecplot needs
+        the case's mesh, kept alive here until the wait."""
+        keep = []
+        hm = _hp_mesh(mesh, keep) if mesh is not None else None
+        t = ctypes.c_int32()
+        _check(self.L.hp_output_async(self.h, 0, ctypes.byref(hm) if hm is not None else None,
+                                      restart_path.encode() if restart_path else None,
+                                      tecplot_path.encode() if tecplot_path else None, ctypes.byref(t)), self.h)
+        self._out_keep = getattr(self, "_out_keep", {})
+        self._out_keep[t.value] = (keep, hm)
+        return t.value
+
+    def output_wait(self, ticket: int):
+        """Block until the files of an output_async request are written."""
+        try:
+            _check(self.L.hp_output_wait(self.h, int(ticket)), self.h)
+        finally:
+            getattr(self, "_out_keep", {}).pop(int(ticket), None)
 
     def prims(self):
         out = np.zeros(14 * self.neles)
