@@ -328,6 +328,43 @@ def accuracy_run(spec, steps: int) -> dict:
             "nan_cells": {k: int((~np.isfinite(v)).any(axis=0).sum()) for k, v in states.items()}}
 
 
+def output_measure(steps: int = 300) -> dict:
+    """Restart + Tecplot output of the 983k-cell cylinder (mixed variant)
+    written while `steps` steps run (hp_output_async), against the same
+    output written with the steps stopped: wall-clock seconds and the
+    fraction of the write time hidden behind the steps."""
+    import shutil
+    from hydraphase import PREC_MIXED, Case
+    spec = make_workload("cylinder_medium")
+    d = tempfile.mkdtemp(prefix="hp_out_")
+    try:
+        with Case(spec.mesh, spec.params(precision=PREC_MIXED)) as c:
+            c.set_state(0.0, spec.cu, spec.ghost_prims)
+            c.step(3, diagnostics=False)
+            c.sync()
+            t0 = time.perf_counter()
+            c.step(steps, diagnostics=False)
+            c.sync()
+            t_steps = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            c.output_wait(c.output_async(os.path.join(d, "r1.in"), os.path.join(d, "t1.dat"), mesh=spec.mesh))
+            t_write = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            tk = c.output_async(os.path.join(d, "r2.in"), os.path.join(d, "t2.dat"), mesh=spec.mesh)
+            c.step(steps, diagnostics=False)
+            c.sync()
+            t_steps_during = time.perf_counter() - t0
+            c.output_wait(tk)
+            t_both = time.perf_counter() - t0
+            size = os.path.getsize(os.path.join(d, "r2.in")) + os.path.getsize(os.path.join(d, "t2.dat"))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return {"workload": f"cylinder 983,040 cells, mixed, {steps} steps; one restart + Tecplot file ({size / 1e6:.0f} MB)",
+            "steps_s": round(t_steps, 3), "write_stopped_s": round(t_write, 3),
+            "steps_while_writing_s": round(t_steps_during, 3), "steps_and_write_overlapped_s": round(t_both, 3),
+            "hidden_fraction": round((t_steps + t_write - t_both) / t_write, 3) if t_write > 0 else None}
+
+
 def run_reference_arm(args, world, rank, pg):
     if rank != 0:
         return 0
@@ -457,6 +494,8 @@ def run_ours(args, world, rank, local, pg):
         line["mixed"]["accuracy"] = accuracy_run(spec, args.accuracy_steps)
     if world == 1 and rank == 0 and not args.no_overset:
         line["overset"] = overset_measure(max(args.steps // 2, 5))
+    if world == 1 and rank == 0 and not args.no_output:
+        line["output"] = output_measure()
     if world == 1 and rank == 0 and args.serving_cases > 0:
         sv = serving_measure(args.serving_cases, args.serving_steps)
         sv["mixed_served_vs_plain_fp64_value"] = sv["mixed"]["updates_per_s"] / value
@@ -478,6 +517,7 @@ def main():
                     help="cases of the serving stream measured after the step benchmark (0: skip)")
     ap.add_argument("--serving-steps", type=int, default=500)
     ap.add_argument("--no-overset", action="store_true", help="skip the overset cylinder measurement")
+    ap.add_argument("--no-output", action="store_true", help="skip the asynchronous output measurement")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy run on the timed workload (0: skip)")
     args = ap.parse_args()

@@ -294,9 +294,25 @@ extern "C" int hp_read_restart(const char* path, int32_t neles, int32_t nghosts,
 }
 
 namespace {
-void put(FILE* f, double v) {
-    if (std::isnan(v)) std::fputs("                       NaN", f);
-    else std::fprintf(f, " %25.16E", v);
+// One restart value: " %25.16E" (26 characters; NaN right-justified).
+void put26(double v, char* out) {
+    char b[40];
+    if (std::isnan(v)) std::snprintf(b, sizeof b, " %25s", "NaN");
+    else std::snprintf(b, sizeof b, " %25.16E", v);
+    std::memcpy(out, b, 26);
+}
+
+// Values of one record, formatted in parallel blocks of fixed-width fields.
+bool put_record(FILE* f, const double* v, size_t n, std::vector<char>& buf) {
+    const size_t block = (size_t)1 << 20;
+    buf.resize(block * 26);
+    for (size_t s = 0; s < n; s += block) {
+        const long long m = (long long)std::min(block, n - s);
+#pragma omp parallel for schedule(static)
+        for (long long k = 0; k < m; k++) put26(v[s + k], buf.data() + 26 * k);
+        if (std::fwrite(buf.data(), 26, (size_t)m, f) != (size_t)m) return false;
+    }
+    return std::fputc('\n', f) != EOF;
 }
 }  // namespace
 
@@ -305,15 +321,10 @@ extern "C" int hp_write_restart(const char* path, int32_t neles, int32_t nghosts
     if (!path || !cu_elem || !ghost_prims) return HP_E_ARG;
     FILE* f = std::fopen(path, "w");
     if (!f) return HP_E_IO;
-    put(f, time);
-    std::fputc('\n', f);
-    for (size_t i = 0; i < (size_t)neles * 10; i++) put(f, cu_elem[i]);
-    std::fputc('\n', f);
-    for (int v = 0; v < 6; v++) {
-        for (int g = 0; g < nghosts; g++) put(f, ghost_prims[(size_t)v * nghosts + g]);
-        std::fputc('\n', f);
-    }
-    return std::fclose(f) == 0 ? HP_OK : HP_E_IO;
+    std::vector<char> buf;
+    bool ok = put_record(f, &time, 1, buf) && put_record(f, cu_elem, (size_t)neles * 10, buf);
+    for (int v = 0; v < 6 && ok; v++) ok = put_record(f, ghost_prims + (size_t)v * nghosts, (size_t)nghosts, buf);
+    return (std::fclose(f) == 0 && ok) ? HP_OK : HP_E_IO;
 }
 
 // ---------------------------------------------------------------------------
