@@ -256,14 +256,15 @@ def serving_measure(n_cases: int, steps: int):
                        f"from arrival to the final state on the host",
            "cells_total": int(sum(r.spec.mesh.neles for r in reqs)), "generation_s": round(gen_s, 2)}
     for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64_PARITY)):
-        blocks = {}
+        blocks, modes = {}, {}
         for r in reqs:
             cls = tune.size_class(r.spec.mesh.neles)
             if cls not in blocks:
                 blocks[cls] = tune.tune_block_size(r.spec, precision=prec, steps=4)[0]
+                modes[cls] = tune.tune_face_mode(r.spec, precision=prec, block_size=blocks[cls], steps=4)[0]
         rep_ = Server(150 << 30, precision=prec, max_active=16, chunk=25, batch_cells=200000,
-                      block_size=blocks, keep_state=True).run(reqs)
-        out[name] = {**rep_.summary(), "block_size": blocks}
+                      block_size=blocks, face_mode=modes, keep_state=True).run(reqs)
+        out[name] = {**rep_.summary(), "block_size": blocks, "face_mode": modes}
     out["speedup_mixed_vs_fp64"] = out["mixed"]["updates_per_s"] / out["fp64"]["updates_per_s"]
     return out
 

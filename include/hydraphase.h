@@ -65,7 +65,10 @@ typedef struct hp_params {
     int32_t myorder;         /* 1 or 2 */
     double as, ts;           /* Sutherland constants */
     /* --- additions; zero-initialised values reproduce the reference --- */
-    int32_t reserved0;
+    int32_t face_mode;       /* FP32-arithmetic variants: 0 = fluxes evaluated
+                                once per face where the mesh allows, 1 = once
+                                from each side (four lanes per cell);
+                                hydraphase.tune picks it */
     double venkat_k;         /* limiter eps^2 = (K*dl)^3; 0 selects 0.3 */
     int32_t rk_scheme;       /* 0: reference 4-stage ESSPRK; 1: SSP-RK3 */
     int32_t inviscid;        /* 1: viscous face fluxes off */

@@ -549,7 +549,7 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     // when the other side is a ghost); meshes whose neighbour lists are not
     // mutual, and aliased meshes, keep the cell-centric fluxes ---
     std::vector<int> hf_i, hf_code, hcface;
-    if (gb != D && !h->aliased) {
+    if (gb != D && !h->aliased && h->prm.face_mode == 0) {
         hcface.assign(4 * (size_t)ld, 0);
         bool mutual = true;
         for (int t = 0; t < neles && mutual; t++)
@@ -1033,7 +1033,7 @@ extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, i
     const size_t gb = (params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32) ? sizeof(float)
                                                                                                 : sizeof(double);
     Arena probe;
-    const int nface = gb == sizeof(double) ? 0 : (int)((4LL * mesh->neles + mesh->nghosts) / 2);
+    const int nface = gb == sizeof(double) || params->face_mode ? 0 : (int)((4LL * mesh->neles + mesh->nghosts) / 2);
     plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb, 1, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
@@ -1053,7 +1053,7 @@ extern "C" int hp_estimate_batch_bytes(const hp_mesh* meshes, int32_t ncase, con
     const size_t gb = (params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32) ? sizeof(float)
                                                                                                 : sizeof(double);
     Arena probe;
-    const int nface = gb == sizeof(double) ? 0 : (int)((4 * ne + ng) / 2);
+    const int nface = gb == sizeof(double) || params->face_mode ? 0 : (int)((4 * ne + ng) / 2);
     plan_arena(&probe_h, probe, (int)ne, (int)ng, ld, gb, ncase, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;

@@ -857,6 +857,15 @@ __device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& p
     }
 }
 
+// face-state loads through the read-only data path (1) or plain (0)
+#ifndef HP_FACE_LDG
+#define HP_FACE_LDG 1
+#endif
+#if HP_FACE_LDG
+#define PLD(p) ldg(p)
+#else
+#define PLD(p) (*(p))
+#endif
 // F selects the division form (see mdiv); bad collects its out-of-range flag.
 template <int F, class PT>
 __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s, const DevParams& P,
@@ -869,16 +878,16 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     const R area = sqrt(scx * scx + scy * scy + scz * scz);
     const R rarea = mrcp<F>(area, bad);
     const R enx = mdiv<F>(scx, area, rarea, bad), eny = mdiv<F>(scy, area, rarea, bad), enz = mdiv<F>(scz, area, rarea, bad);
-    R ugL = (R)COL(pr, P_UG)[i], vgL = (R)COL(pr, P_VG)[i], wgL = (R)COL(pr, P_WG)[i];
-    R tgL = (R)COL(pr, P_TG)[i], phigL = (R)COL(pr, P_PHIG)[i];
-    R upL = (R)COL(pr, P_UP)[i], vpL = (R)COL(pr, P_VP)[i], wpL = (R)COL(pr, P_WP)[i];
-    R tpL = (R)COL(pr, P_TP)[i], pgL = (R)COL(pr, P_PG)[i], ppL = (R)COL(pr, P_PP)[i];
-    R ugR = (R)COL(pr, P_UG)[neigh], vgR = (R)COL(pr, P_VG)[neigh], wgR = (R)COL(pr, P_WG)[neigh];
-    R tgR = (R)COL(pr, P_TG)[neigh], phigR = (R)COL(pr, P_PHIG)[neigh];
-    R upR = (R)COL(pr, P_UP)[neigh], vpR = (R)COL(pr, P_VP)[neigh], wpR = (R)COL(pr, P_WP)[neigh];
-    R tpR = (R)COL(pr, P_TP)[neigh], pgR = (R)COL(pr, P_PG)[neigh], ppR = (R)COL(pr, P_PP)[neigh];
+    R ugL = (R)PLD(COL(pr, P_UG) + i), vgL = (R)PLD(COL(pr, P_VG) + i), wgL = (R)PLD(COL(pr, P_WG) + i);
+    R tgL = (R)PLD(COL(pr, P_TG) + i), phigL = (R)PLD(COL(pr, P_PHIG) + i);
+    R upL = (R)PLD(COL(pr, P_UP) + i), vpL = (R)PLD(COL(pr, P_VP) + i), wpL = (R)PLD(COL(pr, P_WP) + i);
+    R tpL = (R)PLD(COL(pr, P_TP) + i), pgL = (R)PLD(COL(pr, P_PG) + i), ppL = (R)PLD(COL(pr, P_PP) + i);
+    R ugR = (R)PLD(COL(pr, P_UG) + neigh), vgR = (R)PLD(COL(pr, P_VG) + neigh), wgR = (R)PLD(COL(pr, P_WG) + neigh);
+    R tgR = (R)PLD(COL(pr, P_TG) + neigh), phigR = (R)PLD(COL(pr, P_PHIG) + neigh);
+    R upR = (R)PLD(COL(pr, P_UP) + neigh), vpR = (R)PLD(COL(pr, P_VP) + neigh), wpR = (R)PLD(COL(pr, P_WP) + neigh);
+    R tpR = (R)PLD(COL(pr, P_TP) + neigh), pgR = (R)PLD(COL(pr, P_PG) + neigh), ppR = (R)PLD(COL(pr, P_PP) + neigh);
     if (P.myorder == 2 && (kind & FK_RECON)) {
-        const R phimin = (R)mn2(s.phi[i], s.phi[neigh]);
+        const R phimin = (R)mn2(PLD(s.phi + i), PLD(s.phi + neigh));
         const double xf = ldg(COL(m.fch, f) + i), yf = ldg(COL(m.fch, 4 + f) + i),
                      zf = ldg(COL(m.fch, 8 + f) + i);
         const R xf0 = (R)(xf - ldg(m.xc + i)), yf0 = (R)(yf - ldg(m.yc + i)), zf0 = (R)(zf - ldg(m.zc + i));
@@ -886,7 +895,7 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
                 zfn = (R)(zf - ldg(m.zc + neigh));
         const R* g = s.gr;
 #define REC(v, X, Y, Z, G, c) \
-    v = v + phimin * (X * COL(g, G)[c] + Y * COL(g, G + 1)[c] + Z * COL(g, G + 2)[c])
+    v = v + phimin * (X * PLD(COL(g, G) + c) + Y * PLD(COL(g, G + 1) + c) + Z * PLD(COL(g, G + 2) + c))
         REC(phigL, xf0, yf0, zf0, G_PHIG, i); REC(ugL, xf0, yf0, zf0, G_UG, i);
         REC(vgL, xf0, yf0, zf0, G_VG, i); REC(wgL, xf0, yf0, zf0, G_WG, i);
         REC(tgL, xf0, yf0, zf0, G_TG, i); REC(pgL, xf0, yf0, zf0, G_PG, i);

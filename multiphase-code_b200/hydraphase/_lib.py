@@ -33,7 +33,7 @@ class HpParams(ctypes.Structure):
         "gamag", "cpp", "cpg", "amolg", "prg", "epslnmax", "epslnmin", "epslninf", "phipzero",
         "cfl")] + [
         ("niter", _I), ("itersub", _I), ("istart", _I), ("diap", _D), ("surfacetension", _D),
-        ("myflux", _I), ("myorder", _I), ("as_", _D), ("ts", _D), ("reserved0", _I),
+        ("myflux", _I), ("myorder", _I), ("as_", _D), ("ts", _D), ("face_mode", _I),
         ("venkat_k", _D), ("rk_scheme", _I), ("inviscid", _I), ("twall", _D), ("precision", _I),
         ("renumber", _I), ("block_size", _I), ("use_graph", _I), ("pad_", _D * 4)]
 

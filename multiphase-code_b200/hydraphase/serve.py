@@ -120,11 +120,12 @@ class Server:
     max_batch: cases per batch at most
     block_size: threads per block of the per-cell kernels: an int, a dict
         from hydraphase.tune.size_class() to an int, or None (256)
+    face_mode: hp_params.face_mode, an int or a dict by size class (None: 0)
     """
 
     def __init__(self, hbm_budget: int, precision: int = PREC_MIXED, max_active: int = 12, chunk: int = 25,
                  setup_workers: int = 8, keep_state: bool = True, param_overrides: dict | None = None,
-                 batch_cells: int = 0, max_batch: int = 64, block_size=None):
+                 batch_cells: int = 0, max_batch: int = 64, block_size=None, face_mode=None):
         self.budget = int(hbm_budget)
         self.precision = precision
         self.max_active = max_active
@@ -135,15 +136,20 @@ class Server:
         self.batch_cells = int(batch_cells)
         self.max_batch = int(max_batch)
         self.block_size = block_size
+        self.face_mode = face_mode
 
     def _params(self, spec, cells: int):
+        from .tune import size_class
         over = dict(self.over)
-        b = self.block_size
+        b, fm = self.block_size, self.face_mode
         if isinstance(b, dict):
-            from .tune import size_class
             b = b.get(size_class(cells))
+        if isinstance(fm, dict):
+            fm = fm.get(size_class(cells))
         if b and "block_size" not in over:
             over["block_size"] = int(b)
+        if fm and "face_mode" not in over:
+            over["face_mode"] = int(fm)
         return spec.params(precision=self.precision, **over)
 
     @staticmethod

@@ -3,12 +3,16 @@ for each mesh-size class, and caches the choices.
 
 Two levels are tuned:
 
-* **Kernels** (`tune_block_size`). These are the threads per block of the
-  one-thread-per-cell kernels: primitive recovery, JST smoothing and ghost
-  fill. Every candidate runs a few device-timed steps (CUDA events) of a
-  representative case of the class, and the fastest is kept. The four-lane
-  gradient, flux and viscous kernels have their block size fixed by their
-  launch bounds, tuned per precision variant at build time.
+* **Kernels** (`tune_block_size`, `tune_face_mode`). These are the threads
+  per block of the one-thread-per-cell kernels (primitive recovery, JST
+  smoothing, ghost fill, and the gradients and face gathers of the
+  FP32-arithmetic variants) and, for those variants, whether the HLLC and
+  viscous fluxes are evaluated once per face (a face list, one thread per
+  face, then a per-cell gather) or once from each side (four lanes per cell,
+  one kernel fewer per stage). Every candidate runs a few device-timed steps
+  (CUDA events) of a representative case of the class, and the fastest is
+  kept. The four-lane kernels have their block size fixed by their launch
+  bounds, tuned per precision variant at build time.
 * **Serving** (`tune_serving`). These are the units in flight, the
   multi-mesh batch size and the steps enqueued per turn. Every candidate
   serves a short sample of the stream with all cases arriving at once, and
@@ -25,7 +29,7 @@ import json
 import os
 import time
 
-from ._lib import PREC_MIXED
+from ._lib import PREC_FP32, PREC_MIXED
 from .engine import Case
 
 SIZE_CLASSES = ((0, 20000, "xs"), (20000, 100000, "s"), (100000, 400000, "m"), (400000, 1 << 62, "l"))
@@ -88,6 +92,32 @@ def tune_block_size(spec, precision: int = PREC_MIXED, candidates=BLOCK_CANDIDAT
             c.set_state(0.0, spec.cu, spec.ghost_prims)
             c.step(2, diagnostics=False)
             ms[int(b)] = min(c.step_timed(steps), c.step_timed(steps)) / steps
+    best = min(ms, key=ms.get)
+    data = _load()
+    data[key] = {"best": best, "ms": {str(k): v for k, v in ms.items()}, "cells": spec.mesh.neles,
+                 "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+    _store(data)
+    return best, ms
+
+
+def tune_face_mode(spec, precision: int = PREC_MIXED, block_size: int = 0, steps: int = 6,
+                   use_cache: bool = True) -> tuple[int, dict]:
+    """hp_params.face_mode for the size class of `spec` in the
+    FP32-arithmetic variants: 0 (once per face) or 1 (once from each side);
+    returns (best, {mode: ms per step}).  The FP64 variants have one mode."""
+    if precision not in (PREC_MIXED, PREC_FP32):
+        return 0, {}
+    key = _key(precision, size_class(spec.mesh.neles), f"face_mode_b{block_size}")
+    if use_cache:
+        hit = _load().get(key)
+        if hit:
+            return int(hit["best"]), {int(k): v for k, v in hit["ms"].items()}
+    ms = {}
+    for mode in (0, 1):
+        with Case(spec.mesh, spec.params(precision=precision, block_size=int(block_size), face_mode=mode)) as c:
+            c.set_state(0.0, spec.cu, spec.ghost_prims)
+            c.step(2, diagnostics=False)
+            ms[mode] = min(c.step_timed(steps), c.step_timed(steps)) / steps
     best = min(ms, key=ms.get)
     data = _load()
     data[key] = {"best": best, "ms": {str(k): v for k, v in ms.items()}, "cells": spec.mesh.neles,

@@ -104,13 +104,15 @@ def _alpha_g(cu, flow):
     return cu[0] * (gg - 1) * eg / pg
 
 
-def test_mixed_within_tolerance():
+@pytest.mark.parametrize("face_mode", [0, 1])
+def test_mixed_within_tolerance(face_mode):
     """Mixed path (FP32 gradients/limiter/fluxes/viscous, FP64 state, EOS
     and reductions) against the FP64 oracle: mixture density, alpha_g and
-    the air energy within 1e-5 relative L2."""
+    the air energy within 1e-5 relative L2, with the fluxes evaluated once
+    per face (face_mode 0) and once from each side (1)."""
     spec = SPECS["cylinder"]()
     _, _, _, cu_o, _ = _oracle_run(spec, 5)
-    _, _, cu_g, _ = _gpu_run(spec, 5, PREC_MIXED)
+    _, _, cu_g, _ = _gpu_run(spec, 5, PREC_MIXED, face_mode=face_mode)
     assert np.all(np.isfinite(cu_g))
     rho_o, rho_g = cu_o[0] + cu_o[5], cu_g[0] + cu_g[5]
     assert np.linalg.norm(rho_g - rho_o) / np.linalg.norm(rho_o) < 1e-5

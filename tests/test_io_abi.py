@@ -166,5 +166,5 @@ def test_params_layout_matches_header():
     # bind(C) interfaces: fixed size and offsets
     assert ctypes.sizeof(HpParams) == 376
     assert HpParams.cfl.offset == 29 * 8
-    assert HpParams.reserved0.offset == 296
-    assert HpParams.venkat_k.offset == HpParams.reserved0.offset + 8
+    assert HpParams.face_mode.offset == 296
+    assert HpParams.venkat_k.offset == HpParams.face_mode.offset + 8

@@ -95,3 +95,14 @@ def test_block_size_tuner_measures_and_caches(tmp_path, monkeypatch):
     assert best in (128, 256) and set(ms) == {128, 256}
     best2, ms2 = tune.tune_block_size(spec, candidates=(128, 256), steps=2)
     assert best2 == best and ms2 == ms
+
+
+@pytest.mark.gpu
+def test_face_mode_tuner_measures_and_caches(tmp_path, monkeypatch):
+    from hydraphase import PREC_FP64_PARITY, tune
+    monkeypatch.setenv("HYDRAPHASE_TUNE_CACHE", str(tmp_path / "t.json"))
+    spec = cases.shock_bubble(n=8, alpha_min=0.1)
+    best, ms = tune.tune_face_mode(spec, steps=2)
+    assert best in (0, 1) and set(ms) == {0, 1}
+    assert tune.tune_face_mode(spec, steps=2) == (best, ms)
+    assert tune.tune_face_mode(spec, precision=PREC_FP64_PARITY) == (0, {})
