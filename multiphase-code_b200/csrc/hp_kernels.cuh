@@ -86,21 +86,6 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 #ifndef HP_S
 #define HP_S double
 #endif
-// face-based variants: one thread per cell (1) or four lanes per cell (0)
-// gather the face fluxes, add the sources and update the state
-#ifndef HP_FACE_CELL1
-#define HP_FACE_CELL1 1
-#endif
-// FP32-arithmetic variants: one-thread-per-cell gradients (1) or four lanes
-// per cell (0)
-#ifndef HP_GRAD_CELL1
-#define HP_GRAD_CELL1 1
-#endif
-// FP32-arithmetic variants: one-thread-per-cell viscous fluxes (1) or four
-// lanes per cell (0)
-#ifndef HP_VISC_CELL1
-#define HP_VISC_CELL1 0
-#endif
 // FP32-arithmetic variants with a face list: viscous fluxes evaluated once
 // per face (1) instead of once from each side (0)
 #ifndef HP_FACE_VISC
@@ -1408,7 +1393,7 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
 // form (see mdiv).  The fast form returns false, before any store, when a lane
 // of the warp flagged an operand (cn is read and written here, so the stores
 // must wait for that vote).
-template <int F, bool FACE>
+template <int F>
 __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int stage,
                                            int i, int q, bool active) {
     unsigned bad = 0;
@@ -1416,18 +1401,7 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     // this lane's face
     R eff[10];
     int flags;
-    if constexpr (FACE) {
-        // the face's flux, evaluated once by k_faceflux in the owner's
-        // orientation: outgoing for the owner, incoming for the other cell
-        const int code = ldg(COL(m.cface, q) + i);
-        const int fid = (code > 0 ? code : -code) - 1;
-        const R sg = code > 0 ? R(1) : R(-1);
-        R rec[FACE_REC];
-        load_frec(s.ff + (size_t)FACE_REC * (size_t)fid, rec);
-#pragma unroll
-        for (int k = 0; k < 10; k++) eff[k] = sg * rec[k];
-        flags = rec[10] != R(0) ? 1 : 6;
-    } else {
+    {
         FaceOut o;
         face_eval<F>(m, s, P, i, q, o, bad, s.prr);
         if (o.wall) {
@@ -1590,7 +1564,6 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     return true;
 }
 
-template <bool FACE>
 __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
@@ -1598,10 +1571,10 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevStat
     const bool valid = i < m.neles;
     if (!valid) i = m.neles - 1;
     const bool active = valid && ldg(m.iblank + i) == 1;
-    if constexpr (HP_FAST(2) && !FACE) {
-        if (!flux4_body<1, false>(m, s, P, stage, i, q, active)) flux4_body<0, false>(m, s, P, stage, i, q, active);
+    if constexpr (HP_FAST(2)) {
+        if (!flux4_body<1>(m, s, P, stage, i, q, active)) flux4_body<0>(m, s, P, stage, i, q, active);
     } else {
-        flux4_body<0, FACE>(m, s, P, stage, i, q, active);
+        flux4_body<0>(m, s, P, stage, i, q, active);
     }
 }
 
@@ -1727,7 +1700,6 @@ __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s
 }
 
 // one thread per cell (aliased meshes)
-template <bool FPR>
 __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParams P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
@@ -1742,8 +1714,7 @@ __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParam
     for (int f = 0; f < 4; f++) {
         double c[8];
         unsigned bad_ = 0;
-        if constexpr (FPR) visc_face<0>(m, s, P, i, f, nci, c, bad_, s.prr);
-        else visc_face<0>(m, s, P, i, f, nci, c, bad_, s.pr);
+        visc_face<0>(m, s, P, i, f, nci, c, bad_, s.pr);
 #pragma unroll
         for (int k = 0; k < 8; k++) acc[k] = acc[k] + c[k];
     }
@@ -1901,12 +1872,10 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     if (!P.inviscid) {
         MARK(KK_VISC);
         if (m.aliased) {
-            k_visc<false><<<gf, b, 0, st>>>(m, s, P);
+            k_visc<<<gf, b, 0, st>>>(m, s, P);
         } else if (sizeof(R) != sizeof(double) && HP_FACE_VISC && m.nface > 0) {
             k_facevisc<<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
             k_vis_gather<<<grid_for(m.neles, 256), 256, 0, st>>>(m, s);
-        } else if (sizeof(R) != sizeof(double) && HP_VISC_CELL1) {
-            k_visc<true><<<gf, b, 0, st>>>(m, s, P);
         } else {
             k_visc4<<<g4, 128, 0, st>>>(m, s, P);
         }
@@ -1923,7 +1892,7 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
         if (P.myorder == 2) {
             MARK(KK_GRAD);
             if (m.aliased) k_grad<false><<<gf, b, 0, st>>>(m, s, P);
-            else if (sizeof(R) != sizeof(double) && HP_GRAD_CELL1) k_grad<true><<<gf, b, 0, st>>>(m, s, P);
+            else if (sizeof(R) != sizeof(double)) k_grad<true><<<gf, b, 0, st>>>(m, s, P);
             else k_grad4<<<g4, 128, 0, st>>>(m, s, P);
             if (m.aliased) { MARK(KK_SERIAL); k_phi_copy_serial<<<1, 1, 0, st>>>(m, s); }
         }
@@ -1934,10 +1903,9 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             k_flux_carry<<<1, 1, 0, st>>>(m, s, P);
         } else if (sizeof(R) != sizeof(double) && m.nface > 0) {
             k_faceflux<<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
-            if (HP_FACE_CELL1) k_flux<false, true><<<gf, 128, 0, st>>>(m, s, P, stage);
-            else k_flux4<true><<<g4, 128, 0, st>>>(m, s, P, stage);
+            k_flux<false, true><<<gf, 128, 0, st>>>(m, s, P, stage);
         } else {
-            k_flux4<false><<<g4, 128, 0, st>>>(m, s, P, stage);
+            k_flux4<<<g4, 128, 0, st>>>(m, s, P, stage);
         }
         if (m.nfringe > 0) {
             MARK(KK_OVERSET);
