@@ -234,12 +234,21 @@ class Case:
                                        cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n), self.h)
         return {"kinds": list(KERNEL_KINDS), "ms": ms.tolist(), "launches": cnt.tolist()}
 
-    def state(self):
+    def state(self, out=None):
+        """(time, cu (10, neles), ghost primitives (6, nghosts)).  out =
+        (cu, gp): caller buffers (C-contiguous float64 of 10 * neles and at
+        least 6 * nghosts values, e.g. pinned memory) to fill instead."""
         t = ctypes.c_double()
-        cu = np.zeros(10 * self.neles)
-        gp = np.zeros(6 * max(self.nghosts, 1))
+        if out is None:
+            cu = np.zeros(10 * self.neles)
+            gp = np.zeros(6 * max(self.nghosts, 1))
+        else:
+            cu, gp = out
+            if (cu.dtype != np.float64 or gp.dtype != np.float64 or not cu.flags.c_contiguous
+                    or not gp.flags.c_contiguous or cu.size != 10 * self.neles or gp.size < 6 * self.nghosts):
+                raise ValueError("out must be C-contiguous float64 buffers of 10*neles and 6*nghosts values")
         _check(self.L.hp_get_state(self.h, ctypes.byref(t), _dp(cu), _dp(gp)), self.h)
-        return t.value, cu.reshape(10, self.neles), gp[:6 * self.nghosts].reshape(6, self.nghosts)
+        return t.value, cu.reshape(10, self.neles), gp.reshape(-1)[:6 * self.nghosts].reshape(6, self.nghosts)
 
     def output_async(self, restart_path=None, tecplot_path=None, mesh: MeshArrays | None = None) -> int:
         """Start writing the current state (after the steps enqueued so far)

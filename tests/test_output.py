@@ -135,3 +135,22 @@ def test_async_output_matches_synchronous(tmp_path, precision):
     assert (tmp_path / "t_async.dat").read_text() == expected_tecplot(m, tecplot_fields(cu, spec.flow))
     np.testing.assert_array_equal(cu2a, cu2)   # output did not disturb the steps
     assert (tmp_path / "r_async2.in").stat().st_size > 0
+
+
+@pytest.mark.gpu
+def test_state_into_caller_buffers():
+    """Case.state(out=...) fills caller buffers (e.g. pinned memory) with the
+    same values as a fresh read-back."""
+    spec = cases.shock_bubble(n=6, alpha_min=0.1)
+    m = spec.mesh
+    with Case(m, spec.params(precision=PREC_FP64_PARITY)) as c:
+        c.set_state(0.0, spec.cu, spec.ghost_prims)
+        c.step(3, diagnostics=False)
+        t, cu, gp = c.state()
+        bufs = (np.full(10 * m.neles, np.nan), np.full(6 * m.nghosts + 5, np.nan))
+        t2, cu2, gp2 = c.state(out=bufs)
+        with pytest.raises(ValueError):
+            c.state(out=(np.zeros(3), bufs[1]))
+    assert t2 == t
+    np.testing.assert_array_equal(cu2, cu)
+    np.testing.assert_array_equal(gp2, gp)
