@@ -119,14 +119,37 @@ static int fail(hp_handle* h, int code, const std::string& msg) {
     } while (0)
 
 // ---------------------------------------------------------------------------
-// 30-bit Morton key of a point in the unit cube (10 bits per axis).
-static inline uint32_t spread10(uint32_t v) {
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
+// 30-bit Hilbert index of a point with 10-bit integer coordinates
+// (Skilling's transpose algorithm, "Programming the Hilbert curve", AIP
+// Conf. Proc. 707, 2004): undo the excess work per level, Gray-encode, then
+// interleave the transposed bits.  Consecutive indices are face-adjacent
+// cells of the 1024^3 grid, so neighbours stay closer in the sorted order
+// than along a Morton curve.
+static inline uint32_t hilbert10(uint32_t x0, uint32_t x1, uint32_t x2) {
+    uint32_t x[3] = {x0, x1, x2};
+    const uint32_t M = 1u << 9;
+    for (uint32_t Q = M; Q > 1; Q >>= 1) {
+        const uint32_t P = Q - 1;
+        for (int i = 0; i < 3; i++) {
+            if (x[i] & Q) {
+                x[0] ^= P;
+            } else {
+                const uint32_t t = (x[0] ^ x[i]) & P;
+                x[0] ^= t;
+                x[i] ^= t;
+            }
+        }
+    }
+    x[1] ^= x[0];
+    x[2] ^= x[1];
+    uint32_t t = 0;
+    for (uint32_t Q = M; Q > 1; Q >>= 1)
+        if (x[2] & Q) t ^= Q - 1;
+    for (int i = 0; i < 3; i++) x[i] ^= t;
+    uint32_t key = 0;
+    for (int j = 9; j >= 0; j--)
+        for (int i = 0; i < 3; i++) key = (key << 1) | ((x[i] >> j) & 1u);
+    return key;
 }
 
 extern "C" const char* hp_create_error(void) { return g_create_error.c_str(); }
@@ -379,21 +402,25 @@ static int fill_case(const hp_mesh* mesh, const hp_params* params, Layout& L, Ca
     std::vector<int> perm(neles + 1);   // 1-based reference id -> 0-based internal
     std::iota(perm.begin(), perm.end(), -1);
     if (params->renumber && !cr.aliased) {
+        // centroids on a 1024^3 grid over the bounding cube (one scale for
+        // all axes, so a thin domain does not stretch the curve), sorted by
+        // Hilbert index
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
         for (int i = 1; i <= neles; i++) {
             double p[3] = {xcel[i], ycel[i], zcel[i]};
             for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], p[d]); hi[d] = std::max(hi[d], p[d]); }
         }
+        const double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
         std::vector<std::pair<uint32_t, int>> key(neles);
 #pragma omp parallel for schedule(static)
         for (int i = 1; i <= neles; i++) {
             double p[3] = {xcel[i], ycel[i], zcel[i]};
             uint32_t q[3];
             for (int d = 0; d < 3; d++) {
-                double t = (hi[d] > lo[d]) ? (p[d] - lo[d]) / (hi[d] - lo[d]) : 0.0;
+                double t = ext > 0.0 ? (p[d] - lo[d]) / ext : 0.0;
                 q[d] = (uint32_t)std::min(1023.0, std::max(0.0, t * 1023.0));
             }
-            key[i - 1] = {spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2), i};
+            key[i - 1] = {hilbert10(q[0], q[1], q[2]), i};
         }
         std::stable_sort(key.begin(), key.end());
         for (int r = 0; r < neles; r++) perm[key[r].second] = r;
