@@ -227,6 +227,12 @@ int hp_output_wait(hp_handle *h, int32_t ticket);
  * bytes hp_create would allocate for this mesh and precision (admission
  * against an HBM budget before creating). */
 int hp_estimate_bytes(const hp_mesh *mesh, const hp_params *params, int64_t *bytes);
+/* Host threads of the set-up loops (geometry, least-squares tables, cell
+ * order) that hp_create runs on the calling thread; 0 = one per core.  A
+ * server that sets up several cases at once on worker threads gives each
+ * worker a share of the cores, so the workers do not oversubscribe the host
+ * (and starve the thread that feeds the GPU). */
+int hp_set_host_threads(int32_t n);
 int hp_estimate_batch_bytes(const hp_mesh *meshes, int32_t ncase, const hp_params *params,
                             int64_t *bytes);
 /* *busy = 1 while steps queued on the handle's stream are still running,

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include "../../include/hydraphase.h"
 #include "hp_device.h"
@@ -153,6 +154,13 @@ static inline uint32_t hilbert10(uint32_t x0, uint32_t x1, uint32_t x2) {
 }
 
 extern "C" const char* hp_create_error(void) { return g_create_error.c_str(); }
+
+// See include/hydraphase.h.
+extern "C" int hp_set_host_threads(int32_t n) {
+    if (n < 0) return HP_E_ARG;
+    omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+    return HP_OK;
+}
 
 extern "C" const char* hp_last_error(const hp_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
@@ -602,8 +610,24 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     Arena probe;
     plan(probe);
     A.size = probe.used + 256;
+    // The arenas come from the device's stream-ordered pool.  Keeping freed
+    // arenas in the pool (release threshold: never) lets a server that
+    // creates and destroys cases reuse their memory instead of mapping new
+    // memory for each case; memory the pool holds but does not use counts
+    // as free below.
+    cudaMemPool_t pool = nullptr;
+    size_t pool_spare = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX, reserved = 0, used = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+            pool_spare = (size_t)(reserved - used);
+    }
+    cudaGetLastError();
     size_t freeb = 0, totalb = 0;
     cudaMemGetInfo(&freeb, &totalb);
+    freeb += pool_spare;
     if (A.size > freeb) {
         delete h;
         return fail(nullptr, HP_E_NOMEM, "case needs " + std::to_string(A.size >> 20) + " MiB, " +

@@ -100,6 +100,7 @@ def lib():
     L.hp_set_overset.argtypes = [vp, ctypes.POINTER(HpOverset)]
     L.hp_estimate_bytes.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(HpParams), ctypes.POINTER(ctypes.c_int64)]
     L.hp_poll.argtypes = [vp, ctypes.POINTER(_I)]
+    L.hp_set_host_threads.argtypes = [_I]
     L.hp_dt_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, _I,
                                 ctypes.POINTER(HpParams), ctypes.c_void_p, ctypes.c_void_p]
     L.hp_read_flow.argtypes = [ctypes.c_char_p, ctypes.POINTER(HpParams)]
@@ -117,7 +118,7 @@ def lib():
                "hp_estimate_batch_bytes", "hp_overset_build", "hp_overset_build_gpu", "hp_set_overset",
                "hp_get_state", "hp_get_prims", "hp_device_state", "hp_info", "hp_read_flow",
                "hp_read_mesh", "hp_read_restart", "hp_write_restart", "hp_write_tecplot", "hp_output_async",
-               "hp_output_wait"):
+               "hp_output_wait", "hp_set_host_threads"):
         getattr(L, fn).restype = ctypes.c_int
     _lib = L
     return L
@@ -133,5 +134,6 @@ EXPORTED_SYMBOLS = (
     "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll", "hp_create_batch", "hp_case_count",
     "hp_set_state_case", "hp_get_state_case", "hp_estimate_batch_bytes", "hp_overset_build", "hp_free_overset",
     "hp_set_overset", "hp_overset_build_gpu", "hp_write_tecplot", "hp_output_async", "hp_output_wait",
+    "hp_set_host_threads",
 )
 NOALLOC_MAX_CELLS = 1 << 24

@@ -111,6 +111,9 @@ class Server:
     hbm_budget: device bytes the admitted units may hold together
     max_active: units in flight (set up or running)
     chunk: steps enqueued per unit per turn of the loop
+    chunk_cell_steps: if set, a unit of c cells gets max(chunk,
+        chunk_cell_steps // c) steps per turn, so small units go back to the
+        host loop no more often than large ones
     setup_workers: host threads running hp_create + hp_set_state; with 4,
         the 48-case stream of the benchmark queued for set-up (median wait
         1.8 s), with 8 it did not (0.1 s)
@@ -121,11 +124,15 @@ class Server:
     block_size: threads per block of the per-cell kernels: an int, a dict
         from hydraphase.tune.size_class() to an int, or None (256)
     face_mode: hp_params.face_mode, an int or a dict by size class (None: 0)
+    host_threads: OpenMP threads of each set-up worker's hp_create (None: the
+        cores divided among the workers, so that concurrent set-ups do not
+        oversubscribe the host and delay the loop that feeds the GPU)
     """
 
     def __init__(self, hbm_budget: int, precision: int = PREC_MIXED, max_active: int = 12, chunk: int = 25,
                  setup_workers: int = 8, keep_state: bool = True, param_overrides: dict | None = None,
-                 batch_cells: int = 0, max_batch: int = 64, block_size=None, face_mode=None):
+                 batch_cells: int = 0, max_batch: int = 64, block_size=None, face_mode=None,
+                 chunk_cell_steps: int | None = None, host_threads: int | None = None):
         self.budget = int(hbm_budget)
         self.precision = precision
         self.max_active = max_active
@@ -137,6 +144,8 @@ class Server:
         self.max_batch = int(max_batch)
         self.block_size = block_size
         self.face_mode = face_mode
+        self.chunk_cell_steps = chunk_cell_steps
+        self.host_threads = host_threads
 
     def _params(self, spec, cells: int):
         from .tune import size_class
@@ -164,6 +173,13 @@ class Server:
             b.set_state(k, 0.0, r.spec.cu, r.spec.ghost_prims)
         return b
 
+    def _chunk_for(self, unit) -> int:
+        """Steps per turn for a unit (its cases' total cells)."""
+        if not self.chunk_cell_steps:
+            return self.chunk
+        cells = sum(r.spec.mesh.neles for r in unit)
+        return max(self.chunk, int(self.chunk_cell_steps) // max(cells, 1))
+
     def _take_unit(self, queue):
         """The next unit from the head of the queue: one case, or the longest
         run of small compatible cases that fits in batch_cells."""
@@ -190,7 +206,10 @@ class Server:
         used = 0
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
-        with ThreadPoolExecutor(self.workers) as pool:
+        import os
+        from ._lib import lib
+        nthr = self.host_threads if self.host_threads is not None else max(1, (os.cpu_count() or 1) // self.workers)
+        with ThreadPoolExecutor(self.workers, initializer=lambda: lib().hp_set_host_threads(int(nthr))) as pool:
             while pending or queue or setting_up or active:
                 progressed = False
                 t = now()
@@ -227,7 +246,7 @@ class Server:
                             rep.results.append(CaseResult(r.rid, r.spec.mesh.neles, r.steps, r.arrival, ta, ta,
                                                           now(), b // len(unit), error=str(e)))
                         continue
-                    n = min(self.chunk, unit[0].steps)
+                    n = min(self._chunk_for(unit), unit[0].steps)
                     handle.step(n, diagnostics=False)
                     active.append(_Active(unit, handle, b, ta, now(), unit[0].steps - n))
                 setting_up = still
@@ -240,7 +259,7 @@ class Server:
                         continue
                     progressed = True
                     if a.remaining > 0:
-                        n = min(self.chunk, a.remaining)
+                        n = min(self._chunk_for(a.reqs), a.remaining)
                         a.handle.step(n, diagnostics=False)
                         a.remaining -= n
                         keep.append(a)
