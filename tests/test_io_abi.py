@@ -168,3 +168,12 @@ def test_params_layout_matches_header():
     assert HpParams.cfl.offset == 29 * 8
     assert HpParams.face_mode.offset == 296
     assert HpParams.venkat_k.offset == HpParams.face_mode.offset + 8
+
+
+def test_host_thread_share():
+    """hp_set_host_threads sets the calling thread's set-up threads (0 = one
+    per core) and rejects a negative count; no GPU needed."""
+    from hydraphase import HP_E_ARG, lib
+    assert lib().hp_set_host_threads(2) == 0
+    assert lib().hp_set_host_threads(0) == 0
+    assert lib().hp_set_host_threads(-1) == HP_E_ARG
