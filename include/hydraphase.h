@@ -197,6 +197,23 @@ int hp_overset_build(const hp_mesh *mesh, const int32_t *block, int32_t layers, 
  * HP_E_CUDA if a device call fails. */
 int hp_overset_build_gpu(const hp_mesh *mesh, const int32_t *block, int32_t layers, int32_t outer_type,
                          int32_t *iblank_out, hp_overset *out);
+/* Hole cut, the step before hp_overset_build (new work: the reference takes
+ * it from TIOGA).  The wall surface is the set of faces of component
+ * (block 1) elements whose neighbour is a ghost of type wall_type (face k:
+ * the element's nodes other than node k).  A background (block 0) cell with
+ * iblank 1 becomes a hole, iblank_out = 0, when its centroid lies within
+ * `margin` (>= 0) of a wall triangle or is enclosed by the surface (the ray
+ * from it towards +x crosses an odd number of wall triangles; edges and
+ * vertices counted once); every other cell keeps the mesh's iblank.  The
+ * surface must be closed, or open only across planes parallel to the x axis
+ * (a body extruded between planes z = const).  *nholes (may be NULL) = cells
+ * cut.  HP_E_ARG on bad arguments or when no face has type wall_type.  The
+ * _gpu form tests the cells on the current CUDA device (temporary device
+ * memory; HP_E_CUDA if a device call fails) and returns the same iblank. */
+int hp_overset_hole_cut(const hp_mesh *mesh, const int32_t *block, int32_t wall_type, double margin,
+                        int32_t *iblank_out, int32_t *nholes);
+int hp_overset_hole_cut_gpu(const hp_mesh *mesh, const int32_t *block, int32_t wall_type, double margin,
+                            int32_t *iblank_out, int32_t *nholes);
 void hp_free_overset(hp_overset *ov);
 /* Single-case handles only; replaces any earlier table. */
 int hp_set_overset(hp_handle *h, const hp_overset *ov);

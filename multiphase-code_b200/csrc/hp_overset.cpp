@@ -164,7 +164,139 @@ int prepare(const hp_mesh* mesh, const int32_t* block, int32_t layers, int32_t o
     return HP_OK;
 }
 
+// Wall triangles of the component (block 1): face k of an element (the nodes
+// other than node k, in the order of src/sr_geometry.F90:149-158) whose
+// neighbour is a ghost of type wall_type, in (element, face) order; then the
+// two search grids of HoleView.  r3 exceeds the margin by a relative 1e-6
+// and both grids add 1e-9 of the surface's extent, so every triangle that can
+// pass a test at p sits in p's grid cell and the result equals a test of all
+// triangles.
+int prepare_hole(const hp_mesh* mesh, const int32_t* block, int32_t wall_type, double margin, HolePrep& H) {
+    static const int FACE[4][3] = {{2, 3, 4}, {4, 3, 1}, {2, 4, 1}, {3, 2, 1}};
+    if (!mesh || !block || !(margin >= 0.0) || !(margin < 1e300) || mesh->neles <= 0 || mesh->nghosts < 0 ||
+        !mesh->elem || (mesh->nghosts && !mesh->ghost) || !mesh->x || !mesh->y || !mesh->z)
+        return HP_E_ARG;
+    const int neles = mesh->neles, ntot = neles + mesh->nghosts;
+    Mesh M{mesh};
+    std::vector<int> gtype(ntot + 2, 0);
+    for (int g = 0; g < mesh->nghosts; g++) {
+        const int id = mesh->ghost[4 * g + 1];
+        if (id >= 1 && id <= ntot) gtype[id] = mesh->ghost[4 * g + 2];
+    }
+    H.tri.clear();
+    for (int e = 1; e <= neles; e++) {
+        const int32_t* r = M.row(e);
+        for (int k = 0; k < 4; k++)
+            if (r[k] < 1 || r[k] > mesh->nodes || r[4 + k] < 1 || r[4 + k] > ntot) return HP_E_ARG;
+        if (block[e - 1] != 0 && block[e - 1] != 1) return HP_E_ARG;
+        if (block[e - 1] != 1) continue;
+        for (int k = 0; k < 4; k++) {
+            const int n = r[4 + k];
+            if (n <= neles || gtype[n] != wall_type) continue;
+            for (int v = 0; v < 3; v++) {
+                double q[3];
+                M.node(r[FACE[k][v] - 1], q);
+                H.tri.insert(H.tri.end(), q, q + 3);
+            }
+        }
+    }
+    const int ntri = (int)(H.tri.size() / 9);
+    if (ntri == 0) return HP_E_ARG;
+    double blo[3] = {1e300, 1e300, 1e300}, bhi[3] = {-1e300, -1e300, -1e300}, mean_ext = 0.0;
+    std::vector<double> tlo(3 * (size_t)ntri), thi(3 * (size_t)ntri);
+    for (int t = 0; t < ntri; t++) {
+        const double* T = &H.tri[9 * (size_t)t];
+        double te = 0.0;
+        for (int d = 0; d < 3; d++) {
+            const double lo = std::min(std::min(T[d], T[3 + d]), T[6 + d]);
+            const double hi = std::max(std::max(T[d], T[3 + d]), T[6 + d]);
+            tlo[3 * t + d] = lo; thi[3 * t + d] = hi;
+            blo[d] = std::min(blo[d], lo); bhi[d] = std::max(bhi[d], hi);
+            te = std::max(te, hi - lo);
+        }
+        mean_ext += te;
+    }
+    mean_ext /= ntri;
+    const double L = std::max(std::max(bhi[0] - blo[0], bhi[1] - blo[1]), bhi[2] - blo[2]);
+    const double tol = 1e-9 * L + 1e-300;
+    const double r3 = margin * (1.0 + 1e-6) + tol;
+    HoleView& V = H.v;
+    V.m2 = margin * margin;
+    // grid cells: g3 at least r3 / 2 and the mean triangle size, at most 64
+    // per axis; g2 square cells of 1/256 of the projected extent
+    auto setup = [&](GridParams& g, const double lo[3], const double hi[3], double h, bool yz, int cap) {
+        g = GridParams{};
+        g.h = h > 0.0 ? h : 1.0;
+        for (int d = 0; d < 3; d++) {
+            g.lo[d] = yz && d == 0 ? 0.0 : lo[d];
+            g.n[d] = yz && d == 0 ? 1 : std::max(1, std::min(cap, (int)((hi[d] - lo[d]) / g.h) + 1));
+        }
+    };
+    auto bin = [&](const GridParams& g, double grow, bool yz, std::vector<int>& start, std::vector<int>& items) {
+        const size_t ncell = (size_t)g.n[0] * g.n[1] * g.n[2];
+        start.assign(ncell + 1, 0);
+        for (int pass = 0; pass < 2; pass++) {
+            std::vector<int> fill;
+            if (pass) { fill.assign(start.begin(), start.end() - 1); items.assign(start[ncell], 0); }
+            for (int t = 0; t < ntri; t++) {
+                int a[3], b[3];
+                for (int d = 0; d < 3; d++) {
+                    if (yz && d == 0) { a[d] = b[d] = 0; continue; }
+                    a[d] = grid_index(g, d, tlo[3 * t + d] - grow);
+                    b[d] = grid_index(g, d, thi[3 * t + d] + grow);
+                }
+                for (int i = a[0]; i <= b[0]; i++)
+                    for (int j = a[1]; j <= b[1]; j++)
+                        for (int k = a[2]; k <= b[2]; k++) {
+                            const size_t c = ((size_t)i * g.n[1] + j) * g.n[2] + k;
+                            if (pass) items[fill[c]++] = t; else start[c + 1]++;
+                        }
+            }
+            if (!pass)
+                for (size_t c = 0; c < ncell; c++) start[c + 1] += start[c];
+        }
+    };
+    for (int d = 0; d < 3; d++) {
+        V.lo3[d] = blo[d] - r3; V.hi3[d] = bhi[d] + r3;
+        V.lo2[d] = blo[d] - tol; V.hi2[d] = bhi[d] + tol;
+    }
+    const double L3 = L + 2.0 * r3;
+    setup(V.g3, V.lo3, V.hi3, std::max(std::max(L3 / 64.0, 0.5 * r3), mean_ext), false, 64);
+    const double L2 = std::max(V.hi2[1] - V.lo2[1], V.hi2[2] - V.lo2[2]);
+    setup(V.g2, V.lo2, V.hi2, L2 / 256.0, true, 256);
+    bin(V.g3, r3, false, H.start3, H.items3);
+    bin(V.g2, tol, true, H.start2, H.items2);
+    V.tri = H.tri.data();
+    V.start3 = H.start3.data(); V.items3 = H.items3.data();
+    V.start2 = H.start2.data(); V.items2 = H.items2.data();
+    return HP_OK;
+}
+
 }  // namespace hp_ov
+
+// See include/hydraphase.h.
+extern "C" int hp_overset_hole_cut(const hp_mesh* mesh, const int32_t* block, int32_t wall_type, double margin,
+                                   int32_t* iblank_out, int32_t* nholes) {
+    if (!iblank_out) return HP_E_ARG;
+    hp_ov::HolePrep H;
+    const int rc = hp_ov::prepare_hole(mesh, block, wall_type, margin, H);
+    if (rc != HP_OK) return rc;
+    Mesh M{mesh};
+    const hp_ov::HoleView V = H.v;
+    int nh = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : nh)
+    for (int e = 1; e <= mesh->neles; e++) {
+        int ib = M.row(e)[8];
+        if (block[e - 1] == 0 && ib == 1) {
+            double p[3];
+            M.centroid(e, p);
+            if (hp_ov::hole_test(V, p)) { ib = 0; nh++; }
+        }
+        iblank_out[e - 1] = ib;
+    }
+    if (nholes) *nholes = nh;
+    return HP_OK;
+}
 
 // See include/hydraphase.h.
 extern "C" int hp_overset_build(const hp_mesh* mesh, const int32_t* block, int32_t layers, int32_t outer_type,

@@ -223,6 +223,20 @@ __global__ void k_weights(DMesh M, const int* block, const int* iblank, const in
                 }
 }
 
+// Hole cut: one thread per element; background field cells whose centroid
+// passes hole_test become holes (iblank 0).
+__global__ void k_hole_cut(DMesh M, const int* block, hp_ov::HoleView H, int32_t* iblank, int* nholes) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (e > M.neles) return;
+    int ib = row(M, e)[8];
+    if (block[e - 1] == 0 && ib == 1) {
+        double p[3];
+        centroid(M, e, p);
+        if (hp_ov::hole_test(H, p)) { ib = 0; atomicAdd(nholes, 1); }
+    }
+    iblank[e - 1] = ib;
+}
+
 // Device buffers of one build, freed on every exit.
 struct Buffers {
     std::vector<void*> p;
@@ -356,5 +370,60 @@ extern "C" int hp_overset_build_gpu(const hp_mesh* mesh, const int32_t* block, i
         if (st) cudaStreamDestroy(st);
     }
     if (rc != HP_OK) hp_free_overset(out);
+    return rc;
+}
+
+// See include/hydraphase.h.
+extern "C" int hp_overset_hole_cut_gpu(const hp_mesh* mesh, const int32_t* block, int32_t wall_type, double margin,
+                                       int32_t* iblank_out, int32_t* nholes) {
+    if (!iblank_out) return HP_E_ARG;
+    hp_ov::HolePrep HP;
+    int rc = hp_ov::prepare_hole(mesh, block, wall_type, margin, HP);
+    if (rc != HP_OK) return rc;
+    const int neles = mesh->neles, nodes = mesh->nodes;
+    {
+        Buffers buf;
+        cudaStream_t st = nullptr;
+        double *x = nullptr, *y = nullptr, *z = nullptr, *tri = nullptr;
+        int32_t *elem = nullptr, *ib = nullptr;
+        int *blk = nullptr, *s3 = nullptr, *i3 = nullptr, *s2 = nullptr, *i2 = nullptr, *cnt = nullptr;
+        int hcount = 0;
+        hp_ov::HoleView V = HP.v;
+        OV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        OV_CUDA(buf.get(&x, nodes));
+        OV_CUDA(buf.get(&y, nodes));
+        OV_CUDA(buf.get(&z, nodes));
+        OV_CUDA(buf.get(&elem, 9 * (size_t)neles));
+        OV_CUDA(buf.get(&blk, neles));
+        OV_CUDA(buf.get(&ib, neles));
+        OV_CUDA(buf.get(&cnt, 1));
+        OV_CUDA(buf.get(&tri, HP.tri.size()));
+        OV_CUDA(buf.get(&s3, HP.start3.size()));
+        OV_CUDA(buf.get(&i3, HP.items3.size()));
+        OV_CUDA(buf.get(&s2, HP.start2.size()));
+        OV_CUDA(buf.get(&i2, HP.items2.size()));
+        OV_CUDA(cudaMemcpyAsync(x, mesh->x, nodes * sizeof(double), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(y, mesh->y, nodes * sizeof(double), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(z, mesh->z, nodes * sizeof(double), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(elem, mesh->elem, 9 * (size_t)neles * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(blk, block, neles * sizeof(int), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(tri, HP.tri.data(), HP.tri.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(s3, HP.start3.data(), HP.start3.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(i3, HP.items3.data(), HP.items3.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(s2, HP.start2.data(), HP.start2.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemcpyAsync(i2, HP.items2.data(), HP.items2.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        OV_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+        V.tri = tri;
+        V.start3 = s3; V.items3 = i3;
+        V.start2 = s2; V.items2 = i2;
+        k_hole_cut<<<blocks_for(neles, 128), 128, 0, st>>>(DMesh{x, y, z, elem, neles}, blk, V, ib, cnt);
+        OV_CUDA(cudaGetLastError());
+        OV_CUDA(cudaMemcpyAsync(iblank_out, ib, neles * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        OV_CUDA(cudaMemcpyAsync(&hcount, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+        OV_CUDA(cudaStreamSynchronize(st));
+        if (nholes) *nholes = hcount;
+    done:
+        if (st) cudaStreamDestroy(st);
+    }
     return rc;
 }

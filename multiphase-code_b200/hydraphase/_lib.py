@@ -95,6 +95,9 @@ def lib():
     L.hp_overset_build.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(_I), _I, _I, ctypes.POINTER(_I),
                                    ctypes.POINTER(HpOverset)]
     L.hp_overset_build_gpu.argtypes = L.hp_overset_build.argtypes
+    L.hp_overset_hole_cut.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(_I), _I, _D, ctypes.POINTER(_I),
+                                      ctypes.POINTER(_I)]
+    L.hp_overset_hole_cut_gpu.argtypes = L.hp_overset_hole_cut.argtypes
     L.hp_free_overset.argtypes = [ctypes.POINTER(HpOverset)]
     L.hp_free_overset.restype = None
     L.hp_set_overset.argtypes = [vp, ctypes.POINTER(HpOverset)]
@@ -118,7 +121,7 @@ def lib():
                "hp_estimate_batch_bytes", "hp_overset_build", "hp_overset_build_gpu", "hp_set_overset",
                "hp_get_state", "hp_get_prims", "hp_device_state", "hp_info", "hp_read_flow",
                "hp_read_mesh", "hp_read_restart", "hp_write_restart", "hp_write_tecplot", "hp_output_async",
-               "hp_output_wait", "hp_set_host_threads"):
+               "hp_output_wait", "hp_set_host_threads", "hp_overset_hole_cut", "hp_overset_hole_cut_gpu"):
         getattr(L, fn).restype = ctypes.c_int
     _lib = L
     return L
@@ -134,6 +137,6 @@ EXPORTED_SYMBOLS = (
     "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll", "hp_create_batch", "hp_case_count",
     "hp_set_state_case", "hp_get_state_case", "hp_estimate_batch_bytes", "hp_overset_build", "hp_free_overset",
     "hp_set_overset", "hp_overset_build_gpu", "hp_write_tecplot", "hp_output_async", "hp_output_wait",
-    "hp_set_host_threads",
+    "hp_set_host_threads", "hp_overset_hole_cut", "hp_overset_hole_cut_gpu",
 )
 NOALLOC_MAX_CELLS = 1 << 24

@@ -371,14 +371,17 @@ class OversetSpec:
 
 
 def overset_cylinder(bg=(200, 120, 20), comp=(96, 256, 20), hole_r=1.2, comp_r_out=3.0, layers=2, seed=1,
-                     box=((-10.0, -12.0, 0.0), (30.0, 12.0, 4.0)), **flow_kw) -> OversetSpec:
+                     box=((-10.0, -12.0, 0.0), (30.0, 12.0, 4.0)), hole_cut="radius", **flow_kw) -> OversetSpec:
     """Overset cylinder: a background box of bg hexes on [-10,30]x[-12,12]x[0,4]
     (6 tets each; far field on its x/y faces, symmetry 53 on z; `box` moves
     its corners, the span must stay [0, 4]) and an O-grid
     component of comp = (radial, azimuthal, spanwise) hexes around the
     cylinder (D = 1) out to comp_r_out; background cells whose centroid lies
-    within hole_r of the cylinder axis are holes (iblank 0).  Flow as in
-    cylinder() (Mach 0.3, Re_D 150, droplets)."""
+    within hole_r of the cylinder axis are holes (iblank 0).  hole_cut="wall"
+    cuts them with the library instead (hp_overset_hole_cut: within
+    hole_r - 0.5 of the cylinder's wall faces, or inside them), which differs
+    from the radius rule only within the polygonal wall's deviation from the
+    circle.  Flow as in cylinder() (Mach 0.3, Re_D 150, droplets)."""
     nx, ny, nz = bg
 
     def bg_types(fc):
@@ -390,8 +393,14 @@ def overset_cylinder(bg=(200, 120, 20), comp=(96, 256, 20), hole_r=1.2, comp_r_o
     nr, nt, nzc = comp
     b = ogrid_mesh(nr, nt, nzc, r_in=0.5, r_out=comp_r_out, dr0=0.005, seed=seed + 1)
     u, block = union_mesh(a, b)
-    hole = (block == 0) & (np.hypot(u.xc[:, 0], u.xc[:, 1]) < hole_r)
-    u.mesh.elem[hole, 8] = 0
+    if hole_cut == "wall":
+        from .engine import overset_hole_cut
+        u.mesh.elem[:, 8], _ = overset_hole_cut(u.mesh, block, wall_type=6, margin=hole_r - 0.5)
+    elif hole_cut == "radius":
+        hole = (block == 0) & (np.hypot(u.xc[:, 0], u.xc[:, 1]) < hole_r)
+        u.mesh.elem[hole, 8] = 0
+    else:
+        raise ValueError(f"hole_cut must be 'radius' or 'wall', not {hole_cut!r}")
     spec = _cylinder_flow(u, "overset_cylinder", seed=seed, **flow_kw)
     return OversetSpec(spec, block, 7, layers)
 

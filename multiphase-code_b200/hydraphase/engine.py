@@ -120,6 +120,23 @@ def overset_build(mesh: MeshArrays, block, layers: int = 2, outer_type: int = 7,
         lib().hp_free_overset(ctypes.byref(ov))
 
 
+def overset_hole_cut(mesh: MeshArrays, block, wall_type: int = 6, margin: float = 0.0, device: bool = False):
+    """Hole cut of a two-block overset mesh (hp_overset_hole_cut): background
+    field cells within `margin` of, or enclosed by, the wall surface of the
+    component block (its faces on ghosts of type wall_type) get iblank 0.
+    Returns (iblank, nholes); put iblank into the mesh given to
+    overset_build.  device=True tests the cells on the current CUDA device
+    (hp_overset_hole_cut_gpu); the result is the same."""
+    keep = []
+    hm = _hp_mesh(mesh, keep)
+    bl = np.ascontiguousarray(block, np.int32)
+    ib = np.zeros(mesh.neles, np.int32)
+    nh = ctypes.c_int32()
+    cut = lib().hp_overset_hole_cut_gpu if device else lib().hp_overset_hole_cut
+    _check(cut(ctypes.byref(hm), _ip(bl), int(wall_type), float(margin), _ip(ib), ctypes.byref(nh)))
+    return ib, nh.value
+
+
 def write_tecplot(path: str, mesh: MeshArrays, fields: np.ndarray):
     """The reference's Tecplot file (hp_write_tecplot) from the 13
     cell-centred fields (13, neles)."""

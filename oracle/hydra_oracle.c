@@ -1485,3 +1485,157 @@ static void overset_apply(or_case *S) {
             CN(i, j) = w[0] * CN(d[0], j) + w[1] * CN(d[1], j) + w[2] * CN(d[2], j) + w[3] * CN(d[3], j);
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* Overset hole cut.  New work: the reference takes its hole cut from
+ * TIOGA, outside the path, and only freezes cells with iblank != 1
+ * (src/sr_RK.F90:31).  Test infrastructure: the library's
+ * hp_overset_hole_cut (csrc/hp_overset.cpp) and hp_overset_hole_cut_gpu
+ * (csrc/hp_overset_gpu.cu) are checked against this brute-force
+ * restatement of the rule.
+ *
+ * Wall surface: the faces of component (block 1) elements whose neighbour
+ * is a ghost of type wall_type; face k of an element is the triangle of its
+ * nodes other than node k, in the node order of src/sr_geometry.F90:149-158
+ * ((2,3,4), (4,3,1), (2,4,1), (3,2,1)).  A background (block 0) field cell
+ * (iblank 1) becomes a hole (iblank 0) when its centroid p
+ *   - lies within `margin` of the surface: the squared distance to some wall
+ *     triangle is <= margin*margin, or
+ *   - is enclosed by it: the ray from p towards +x crosses an odd number of
+ *     wall triangles.
+ * A crossing is decided in the (y, z) projection.  Each edge function is
+ * evaluated from the lexicographically lower end of its edge, so the two
+ * triangles that share an edge see exactly opposite values; where an edge
+ * function is zero it takes the sign it has once p moves by (0, eps, eps^2)
+ * (simulation of simplicity), so a ray through an edge or a vertex counts
+ * one triangle of those around it.  The crossing counts when the hit point
+ * lies at x > p.x.  The surface must be closed, or open only across planes
+ * parallel to the x axis (an extruded body between planes z = const).
+ * Other cells keep their iblank. */
+static double hc_dot(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+static void hc_cross3(const double a[3], const double b[3], double o[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* squared distance from p to the segment u-v */
+static double hc_seg2(const double p[3], const double u[3], const double v[3]) {
+    double w[3], d[3];
+    for (int k = 0; k < 3; k++) { w[k] = v[k] - u[k]; d[k] = p[k] - u[k]; }
+    double ww = hc_dot(w, w), t = hc_dot(d, w);
+    if (t <= 0.0 || ww == 0.0) return hc_dot(d, d);
+    if (t >= ww) {
+        double q[3] = {p[0] - v[0], p[1] - v[1], p[2] - v[2]};
+        return hc_dot(q, q);
+    }
+    double s = t / ww, q[3];
+    for (int k = 0; k < 3; k++) q[k] = d[k] - s * w[k];
+    return hc_dot(q, q);
+}
+
+/* squared distance from p to the triangle a, b, c */
+static double hc_dist2(const double p[3], const double a[3], const double b[3], const double c[3]) {
+    double ab[3], ac[3], n[3];
+    for (int k = 0; k < 3; k++) { ab[k] = b[k] - a[k]; ac[k] = c[k] - a[k]; }
+    hc_cross3(ab, ac, n);
+    double nn = hc_dot(n, n);
+    if (nn > 0.0) {
+        const double *V[3] = {a, b, c};
+        int in = 1;
+        for (int q = 0; q < 3 && in; q++) {
+            const double *u = V[q], *v = V[(q + 1) % 3];
+            double e[3], d[3], x[3];
+            for (int k = 0; k < 3; k++) { e[k] = v[k] - u[k]; d[k] = p[k] - u[k]; }
+            hc_cross3(e, d, x);
+            in = hc_dot(n, x) >= 0.0;
+        }
+        if (in) {
+            double ap[3] = {p[0] - a[0], p[1] - a[1], p[2] - a[2]};
+            double h = hc_dot(ap, n);
+            return h * h / nn;
+        }
+    }
+    double d0 = hc_seg2(p, a, b), d1 = hc_seg2(p, b, c), d2 = hc_seg2(p, c, a);
+    return d0 < d1 ? (d0 < d2 ? d0 : d2) : (d1 < d2 ? d1 : d2);
+}
+
+/* sign (+1/-1) of the projected edge function of u->v at p (value in *val);
+ * 0 when u and v coincide in projection */
+static int hc_edge(const double u[3], const double v[3], const double p[3], double *val) {
+    int swap = u[1] > v[1] || (u[1] == v[1] && u[2] > v[2]);
+    const double *s = swap ? v : u, *t = swap ? u : v;
+    double dy = t[1] - s[1], dz = t[2] - s[2];
+    if (dy == 0.0 && dz == 0.0) { *val = 0.0; return 0; }
+    double e = dy * (p[2] - s[2]) - dz * (p[1] - s[1]);
+    int sg = e > 0.0 ? 1 : e < 0.0 ? -1 : (dz != 0.0 ? (dz > 0.0 ? -1 : 1) : 1);
+    *val = swap ? -e : e;
+    return swap ? -sg : sg;
+}
+
+/* 1 if the ray from p towards +x crosses the triangle a, b, c */
+static int hc_ray(const double p[3], const double a[3], const double b[3], const double c[3]) {
+    double ea, eb, ec;
+    int sa = hc_edge(b, c, p, &ea), sb = hc_edge(c, a, p, &eb), sc = hc_edge(a, b, p, &ec);
+    if (sa == 0 || sb == 0 || sc == 0 || sa != sb || sb != sc) return 0;
+    double den = ea + eb + ec;
+    double xh = den != 0.0 ? (ea * a[0] + eb * b[0] + ec * c[0]) / den : a[0];
+    return xh > p[0];
+}
+
+int or_overset_hole_cut(int32_t nodes, int32_t neles, int32_t nghosts, const double *x, const double *y,
+                        const double *z, const int32_t *elem, const int32_t *ghost, const int32_t *block,
+                        int32_t wall_type, double margin, int32_t *iblank_out, int32_t *nholes) {
+    (void)nodes;
+    static const int FACE[4][3] = {{2, 3, 4}, {4, 3, 1}, {2, 4, 1}, {3, 2, 1}};
+    const int ntot = neles + nghosts;
+    int *gtype = ialloc(ntot + 2);
+    for (int g = 0; g < nghosts; g++) {
+        int id = ghost[4 * g + 1];
+        if (id >= 1 && id <= ntot) gtype[id] = ghost[4 * g + 2];
+    }
+    int ntri = 0;
+    for (int e = 1; e <= neles; e++)
+        for (int k = 0; k < 4; k++) {
+            int n = elem[9 * (size_t)(e - 1) + 4 + k];
+            ntri += block[e - 1] == 1 && n > neles && gtype[n] == wall_type;
+        }
+    double *tri = dalloc(9 * (size_t)ntri + 1);
+    int t = 0;
+    for (int e = 1; e <= neles; e++)
+        for (int k = 0; k < 4; k++) {
+            const int32_t *r = elem + 9 * (size_t)(e - 1);
+            int n = r[4 + k];
+            if (!(block[e - 1] == 1 && n > neles && gtype[n] == wall_type)) continue;
+            for (int v = 0; v < 3; v++) {
+                int nd = r[FACE[k][v] - 1];
+                tri[9 * (size_t)t + 3 * v + 0] = x[nd - 1];
+                tri[9 * (size_t)t + 3 * v + 1] = y[nd - 1];
+                tri[9 * (size_t)t + 3 * v + 2] = z[nd - 1];
+            }
+            t++;
+        }
+    const double m2 = margin * margin;
+    int nh = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : nh)
+    for (int e = 1; e <= neles; e++) {
+        const int32_t *r = elem + 9 * (size_t)(e - 1);
+        int ib = r[8];
+        if (block[e - 1] == 0 && ib == 1) {
+            double p[3];
+            ov_centroid(x, y, z, r, p);
+            int hole = 0, par = 0;
+            for (int q = 0; q < ntri && !hole; q++) {
+                const double *T = tri + 9 * (size_t)q;
+                hole = hc_dist2(p, T, T + 3, T + 6) <= m2;
+                par ^= hc_ray(p, T, T + 3, T + 6);
+            }
+            if (hole || par) { ib = 0; nh++; }
+        }
+        iblank_out[e - 1] = ib;
+    }
+    *nholes = nh;
+    free(gtype); free(tri);
+    return ntri > 0 ? 0 : -1;
+}

@@ -112,6 +112,12 @@ int or_overset_build(int32_t nodes, int32_t neles, int32_t nghosts, const double
                      int32_t *fringe, int32_t *donor, double *weight, int32_t *nfallback);
 void or_set_overset(or_case *c, int32_t nfringe, const int32_t *fringe, const int32_t *donor,
                     const double *weight);
+/* Hole cut of an overset mesh (rule in hydra_oracle.c): iblank_out[neles]
+ * is 0 on background field cells within `margin` of, or enclosed by, the
+ * wall surface of the component block; -1 if there is no wall face. */
+int or_overset_hole_cut(int32_t nodes, int32_t neles, int32_t nghosts, const double *x, const double *y,
+                        const double *z, const int32_t *elem, const int32_t *ghost, const int32_t *block,
+                        int32_t wall_type, double margin, int32_t *iblank_out, int32_t *nholes);
 
 #ifdef __cplusplus
 }

@@ -238,6 +238,9 @@ def lib():
                                        ctypes.c_int32, ctypes.c_int32, ip, i32p, ip, ip, dp, i32p]
         L.or_overset_build.restype = ctypes.c_int
         L.or_set_overset.argtypes = [ctypes.c_void_p, ctypes.c_int32, ip, ip, dp]
+        L.or_overset_hole_cut.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, dp, dp, dp, ip, ip,
+                                          ip, ctypes.c_int32, ctypes.c_double, ip, i32p]
+        L.or_overset_hole_cut.restype = ctypes.c_int
     return _lib
 
 
@@ -273,6 +276,23 @@ def overset_build(mesh: Mesh, block, layers: int, outer_type: int):
                            ctypes.byref(nfb))
     n = nf.value
     return ib, fr[:n].copy(), dn[:4 * n].reshape(n, 4).copy(), w[:4 * n].reshape(n, 4).copy(), nfb.value
+
+
+def overset_hole_cut(mesh: Mesh, block, wall_type: int, margin: float):
+    """Hole cut of a two-block overset mesh by the oracle's restatement of
+    the rule: returns (iblank, nholes); background field cells within
+    `margin` of, or enclosed by, the component's wall surface become 0."""
+    keep = [np.ascontiguousarray(mesh.x, np.float64), np.ascontiguousarray(mesh.y, np.float64),
+            np.ascontiguousarray(mesh.z, np.float64), np.ascontiguousarray(mesh.elem, np.int32),
+            np.ascontiguousarray(mesh.ghost, np.int32), np.ascontiguousarray(block, np.int32)]
+    x, y, z, el, gh, bl = keep
+    ib = np.zeros(mesh.neles, np.int32)
+    nh = ctypes.c_int32()
+    rc = lib().or_overset_hole_cut(mesh.nodes, mesh.neles, mesh.nghosts, _dp(x), _dp(y), _dp(z), _ip(el), _ip(gh),
+                                   _ip(bl), int(wall_type), float(margin), _ip(ib), ctypes.byref(nh))
+    if rc != 0:
+        raise ValueError("no wall face of the given type on the component block")
+    return ib, nh.value
 
 
 class Oracle:

@@ -10,13 +10,17 @@ stage) equal the oracle bit for bit in the FP64 parity variant, and the mixed
 variant stays within 1e-5 in mixture density and alpha_g; the device builder
 (hp_overset_build_gpu) returns the host builder's tables bit for bit,
 nearest-centroid fallbacks included.
+Hole cut: background cells within a margin of, or enclosed by, the
+component's wall faces; the library equals the oracle and the geometric
+answer on CPU (rays through shared edges and vertices counted once), and the
+device cut equals the host's.
 """
 import numpy as np
 import pytest
 
 import oracle as O
 from hydraphase import HP_E_UNSUPPORTED, PREC_FP64_PARITY, PREC_MIXED, Batch, Case, HydraError, cases
-from hydraphase.engine import MeshArrays, overset_build
+from hydraphase.engine import MeshArrays, overset_build, overset_hole_cut
 
 
 def _small():
@@ -155,3 +159,98 @@ def test_device_tables_with_nearest_fallback():
     np.testing.assert_array_equal(th.donor, td.donor)
     np.testing.assert_array_equal(th.weight, td.weight)
     assert th.nfallback == td.nfallback
+
+
+# --- hole cut (hp_overset_hole_cut / _gpu) ------------------------------------
+def _cube_in_box():
+    """A unit cube of wall faces (component, 2x2x2 hexes, type 6) inside a
+    background box whose tet centroids put many +x rays exactly through the
+    cube's face edges and vertices (y, z on multiples of 1/8; cube nodes at
+    multiples of 1/2); no centroid lies on the cube's surface."""
+    bg = cases.box_mesh(10, 10, 10, lo=(-2.05, -2.0, -2.0), hi=(2.95, 3.0, 3.0), bc_type=7)
+    cube = cases.box_mesh(2, 2, 2, bc_type=6)
+    u, block = cases.union_mesh(bg, cube)
+    return u, block
+
+
+def _unblanked(mesh):
+    el = mesh.elem.copy()
+    el[:, 8] = 1
+    return MeshArrays(mesh.x, mesh.y, mesh.z, el, mesh.ghost)
+
+
+@pytest.mark.parametrize("margin", [0.0, 0.3])
+def test_hole_cut_cube_equals_geometry_and_oracle(margin):
+    """Holes are exactly the background cells inside the cube or within the
+    margin of it (Euclidean distance to the solid cube), rays through shared
+    edges and vertices included; the library equals the oracle."""
+    u, block = _cube_in_box()
+    ib, nh = overset_hole_cut(u.mesh, block, wall_type=6, margin=margin)
+    ib_o, nh_o = O.overset_hole_cut(O.Mesh(u.mesh.x, u.mesh.y, u.mesh.z, u.mesh.elem, u.mesh.ghost), block, 6,
+                                    margin)
+    xc = u.xc
+    gap = np.maximum(0.0, np.maximum(-xc, xc - 1.0))
+    inside = np.all((xc > 0.0) & (xc < 1.0), axis=1)
+    expect = (block == 0) & (inside | (np.sqrt((gap ** 2).sum(axis=1)) <= margin))
+    np.testing.assert_array_equal(ib == 0, expect)
+    np.testing.assert_array_equal(ib, ib_o)
+    assert nh == nh_o == expect.sum() > 0
+
+
+@pytest.mark.parametrize("sizes", [((24, 24, 2), (12, 48, 2)), ((40, 30, 3), (16, 64, 3))])
+def test_hole_cut_cylinder_equals_radius_rule(sizes):
+    """Within hole_r - 0.5 of the cylinder's wall faces or inside them: the
+    same holes as the radius rule r < hole_r on these meshes (no centroid in
+    the band where the polygonal wall departs from the circle), equal to the
+    oracle, background field cells only."""
+    bg, comp = sizes
+    box = ((-6.0, -6.0, 0.0), (6.0, 6.0, 4.0))
+    ovr = cases.overset_cylinder(bg=bg, comp=comp, box=box)
+    ovw = cases.overset_cylinder(bg=bg, comp=comp, box=box, hole_cut="wall")
+    np.testing.assert_array_equal(ovr.spec.mesh.elem[:, 8], ovw.spec.mesh.elem[:, 8])
+    m = _unblanked(ovr.spec.mesh)
+    ib, nh = overset_hole_cut(m, ovr.block, wall_type=6, margin=0.7)
+    ib_o, nh_o = O.overset_hole_cut(O.Mesh(m.x, m.y, m.z, m.elem, m.ghost), ovr.block, 6, 0.7)
+    np.testing.assert_array_equal(ib, ib_o)
+    assert nh == nh_o == (ib == 0).sum() > 0 and np.all(ovr.block[ib == 0] == 0)
+    ib0, _ = overset_hole_cut(m, ovr.block, wall_type=6, margin=0.0)     # the body alone
+    xc = ovr.spec.mesh.x[m.elem[:, :4] - 1].mean(axis=1), ovr.spec.mesh.y[m.elem[:, :4] - 1].mean(axis=1)
+    r = np.hypot(*xc)
+    assert np.all(r[ib0 == 0] < 0.5) and np.all(ib0[(ovr.block == 0) & (r < 0.49)] == 0)
+
+
+def test_hole_cut_rejects_bad_arguments():
+    u, block = _cube_in_box()
+    with pytest.raises(HydraError):
+        overset_hole_cut(u.mesh, block, wall_type=6, margin=-1.0)
+    with pytest.raises(HydraError):
+        overset_hole_cut(u.mesh, block, wall_type=99, margin=0.0)       # no wall face of that type
+    bad = block.copy()
+    bad[0] = 2
+    with pytest.raises(HydraError):
+        overset_hole_cut(u.mesh, bad, wall_type=6, margin=0.0)
+
+
+@pytest.mark.gpu
+def test_hole_cut_device_equals_host():
+    """hp_overset_hole_cut_gpu returns the host's iblank bit for bit, and the
+    whole device chain (hole cut, donor search) gives the host chain's
+    tables."""
+    u, block = _cube_in_box()
+    for margin in (0.0, 0.3):
+        ib_h, nh_h = overset_hole_cut(u.mesh, block, 6, margin)
+        ib_d, nh_d = overset_hole_cut(u.mesh, block, 6, margin, device=True)
+        np.testing.assert_array_equal(ib_h, ib_d)
+        assert nh_h == nh_d
+    ov = cases.overset_cylinder(bg=(40, 30, 3), comp=(16, 64, 3), box=((-6.0, -6.0, 0.0), (6.0, 6.0, 4.0)))
+    m = _unblanked(ov.spec.mesh)
+    ib_h, nh_h = overset_hole_cut(m, ov.block, 6, 0.7)
+    ib_d, nh_d = overset_hole_cut(m, ov.block, 6, 0.7, device=True)
+    np.testing.assert_array_equal(ib_h, ib_d)
+    assert nh_h == nh_d > 0
+    mh = _with_iblank(m, ib_h)
+    fh, th = overset_build(mh, ov.block, ov.layers, ov.outer_type)
+    fd, td = overset_build(_with_iblank(m, ib_d), ov.block, ov.layers, ov.outer_type, device=True)
+    np.testing.assert_array_equal(fh, fd)
+    np.testing.assert_array_equal(th.donor, td.donor)
+    np.testing.assert_array_equal(th.weight, td.weight)
