@@ -148,7 +148,7 @@ int hp_step_timed(hp_handle *h, int32_t nsteps, double *device_ms);
 /* nsteps launched eagerly with a CUDA event between every two kernels;
  * accumulates device time and launch counts per kernel kind (nkinds >= 14:
  * prim_start, step_begin, smooth1, smooth2, bc_visc, visc, prim_stage, bc,
- * grad, flux, prim_end, step_end, serial, overset). */
+ * grad, flux, prim_end, step_end, serial, overset, halo). */
 int hp_profile_steps(hp_handle *h, int32_t nsteps, double *ms_per_kind,
                      int64_t *launches_per_kind, int32_t nkinds);
 
@@ -217,6 +217,54 @@ int hp_overset_hole_cut_gpu(const hp_mesh *mesh, const int32_t *block, int32_t w
 void hp_free_overset(hp_overset *ov);
 /* Single-case handles only; replaces any earlier table. */
 int hp_set_overset(hp_handle *h, const hp_overset *ov);
+
+/* --- partitioned meshes ------------------------------------------------------ */
+/* The reference runs one partition per MPI rank, with one layer of partition
+ * ghosts whose conserved state is exchanged after every RK stage
+ * (src/sr_mpiexchangecn.F90:1-96, called from src/sr_RK.F90) and an
+ * MPI_Allreduce of the time step (src/main.F90:552).  Here a part is an
+ * ordinary mesh: its own cells, then two layers of the neighbouring parts'
+ * cells as elements with their nodes (iblank HP_IBLANK_HALO1: gradients and
+ * limiter evaluated, no RK update; HP_IBLANK_HALO2: frozen), with the
+ * bounding-box nodes of the whole mesh appended.  Every owned cell then sees
+ * the inputs it has in the whole mesh, and the parts reproduce the
+ * single-mesh run bit for bit.  hydraphase.partition builds the parts. */
+enum { HP_IBLANK_HALO1 = 2, HP_IBLANK_HALO2 = 3 };
+/* Parts on one device, as the cases of a batch: after every RK stage, halo
+ * element dst_elem[t] of case dst_case[t] takes the conserved state of element
+ * src_elem[t] of case src_case[t] (1-based elements, 0-based cases; a
+ * destination is no source), and every case takes one dt, the minimum over
+ * the parts.  n = 0 removes the table.  Set before the first step. */
+int hp_set_halo(hp_handle *h, int32_t n, const int32_t *dst_case, const int32_t *dst_elem,
+                const int32_t *src_case, const int32_t *src_elem);
+/* Parts on several GPUs, one single-case handle per process.  The library
+ * calls fn(user, point, stream) on the thread that enqueues the steps, with
+ * the handle's cudaStream_t:
+ *   HP_X_DT    before each step forms its dt: the part's partial minimum
+ *              (*hp_dtmin_ptr: the bit pattern of a positive double, so the
+ *              minimum over parts is the unsigned minimum) is complete in
+ *              stream order; the callback enqueues its replacement by the
+ *              minimum over all parts (an allreduce(MIN) on the stream);
+ *   HP_X_HALO  after each RK stage: the callback enqueues hp_halo_pack, the
+ *              exchange between parts and hp_halo_unpack on the stream.
+ * Steps of a handle with a callback are not captured in CUDA graphs.  fn =
+ * NULL removes it. */
+enum { HP_X_DT = 0, HP_X_HALO = 1 };
+typedef void (*hp_exchange_fn)(void *user, int32_t point, void *stream);
+int hp_set_exchange(hp_handle *h, hp_exchange_fn fn, void *user);
+/* Cells this part sends (send_elem, its own elements) and receives
+ * (recv_elem, its halo elements), 1-based, each list in the order of the
+ * exchange buffers. */
+int hp_set_halo_lists(hp_handle *h, int32_t nsend, const int32_t *send_elem, int32_t nrecv,
+                      const int32_t *recv_elem);
+/* Enqueued on the handle's stream: buf[10 * t + k] = cn(send_elem[t], k+1)
+ * for the 10 conserved variables, and cn(recv_elem[t], k+1) =
+ * buf[10 * t + k] (cell major: one peer's cells are one contiguous block).
+ * Device buffers of 10 * nsend and 10 * nrecv doubles. */
+int hp_halo_pack(hp_handle *h, double *buf);
+int hp_halo_unpack(hp_handle *h, const double *buf);
+/* Device address of case 0's partial dt minimum (uint64 bit pattern). */
+int hp_dtmin_ptr(hp_handle *h, uint64_t **bits);
 
 /* --- output ------------------------------------------------------------------ */
 /* The Tecplot file of src/main.F90:956-1268 (two-phase build): node

@@ -11,6 +11,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/hydraphase.h"   // HP_IBLANK_HALO*, HP_X_*
+
 namespace hp {
 
 enum { NEQ = 10, NPR = 14, NGR = 33 };
@@ -78,6 +80,12 @@ struct DevMesh {
     const int* fr;
     const int* fdon;
     const double* fw;
+    // partition halo (nhalo = 0: none): after every RK stage cell hdst[t]
+    // takes the conserved state of cell hsrc[t] (the parts of one mesh as
+    // the cases of a batch); the cases then share one dt
+    int nhalo;
+    const int* hdst;
+    const int* hsrc;
 };
 
 // Per-case scalars (one entry per case of the handle).
@@ -120,14 +128,18 @@ struct DevState {
 enum KernelKind {
     KK_PRIM_START = 0, KK_STEP_BEGIN, KK_SMOOTH1, KK_SMOOTH2, KK_BC_VISC, KK_VISC,
     KK_PRIM_STAGE, KK_BC, KK_GRAD, KK_FLUX, KK_PRIM_END, KK_STEP_END, KK_SERIAL,
-    KK_OVERSET, KK_COUNT
+    KK_OVERSET, KK_HALO, KK_COUNT
 };
 
 // Optional hook called before every launch (and with KK_COUNT after the
 // last one) so the host can bracket each kernel with CUDA events.
 struct StepHook {
-    void (*mark)(void* ctx, int kind);
+    void (*mark)(void* ctx, int kind);      // before each kernel (may be null)
     void* ctx;
+    // exchange points of a part run on several GPUs (may be null):
+    // HP_X_DT before the step's dt is formed, HP_X_HALO after each RK stage
+    void (*exchange)(void* ctx, int point);
+    void* xctx;
 };
 
 // What one precision variant provides to the host.

@@ -91,6 +91,11 @@ struct hp_handle {
     std::vector<int> perm;      // [neles] case c's reference element i -> slot, at cases[c].e0 + i
     std::vector<int> ghost_id;  // [nghosts] case c's ghost g -> slot, at cases[c].g0 + g
     void* d_overset = nullptr;  // overset fringe table (hp_set_overset)
+    int* d_halo = nullptr;      // partition halo table (hp_set_halo): dst, then src
+    hp_exchange_fn xfn = nullptr;   // exchange callback of a part on several GPUs
+    void* xuser = nullptr;
+    int* d_xlist = nullptr;     // send cells, then receive cells (hp_set_halo_lists)
+    int nsend = 0, nrecv = 0;
     int* d_perm = nullptr;      // the two maps above, on the device
     int* d_gid = nullptr;
     double* d_gstage = nullptr; // 6 x nghosts staging of ghost primitives
@@ -732,6 +737,8 @@ extern "C" int hp_destroy(hp_handle* h) {
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
     if (h->d_overset) cudaFreeAsync(h->d_overset, h->stream);
+    if (h->d_halo) cudaFreeAsync(h->d_halo, h->stream);
+    if (h->d_xlist) cudaFreeAsync(h->d_xlist, h->stream);
     if (h->arena.base) {
         cudaFreeAsync(h->arena.base, h->stream);
         cudaStreamSynchronize(h->stream);
@@ -907,6 +914,13 @@ static cudaError_t reset_step_counters(hp_handle* h) {
     return cudaMemset2DAsync(&h->ds.s->step_in_call, sizeof(DevScalars), 0, sizeof(int), h->ncase, h->stream);
 }
 
+// exchange points of a part on several GPUs: the caller's callback with the
+// handle's stream
+static void exchange_point(void* ctx, int point) {
+    hp_handle* h = static_cast<hp_handle*>(ctx);
+    h->xfn(h->xuser, point, static_cast<void*>(h->stream));
+}
+
 static int run_steps(hp_handle* h, int n) {
     cudaStream_t st = h->stream;
     const int block = h->prm.block_size;
@@ -914,7 +928,10 @@ static int run_steps(hp_handle* h, int n) {
         h->var->enqueue_start(h->dm, &h->ds, h->dp, st, block, nullptr);
         h->started = true;
     }
-    if (h->prm.use_graph) {
+    if (h->xfn) {
+        const StepHook hook{nullptr, nullptr, exchange_point, h};
+        for (int k = 0; k < n; k++) h->var->enqueue_step(h->dm, &h->ds, h->dp, st, block, &hook);
+    } else if (h->prm.use_graph) {
         if (!h->gexec) {
             CUDA_OK(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             h->var->enqueue_step(h->dm, &h->ds, h->dp, st, block, nullptr);
@@ -1008,7 +1025,7 @@ extern "C" int hp_profile_steps(hp_handle* h, int32_t nsteps, double* ms_per_kin
     for (int k = 0; k < nkinds; k++) { ms_per_kind[k] = 0.0; launches_per_kind[k] = 0; }
     ProfCtx ctx;
     ctx.st = h->stream;
-    StepHook hook{prof_mark, &ctx};
+    StepHook hook{prof_mark, &ctx, h->xfn ? exchange_point : nullptr, h};
     if (!h->started) {
         h->var->enqueue_start(h->dm, &h->ds, h->dp, h->stream, h->prm.block_size, nullptr);
         h->started = true;
@@ -1074,6 +1091,124 @@ extern "C" int hp_set_overset(hp_handle* h, const hp_overset* ov) {
     // a captured step holds the mesh description it was launched with
     if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
     if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    return HP_OK;
+}
+
+// a captured step holds the mesh description it was launched with
+static void drop_graph(hp_handle* h) {
+    if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+}
+
+// Slot of element e (1-based, reference order) of case c; -1 if out of range.
+static int slot_of(const hp_handle* h, int c, int e) {
+    if (c < 0 || c >= h->ncase || e < 1 || e > h->cases[c].ne) return -1;
+    return h->perm[(size_t)h->cases[c].e0 + e - 1];
+}
+
+extern "C" int hp_set_halo(hp_handle* h, int32_t n, const int32_t* dst_case, const int32_t* dst_elem,
+                           const int32_t* src_case, const int32_t* src_elem) {
+    if (!h || n < 0 || (n > 0 && (!dst_case || !dst_elem || !src_case || !src_elem))) return HP_E_ARG;
+    if (h->started) return fail(h, HP_E_STATE, "hp_set_halo after the first step");
+    std::vector<int> iv(2 * (size_t)n);
+    std::vector<char> role(h->neles, 0);   // 1 destination, 2 source
+    for (int t = 0; t < n; t++) {
+        const int d = slot_of(h, dst_case[t], dst_elem[t]), q = slot_of(h, src_case[t], src_elem[t]);
+        if (d < 0 || q < 0) return fail(h, HP_E_ARG, "halo table: case or element out of range");
+        if (role[d] != 0 || role[q] == 1)
+            return fail(h, HP_E_ARG, "halo table: a destination repeats or is also a source");
+        role[d] = 1;
+        role[q] = 2;
+        iv[t] = d;
+        iv[(size_t)n + t] = q;
+    }
+    cudaStream_t st = h->stream;
+    if (h->d_halo) {
+        CUDA_OK(h, cudaFreeAsync(h->d_halo, st));
+        h->d_halo = nullptr;
+    }
+    h->dm.nhalo = 0;
+    h->dm.hdst = nullptr; h->dm.hsrc = nullptr;
+    if (n > 0) {
+        CUDA_OK(h, cudaMallocAsync(reinterpret_cast<void**>(&h->d_halo), iv.size() * sizeof(int), st));
+        CUDA_OK(h, cudaMemcpyAsync(h->d_halo, iv.data(), iv.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        h->dm.nhalo = n;
+        h->dm.hdst = h->d_halo;
+        h->dm.hsrc = h->d_halo + n;
+    }
+    CUDA_OK(h, cudaStreamSynchronize(st));
+    drop_graph(h);
+    return HP_OK;
+}
+
+extern "C" int hp_set_exchange(hp_handle* h, hp_exchange_fn fn, void* user) {
+    if (!h) return HP_E_ARG;
+    if (fn && h->ncase != 1) return fail(h, HP_E_UNSUPPORTED, "exchange callbacks: single-case handles only");
+    h->xfn = fn;
+    h->xuser = user;
+    drop_graph(h);
+    return HP_OK;
+}
+
+extern "C" int hp_set_halo_lists(hp_handle* h, int32_t nsend, const int32_t* send_elem, int32_t nrecv,
+                                 const int32_t* recv_elem) {
+    if (!h || nsend < 0 || nrecv < 0 || (nsend && !send_elem) || (nrecv && !recv_elem)) return HP_E_ARG;
+    if (h->ncase != 1) return fail(h, HP_E_UNSUPPORTED, "halo lists: single-case handles only");
+    std::vector<int> iv((size_t)nsend + nrecv);
+    for (int t = 0; t < nsend + nrecv; t++) {
+        const int s = slot_of(h, 0, t < nsend ? send_elem[t] : recv_elem[t - nsend]);
+        if (s < 0) return fail(h, HP_E_ARG, "halo lists: element out of range");
+        iv[t] = s;
+    }
+    cudaStream_t st = h->stream;
+    if (h->d_xlist) {
+        CUDA_OK(h, cudaFreeAsync(h->d_xlist, st));
+        h->d_xlist = nullptr;
+    }
+    h->nsend = h->nrecv = 0;
+    if (!iv.empty()) {
+        CUDA_OK(h, cudaMallocAsync(reinterpret_cast<void**>(&h->d_xlist), iv.size() * sizeof(int), st));
+        CUDA_OK(h, cudaMemcpyAsync(h->d_xlist, iv.data(), iv.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    }
+    h->nsend = nsend;
+    h->nrecv = nrecv;
+    CUDA_OK(h, cudaStreamSynchronize(st));
+    return HP_OK;
+}
+
+// buf[10 * t + k] <-> cn(list[t], k) for the 10 conserved variables (cell
+// major, so the cells of one peer form one contiguous block)
+template <bool PACK>
+__global__ void k_halo_buf(double* cn, long long ld, const int* list, int n, double* buf) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = list[t];
+    for (int k = 0; k < 10; k++) {
+        if (PACK) buf[10 * (size_t)t + k] = cn[(size_t)k * ld + i];
+        else cn[(size_t)k * ld + i] = buf[10 * (size_t)t + k];
+    }
+}
+
+extern "C" int hp_halo_pack(hp_handle* h, double* buf) {
+    if (!h || (h->nsend > 0 && !buf)) return HP_E_ARG;
+    if (h->nsend > 0)
+        k_halo_buf<true><<<(h->nsend + 255) / 256, 256, 0, h->stream>>>(h->ds.cn, h->ld, h->d_xlist, h->nsend, buf);
+    CUDA_OK(h, cudaGetLastError());
+    return HP_OK;
+}
+
+extern "C" int hp_halo_unpack(hp_handle* h, const double* buf) {
+    if (!h || (h->nrecv > 0 && !buf)) return HP_E_ARG;
+    if (h->nrecv > 0)
+        k_halo_buf<false><<<(h->nrecv + 255) / 256, 256, 0, h->stream>>>(h->ds.cn, h->ld, h->d_xlist + h->nsend,
+                                                                          h->nrecv, const_cast<double*>(buf));
+    CUDA_OK(h, cudaGetLastError());
+    return HP_OK;
+}
+
+extern "C" int hp_dtmin_ptr(hp_handle* h, uint64_t** bits) {
+    if (!h || !bits) return HP_E_ARG;
+    *bits = reinterpret_cast<uint64_t*>(&h->ds.s[0].dtmin_bits);
     return HP_OK;
 }
 

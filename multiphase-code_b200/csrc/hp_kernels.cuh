@@ -321,7 +321,8 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
                 bad |= (c[k] != c[k]);
                 COL(s.cu, k)[i] = c[k];
             }
-            nanc = bad ? 1 : 0;
+            // halo cells are counted by the part that owns them
+            nanc = (bad && ldg(m.iblank + i) < HP_IBLANK_HALO1) ? 1 : 0;
             DevScalars& sc = s.s[case_of(m, i)];
             if (i == sc.cell1) sc.velmag = sqrt(q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
         }
@@ -380,15 +381,28 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
 }
 
 // dt = cfl * dtmin, time += dt (src/main.F90:521-556); one thread per case.
-__global__ void k_step_begin(DevState<R> s, DevParams P, int ncase) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncase) return;
-    DevScalars* sc = s.s + c;
-    double dtmin = __longlong_as_double((long long)sc->dtmin_bits);
+__device__ __forceinline__ void step_begin_case(DevScalars* sc, const DevParams& P, unsigned long long bits) {
+    double dtmin = __longlong_as_double((long long)bits);
     sc->dt = dtmin * P.cfl;
     sc->time = sc->time + sc->dt;
     sc->total = sc->total + 1;
     sc->dtmin_bits = (unsigned long long)__double_as_longlong(1.0e8);
+}
+
+// One thread per case.  coupled: the cases are the parts of one mesh and all
+// take the minimum over all of them (the positive dt contributions order as
+// their bit patterns); launched as one block, which reads every case before
+// any is reset.
+__global__ void k_step_begin(DevState<R> s, DevParams P, int ncase, int coupled) {
+    if (coupled) {
+        unsigned long long bits = ~0ull;
+        for (int k = 0; k < ncase; k++) bits = min(bits, s.s[k].dtmin_bits);
+        __syncthreads();
+        for (int c = threadIdx.x; c < ncase; c += blockDim.x) step_begin_case(s.s + c, P, bits);
+        return;
+    }
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncase) step_begin_case(s.s + c, P, s.s[c].dtmin_bits);
 }
 
 // per-step diagnostics and reset of the residual accumulators; one thread
@@ -702,9 +716,14 @@ __global__ void __launch_bounds__(512) k_smooth2(DevMesh m, DevState<R> s, DevPa
     }
 }
 
+// Cells whose gradients and limiter are evaluated: active cells and the
+// first halo layer of a partition part (iblank HP_IBLANK_HALO1), which its
+// owner evaluates the same way; the halo is never RK-updated.
+__device__ __forceinline__ bool grad_cell(int ib) { return ib == 1 || ib == HP_IBLANK_HALO1; }
+
 // ---------------------------------------------------------------------------
 // LSQ gradients (src/sr_derivative.F90:45-322) fused with the
-// Venkatakrishnan limiter (src/sr_VK.F90:32-272).  iblank == 1 cells.
+// Venkatakrishnan limiter (src/sr_VK.F90:32-272).  grad_cell() cells.
 // FPR: read the primitives in R (the float copy of the FP32-arithmetic
 // variants) instead of the FP64 columns; false on aliased meshes.
 template <bool FPR>
@@ -713,7 +732,7 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParam
     const PT* const prb = reinterpret_cast<const PT*>(FPR ? (const void*)s.prr : (const void*)s.pr);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
-    if (ldg(m.iblank + i) != 1) return;
+    if (!grad_cell(ldg(m.iblank + i))) return;
     int n[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
@@ -1376,7 +1395,7 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
     int i = (int)(gt >> 2);
     const bool valid = i < m.neles;
     if (!valid) i = m.neles - 1;
-    const bool active = valid && ldg(m.iblank + i) == 1;
+    const bool active = valid && grad_cell(ldg(m.iblank + i));
     if constexpr (HP_FAST(1)) {
         // the outputs are not inputs of this kernel, so a warp that flagged
         // an operand simply recomputes and overwrites them
@@ -1828,11 +1847,23 @@ __global__ void __launch_bounds__(256) k_overset(DevMesh m, DevState<R> s) {
     for (int k = 0; k < 10; k++) COL(s.cn, k)[i] = v[k];
 }
 
+// Partition halo: each halo cell takes the conserved state of the cell that
+// owns it in another part of the batch, after every RK stage.  Destinations
+// are halo cells, which no RK update writes; sources are owned cells.
+__global__ void __launch_bounds__(256) k_halo(DevMesh m, DevState<R> s) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.nhalo) return;
+    const int i = ldg(m.hdst + t), j = ldg(m.hsrc + t);
+#pragma unroll
+    for (int k = 0; k < 10; k++) COL(s.cn, k)[i] = COL(s.cn, k)[j];
+}
+
 static inline unsigned grid_for(long long n, int block) {
     return (unsigned)((n + block - 1) / block);
 }
 
-#define MARK(k) do { if (hook) hook->mark(hook->ctx, (k)); } while (0)
+#define MARK(k) do { if (hook && hook->mark) hook->mark(hook->ctx, (k)); } while (0)
+#define EXCHANGE(p) do { if (hook && hook->exchange) hook->exchange(hook->xctx, (p)); } while (0)
 
 static void enqueue_start(const DevMesh& m, const void* stp, const DevParams& P, cudaStream_t st,
                           int block, const StepHook* hook) {
@@ -1853,8 +1884,10 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     const int cb = block > 0 ? block : 256, b = 128;
     const unsigned ge = grid_for(m.neles, cb), gf = grid_for(m.neles, b);
     const unsigned gg = grid_for(m.nghosts > 0 ? m.nghosts : 1, cb);
+    EXCHANGE(HP_X_DT);
     MARK(KK_STEP_BEGIN);
-    k_step_begin<<<grid_for(m.ncase, 128), 128, 0, st>>>(s, P, m.ncase);
+    if (m.nhalo > 0) k_step_begin<<<1, 128, 0, st>>>(s, P, m.ncase, 1);
+    else k_step_begin<<<grid_for(m.ncase, 128), 128, 0, st>>>(s, P, m.ncase, 0);
     // JST dissipation, src/sr_smooth.F90 (once per step)
     if (m.aliased) { MARK(KK_SERIAL); k_smooth_copy_serial<<<1, 1, 0, st>>>(m, s, 0); }
     MARK(KK_SMOOTH1);
@@ -1911,6 +1944,11 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             MARK(KK_OVERSET);
             k_overset<<<grid_for(m.nfringe, 256), 256, 0, st>>>(m, s);
         }
+        if (m.nhalo > 0) {
+            MARK(KK_HALO);
+            k_halo<<<grid_for(m.nhalo, 256), 256, 0, st>>>(m, s);
+        }
+        EXCHANGE(HP_X_HALO);
     }
     // src/main.F90:595-641: primitive, residual norms, cu = cn
     MARK(KK_PRIM_END);
@@ -1923,6 +1961,7 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     MARK(KK_COUNT);
 }
 #undef MARK
+#undef EXCHANGE
 
 }  // namespace HP_NS
 }  // namespace hp

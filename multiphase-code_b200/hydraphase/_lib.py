@@ -15,6 +15,10 @@ LIB_PATH = os.environ.get("HYDRAPHASE_LIB", os.path.join(HERE, "libhydraphase.so
 
 HP_OK, HP_E_ARG, HP_E_CUDA, HP_E_NOMEM, HP_E_IO, HP_E_STATE, HP_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
 PREC_FP64_PARITY, PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2, 3
+HP_IBLANK_HALO1, HP_IBLANK_HALO2 = 2, 3      # partition halo layers
+HP_X_DT, HP_X_HALO = 0, 1                    # exchange points (hp_set_exchange)
+# hp_exchange_fn: (user, point, stream)
+HP_EXCHANGE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p)
 
 ERROR_NAMES = {HP_E_ARG: "HP_E_ARG", HP_E_CUDA: "HP_E_CUDA", HP_E_NOMEM: "HP_E_NOMEM",
                HP_E_IO: "HP_E_IO", HP_E_STATE: "HP_E_STATE", HP_E_UNSUPPORTED: "HP_E_UNSUPPORTED"}
@@ -98,6 +102,13 @@ def lib():
     L.hp_overset_hole_cut.argtypes = [ctypes.POINTER(HpMesh), ctypes.POINTER(_I), _I, _D, ctypes.POINTER(_I),
                                       ctypes.POINTER(_I)]
     L.hp_overset_hole_cut_gpu.argtypes = L.hp_overset_hole_cut.argtypes
+    L.hp_set_halo.argtypes = [vp, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                              ctypes.POINTER(_I)]
+    L.hp_set_exchange.argtypes = [vp, HP_EXCHANGE_FN, vp]
+    L.hp_set_halo_lists.argtypes = [vp, _I, ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]
+    L.hp_halo_pack.argtypes = [vp, vp]
+    L.hp_halo_unpack.argtypes = [vp, vp]
+    L.hp_dtmin_ptr.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint64))]
     L.hp_free_overset.argtypes = [ctypes.POINTER(HpOverset)]
     L.hp_free_overset.restype = None
     L.hp_set_overset.argtypes = [vp, ctypes.POINTER(HpOverset)]
@@ -121,14 +132,16 @@ def lib():
                "hp_estimate_batch_bytes", "hp_overset_build", "hp_overset_build_gpu", "hp_set_overset",
                "hp_get_state", "hp_get_prims", "hp_device_state", "hp_info", "hp_read_flow",
                "hp_read_mesh", "hp_read_restart", "hp_write_restart", "hp_write_tecplot", "hp_output_async",
-               "hp_output_wait", "hp_set_host_threads", "hp_overset_hole_cut", "hp_overset_hole_cut_gpu"):
+               "hp_output_wait", "hp_set_host_threads", "hp_overset_hole_cut", "hp_overset_hole_cut_gpu",
+               "hp_set_halo", "hp_set_exchange", "hp_set_halo_lists", "hp_halo_pack", "hp_halo_unpack",
+               "hp_dtmin_ptr"):
         getattr(L, fn).restype = ctypes.c_int
     _lib = L
     return L
 
 
 KERNEL_KINDS = ("prim_start", "step_begin", "smooth1", "smooth2", "bc_visc", "visc", "prim_stage",
-                "bc", "grad", "flux", "prim_end", "step_end", "serial", "overset")
+                "bc", "grad", "flux", "prim_end", "step_end", "serial", "overset", "halo")
 
 EXPORTED_SYMBOLS = (
     "hp_create", "hp_destroy", "hp_last_error", "hp_create_error", "hp_init_uniform",
@@ -137,6 +150,7 @@ EXPORTED_SYMBOLS = (
     "hp_write_restart", "hp_dt_noalloc", "hp_estimate_bytes", "hp_poll", "hp_create_batch", "hp_case_count",
     "hp_set_state_case", "hp_get_state_case", "hp_estimate_batch_bytes", "hp_overset_build", "hp_free_overset",
     "hp_set_overset", "hp_overset_build_gpu", "hp_write_tecplot", "hp_output_async", "hp_output_wait",
-    "hp_set_host_threads", "hp_overset_hole_cut", "hp_overset_hole_cut_gpu",
+    "hp_set_host_threads", "hp_overset_hole_cut", "hp_overset_hole_cut_gpu", "hp_set_halo", "hp_set_exchange",
+    "hp_set_halo_lists", "hp_halo_pack", "hp_halo_unpack", "hp_dtmin_ptr",
 )
 NOALLOC_MAX_CELLS = 1 << 24
