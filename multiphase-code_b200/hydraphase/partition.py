@@ -363,7 +363,7 @@ class RankPart:
         return self.case.state()
 
     def close(self):
-        lib().hp_set_exchange(self.case.h, None, None)
+        lib().hp_set_exchange(self.case.h, HP_EXCHANGE_FN(), None)     # NULL: no callback
         self.case.close()
 
 
