@@ -351,6 +351,38 @@ def overset_measure(steps: int):
     return out
 
 
+def partition_measure(spec, nparts: int, steps: int, check_steps: int = 3) -> dict:
+    """The workload split into nparts parts with two halo layers
+    (hydraphase.partition), run on this one GPU as the cases of one batch
+    coupled by hp_set_halo (one dt; halo cells copied from their owners after
+    every RK stage): device-timed steps, the halo share of the cells, and
+    whether check_steps steps reproduce the single-mesh FP64 parity run bit
+    for bit."""
+    from hydraphase import PREC_FP64_PARITY, Case
+    from hydraphase.partition import PartitionedCase, partition_case
+    t0 = time.perf_counter()
+    P = partition_case(spec, nparts)
+    t1 = time.perf_counter()
+    local = sum(p.spec.mesh.neles for p in P.parts)
+    prm = spec.params(precision=PREC_FP64_PARITY)
+    with PartitionedCase(P, prm) as pc:
+        pc.set_state(0.0, spec.cu, spec.ghost_prims)
+        dp = pc.step(check_steps)
+        _, cu_p, gp_p = pc.state()
+        ms = pc.step_timed(steps)
+    with Case(spec.mesh, prm) as c:
+        c.set_state(0.0, spec.cu, spec.ghost_prims)
+        ds = c.step(check_steps)
+        _, cu_s, gp_s = c.state()
+    same = bool(np.array_equal(cu_p, cu_s) and np.array_equal(gp_p, gp_s) and
+                all(np.array_equal(dp[k], ds[k]) for k in ("time", "dt", "velmag", "diff")))
+    stages = 3 if spec.extra.get("rk_scheme", 0) == 1 else 4
+    return {"parts": nparts, "layout": "one GPU, the parts as one coupled batch",
+            "cells": spec.mesh.neles, "local_cells": local, "halo_frac": local / spec.mesh.neles - 1.0,
+            "value": spec.mesh.neles * stages * steps / (ms / 1e3), "ms_per_step": ms / steps, "unit": UNIT,
+            "partition_s": round(t1 - t0, 2), f"bit_exact_vs_single_mesh_{check_steps}_steps": same}
+
+
 def accuracy_run(spec, steps: int) -> dict:
     """The mixed variant against the FP64 parity variant after `steps` steps
     from the same initial state, on the timed workload (rel L2 of mixture
@@ -543,6 +575,8 @@ def run_ours(args, world, rank, local, pg):
         line["mixed"]["accuracy"] = accuracy_run(spec, args.accuracy_steps)
     if world == 1 and rank == 0 and not args.no_overset:
         line["overset"] = overset_measure(max(args.steps // 2, 5))
+    if world == 1 and rank == 0 and args.partition_parts > 1:
+        line["partitioned"] = partition_measure(spec, args.partition_parts, max(args.steps // 2, 5))
     if world == 1 and rank == 0 and not args.no_output:
         line["output"] = output_measure()
     if world == 1 and rank == 0 and args.serving_cases > 0:
@@ -567,6 +601,8 @@ def main():
     ap.add_argument("--serving-steps", type=int, default=500)
     ap.add_argument("--no-overset", action="store_true", help="skip the overset cylinder measurement")
     ap.add_argument("--no-output", action="store_true", help="skip the asynchronous output measurement")
+    ap.add_argument("--partition-parts", type=int, default=4,
+                    help="parts of the partitioned-mesh measurement on this GPU (0 or 1: skip)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy run on the timed workload (0: skip)")
     args = ap.parse_args()
