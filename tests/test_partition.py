@@ -28,6 +28,7 @@ from hydraphase.partition import HALO_EDGE_TYPE, partition_case
 
 SPECS = {
     "shock_bubble": lambda: cases.shock_bubble(n=6, alpha_min=0.1),
+    "shock_bubble_ref": lambda: cases.shock_bubble(n=6, alpha_min=0.1, reference_scheme=True),
     "cylinder": lambda: cases.cylinder(nr=6, nt=16, nz=2),
 }
 
@@ -250,3 +251,38 @@ def test_rank_parts_with_thread_exchange_bit_exact(nparts):
          "diff": np.max(np.stack([o["diff"] for o in out]), axis=0),
          "nan_cells": np.sum(np.stack([o["nan_cells"] for o in out]), axis=0)}
     _assert_same(d, cu, gp, ref)
+
+
+def _nccl_rank(rank, world, port, out_dir):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from hydraphase.partition import DistComm, RankPart
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    spec = SPECS["cylinder"]()
+    ref = _single(spec, 3)
+    P = partition_case(spec, 1)
+    rp = RankPart(P, 0, spec.params(precision=PREC_FP64_PARITY), DistComm())
+    cp, gp = P.scatter_state(spec.cu, spec.ghost_prims)[0]
+    rp.set_state(0.0, cp, gp)
+    d = rp.step(3)
+    _, cu, gpo = rp.state()
+    rp.close()
+    dist.destroy_process_group()
+    same = all(np.array_equal(d[k], ref[0][k]) for k in ("time", "dt", "velmag", "diff")) and \
+        np.array_equal(cu, ref[1]) and np.array_equal(gpo, ref[2])
+    np.save(os.path.join(out_dir, "nccl.npy"), np.array([same]))
+
+
+@pytest.mark.gpu
+def test_rank_part_dt_allreduce_over_nccl_single_rank(tmp_path):
+    """DistComm over NCCL with one rank (one GPU in this run): the library
+    calls back at every exchange point and the dt word is allreduced in
+    place on the library's stream; the run equals the plain single-mesh
+    run bit for bit."""
+    mp.spawn(_nccl_rank, args=(1, _free_port(), str(tmp_path)), nprocs=1, join=True)
+    assert bool(np.load(tmp_path / "nccl.npy")[0])
