@@ -33,7 +33,7 @@ enum {
     HP_E_NOMEM = -3,      /* device allocation failed or over the HBM budget */
     HP_E_IO = -4,         /* file could not be opened / parsed */
     HP_E_STATE = -5,      /* call out of order (e.g. step before set_state) */
-    HP_E_UNSUPPORTED = -6 /* feature outside this build (partition ghosts) */
+    HP_E_UNSUPPORTED = -6 /* feature outside this build (proc_bc partition ghosts) */
 };
 
 /* Arithmetic of the hot kernels. */
@@ -86,7 +86,8 @@ typedef struct hp_params {
  *   x, y, z[nodes]                   node coordinates
  *   elem[neles*9] row-major          nod1..nod4, nc1..nc4, iblank (1-based)
  *   ghost[nghosts*4] row-major       nparent, nghost, ntype, nside
- * Partition ghosts (proc_bc) must be zero: one partition per GPU. */
+ * Partition ghosts (proc_bc) must be zero: a part of a partitioned mesh is an
+ * ordinary mesh whose halo cells are elements (see hp_set_halo). */
 typedef struct hp_mesh {
     int32_t nodes, neles, nghosts, pghosts;
     const double *x, *y, *z;

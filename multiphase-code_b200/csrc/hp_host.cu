@@ -510,7 +510,9 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
         const hp_mesh* mesh = meshes + c;
         const std::string tag = ncase > 1 ? "case " + std::to_string(c) + ": " : "";
         if (mesh->pghosts != 0)
-            return fail(nullptr, HP_E_UNSUPPORTED, tag + "partition ghosts: one partition per GPU only");
+            return fail(nullptr, HP_E_UNSUPPORTED,
+                        tag + "proc_bc partition ghosts: give a partitioned mesh's parts halo elements instead "
+                              "(hydraphase.partition, hp_set_halo)");
         if (mesh->nodes <= 0 || mesh->neles <= 0 || mesh->nghosts < 0 || !mesh->x || !mesh->y || !mesh->z ||
             !mesh->elem || (mesh->nghosts > 0 && !mesh->ghost))
             return fail(nullptr, HP_E_ARG, tag + "empty or incomplete mesh");

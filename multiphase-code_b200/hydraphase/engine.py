@@ -313,7 +313,8 @@ def read_mesh(case_dir: str, rank: int = 0) -> MeshArrays:
     _check(L.hp_read_mesh(case_dir.encode(), rank, ctypes.byref(m)))
     try:
         if m.pghosts:
-            raise HydraError(-6, "partition ghosts are not supported (one partition per GPU)")
+            raise HydraError(-6, "proc_bc partition ghosts are not read: partition the whole mesh with "
+                                 "hydraphase.partition instead")
         x = np.ctypeslib.as_array(m.x, (m.nodes,)).copy()
         y = np.ctypeslib.as_array(m.y, (m.nodes,)).copy()
         z = np.ctypeslib.as_array(m.z, (m.nodes,)).copy()
