@@ -588,6 +588,58 @@ def run_ours(args, world, rank, local, pg):
     return 0
 
 
+def run_partitioned(args, world, rank, local, pg):
+    """--partitioned: strong scaling of the workload over the ranks.  The
+    mesh is split into one part per rank with two halo layers
+    (hydraphase.partition); each rank steps its part in the FP64 parity
+    variant, exchanging the halo after every RK stage and the dt minimum
+    before every step through NCCL on the library's stream (DistComm; with
+    one process, a single part and ThreadComm).  value = the whole mesh's
+    cell-stage updates over the max-over-ranks device time."""
+    import torch
+    from hydraphase import PREC_FP64_PARITY
+    from hydraphase.partition import DistComm, RankPart, ThreadComm, partition_case
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    spec = make_workload(args.workload)
+    stages = 3 if spec.extra.get("rk_scheme", 0) == 1 else 4
+    t0 = time.perf_counter()
+    P = partition_case(spec, world)
+    part_s = time.perf_counter() - t0
+    comm = DistComm() if pg is not None else ThreadComm(1).bind(0)
+    rp = RankPart(P, rank, spec.params(precision=PREC_FP64_PARITY), comm)
+    cp, gp = P.scatter_state(spec.cu, spec.ghost_prims)[rank]
+    rp.set_state(0.0, cp, gp)
+    rp.step(args.warmup, diagnostics=False)
+    rp.case.sync()
+    if pg is not None:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = rp.case.step_timed(args.steps)
+    clk = clocks.stop()
+    if rp.error is not None:
+        raise rp.error
+    t_max = barrier_max(pg, ms, device) / 1e3
+    local_cells = barrier_sum(pg, float(P.parts[rank].spec.mesh.neles), device)
+    kernels = int(rp.case.info()["kernels_per_step"]) * args.steps
+    rp.close()
+    line = {
+        "metric": METRIC, "value": spec.mesh.neles * stages * args.steps / t_max, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (O-grid cylinder generated in the reference's formats)",
+        "config": {**workload_config(spec, args.workload),
+                   "parallelism": f"partitioned x{world} (two-layer halo, exchange after every RK stage)",
+                   "precision": "fp64 bit-parity (no FMA)", "halo_frac": local_cells / spec.mesh.neles - 1.0,
+                   "partition_s": round(part_s, 2)},
+        "gpu_launches": kernels, "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -603,6 +655,9 @@ def main():
     ap.add_argument("--no-output", action="store_true", help="skip the asynchronous output measurement")
     ap.add_argument("--partition-parts", type=int, default=4,
                     help="parts of the partitioned-mesh measurement on this GPU (0 or 1: skip)")
+    ap.add_argument("--partitioned", action="store_true",
+                    help="strong scaling: one part of the workload mesh per rank, halo exchange over NCCL "
+                         "(instead of one replica per rank)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy run on the timed workload (0: skip)")
     args = ap.parse_args()
@@ -611,6 +666,8 @@ def main():
     try:
         if args.impl == "reference":
             rc = run_reference_arm(args, world, rank, pg)
+        elif args.partitioned:
+            rc = run_partitioned(args, world, rank, local, pg)
         else:
             rc = run_ours(args, world, rank, local, pg)
     finally:
