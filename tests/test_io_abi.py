@@ -177,3 +177,13 @@ def test_host_thread_share():
     assert lib().hp_set_host_threads(2) == 0
     assert lib().hp_set_host_threads(0) == 0
     assert lib().hp_set_host_threads(-1) == HP_E_ARG
+
+
+def test_partition_constants_match_header():
+    """The Python mirror's halo iblank codes and exchange points are the
+    header's enums."""
+    from hydraphase._lib import HP_IBLANK_HALO1, HP_IBLANK_HALO2, HP_X_DT, HP_X_HALO
+    hdr = open(os.path.join(ROOT, "include", "hydraphase.h")).read()
+    vals = {k: int(v) for k, v in re.findall(r"\b(HP_IBLANK_HALO[12]|HP_X_DT|HP_X_HALO)\s*=\s*(\d+)", hdr)}
+    assert vals == {"HP_IBLANK_HALO1": HP_IBLANK_HALO1, "HP_IBLANK_HALO2": HP_IBLANK_HALO2,
+                    "HP_X_DT": HP_X_DT, "HP_X_HALO": HP_X_HALO}
