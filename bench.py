@@ -273,6 +273,7 @@ def serving_measure(n_cases: int, steps: int):
                        f"{steps} SSP-RK3 steps each, CFL 0.05, HBM budget 150 GiB; time-to-solution "
                        f"from arrival to the final state on the host; after an untimed 12-case warm-up",
            "cells_total": int(sum(r.spec.mesh.neles for r in reqs)), "generation_s": round(gen_s, 2)}
+    reports = {}
     for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64_PARITY)):
         blocks, modes = {}, {}
         for r in reqs:
@@ -287,8 +288,20 @@ def serving_measure(n_cases: int, steps: int):
         # growth, worker start-up)
         server.run([type(r)(r.rid, 0.0, 25, r.spec) for r in reqs[:12]], realtime=False)
         rep_ = server.run(reqs)
+        reports[name] = rep_
         out[name] = {**rep_.summary(), "block_size": blocks, "face_mode": modes}
     out["speedup_mixed_vs_fp64"] = out["mixed"]["updates_per_s"] / out["fp64"]["updates_per_s"]
+    # each served mixed result against the served FP64 result of the same case
+    fp = {r.rid: r for r in reports["fp64"].results}
+    err = []
+    for r in reports["mixed"].results:
+        f = fp.get(r.rid)
+        if r.error is None and f is not None and f.error is None and r.cu is not None and f.cu is not None:
+            rho_m, rho_f = r.cu[0] + r.cu[5], f.cu[0] + f.cu[5]
+            err.append(float(np.linalg.norm(rho_m - rho_f) / np.linalg.norm(rho_f)))
+    if err:
+        out["mixed_vs_fp64_density_rel_l2"] = {"median": float(np.median(err)), "max": float(np.max(err)),
+                                               "cases": len(err), "steps": steps}
     return out
 
 
