@@ -9,9 +9,10 @@ Two levels are tuned:
   FP32-arithmetic variants) and, for those variants, whether the HLLC and
   viscous fluxes are evaluated once per face (a face list, one thread per
   face, then a per-cell gather) or once from each side (four lanes per cell,
-  one kernel fewer per stage). Every candidate runs a few device-timed steps
-  (CUDA events) of a representative case of the class, and the fastest is
-  kept. The four-lane kernels have their block size fixed by their launch
+  one kernel fewer per stage). Every candidate runs device-timed steps (CUDA
+  events) of a representative case of the class: the best of three runs from
+  the initial state, each of at least 20 ms (up to 200 steps).  The fastest
+  is kept. The four-lane kernels have their block size fixed by their launch
   bounds, tuned per precision variant at build time.
 * **Serving** (`tune_serving`). These are the units in flight, the
   multi-mesh batch size and the steps enqueued per turn. Every candidate
@@ -26,6 +27,7 @@ read the cache instead of measuring again.
 from __future__ import annotations
 
 import json
+import math
 import os
 import time
 
@@ -77,6 +79,24 @@ def _key(precision: int, cls: str, what: str) -> str:
     return f"{_gpu_name()}|prec{precision}|{cls}|{what}"
 
 
+def _ms_per_step(c, spec, steps: int, min_ms: float = 20.0, max_steps: int = 200, repeats: int = 3) -> float:
+    """Device ms per step of an open Case: the best of `repeats` timed runs
+    from the initial state, each of at least `steps` steps and, up to
+    max_steps, of at least min_ms in all.  Small meshes step in a fraction of
+    a millisecond, where a few steps time mostly launch noise and the choice
+    between candidates would be a coin toss."""
+    c.set_state(0.0, spec.cu, spec.ghost_prims)
+    c.step(2, diagnostics=False)
+    probe = c.step_timed(steps) / steps
+    n = min(max_steps, max(steps, int(math.ceil(min_ms / max(probe, 1e-3)))))
+    best = float("inf")
+    for _ in range(repeats):
+        c.set_state(0.0, spec.cu, spec.ghost_prims)
+        c.step(1, diagnostics=False)
+        best = min(best, c.step_timed(n) / n)
+    return best
+
+
 def tune_block_size(spec, precision: int = PREC_MIXED, candidates=BLOCK_CANDIDATES, steps: int = 6,
                     use_cache: bool = True) -> tuple[int, dict]:
     """Threads per block of the per-cell kernels for the size class of
@@ -89,9 +109,7 @@ def tune_block_size(spec, precision: int = PREC_MIXED, candidates=BLOCK_CANDIDAT
     ms = {}
     for b in candidates:
         with Case(spec.mesh, spec.params(precision=precision, block_size=int(b))) as c:
-            c.set_state(0.0, spec.cu, spec.ghost_prims)
-            c.step(2, diagnostics=False)
-            ms[int(b)] = min(c.step_timed(steps), c.step_timed(steps)) / steps
+            ms[int(b)] = _ms_per_step(c, spec, steps)
     best = min(ms, key=ms.get)
     data = _load()
     data[key] = {"best": best, "ms": {str(k): v for k, v in ms.items()}, "cells": spec.mesh.neles,
@@ -115,9 +133,7 @@ def tune_face_mode(spec, precision: int = PREC_MIXED, block_size: int = 0, steps
     ms = {}
     for mode in (0, 1):
         with Case(spec.mesh, spec.params(precision=precision, block_size=int(block_size), face_mode=mode)) as c:
-            c.set_state(0.0, spec.cu, spec.ghost_prims)
-            c.step(2, diagnostics=False)
-            ms[mode] = min(c.step_timed(steps), c.step_timed(steps)) / steps
+            ms[mode] = _ms_per_step(c, spec, steps)
     best = min(ms, key=ms.get)
     data = _load()
     data[key] = {"best": best, "ms": {str(k): v for k, v in ms.items()}, "cells": spec.mesh.neles,
