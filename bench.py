@@ -271,7 +271,7 @@ def serving_measure(n_cases: int, steps: int):
     gen_s = time.perf_counter() - t0
     out = {"workload": f"shock-bubble stream: {n_cases} cases, cells log-U[6000, 400000], Poisson 40/s, "
                        f"{steps} SSP-RK3 steps each, CFL 0.05, HBM budget 150 GiB; time-to-solution "
-                       f"from arrival to the final state on the host; after an untimed 12-case warm-up",
+                       f"from arrival to the final state on the host; after an untimed 25-step warm-up of every case",
            "cells_total": int(sum(r.spec.mesh.neles for r in reqs)), "generation_s": round(gen_s, 2)}
     reports = {}
     for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64_PARITY)):
@@ -283,10 +283,10 @@ def serving_measure(n_cases: int, steps: int):
                 modes[cls] = tune.tune_face_mode(r.spec, precision=prec, block_size=blocks[cls], steps=4)[0]
         server = Server(150 << 30, precision=prec, max_active=16, chunk=25, chunk_cell_steps=10_000_000,
                         batch_cells=200000, block_size=blocks, face_mode=modes, keep_state=True)
-        # warm-up (untimed): a few cases of every size, all arriving at once,
-        # so the measured run pays no first-use costs (module loading, pool
-        # growth, worker start-up)
-        server.run([type(r)(r.rid, 0.0, 25, r.spec) for r in reqs[:12]], realtime=False)
+        # warm-up (untimed): every case of the stream for 25 steps, all
+        # arriving at once, so the measured run pays no first-use costs
+        # (module loading, pool growth to the stream's peak, worker start-up)
+        server.run([type(r)(r.rid, 0.0, 25, r.spec) for r in reqs], realtime=False)
         rep_ = server.run(reqs)
         reports[name] = rep_
         out[name] = {**rep_.summary(), "block_size": blocks, "face_mode": modes}
