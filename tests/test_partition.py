@@ -286,3 +286,41 @@ def test_rank_part_dt_allreduce_over_nccl_single_rank(tmp_path):
     run bit for bit."""
     mp.spawn(_nccl_rank, args=(1, _free_port(), str(tmp_path)), nprocs=1, join=True)
     assert bool(np.load(tmp_path / "nccl.npy")[0])
+
+
+@pytest.mark.gpu
+def test_halo_and_exchange_argument_errors():
+    """hp_set_halo rejects ids out of range, a repeated destination and a
+    destination that is also a source, and a table set after the first step;
+    hp_set_exchange and hp_set_halo_lists take single-case handles only."""
+    import ctypes
+
+    from hydraphase import HP_E_ARG, HP_E_STATE, HP_E_UNSUPPORTED, Batch
+    from hydraphase._lib import HP_EXCHANGE_FN, lib
+    spec = SPECS["shock_bubble"]()
+    P = partition_case(spec, 2)
+    L = lib()
+    ip = lambda a: np.ascontiguousarray(a, np.int32).ctypes.data_as(ctypes.POINTER(ctypes.c_int32))  # noqa: E731
+    with Batch([p.spec.mesh for p in P.parts], spec.params(precision=PREC_FP64_PARITY)) as b:
+        dc, de, sc, se = (np.ascontiguousarray(a, np.int32) for a in P.halo_table())
+        bad = de.copy()
+        bad[0] = 10 ** 7
+        assert L.hp_set_halo(b.h, dc.size, ip(dc), ip(bad), ip(sc), ip(se)) == HP_E_ARG
+        rep = de.copy()
+        rep[1] = rep[0]
+        rep_c = dc.copy()
+        rep_c[1] = rep_c[0]
+        assert L.hp_set_halo(b.h, dc.size, ip(rep_c), ip(rep), ip(sc), ip(se)) == HP_E_ARG
+        # a destination that is another entry's source
+        d1 = np.array([dc[0], sc[0]], np.int32)
+        e1 = np.array([de[0], se[0]], np.int32)
+        s1 = np.array([sc[0], dc[0]], np.int32)
+        f1 = np.array([se[0], de[0]], np.int32)
+        assert L.hp_set_halo(b.h, 2, ip(d1), ip(e1), ip(s1), ip(f1)) == HP_E_ARG
+        assert L.hp_set_exchange(b.h, HP_EXCHANGE_FN(lambda u, p, s: None), None) == HP_E_UNSUPPORTED
+        assert L.hp_set_halo_lists(b.h, 0, None, 0, None) == HP_E_UNSUPPORTED
+        assert L.hp_set_halo(b.h, dc.size, ip(dc), ip(de), ip(sc), ip(se)) == 0
+        for c, (cp, gp) in enumerate(P.scatter_state(spec.cu, spec.ghost_prims)):
+            b.set_state(c, 0.0, cp, gp)
+        b.step(1, diagnostics=False)
+        assert L.hp_set_halo(b.h, dc.size, ip(dc), ip(de), ip(sc), ip(se)) == HP_E_STATE
