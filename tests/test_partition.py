@@ -39,7 +39,7 @@ def _neighbours(el, ids, ne):
 
 
 @pytest.mark.parametrize("name", list(SPECS))
-@pytest.mark.parametrize("nparts", [1, 2, 5])
+@pytest.mark.parametrize("nparts", [1, 2, 5, 37])
 def test_parts_structure(name, nparts):
     spec = SPECS[name]()
     m = spec.mesh
@@ -178,7 +178,7 @@ def _assert_same(d, cu, gp, ref):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(SPECS))
-@pytest.mark.parametrize("nparts", [2, 5])
+@pytest.mark.parametrize("nparts", [2, 5, 37])
 def test_partitioned_batch_bit_exact(name, nparts):
     from hydraphase.partition import PartitionedCase
     spec = SPECS[name]()
