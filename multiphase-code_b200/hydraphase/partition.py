@@ -51,7 +51,7 @@ import numpy as np
 
 from . import cases
 from ._lib import HP_EXCHANGE_FN, HP_IBLANK_HALO1, HP_IBLANK_HALO2, HP_X_DT, HpParams, lib
-from .engine import Batch, Case, MeshArrays, _check, _dp, _ip
+from .engine import Batch, Case, MeshArrays, _check, _ip
 
 HALO_EDGE_TYPE = 2     # boundary type of the ghosts closing the second halo layer
 
