@@ -7,8 +7,8 @@
  * calls argument-less subroutines that share module globals
  * (src/mod_GlobalVariables.F90).  This header replaces that loop.  A Fortran
  * host keeps its own Read_flow, mesh reader and restart/Tecplot writers and
- * calls these entry points through ISO_C_BINDING interfaces (see
- * INTEGRATION.md); plain pointers and sizes only, 1-based cell ids as the
+ * calls these entry points through ISO_C_BINDING interfaces (one bind(C)
+ * interface per function below); plain pointers and sizes only, 1-based cell ids as the
  * reference stores them, column-major conserved state.
  *
  * Conventions: every entry point returns 0 on success and a negative
@@ -323,7 +323,12 @@ int hp_poll(hp_handle *h, int32_t *busy);
  * cells that each GPU using the library keeps until exit; larger ncells is
  * rejected with HP_E_ARG.  All calls share that array, so calls that overlap
  * on the GPU race.  The first call on each device looks up the array's device
- * address; make it before any stream capture. */
+ * address; make it before any stream capture.  The lookup is repeated when
+ * the device's context changes (after cudaDeviceReset, or a runtime that
+ * shuts the device down and opens it again), so the call stays valid across
+ * such a reset.  If an earlier CUDA call of the caller left an error pending,
+ * the call returns HP_E_CUDA without launching and leaves that error for the
+ * caller to read. */
 #define HP_NOALLOC_MAX_CELLS (1 << 24)
 int hp_dt_noalloc(const double *cn_dev, int64_t ld, const double *dl_dev,
                   int32_t ncells, const hp_params *params, double *dt_dev,

@@ -22,6 +22,8 @@
 #define HP_LSQ_TABLE 1
 #include "hp_kernels.cuh"
 
+#include <cuda.h>
+
 #include <mutex>
 
 #include "../../include/hydraphase.h"
@@ -39,20 +41,56 @@ static __device__ __align__(256) unsigned long long g_dt_partial[kMaxBlocks];
 
 std::mutex g_mu;
 constexpr int kMaxDevices = 64;
-unsigned long long* g_dev_ptr[kMaxDevices] = {};
+// Device address of g_dt_partial per device, with the id of the CUDA context
+// it was looked up in.  A context torn down and made again on the same device
+// (cudaDeviceReset, or an OpenACC runtime that shuts the device down and
+// opens a new data region) reloads this module at a new address, so the
+// address is looked up again whenever the current context's id changes
+// (context ids are never reused within a process).
+struct Scratch { unsigned long long ctx_id; unsigned long long* ptr; };
+Scratch g_dev[kMaxDevices] = {};
 
-// Device address of g_dt_partial on the current device, looked up once per
-// device (the host-side name of the array is only a stand-in; a kernel must
-// be given the device address).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Id of the current context, through the driver entry points the runtime
+// hands out (no link-time dependency on the driver library).
+cudaError_t current_ctx_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            return cudaErrorNotSupported;
+        get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return cudaErrorContextIsDestroyed;
+    return get_id(ctx, id) == CUDA_SUCCESS ? cudaSuccess : cudaErrorContextIsDestroyed;
+}
+
+// Device address of g_dt_partial on the current device and context (the
+// host-side name of the array is only a stand-in; a kernel must be given the
+// device address).  Looked up once per device and context.
 cudaError_t scratch_on_device(int dev, unsigned long long** out) {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_dev_ptr[dev]) {
+    unsigned long long id = 0;
+    cudaError_t e = current_ctx_id(&id);
+    if (e != cudaSuccess) return e;
+    if (!g_dev[dev].ptr || g_dev[dev].ctx_id != id) {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_dt_partial);
+        e = cudaGetSymbolAddress(&p, g_dt_partial);
         if (e != cudaSuccess) return e;
-        g_dev_ptr[dev] = static_cast<unsigned long long*>(p);
+        g_dev[dev].ptr = static_cast<unsigned long long*>(p);
+        g_dev[dev].ctx_id = id;
     }
-    *out = g_dev_ptr[dev];
+    *out = g_dev[dev].ptr;
     return cudaSuccess;
 }
 
@@ -115,6 +153,9 @@ extern "C" int hp_dt_noalloc(const double* cn_dev, int64_t ld, const double* dl_
                              const hp_params* params, double* dt_dev, void* stream) {
     if (!cn_dev || !dl_dev || !params || !dt_dev || ncells < 1 || ld < ncells) return HP_E_ARG;
     if (ncells > HP_NOALLOC_MAX_CELLS) return HP_E_ARG;   // beyond the scratch array
+    // an error left pending by the caller's own CUDA work stays the caller's:
+    // report it without launching and without clearing it
+    if (cudaPeekAtLastError() != cudaSuccess) return HP_E_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return HP_E_CUDA;
     unsigned long long* part = nullptr;
@@ -131,5 +172,6 @@ extern "C" int hp_dt_noalloc(const double* cn_dev, int64_t ld, const double* dl_
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     k_dt_partial<<<nblocks, kBlock, 0, st>>>(cn_dev, ld, dl_dev, ncells, P, part);
     k_dt_final<<<1, 1024, 0, st>>>(part, nblocks, p.cfl, dt_dev);
+    // nothing was pending on entry, so an error now is this call's launch
     return cudaGetLastError() == cudaSuccess ? HP_OK : HP_E_CUDA;
 }

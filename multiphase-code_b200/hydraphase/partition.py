@@ -459,9 +459,13 @@ class _ThreadRank:
         s = torch.cuda.ExternalStream(stream)
         with torch.cuda.stream(s):
             self._post(s, t, None)
-            for q in range(hub.n):
-                s.wait_event(hub.ready[q][1])
-            m = torch.min(torch.cat([hub.ready[q][0] for q in range(hub.n)])).reshape(1)
+            try:
+                for q in range(hub.n):
+                    s.wait_event(hub.ready[q][1])
+                m = torch.min(torch.cat([hub.ready[q][0] for q in range(hub.n)])).reshape(1)
+            except BaseException:
+                hub.barrier.abort()      # the peers fail at once, not at the timeout
+                raise
             self._finish(s, [q for q in range(hub.n) if q != self.rank])
             t.copy_(m)
 
@@ -475,15 +479,22 @@ class _ThreadRank:
             o += int(ns)
         with torch.cuda.stream(s):
             self._post(s, sendbuf, offs)
-            ro = 0
-            for q, nr in zip(peers, rcount):
-                nr = int(nr)
-                buf, qev, qoffs = hub.ready[q]
-                so, ns = qoffs[r]
-                if ns != nr:
-                    raise RuntimeError(f"part {r} expects {nr} cells from part {q}, which sends {ns}")
-                if nr:
-                    s.wait_event(qev)
-                    recvbuf[10 * ro:10 * (ro + nr)].copy_(buf[10 * so:10 * (so + ns)])
-                ro += nr
+            try:
+                ro = 0
+                for q, nr in zip(peers, rcount):
+                    nr = int(nr)
+                    buf, qev, qoffs = hub.ready[q]
+                    so, ns = qoffs.get(r, (0, 0))
+                    if ns != nr:
+                        raise RuntimeError(f"part {r} expects {nr} cells from part {q}, which sends {ns}")
+                    if nr:
+                        s.wait_event(qev)
+                        recvbuf[10 * ro:10 * (ro + nr)].copy_(buf[10 * so:10 * (so + ns)])
+                    ro += nr
+            except BaseException:
+                # a part that fails between posting and finishing would leave
+                # its peers at the second barrier until the timeout; breaking
+                # the barrier ends their exchange at once with an error
+                hub.barrier.abort()
+                raise
             self._finish(s, peers)

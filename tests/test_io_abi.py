@@ -63,6 +63,33 @@ def test_shipped_flow_and_mesh(reference_dir):
     np.testing.assert_array_equal(m.ghost, om.ghost)
 
 
+def test_shipped_mesh_through_reference_format(tmp_path):
+    """The shipped mesh (committed fixture), written back in the reference's
+    grid/bc text layout with 17 significant digits as its list-directed
+    output has them, and read by the library's reader: identical arrays.
+    Runs without the reference checkout."""
+    from conftest import shipped_case
+    flow, om = shipped_case()
+    g = tmp_path / "geometry_files"
+    g.mkdir()
+    (tmp_path / "flow.in").write_text(str(np.load(os.path.join(ROOT, "tests", "golden",
+                                                               "shipped_mesh.npz"))["flow_in"]))
+    with open(g / "grid_proc0000.dat", "w") as f:
+        f.write(f"{om.nodes:12d}{om.neles:12d}\n")
+        nd = np.column_stack([np.arange(1, om.nodes + 1), om.x, om.y, om.z, om.gid, om.gid])
+        np.savetxt(f, nd, fmt="%12d %25.16E %25.16E %25.16E %16d %11d")
+        np.savetxt(f, np.column_stack([np.arange(1, om.neles + 1), om.elem]), fmt="%12d")
+    with open(g / "bc_proc0000.in", "w") as f:
+        f.write(f"{om.nghosts:12d}\n")
+        np.savetxt(f, om.ghost, fmt="%12d")
+    (g / "proc_bc0000.in").write_text("           0           0\n")
+    p = read_flow(str(tmp_path / "flow.in"))
+    assert (p.myflux, p.myorder, p.niter, p.itersub) == (2, 2, 2, 5)
+    m = read_mesh(str(tmp_path))
+    for k in ("x", "y", "z", "elem", "ghost"):
+        np.testing.assert_array_equal(getattr(m, k), getattr(om, k), err_msg=k)
+
+
 @pytest.mark.skipif(not have_reference(), reason="reference checkout not mounted")
 def test_shipped_restart_reader(reference_dir):
     m = read_mesh(reference_dir)

@@ -3,8 +3,9 @@
 The shipped case (flow.in: HLLC-Batten, 2nd order, CFL 0.01, 2x5 steps from a
 uniform state) runs 10 steps on the merged overset mesh (266,688 tets).  The
 reference wrote Velocity.dat (time and |u_g| of cell 1 per step) and
-restart_files/restart0000.in (full conserved state).  Fixtures extracted by
-tests/golden/make_golden.py.
+restart_files/restart0000.in (full conserved state).  The inputs (mesh and
+flow.in) and the golden outputs are fixtures extracted by
+tests/golden/make_golden.py, so these tests need no reference checkout.
 
 Everything is pinned bit for bit:
   * all 10 (time, |u_g(1)|) records; cell 1 borders a corrupted overset cell
@@ -25,12 +26,24 @@ import numpy as np
 import pytest
 
 import oracle as O
-from conftest import GOLDEN_DIR
+from conftest import GOLDEN_DIR, have_reference, shipped_case, REFERENCE_DIR
+
+
+def test_fixture_equals_reference_files():
+    """The committed mesh fixture decodes to exactly what the reference's
+    files hold (checked where the reference checkout is mounted)."""
+    if not have_reference():
+        pytest.skip("HYDRA_REFERENCE_DIR not set")
+    flow, mesh = shipped_case()
+    flow_r, mesh_r = O.read_case_dir(REFERENCE_DIR)
+    assert flow == flow_r
+    for k in ("x", "y", "z", "elem", "ghost", "gid"):
+        np.testing.assert_array_equal(getattr(mesh, k), getattr(mesh_r, k), err_msg=k)
 
 
 @pytest.fixture(scope="module")
-def shipped_run(reference_dir):
-    flow, mesh = O.read_case_dir(reference_dir)
+def shipped_run():
+    flow, mesh = shipped_case()
     orc = O.Oracle(O.params_from_flow(flow), mesh)
     orc.init_uniform()
     nst = flow["niter"] * flow["itersub"]

@@ -159,6 +159,61 @@ def test_exchange_over_gloo(tmp_path, world):
         assert ok and word == 1000
 
 
+class _FakeEvent:
+    def record(self, stream=None):
+        pass
+
+
+class _FakeStream:
+    def __init__(self, handle=None):
+        pass
+
+    def wait_event(self, ev):
+        pass
+
+
+def test_thread_exchange_failure_ends_all_parts_promptly(monkeypatch):
+    """A part whose receive count disagrees with its peer's send count raises
+    between posting its buffer and finishing the exchange.  It breaks the
+    hub's barrier on the way out, so the peer's exchange ends with an error at
+    once instead of waiting for the barrier's timeout.  Host-only: CUDA events
+    and streams are replaced by no-op fakes and the buffers are CPU tensors."""
+    import contextlib
+    import threading
+    import time
+
+    import torch
+    from hydraphase.partition import ThreadComm
+    monkeypatch.setattr(torch.cuda, "Event", _FakeEvent)
+    monkeypatch.setattr(torch.cuda, "ExternalStream", _FakeStream)
+    monkeypatch.setattr(torch.cuda, "stream", lambda s: contextlib.nullcontext())
+    hub = ThreadComm(2, timeout=60.0)
+    errors = [None, None]
+
+    def part(rank):
+        # part 0 sends 2 cells to part 1; part 1 sends 3 to part 0, which
+        # expects 4
+        scount = [2] if rank == 0 else [3]
+        rcount = [4] if rank == 0 else [2]
+        send = torch.zeros(10 * scount[0], dtype=torch.float64)
+        recv = torch.zeros(10 * rcount[0], dtype=torch.float64)
+        try:
+            hub.bind(rank).exchange(send, scount, recv, rcount, [1 - rank], None)
+        except Exception as e:      # noqa: BLE001 -- the test inspects it
+            errors[rank] = e
+
+    t0 = time.monotonic()
+    threads = [threading.Thread(target=part, args=(r,)) for r in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=30.0)
+    assert not any(t.is_alive() for t in threads)
+    assert time.monotonic() - t0 < 10.0
+    assert isinstance(errors[0], RuntimeError) and "expects 4 cells" in str(errors[0])
+    assert isinstance(errors[1], threading.BrokenBarrierError)
+
+
 # --- GPU ---------------------------------------------------------------------
 def _single(spec, n, prec=PREC_FP64_PARITY):
     with Case(spec.mesh, spec.params(precision=prec)) as c:
