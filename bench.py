@@ -14,7 +14,7 @@ Arms:
   default          the CUDA engine through its C ABI (libhydraphase.so)
   --impl reference the reference algorithm on the host cores (the FP64 CPU
                    restatement in oracle/, since the Fortran reference cannot
-                   be built here), on a bounded sample of the same workload.
+                   be built here), on the same workload and step counts.
 """
 from __future__ import annotations
 
@@ -230,32 +230,38 @@ def profiled_traffic_per_cell(kernel: str):
     return None
 
 
-def cpu_oracle_sample(name: str, threads: int, seconds_target: float = 15.0):
-    """The CPU restatement on a bounded sample: same physics and scheme on a
-    coarser O-grid, timed over whole steps."""
+def cpu_oracle_run(spec, threads: int, warmup: int, steps: int | None = None,
+                   seconds_target: float | None = None):
+    """The CPU restatement of the reference (oracle/, FP64, OpenMP over cells
+    on `threads` host threads) on the same workload as the GPU arm: `warmup`
+    untimed whole steps, then either `steps` timed steps or whole steps until
+    `seconds_target` seconds of stepping have passed.  Returns
+    (cell-stage updates/s, steps timed, seconds)."""
     import oracle as O
-    from hydraphase import cases
-    if name.startswith("cylinder"):
-        spec = cases.cylinder(nr=40, nt=64, nz=8, seed=1, alpha_w_drop=1e-5, alpha_w_bg=1e-6)
-        what = "O-grid 40x64x8"
-    else:
-        spec = cases.shock_bubble(n=8, alpha_min=0.1)
-        spec.flow["cfl"] = 0.05
-        what = "box 8^3 hexes"
     m = spec.mesh
     O.set_threads(threads)
     orc = O.Oracle(O.params_from_flow(spec.flow, **spec.extra), O.Mesh(m.x, m.y, m.z, m.elem, m.ghost))
     orc.set_state(0.0, spec.cu, spec.ghost_prims)
-    orc.run(1)   # warm-up
+    if warmup > 0:
+        orc.run(warmup)
     stages = 3 if spec.extra.get("rk_scheme", 0) == 1 else 4
-    steps, t_used = 0, 0.0
-    while t_used < seconds_target and steps < 200:
+    n, t_used = 0, 0.0
+    while (steps is not None and n < steps) or (steps is None and t_used < seconds_target):
         t0 = time.perf_counter()
         orc.run(1)
         t_used += time.perf_counter() - t0
-        steps += 1
-    return {"value": m.neles * stages * steps / t_used, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{m.neles} cells ({what}, same physics), {steps} steps, {t_used:.1f} s"}
+        n += 1
+    orc.close()
+    return m.neles * stages * n / t_used, n, t_used
+
+
+def cpu_baseline(spec, name: str, threads: int, seconds_target: float = 12.0):
+    """cpu_baseline of the GPU arm's line: the oracle on the identical
+    workload, one untimed step, then whole steps for about seconds_target."""
+    v, n, t = cpu_oracle_run(spec, threads, 1, seconds_target=seconds_target)
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"the timed workload itself ({name}, {spec.mesh.neles} cells): {n} whole steps after "
+                      f"1 untimed, {t:.1f} s", "same_config": True}
 
 
 def serving_measure(n_cases: int, steps: int):
@@ -449,16 +455,26 @@ def output_measure(steps: int = 300) -> dict:
 
 
 def run_reference_arm(args, world, rank, pg):
+    """The reference's algorithm on the host cores, on the GPU arm's
+    workload and step counts: the FP64 CPU restatement in oracle/ (the
+    Fortran reference cannot be built here), --warmup untimed steps, then
+    --steps timed whole steps.  Rank 0 only."""
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    res = cpu_oracle_sample(args.workload, threads, seconds_target=max(5.0, min(60.0, 3.0 * args.steps)))
-    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+    spec = make_workload(args.workload)
+    v, n, t = cpu_oracle_run(spec, threads, args.warmup, steps=args.steps)
+    res = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": f"the GPU arm's workload ({args.workload}, {spec.mesh.neles} cells): {n} whole steps "
+                     f"after {args.warmup} untimed, {t:.1f} s", "same_config": True}
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "impl": "reference", "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "note": "CPU restatement of the reference on a bounded sample"},
-            "cpu_baseline": res,
-            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {**workload_config(spec, args.workload), "parallelism": f"replicas x{world}",
+                       "precision": "fp64 bit-parity (no FMA)"},
+            "note": "CPU restatement of the reference (oracle/), all host threads, rank 0",
+            "ms_per_step": t * 1e3 / n, "cpu_baseline": res,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -582,7 +598,7 @@ def run_ours(args, world, rank, local, pg):
         "nan_cells_after": float(d64["nan_cells"][0]),
     }
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_oracle_sample(args.workload, os.cpu_count() or 1)
+        line["cpu_baseline"] = cpu_baseline(spec, args.workload, os.cpu_count() or 1)
     if world == 1 and rank == 0 and args.accuracy_steps > 0:
         line["mixed"]["accuracy"] = accuracy_run(spec, args.accuracy_steps)
     if world == 1 and rank == 0 and not args.no_overset:
