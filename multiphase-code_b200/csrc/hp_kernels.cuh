@@ -771,9 +771,20 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParam
     R gv[13][3];
 #pragma unroll
     for (int v = 0; v < 13; v++) {
-        const PT* q = COL(prb, pcol[v]);
-        PT qi = q[i];
-        R qa = (R)(q[n[0]] - qi), qb = (R)(q[n[1]] - qi), qc = (R)(q[n[2]] - qi), qd = (R)(q[n[3]] - qi);
+        R qa, qb, qc, qd;
+        if (FPR && pcol[v] == P_PHIG) {
+            // alpha_g differences from the FP64 primitives: near alpha_g = 1
+            // the FP32 copies differ by whole ulps (6e-8), as much as a trace
+            // alpha_p = 1 - alpha_g itself, whose reconstruction uses this
+            // gradient
+            const double* q = COL(s.pr, P_PHIG);
+            const double qi = q[i];
+            qa = (R)(q[n[0]] - qi); qb = (R)(q[n[1]] - qi); qc = (R)(q[n[2]] - qi); qd = (R)(q[n[3]] - qi);
+        } else {
+            const PT* q = COL(prb, pcol[v]);
+            PT qi = q[i];
+            qa = (R)(q[n[0]] - qi); qb = (R)(q[n[1]] - qi); qc = (R)(q[n[2]] - qi); qd = (R)(q[n[3]] - qi);
+        }
         R c1 = DW(qa * xa[0], 0) + DW(qb * xa[1], 1) + DW(qc * xa[2], 2) + DW(qd * xa[3], 3);
         R c2;
         if (v == 7)   // cTp2 lacks the /wt4 (src/sr_derivative.F90:225)
@@ -890,6 +901,18 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     R tgR = (R)PLD(COL(pr, P_TG) + neigh), phigR = (R)PLD(COL(pr, P_PHIG) + neigh);
     R upR = (R)PLD(COL(pr, P_UP) + neigh), vpR = (R)PLD(COL(pr, P_VP) + neigh), wpR = (R)PLD(COL(pr, P_WP) + neigh);
     R tpR = (R)PLD(COL(pr, P_TP) + neigh), pgR = (R)PLD(COL(pr, P_PG) + neigh), ppR = (R)PLD(COL(pr, P_PP) + neigh);
+    // alpha_p.  The reference forms it as 1 - alpha_g after reconstruction
+    // (src/sr_hllcbatten.F90:226-227), which the FP64 variants keep.  In FP32
+    // that difference loses everything where the water is a trace: with
+    // alpha_g = 1 - 1e-6 one FP32 ulp of alpha_g is 6% of alpha_p.  The FP32
+    // variants therefore start from the cell's own alpha_p (recovered in FP64)
+    // and subtract the reconstruction increment of alpha_g, which is the same
+    // quantity mathematically and keeps alpha_p to FP32 relative precision.
+    R phipL = R(0), phipR = R(0);
+    if constexpr (sizeof(R) == 4) {
+        phipL = (R)PLD(COL(pr, P_PHIP) + i);
+        phipR = (R)PLD(COL(pr, P_PHIP) + neigh);
+    }
     if (P.myorder == 2 && (kind & FK_RECON)) {
         const R phimin = (R)mn2(PLD(s.phi + i), PLD(s.phi + neigh));
         const double xf = ldg(COL(m.fch, f) + i), yf = ldg(COL(m.fch, 4 + f) + i),
@@ -900,10 +923,21 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
         const R* g = s.gr;
 #define REC(v, X, Y, Z, G, c) \
     v = v + phimin * (X * PLD(COL(g, G) + c) + Y * PLD(COL(g, G + 1) + c) + Z * PLD(COL(g, G + 2) + c))
-        REC(phigL, xf0, yf0, zf0, G_PHIG, i); REC(ugL, xf0, yf0, zf0, G_UG, i);
+        if constexpr (sizeof(R) == 4) {
+            const R dL = xf0 * PLD(COL(g, G_PHIG) + i) + yf0 * PLD(COL(g, G_PHIG + 1) + i) +
+                         zf0 * PLD(COL(g, G_PHIG + 2) + i);
+            const R dR = xfn * PLD(COL(g, G_PHIG) + neigh) + yfn * PLD(COL(g, G_PHIG + 1) + neigh) +
+                         zfn * PLD(COL(g, G_PHIG + 2) + neigh);
+            phigL = phigL + phimin * dL; phipL = phipL - phimin * dL;
+            phigR = phigR + phimin * dR; phipR = phipR - phimin * dR;
+        } else {
+            REC(phigL, xf0, yf0, zf0, G_PHIG, i);
+            REC(phigR, xfn, yfn, zfn, G_PHIG, neigh);
+        }
+        REC(ugL, xf0, yf0, zf0, G_UG, i);
         REC(vgL, xf0, yf0, zf0, G_VG, i); REC(wgL, xf0, yf0, zf0, G_WG, i);
         REC(tgL, xf0, yf0, zf0, G_TG, i); REC(pgL, xf0, yf0, zf0, G_PG, i);
-        REC(phigR, xfn, yfn, zfn, G_PHIG, neigh); REC(ugR, xfn, yfn, zfn, G_UG, neigh);
+        REC(ugR, xfn, yfn, zfn, G_UG, neigh);
         REC(vgR, xfn, yfn, zfn, G_VG, neigh); REC(wgR, xfn, yfn, zfn, G_WG, neigh);
         REC(tgR, xfn, yfn, zfn, G_TG, neigh); REC(pgR, xfn, yfn, zfn, G_PG, neigh);
         REC(upL, xf0, yf0, zf0, G_UP, i); REC(vpL, xf0, yf0, zf0, G_VP, i);
@@ -915,7 +949,10 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
 #undef REC
     }
     const R rrg = (R)P.rrg, gamag = (R)P.gamag, gamap = (R)P.gamap, pinf = (R)P.pinf, cpp = (R)P.cpp;
-    R phipL = R(1) - phigL, phipR = R(1) - phigR;
+    if constexpr (sizeof(R) != 4) {
+        phipL = R(1) - phigL;
+        phipR = R(1) - phigR;
+    }
     blend_phases_r<F>(P, phigL, phipL, ugL, vgL, wgL, tgL, pgL, upL, vpL, wpL, tpL, ppL, bad);
     R rogL = pgL / (rrg * tgL);
     R ropL = gamap * (ppL + pinf) / ((gamap - R(1)) * cpp * tpL);
@@ -1195,17 +1232,25 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
         const R dl = (R)ldg(m.dl + i), voli = (R)ldg(m.vol + i);
         const R amug = (R)P.as * sqrt(tg) / (R(1) + (R)P.ts / tg);
         const R du = ug - up, dv = vg - vp, dw = wg - wp;
-        const R drag = R(0.44) * phig * (phig - R(1)) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        // alpha_g (alpha_g - 1) and 1 - alpha_g in the reference's form in
+        // FP64; from alpha_p in FP32, where the differences would cancel
+        // (see face_eval)
+        R drag;
+        if constexpr (sizeof(R) == 4)
+            drag = -(R(0.44) * phig * phip) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        else
+            drag = R(0.44) * phig * (phig - R(1)) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        const R omg = sizeof(R) == 4 ? phip : R(1) - phig;
         const R fdgx = drag * du, fdgy = drag * dv, fdgz = drag * dw;
         const R qsource = R(6) * phip * amug * (R)P.cpg * R(2) * (tp - tg) / ((R)P.prg * (dl * dl));
         const R delpstar = R(2) * (phig * rog * phip * rop) / (phig * rop + phip * rog) *
                            (du * du + dv * dv + dw * dw);
         const R pint = pg - mn2(delpstar, R(0.01) * pg);
-        const R den = phig * rog + (R(1) - phig) * rop;
+        const R den = phig * rog + omg * rop;
         const R rden = rcp(den);
-        const R uint_ = div_rn(phig * rog * ug + (R(1) - phig) * rop * up, den, rden);
-        const R vint = div_rn(phig * rog * vg + (R(1) - phig) * rop * vp, den, rden);
-        const R wint = div_rn(phig * rog * wg + (R(1) - phig) * rop * wp, den, rden);
+        const R uint_ = div_rn(phig * rog * ug + omg * rop * up, den, rden);
+        const R vint = div_rn(phig * rog * vg + omg * rop * vp, den, rden);
+        const R wint = div_rn(phig * rog * wg + omg * rop * wp, den, rden);
         const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
         R xa[4], ya[4], za[4], pa[4], wt[4];
 #pragma unroll
@@ -1438,7 +1483,8 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     const int nq = ldg(COL(m.nc, q) + i);
     const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
     const R xq = (R)(ldg(m.xc + nq) - x0), yq = (R)(ldg(m.yc + nq) - y0), zq = (R)(ldg(m.zc + nq) - z0);
-    const R pq = (R)(COL(pr, P_PHIG)[nq] - COL(pr, P_PHIG)[i]);
+    // alpha_g differences from the FP64 primitives (see k_grad)
+    const R pq = (R)(COL(s.pr, P_PHIG)[nq] - COL(s.pr, P_PHIG)[i]);
     // residual in face order 1..4 (src/sr_hllcbatten.F90:534-552)
     S rhs[10];
 #pragma unroll
@@ -1484,19 +1530,27 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         const R dl = (R)ldg(m.dl + i), voli = (R)ldg(m.vol + i);
         const R amug = (R)P.as * sqrt(tg) / (R(1) + (R)P.ts / tg);
         const R du = ug - up, dv = vg - vp, dw = wg - wp;
-        const R drag = R(0.44) * phig * (phig - R(1)) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        // alpha_g (alpha_g - 1) and 1 - alpha_g in the reference's form in
+        // FP64; from alpha_p in FP32, where the differences would cancel
+        // (see face_eval)
+        R drag;
+        if constexpr (sizeof(R) == 4)
+            drag = -(R(0.44) * phig * phip) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        else
+            drag = R(0.44) * phig * (phig - R(1)) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        const R omg = sizeof(R) == 4 ? phip : R(1) - phig;
         const R fdgx = drag * du, fdgy = drag * dv, fdgz = drag * dw;
         const R qsource = R(6) * phip * amug * (R)P.cpg * R(2) * (tp - tg) / ((R)P.prg * (dl * dl));
         const R delpstar = R(2) * (phig * rog * phip * rop) / (phig * rop + phip * rog) *
                            (du * du + dv * dv + dw * dw);
         const R pint = pg - mn2(delpstar, R(0.01) * pg);
-        const R den = phig * rog + (R(1) - phig) * rop;
+        const R den = phig * rog + omg * rop;
         // lane q < 3 evaluates component q of the interface velocity, of the
         // right-hand side of the alpha_g LSQ system and of its solution; the
         // results are exchanged with shuffles
         const R gq = q == 0 ? ug : (q == 1 ? vg : wg);
         const R pq_ = q == 0 ? up : (q == 1 ? vp : wp);
-        const R vq_int = (phig * rog * gq + (R(1) - phig) * rop * pq_) / den;
+        const R vq_int = (phig * rog * gq + omg * rop * pq_) / den;
         const R uint_ = qshfl(vq_int, 0), vint = qshfl(vq_int, 1), wint = qshfl(vq_int, 2);
         // geometry-only terms (src/sr_source.F90:100-117), evaluated at set-up
         R wt[4], rw[4];
