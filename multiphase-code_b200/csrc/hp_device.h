@@ -38,6 +38,7 @@ struct DevParams {
     // correctly rounded reciprocals of constant divisors
     double r_emm, r_gm1, r_gamap, r_prg, r_prp;
     int rk_scheme, inviscid, myorder, nstage;
+    int myflux;   // 1 HLLC-Zien, 2 HLLC-Batten (src/mod_Fluxmodule.F90:8-11)
 };
 
 // A handle holds one case or a batch of cases whose meshes are concatenated:

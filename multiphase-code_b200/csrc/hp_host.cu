@@ -499,8 +499,10 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     g_create_error.clear();
     if (!meshes || !params || !out || ncase < 1) return fail(nullptr, HP_E_ARG, "null argument or no case");
     *out = nullptr;
-    if (params->myflux != 2)
-        return fail(nullptr, HP_E_UNSUPPORTED, "myflux must be 2 (HLLC-Batten)");
+    if (params->myflux == 3)
+        return fail(nullptr, HP_E_UNSUPPORTED, "myflux 3 (Jameson central flux) is not built");
+    if (params->myflux != 1 && params->myflux != 2)
+        return fail(nullptr, HP_E_ARG, "myflux must be 1 (HLLC-Zien) or 2 (HLLC-Batten)");
     if (params->myorder != 1 && params->myorder != 2)
         return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
     if (params->block_size != 0 && (params->block_size < 64 || params->block_size > 512 || params->block_size % 32))
@@ -563,7 +565,7 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     P.c23 = (double)(2.00f / 3.00f); P.co2 = (double)(1.00f / 16.00f); P.co4 = (double)(1.00f / 1024.00f);
     P.fsd = 4.0 * p.surfacetension / p.diap;
     P.cfl = p.cfl; P.venkat_k = p.venkat_k > 0 ? p.venkat_k : 0.3; P.twall = p.twall; P.amup = 0.001;
-    P.rk_scheme = p.rk_scheme; P.inviscid = p.inviscid; P.myorder = p.myorder;
+    P.rk_scheme = p.rk_scheme; P.inviscid = p.inviscid; P.myorder = p.myorder; P.myflux = p.myflux;
     P.r_emm = 1.0 / (P.emax - P.emin);
     P.r_gm1 = 1.0 / (P.gamag - 1.0);
     P.r_gamap = 1.0 / P.gamap;

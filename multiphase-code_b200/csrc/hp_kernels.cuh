@@ -872,6 +872,109 @@ __device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& p
     }
 }
 
+// HLLC-Zien for one face (src/sr_hllczien.F90:348-487): wave speeds over
+// both phases, a mixture contact speed, and one branch for all ten fluxes.
+// takeg = takep = whether a branch was taken (NaN states take none).
+template <int F>
+__device__ __forceinline__ void zien_flux(FaceOut& o, unsigned& bad, R area, R enx, R eny, R enz,
+                                          R phigL, R phipL, R rogL, R ropL, R ugL, R vgL, R wgL, R upL, R vpL,
+                                          R wpL, R pgL, R ppL, R egL, R hgL, R qgL, R agL, R epL, R hpL, R qpL,
+                                          R apL, R phigR, R phipR, R rogR, R ropR, R ugR, R vgR, R wgR, R upR,
+                                          R vpR, R wpR, R pgR, R ppR, R egR, R hgR, R qgR, R agR, R epR, R hpR,
+                                          R qpR, R apR) {
+    const R eps8 = (R)(double)1.0e-8f, eps6 = (R)(double)1.0e-6f;
+    // DMIN1 / DMAX1 of five arguments, left to right
+    const R sl = mn2(mn2(mn2(mn2(qgL - agL, qpL - apL), qgR - agR), qpR - apR), eps8);
+    const R sr = mx2(mx2(mx2(mx2(qgL + agL, qpL + apL), qgR + agR), qpR + apR), eps8);
+    const R rol = phigL * rogL + phipL * ropL;
+    const R roql = phigL * rogL * qgL + phipL * ropL * qpL;
+    const R ql = roql / rol;
+    const R prl = phigL * pgL + phipL * ppL;
+    const R ror = phigR * rogR + phipR * ropR;
+    const R roqr = phigR * rogR * qgR + phipR * ropR * qpR;
+    const R qr = roqr / ror;
+    const R prr = phigR * pgR + phipR * ppR;
+    const R sstar = (prr - prl + roql * (sl - ql) - roqr * (sr - qr)) / ((rol * (sl - ql) - ror * (sr - qr)) + eps8);
+    const R pgstar = mx2(pgL + rogL * (qgL - sl) * (qgL - sstar), eps6 * mn2(pgL, pgR));
+    const R ppstar = mx2(ppL + ropL * (qpL - sl) * (qpL - sstar), eps6 * mn2(ppL, ppR));
+    const int br = (sl >= R(0)) ? 1 : (sl <= R(0) && sstar > R(0)) ? 2
+                   : (sstar <= R(0) && sr >= R(0)) ? 3 : (sr <= R(0)) ? 4 : 0;
+    o.takeg = o.takep = br != 0;
+    if (br == 1 || br == 2) {
+        R cn[10], fx[10];
+        cn[0] = phigL * rogL; cn[1] = phigL * rogL * ugL; cn[2] = phigL * rogL * vgL;
+        cn[3] = phigL * rogL * wgL; cn[4] = phigL * rogL * egL;
+        cn[5] = phipL * ropL; cn[6] = phipL * ropL * upL; cn[7] = phipL * ropL * vpL;
+        cn[8] = phipL * ropL * wpL; cn[9] = phipL * ropL * epL;
+        fx[0] = phigL * rogL * qgL;
+        fx[1] = phigL * rogL * qgL * ugL + phigL * pgL * enx;
+        fx[2] = phigL * rogL * qgL * vgL + phigL * pgL * eny;
+        fx[3] = phigL * rogL * qgL * wgL + phigL * pgL * enz;
+        fx[4] = phigL * rogL * qgL * hgL;
+        fx[5] = phipL * ropL * qpL;
+        fx[6] = phipL * ropL * qpL * upL + phipL * ppL * enx;
+        fx[7] = phipL * ropL * qpL * vpL + phipL * ppL * eny;
+        fx[8] = phipL * ropL * qpL * wpL + phipL * ppL * enz;
+        fx[9] = phipL * ropL * qpL * hpL;
+        if (br == 1) {
+#pragma unroll
+            for (int k = 0; k < 10; k++) o.F[k] = fx[k] * area;
+        } else {
+            const R dnr = (sstar - sl) + eps6;
+            const R rd = mrcp<F>(dnr, bad);
+            R cs[10];
+            cs[0] = mdiv<F>((qgL - sl) * cn[0], dnr, rd, bad);
+            cs[1] = mdiv<F>((qgL - sl) * cn[1] + phigL * (pgL * enx - pgstar * enx), dnr, rd, bad);
+            cs[2] = mdiv<F>((qgL - sl) * cn[2] + phigL * (pgL * eny - pgstar * eny), dnr, rd, bad);
+            cs[3] = mdiv<F>((qgL - sl) * cn[3] + phigL * (pgL * enz - pgstar * enz), dnr, rd, bad);
+            cs[4] = mdiv<F>((qgL - sl) * cn[4] + phigL * (pgL * qgL - pgstar * sstar), dnr, rd, bad);
+            cs[5] = mdiv<F>((qpL - sl) * cn[5], dnr, rd, bad);
+            cs[6] = mdiv<F>((qpL - sl) * cn[6] + phipL * (ppL * enx - ppstar * enx), dnr, rd, bad);
+            cs[7] = mdiv<F>((qpL - sl) * cn[7] + phipL * (ppL * eny - ppstar * eny), dnr, rd, bad);
+            cs[8] = mdiv<F>((qpL - sl) * cn[8] + phipL * (ppL * enz - ppstar * enz), dnr, rd, bad);
+            cs[9] = mdiv<F>((qpL - sl) * cn[9] + phipL * (ppL * qpL - ppstar * sstar), dnr, rd, bad);
+#pragma unroll
+            for (int k = 0; k < 10; k++) o.F[k] = (fx[k] + sl * (cs[k] - cn[k])) * area;
+        }
+    } else if (br == 4 || br == 3) {
+        R cn[10], fx[10];
+        cn[0] = phigR * rogR; cn[1] = phigR * rogR * ugR; cn[2] = phigR * rogR * vgR;
+        cn[3] = phigR * rogR * wgR; cn[4] = phigR * rogR * egR;
+        cn[5] = phipR * ropR; cn[6] = phipR * ropR * upR; cn[7] = phipR * ropR * vpR;
+        cn[8] = phipR * ropR * wpR; cn[9] = phipR * ropR * epR;
+        fx[0] = phigR * rogR * qgR;
+        fx[1] = phigR * rogR * qgR * ugR + phigR * pgR * enx;
+        fx[2] = phigR * rogR * qgR * vgR + phigR * pgR * eny;
+        fx[3] = phigR * rogR * qgR * wgR + phigR * pgR * enz;
+        fx[4] = phigR * rogR * qgR * hgR;
+        fx[5] = phipR * ropR * qpR;
+        fx[6] = phipR * ropR * qpR * upR + phipR * ppR * enx;
+        fx[7] = phipR * ropR * qpR * vpR + phipR * ppR * eny;
+        fx[8] = phipR * ropR * qpR * wpR + phipR * ppR * enz;
+        fx[9] = phipR * ropR * qpR * hpR;
+        if (br == 4) {
+#pragma unroll
+            for (int k = 0; k < 10; k++) o.F[k] = fx[k] * area;
+        } else {
+            const R dnr = (sstar - sr) + eps6;
+            const R rd = mrcp<F>(dnr, bad);
+            R cs[10];
+            cs[0] = mdiv<F>((qgR - sr) * cn[0], dnr, rd, bad);
+            cs[1] = mdiv<F>((qgR - sr) * cn[1] + phigR * (pgR * enx - pgstar * enx), dnr, rd, bad);
+            cs[2] = mdiv<F>((qgR - sr) * cn[2] + phigR * (pgR * eny - pgstar * eny), dnr, rd, bad);
+            cs[3] = mdiv<F>((qgR - sr) * cn[3] + phigR * (pgR * enz - pgstar * enz), dnr, rd, bad);
+            cs[4] = mdiv<F>((qgR - sr) * cn[4] + phigR * (pgR * qgR - pgstar * sstar), dnr, rd, bad);
+            cs[5] = mdiv<F>((qpR - sr) * cn[5], dnr, rd, bad);
+            cs[6] = mdiv<F>((qpR - sr) * cn[6] + phipR * (ppR * enx - ppstar * enx), dnr, rd, bad);
+            cs[7] = mdiv<F>((qpR - sr) * cn[7] + phipR * (ppR * eny - ppstar * eny), dnr, rd, bad);
+            cs[8] = mdiv<F>((qpR - sr) * cn[8] + phipR * (ppR * enz - ppstar * enz), dnr, rd, bad);
+            cs[9] = mdiv<F>((qpR - sr) * cn[9] + phipR * (ppR * qpR - ppstar * sstar), dnr, rd, bad);
+#pragma unroll
+            for (int k = 0; k < 10; k++) o.F[k] = (fx[k] + sr * (cs[k] - cn[k])) * area;
+        }
+    }
+}
+
 // face-state loads through the read-only data path (1) or plain (0)
 #ifndef HP_FACE_LDG
 #define HP_FACE_LDG 1
@@ -882,7 +985,9 @@ __device__ __forceinline__ void blend_phases_r(const DevParams& P, R& phig, R& p
 #define PLD(p) (*(p))
 #endif
 // F selects the division form (see mdiv); bad collects its out-of-range flag.
-template <int F, class PT>
+// Z selects the Riemann solver: 0 HLLC-Batten (src/sr_hllcbatten.F90:338-529),
+// 1 HLLC-Zien (src/sr_hllczien.F90:348-487).
+template <int F, int Z, class PT>
 __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s, const DevParams& P,
                                           int i, int f, FaceOut& o, unsigned& bad, const PT* pr) {
     const int neigh = ldg(COL(m.nc, f) + i);
@@ -992,6 +1097,12 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     R hpR = epR + mdiv<F>(ppR, ropR, rropR, bad);
     R qpR = upR * enx + vpR * eny + wpR * enz;
     R apR = sqrt(mdiv<F>(gamap * (ppR + pinf), ropR, rropR, bad));
+    if constexpr (Z == 1) {
+        zien_flux<F>(o, bad, area, enx, eny, enz, phigL, phipL, rogL, ropL, ugL, vgL, wgL, upL, vpL, wpL, pgL,
+                     ppL, egL, hgL, qgL, agL, epL, hpL, qpL, apL, phigR, phipR, rogR, ropR, ugR, vgR, wgR, upR,
+                     vpR, wpR, pgR, ppR, egR, hgR, qgR, agR, epR, hpR, qpR, apR);
+        return;
+    }
     R sgl = mn2(mn2(qgL - agL, qgR - agR), eps8);
     R spl = mn2(mn2(qpL - apL, qpR - apR), eps8);
     R sgr = mx2(mx2(qgL + agL, qgR + agR), eps8);
@@ -1122,6 +1233,7 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
 // cell order, whose wave branch was taken -- what the reference's FSTARA
 // variables hold when a NaN state leaves every branch untaken.  Scans
 // backwards from (i, f); falls back to the carry of the previous call.
+template <int Z>
 __device__ __noinline__ void stale_flux(const DevMesh& m, const DevState<R>& s, const DevParams& P,
                                         int i, int f, bool gas, R* out) {
     int cell = i, face = f - 1;
@@ -1134,7 +1246,7 @@ __device__ __noinline__ void stale_flux(const DevMesh& m, const DevState<R>& s, 
         }
         FaceOut o;
         unsigned bad_ = 0;
-        face_eval<0>(m, s, P, cell, face, o, bad_, s.pr);
+        face_eval<0, Z>(m, s, P, cell, face, o, bad_, s.pr);
         if (!o.wall && (gas ? o.takeg : o.takep)) {
             for (int k = 0; k < 5; k++) out[k] = o.F[(gas ? 0 : 5) + k];
             return;
@@ -1146,14 +1258,15 @@ __device__ __noinline__ void stale_flux(const DevMesh& m, const DevState<R>& s, 
 
 // Updates the stale-flux carry with the last taken face of the sweep; one
 // thread, aliased meshes only.
+template <int Z>
 __global__ void k_flux_carry(DevMesh m, DevState<R> s, DevParams P) {
     R tmp[5];
     int last = m.neles - 1;
     while (last >= 0 && ldg(m.iblank + last) != 1) last--;
     if (last < 0) return;
-    stale_flux(m, s, P, last, 4, true, tmp);
+    stale_flux<Z>(m, s, P, last, 4, true, tmp);
     for (int k = 0; k < 5; k++) s.s->fcarry[k] = (double)tmp[k];
-    stale_flux(m, s, P, last, 4, false, tmp);
+    stale_flux<Z>(m, s, P, last, 4, false, tmp);
     for (int k = 0; k < 5; k++) s.s->fcarry[5 + k] = (double)tmp[k];
 }
 
@@ -1161,7 +1274,7 @@ __global__ void k_flux_carry(DevMesh m, DevState<R> s, DevParams P) {
 // RK stage update of src/sr_RK.F90 fused; iblank == 1 cells.
 // FACE: the four face fluxes are gathered from k_faceflux's output (face-
 // based variants) instead of evaluated here.
-template <bool ALIASED, bool FACE = false>
+template <bool ALIASED, bool FACE, int Z>
 __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParams P, int stage) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
@@ -1194,7 +1307,7 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
     for (int f = 0; f < 4 && !FACE; f++) {
         FaceOut o;
         unsigned bad_ = 0;
-        face_eval<0>(m, s, P, i, f, o, bad_, s.pr);
+        face_eval<0, Z>(m, s, P, i, f, o, bad_, s.pr);
         if (o.wall) {
             rhs[1] = rhs[1] + (double)o.w[0]; rhs[2] = rhs[2] + (double)o.w[1];
             rhs[3] = rhs[3] + (double)o.w[2]; rhs[6] = rhs[6] + (double)o.w[3];
@@ -1205,14 +1318,14 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
             for (int k = 0; k < 5; k++) Fg[k] = o.F[k];
             haveg = true;
         } else if (ALIASED && !haveg) {
-            stale_flux(m, s, P, i, f, true, Fg);
+            stale_flux<Z>(m, s, P, i, f, true, Fg);
             haveg = true;
         }
         if (o.takep) {
             for (int k = 0; k < 5; k++) Fp[k] = o.F[5 + k];
             havep = true;
         } else if (ALIASED && !havep) {
-            stale_flux(m, s, P, i, f, false, Fp);
+            stale_flux<Z>(m, s, P, i, f, false, Fp);
             havep = true;
         }
 #pragma unroll
@@ -1457,7 +1570,7 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
 // form (see mdiv).  The fast form returns false, before any store, when a lane
 // of the warp flagged an operand (cn is read and written here, so the stores
 // must wait for that vote).
-template <int F>
+template <int F, int Z>
 __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int stage,
                                            int i, int q, bool active) {
     unsigned bad = 0;
@@ -1467,7 +1580,7 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     int flags;
     {
         FaceOut o;
-        face_eval<F>(m, s, P, i, q, o, bad, s.prr);
+        face_eval<F, Z>(m, s, P, i, q, o, bad, s.prr);
         if (o.wall) {
 #pragma unroll
             for (int k = 0; k < 10; k++) eff[k] = R(0);
@@ -1637,6 +1750,7 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     return true;
 }
 
+template <int Z>
 __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
@@ -1645,9 +1759,9 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevStat
     if (!valid) i = m.neles - 1;
     const bool active = valid && ldg(m.iblank + i) == 1;
     if constexpr (HP_FAST(2)) {
-        if (!flux4_body<1>(m, s, P, stage, i, q, active)) flux4_body<0>(m, s, P, stage, i, q, active);
+        if (!flux4_body<1, Z>(m, s, P, stage, i, q, active)) flux4_body<0, Z>(m, s, P, stage, i, q, active);
     } else {
-        flux4_body<0>(m, s, P, stage, i, q, active);
+        flux4_body<0, Z>(m, s, P, stage, i, q, active);
     }
 }
 
@@ -1655,13 +1769,14 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevStat
 // ghosts): every face is evaluated once, in its owner cell's orientation,
 // instead of once from each side.  Phases with no HLLC branch taken (only
 // with NaN states) contribute zero here.
+template <int Z>
 __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_faceflux(DevMesh m, DevState<R> s, DevParams P) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= m.nface) return;
     const int i = ldg(m.f_i + t), f = ldg(m.f_code + t) & 3;
     FaceOut o{};
     unsigned bad = 0;
-    face_eval<0>(m, s, P, i, f, o, bad, s.prr);
+    face_eval<0, Z>(m, s, P, i, f, o, bad, s.prr);
     R rec[FACE_REC];
     if (o.wall) {
 #pragma unroll
@@ -1919,6 +2034,24 @@ static inline unsigned grid_for(long long n, int block) {
 #define MARK(k) do { if (hook && hook->mark) hook->mark(hook->ctx, (k)); } while (0)
 #define EXCHANGE(p) do { if (hook && hook->exchange) hook->exchange(hook->xctx, (p)); } while (0)
 
+// residual + RK update of one stage with Riemann solver Z (see face_eval)
+template <int Z>
+static void enqueue_flux(const DevMesh& m, const DevState<R>& s, const DevParams& P, cudaStream_t st, int stage,
+                         const StepHook* hook) {
+    const int b = 128;
+    const unsigned gf = grid_for(m.neles, b), g4 = grid_for(4ll * m.neles, 128);
+    if (m.aliased) {
+        k_flux<true, false, Z><<<gf, b, 0, st>>>(m, s, P, stage);
+        MARK(KK_SERIAL);
+        k_flux_carry<Z><<<1, 1, 0, st>>>(m, s, P);
+    } else if (sizeof(R) != sizeof(double) && m.nface > 0) {
+        k_faceflux<Z><<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
+        k_flux<false, true, Z><<<gf, 128, 0, st>>>(m, s, P, stage);
+    } else {
+        k_flux4<Z><<<g4, 128, 0, st>>>(m, s, P, stage);
+    }
+}
+
 static void enqueue_start(const DevMesh& m, const void* stp, const DevParams& P, cudaStream_t st,
                           int block, const StepHook* hook) {
     const DevState<R>& s = *static_cast<const DevState<R>*>(stp);
@@ -1984,16 +2117,8 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             if (m.aliased) { MARK(KK_SERIAL); k_phi_copy_serial<<<1, 1, 0, st>>>(m, s); }
         }
         MARK(KK_FLUX);
-        if (m.aliased) {
-            k_flux<true><<<gf, b, 0, st>>>(m, s, P, stage);
-            MARK(KK_SERIAL);
-            k_flux_carry<<<1, 1, 0, st>>>(m, s, P);
-        } else if (sizeof(R) != sizeof(double) && m.nface > 0) {
-            k_faceflux<<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
-            k_flux<false, true><<<gf, 128, 0, st>>>(m, s, P, stage);
-        } else {
-            k_flux4<<<g4, 128, 0, st>>>(m, s, P, stage);
-        }
+        if (P.myflux == 1) enqueue_flux<1>(m, s, P, st, stage, hook);
+        else enqueue_flux<0>(m, s, P, st, stage, hook);
         if (m.nfringe > 0) {
             MARK(KK_OVERSET);
             k_overset<<<grid_for(m.nfringe, 256), 256, 0, st>>>(m, s);

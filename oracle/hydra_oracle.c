@@ -209,6 +209,7 @@ static void geometry(or_case *S) {
 or_case *or_create(const or_params *p, int32_t nodes, int32_t neles,
                    int32_t nghosts, const double *x, const double *y,
                    const double *z, const int32_t *elem, const int32_t *ghost) {
+    if (p->myflux != 1 && p->myflux != 2) return NULL;   /* mod_Fluxmodule.F90:14-16 stops */
     or_case *S = (or_case *)calloc(1, sizeof(or_case));
     S->p = *p;
     g_nan_mode = p->nan_mode;
@@ -815,8 +816,24 @@ static void face_blend(const or_params *p, double *phig, double *phip, double *u
     }
 }
 
-/* HLLC-Batten face loop, src/sr_hllcbatten.F90:59-556 */
-static void hllc_batten(or_case *S) {
+/* HLLC face loop.  zien = 0: HLLC-Batten, src/sr_hllcbatten.F90:59-556
+ * (wave speeds, contact and branch per phase).  zien = 1: HLLC-Zien,
+ * src/sr_hllczien.F90:62-502: the same reconstruction, blending and wall
+ * terms, then wave speeds over both phases (:348-349), a mixture contact
+ * speed (:351-363), star pressures against it (:365-366) and one branch for
+ * all ten fluxes (:446-487).  The reference does not ship a run of it:
+ * parity for zien = 1 is against this restatement only. */
+static void hllc_zien_face(double *F, double area, double enx, double eny, double enz,
+                           double phigL, double phipL, double rogL, double ropL, double ugL, double vgL,
+                           double wgL, double upL, double vpL, double wpL, double pgL, double ppL,
+                           double egL, double hgL, double qgL, double agL, double epL, double hpL,
+                           double qpL, double apL,
+                           double phigR, double phipR, double rogR, double ropR, double ugR, double vgR,
+                           double wgR, double upR, double vpR, double wpR, double pgR, double ppR,
+                           double egR, double hgR, double qgR, double agR, double epR, double hpR,
+                           double qpR, double apR);
+
+static void hllc_faces(or_case *S, int zien) {
     const or_params *p = &S->p;
     const double eps8 = R4(1.0e-8), eps6 = R4(1.0e-6);
     double rrg = S->rrg, gamag = p->gamag, gamap = p->gamap, pinf = p->pinf, cpp = p->cpp;
@@ -848,7 +865,9 @@ static void hllc_batten(or_case *S) {
                    ropR = S->rop[neigh], upR = S->up[neigh], vpR = S->vp[neigh],
                    wpR = S->wp[neigh], tpR = S->tp[neigh], pgR = S->pg[neigh], ppR = S->pp[neigh];
             (void)rogL; (void)ropL; (void)rogR; (void)ropR;
-            if (p->myorder == 2 && (neigh <= neles || neigh > neles + nghosts)) {
+            /* Zien reconstructs across element faces only (src/sr_hllczien.F90:168);
+             * Batten across partition ghosts too, which this oracle has none of */
+            if (p->myorder == 2 && (neigh <= neles || (!zien && neigh > neles + nghosts))) {
                 double phimin = mn2(S->phi[i], S->phi[neigh]);
                 double xf0 = xf - S->xcel[i], yf0 = yf - S->ycel[i], zf0 = zf - S->zcel[i];
                 double xfn = xf - S->xcel[neigh], yfn = yf - S->ycel[neigh], zfn = zf - S->zcel[neigh];
@@ -896,6 +915,13 @@ static void hllc_batten(or_case *S) {
             double hpR = epR + ppR / ropR;
             double qpR = upR * enx + vpR * eny + wpR * enz;
             double apR = sqrt(gamap * (ppR + pinf) / ropR);
+            if (zien) {
+                hllc_zien_face(F, area, enx, eny, enz, phigL, phipL, rogL, ropL, ugL, vgL, wgL, upL, vpL, wpL,
+                               pgL, ppL, egL, hgL, qgL, agL, epL, hpL, qpL, apL, phigR, phipR, rogR, ropR, ugR,
+                               vgR, wgR, upR, vpR, wpR, pgR, ppR, egR, hgR, qgR, agR, epR, hpR, qpR, apR);
+                for (int k = 1; k <= 10; k++) RHS(i, k) = RHS(i, k) + F[k - 1];
+                continue;
+            }
             double sgl = mn3(qgL - agL, qgR - agR, eps8);
             double spl = mn3(qpL - apL, qpR - apR, eps8);
             double sgr = mx3(qgL + agL, qgR + agR, eps8);
@@ -984,6 +1010,97 @@ static void hllc_batten(or_case *S) {
     }
 }
 
+/* One HLLC-Zien face, src/sr_hllczien.F90:348-487.  F keeps its previous
+ * values when no branch is taken (NaN states), as the reference's FSTARA
+ * variables do. */
+static void hllc_zien_face(double *F, double area, double enx, double eny, double enz,
+                           double phigL, double phipL, double rogL, double ropL, double ugL, double vgL,
+                           double wgL, double upL, double vpL, double wpL, double pgL, double ppL,
+                           double egL, double hgL, double qgL, double agL, double epL, double hpL,
+                           double qpL, double apL,
+                           double phigR, double phipR, double rogR, double ropR, double ugR, double vgR,
+                           double wgR, double upR, double vpR, double wpR, double pgR, double ppR,
+                           double egR, double hgR, double qgR, double agR, double epR, double hpR,
+                           double qpR, double apR) {
+    const double eps8 = R4(1.0e-8), eps6 = R4(1.0e-6);
+    /* DMIN1/DMAX1 of five arguments, left to right */
+    double sl = mn2(mn2(mn2(mn2(qgL - agL, qpL - apL), qgR - agR), qpR - apR), eps8);
+    double sr = mx2(mx2(mx2(mx2(qgL + agL, qpL + apL), qgR + agR), qpR + apR), eps8);
+    double rol = phigL * rogL + phipL * ropL;
+    double roql = phigL * rogL * qgL + phipL * ropL * qpL;
+    double ql = roql / rol;
+    double prl = phigL * pgL + phipL * ppL;
+    double ror = phigR * rogR + phipR * ropR;
+    double roqr = phigR * rogR * qgR + phipR * ropR * qpR;
+    double qr = roqr / ror;
+    double prr = phigR * pgR + phipR * ppR;
+    double snr = prr - prl + roql * (sl - ql) - roqr * (sr - qr);
+    double sdr = rol * (sl - ql) - ror * (sr - qr);
+    double sstar = snr / (sdr + eps8);
+    double pgstar = mx2(pgL + rogL * (qgL - sl) * (qgL - sstar), eps6 * mn2(pgL, pgR));
+    double ppstar = mx2(ppL + ropL * (qpL - sl) * (qpL - sstar), eps6 * mn2(ppL, ppR));
+    double cnl[10], cnr[10], csl[10], csr[10], fl[10], fr[10];
+    cnl[0] = phigL * rogL; cnl[1] = phigL * rogL * ugL; cnl[2] = phigL * rogL * vgL;
+    cnl[3] = phigL * rogL * wgL; cnl[4] = phigL * rogL * egL;
+    cnl[5] = phipL * ropL; cnl[6] = phipL * ropL * upL; cnl[7] = phipL * ropL * vpL;
+    cnl[8] = phipL * ropL * wpL; cnl[9] = phipL * ropL * epL;
+    cnr[0] = phigR * rogR; cnr[1] = phigR * rogR * ugR; cnr[2] = phigR * rogR * vgR;
+    cnr[3] = phigR * rogR * wgR; cnr[4] = phigR * rogR * egR;
+    cnr[5] = phipR * ropR; cnr[6] = phipR * ropR * upR; cnr[7] = phipR * ropR * vpR;
+    cnr[8] = phipR * ropR * wpR; cnr[9] = phipR * ropR * epR;
+    double dnr = (sstar - sl) + eps6;
+    csl[0] = (qgL - sl) * cnl[0] / dnr;
+    csl[1] = ((qgL - sl) * cnl[1] + phigL * (pgL * enx - pgstar * enx)) / dnr;
+    csl[2] = ((qgL - sl) * cnl[2] + phigL * (pgL * eny - pgstar * eny)) / dnr;
+    csl[3] = ((qgL - sl) * cnl[3] + phigL * (pgL * enz - pgstar * enz)) / dnr;
+    csl[4] = ((qgL - sl) * cnl[4] + phigL * (pgL * qgL - pgstar * sstar)) / dnr;
+    csl[5] = (qpL - sl) * cnl[5] / dnr;
+    csl[6] = ((qpL - sl) * cnl[6] + phipL * (ppL * enx - ppstar * enx)) / dnr;
+    csl[7] = ((qpL - sl) * cnl[7] + phipL * (ppL * eny - ppstar * eny)) / dnr;
+    csl[8] = ((qpL - sl) * cnl[8] + phipL * (ppL * enz - ppstar * enz)) / dnr;
+    csl[9] = ((qpL - sl) * cnl[9] + phipL * (ppL * qpL - ppstar * sstar)) / dnr;
+    dnr = (sstar - sr) + eps6;
+    csr[0] = (qgR - sr) * cnr[0] / dnr;
+    csr[1] = ((qgR - sr) * cnr[1] + phigR * (pgR * enx - pgstar * enx)) / dnr;
+    csr[2] = ((qgR - sr) * cnr[2] + phigR * (pgR * eny - pgstar * eny)) / dnr;
+    csr[3] = ((qgR - sr) * cnr[3] + phigR * (pgR * enz - pgstar * enz)) / dnr;
+    csr[4] = ((qgR - sr) * cnr[4] + phigR * (pgR * qgR - pgstar * sstar)) / dnr;
+    csr[5] = (qpR - sr) * cnr[5] / dnr;
+    csr[6] = ((qpR - sr) * cnr[6] + phipR * (ppR * enx - ppstar * enx)) / dnr;
+    csr[7] = ((qpR - sr) * cnr[7] + phipR * (ppR * eny - ppstar * eny)) / dnr;
+    csr[8] = ((qpR - sr) * cnr[8] + phipR * (ppR * enz - ppstar * enz)) / dnr;
+    csr[9] = ((qpR - sr) * cnr[9] + phipR * (ppR * qpR - ppstar * sstar)) / dnr;
+    fl[0] = phigL * rogL * qgL;
+    fl[1] = phigL * rogL * qgL * ugL + phigL * pgL * enx;
+    fl[2] = phigL * rogL * qgL * vgL + phigL * pgL * eny;
+    fl[3] = phigL * rogL * qgL * wgL + phigL * pgL * enz;
+    fl[4] = phigL * rogL * qgL * hgL;
+    fl[5] = phipL * ropL * qpL;
+    fl[6] = phipL * ropL * qpL * upL + phipL * ppL * enx;
+    fl[7] = phipL * ropL * qpL * vpL + phipL * ppL * eny;
+    fl[8] = phipL * ropL * qpL * wpL + phipL * ppL * enz;
+    fl[9] = phipL * ropL * qpL * hpL;
+    fr[0] = phigR * rogR * qgR;
+    fr[1] = phigR * rogR * qgR * ugR + phigR * pgR * enx;
+    fr[2] = phigR * rogR * qgR * vgR + phigR * pgR * eny;
+    fr[3] = phigR * rogR * qgR * wgR + phigR * pgR * enz;
+    fr[4] = phigR * rogR * qgR * hgR;
+    fr[5] = phipR * ropR * qpR;
+    fr[6] = phipR * ropR * qpR * upR + phipR * ppR * enx;
+    fr[7] = phipR * ropR * qpR * vpR + phipR * ppR * eny;
+    fr[8] = phipR * ropR * qpR * wpR + phipR * ppR * enz;
+    fr[9] = phipR * ropR * qpR * hpR;
+    if (sl >= 0.0) {
+        for (int k = 0; k < 10; k++) F[k] = fl[k] * area;
+    } else if (sl <= 0.0 && sstar > 0.0) {
+        for (int k = 0; k < 10; k++) F[k] = (fl[k] + sl * (csl[k] - cnl[k])) * area;
+    } else if (sstar <= 0.0 && sr >= 0.0) {
+        for (int k = 0; k < 10; k++) F[k] = (fr[k] + sr * (csr[k] - cnr[k])) * area;
+    } else if (sr <= 0.0) {
+        for (int k = 0; k < 10; k++) F[k] = fr[k] * area;
+    }
+}
+
 /* Interphase sources, src/sr_source.F90:42-178 */
 static void source(or_case *S) {
     const or_params *p = &S->p;
@@ -1043,10 +1160,13 @@ static void source(or_case *S) {
     }
 }
 
-void or_flux(or_case *S) {               /* src/sr_hllcbatten.F90:29-560 */
+/* CallFluxSolver, src/mod_Fluxmodule.F90:7-21: myflux 1 = HLLC-Zien
+ * (src/sr_hllczien.F90:29-506), 2 = HLLC-Batten (src/sr_hllcbatten.F90:
+ * 29-560); or_create rejects any other value */
+void or_flux(or_case *S) {
     or_primitiveplusbc(S);
     if (S->p.myorder == 2) { or_derivative(S); or_venkat(S); }
-    hllc_batten(S);
+    hllc_faces(S, S->p.myflux == 1);
     source(S);
 }
 

@@ -8,6 +8,10 @@ Config 1 (shock-bubble, 20^3 hexes split into 6 tets):
     interface go NaN in the first step.  A contrast of 1e-3 stays finite;
   * the CFL alone does it too: at air fraction 0.1 / 0.9, CFL 0.4 gives NaN
     cells at step 7 (the shock front).
+Config 5 (precision stress, 5e9 Pa water shock on a 5 x 5 air-bubble
+lattice): air bubbles at a contrast of 1e-6 (or 1e-4) give NaN cells in the
+first step on a reduced 20 x 20 x 30-hex box; a contrast of 1e-3 stays
+finite.
 Config 2 (viscous cylinder): with the reference's convective time step
 (src/main.F90:541-555) the first cell layer at the no-slip wall goes NaN at
 CFL 0.5.  A reduced O-grid of the same wall spacing (40 x 64 x 4 hexes,
@@ -83,6 +87,22 @@ def test_config1_cfl_04_fails_at_step_7():
     orc = _oracle(spec, threads=os.cpu_count() or 1)
     assert spec.flow["cfl"] == 0.4
     assert _first_nan_step(orc, spec.mesh.neles, 10) == 7
+    orc.close()
+
+
+@pytest.mark.parametrize("alpha_min", [1e-6, 1e-4])
+def test_config5_contrast_fails_in_first_step(alpha_min):
+    spec = cases.shock_lattice(nx=20, ny=20, nz=30, alpha_min=alpha_min)
+    orc = _oracle(spec, threads=os.cpu_count() or 1)
+    orc.run(1)
+    assert _nan_cells(orc, spec.mesh.neles).any()
+    orc.close()
+
+
+def test_config5_contrast_1e3_stays_finite():
+    spec = cases.shock_lattice(nx=20, ny=20, nz=30, alpha_min=1e-3)
+    orc = _oracle(spec, threads=os.cpu_count() or 1)
+    assert _first_nan_step(orc, spec.mesh.neles, 20) is None
     orc.close()
 
 

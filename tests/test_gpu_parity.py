@@ -77,6 +77,32 @@ def test_fp64_parity_bit_exact(name, renumber):
     np.testing.assert_array_equal(gp_g, gp_o)
 
 
+@pytest.mark.parametrize("name", ["shock_bubble_ref", "cylinder", "aliased_ghosts"])
+def test_zien_fp64_parity_bit_exact(name):
+    """HLLC-Zien (myflux = 1, src/sr_hllczien.F90): common wave speeds over
+    both phases and one branch for all ten fluxes.  The reference ships no
+    run of it, so the oracle's restatement is the reference here."""
+    spec = SPECS[name]()
+    n = 3
+    t, v, d, cu_o, gp_o = _oracle_run(spec, n, myflux=1)
+    dg, tg, cu_g, gp_g = _gpu_run(spec, n, PREC_FP64_PARITY, myflux=1)
+    np.testing.assert_array_equal(dg["time"], t)
+    np.testing.assert_array_equal(dg["velmag"], v)
+    np.testing.assert_array_equal(cu_g, cu_o)
+    np.testing.assert_array_equal(gp_g, gp_o)
+    _, _, _, cu_b, _ = _oracle_run(spec, n)
+    assert not np.array_equal(cu_o, cu_b)       # a different solver, not Batten again
+
+
+@pytest.mark.parametrize("face_mode", [0, 1])
+def test_zien_mixed_within_tolerance(face_mode):
+    spec = SPECS["cylinder"]()
+    _, _, _, cu_o, _ = _oracle_run(spec, 5, myflux=1)
+    _, _, cu_g, _ = _gpu_run(spec, 5, PREC_MIXED, myflux=1, face_mode=face_mode)
+    rho_o, rho_g = cu_o[0] + cu_o[5], cu_g[0] + cu_g[5]
+    assert np.linalg.norm(rho_g - rho_o) / np.linalg.norm(rho_o) < 1e-5
+
+
 def test_fp64_fma_within_1e10():
     """FMA contraction changes roundings at the 1e-16 level.  The air-phase
     variables (1-5) stay within 1e-10; the trace water phase (alpha_w =

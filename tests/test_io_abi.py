@@ -159,6 +159,9 @@ def test_create_rejects_bad_meshes():
     with pytest.raises(HydraError) as e:
         Case(m, spec.params(myflux=3))           # Jameson flux is not in this build
     assert e.value.code == HP_E_UNSUPPORTED
+    with pytest.raises(HydraError) as e:
+        Case(m, spec.params(myflux=4))           # no such flux (the reference stops)
+    assert e.value.code == HP_E_ARG and "myflux" in str(e.value)
 
 
 def test_partition_ghosts_unsupported():
