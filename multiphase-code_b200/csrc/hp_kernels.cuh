@@ -91,6 +91,11 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 #ifndef HP_FACE_VISC
 #define HP_FACE_VISC 1
 #endif
+// viscous fluxes of the cell-centric variants with eight lanes per cell (one
+// phase each, k_visc8) instead of four (k_visc4)
+#ifndef HP_VISC_SPLIT
+#define HP_VISC_SPLIT 1
+#endif
 // kernels that take the fast form when HP_DIV_FAST is set: 1 gradients,
 // 2 fluxes, 4 viscous fluxes, 8 JST smoothing
 #ifndef HP_FAST_MASK
@@ -1887,6 +1892,88 @@ __device__ __forceinline__ void visc_face(const DevMesh& m, const DevState<R>& s
     c[7] = (double)(phipf * (qxxp * scx + qyyp * scy + qzzp * scz));
 }
 
+// One phase of visc_face: the four contributions c[0..3] of phase ph
+// (0 gas: visug, visvg, viswg, vistg; 1 liquid: visup..vistp) of face f of
+// cell i, every value formed by the same operations in the same order as in
+// visc_face.  The stencil loop runs over the points outermost, so the point
+// offsets are not kept across the fields: every sum still adds its terms in
+// point order 1..nm, starting from the first term.
+#ifndef HP_VISC8_MINB
+#define HP_VISC8_MINB 5
+#endif
+template <int F, class PT>
+__device__ __forceinline__ void visc_face_ph(const DevMesh& m, const DevState<R>& s, const DevParams& P,
+                                             int i, int f, const int nci[4], int ph, double c[4], unsigned& bad,
+                                             const PT* pr) {
+    const int c0 = ph ? P_UP : P_UG;          // u, v, w, T columns of the phase: c0 .. c0 + 3
+    const R c23 = (R)P.c23;
+    const R scx = (R)ldg(COL(m.sc, 3 * f) + i), scy = (R)ldg(COL(m.sc, 3 * f + 1) + i),
+            scz = (R)ldg(COL(m.sc, 3 * f + 2) + i);
+    const double xf = ldg(COL(m.fcv, f) + i), yf = ldg(COL(m.fcv, 4 + f) + i),
+                 zf = ldg(COL(m.fcv, 8 + f) + i);
+    const int neigh = nci[f];
+    R ff[4];
+#pragma unroll
+    for (int v = 0; v < 4; v++) ff[v] = (R)((COL(pr, c0 + v)[i] + COL(pr, c0 + v)[neigh]) * 0.5);
+    const R phif = (R)((COL(pr, P_PHIG + ph)[i] + COL(pr, P_PHIG + ph)[neigh]) * 0.5);
+    R amu, ak;
+    if (ph == 0) {
+        const R tgf = ff[3];
+        amu = (R)P.as * sqrt(tgf) / (R(1) + (R)P.ts / tgf);
+        ak = mdiv<F>(amu * (R)P.cpg, (R)P.prg, (R)P.r_prg, bad);
+    } else {
+        amu = (R)P.amup;
+        ak = mdiv<F>(amu * (R)P.cpp, (R)P.prp, (R)P.r_prp, bad);
+    }
+    const bool bnd = neigh >= m.neles;        // 5-point stencil: the cell's 4 neighbours and the cell
+    R a11, a22, a33, a12, a13, a23, b[4][3];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        if (k >= 5 && bnd) break;
+        const int mk = k < 4 ? nci[k] : (bnd ? i : ldg(COL(m.nc, k - 4) + neigh));
+        const R dx = (R)(ldg(m.xc + mk) - xf), dy = (R)(ldg(m.yc + mk) - yf), dz = (R)(ldg(m.zc + mk) - zf);
+        if (k == 0) {
+            a11 = dx * dx; a22 = dy * dy; a33 = dz * dz; a12 = dx * dy; a13 = dx * dz; a23 = dy * dz;
+        } else {
+            a11 = a11 + dx * dx; a22 = a22 + dy * dy; a33 = a33 + dz * dz;
+            a12 = a12 + dx * dy; a13 = a13 + dx * dz; a23 = a23 + dy * dz;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const R d = (R)COL(pr, c0 + v)[mk] - ff[v];
+            if (k == 0) {
+                b[v][0] = d * dx; b[v][1] = d * dy; b[v][2] = d * dz;
+            } else {
+                b[v][0] = b[v][0] + d * dx; b[v][1] = b[v][1] + d * dy; b[v][2] = b[v][2] + d * dz;
+            }
+        }
+    }
+    const R dnr = det3(a11, a12, a13, a12, a22, a23, a13, a23, a33);
+    const R rdnr = mrcp<F>(dnr, bad);
+    R gr[4][3];
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        gr[v][0] = mdiv<F>(det3(b[v][0], b[v][1], b[v][2], a12, a22, a23, a13, a23, a33), dnr, rdnr, bad);
+        gr[v][1] = mdiv<F>(det3(a11, a12, a13, b[v][0], b[v][1], b[v][2], a13, a23, a33), dnr, rdnr, bad);
+        gr[v][2] = mdiv<F>(det3(a11, a12, a13, a12, a22, a23, b[v][0], b[v][1], b[v][2]), dnr, rdnr, bad);
+    }
+    const R uf = ff[0], vf = ff[1], wf = ff[2];
+    R delv = gr[0][0] + gr[1][1] + gr[2][2];
+    R txx = amu * (R(2) * gr[0][0] - c23 * delv);
+    R tyy = amu * (R(2) * gr[1][1] - c23 * delv);
+    R tzz = amu * (R(2) * gr[2][2] - c23 * delv);
+    R txy = amu * (gr[1][0] + gr[0][1]);
+    R txz = amu * (gr[2][0] + gr[0][2]);
+    R tyz = amu * (gr[1][2] + gr[2][1]);
+    R qxx = uf * txx + vf * txy + wf * txz + ak * gr[3][0];
+    R qyy = uf * txy + vf * tyy + wf * tyz + ak * gr[3][1];
+    R qzz = uf * txz + vf * tyz + wf * tzz + ak * gr[3][2];
+    c[0] = (double)(phif * (txx * scx + txy * scy + txz * scz));
+    c[1] = (double)(phif * (txy * scx + tyy * scy + tyz * scz));
+    c[2] = (double)(phif * (txz * scx + tyz * scy + tzz * scz));
+    c[3] = (double)(phif * (qxx * scx + qyy * scy + qzz * scz));
+}
+
 // one thread per cell (aliased meshes)
 __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParams P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1945,6 +2032,39 @@ __global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevStat
             COL(s.vis, q)[i] = acc[q];
             COL(s.vis, q + 4)[i] = acc[q + 4];
         }
+        if (!__any_sync(0xffffffffu, bad)) break;
+    }
+}
+
+// Eight lanes per cell: each warp takes one phase of 8 cells (warps 2w and
+// 2w+1 the gas and the liquid of the same cells), lane q of a cell face q.
+// The per-cell sums over faces 1..4 are assembled with shuffles as in
+// k_visc4, so vis is identical to k_visc4's.  Splitting the phases halves
+// each lane's live state, which raises the resident warps.
+__global__ void __launch_bounds__(128, HP_VISC8_MINB) k_visc8(DevMesh m, DevState<R> s, DevParams P) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (int)(gt & 3);
+    const int ph = (int)((gt >> 5) & 1);
+    int i = (int)(((gt >> 6) << 3) + ((gt & 31) >> 2));
+    const bool valid = i < m.neles;
+    if (!valid) i = m.neles - 1;
+    const bool active = valid && ldg(m.iblank + i) == 1;
+    int nci[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) nci[f] = ldg(COL(m.nc, f) + i);
+    for (int pass = HP_FAST(4) ? 1 : 0; pass >= 0; pass--) {
+        double c[4];
+        unsigned bad = 0;
+        if (pass) visc_face_ph<1>(m, s, P, i, q, nci, ph, c, bad, s.prr);
+        else visc_face_ph<0>(m, s, P, i, q, nci, ph, c, bad, s.prr);
+        double acc[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) acc[k] = 0.0;
+#pragma unroll
+        for (int f = 0; f < 4; f++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) acc[k] = acc[k] + qshfl(c[k], f);
+        if (active) COL(s.vis, 4 * ph + q)[i] = acc[q];
         if (!__any_sync(0xffffffffu, bad)) break;
     }
 }
@@ -2096,6 +2216,8 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
         } else if (sizeof(R) != sizeof(double) && HP_FACE_VISC && m.nface > 0) {
             k_facevisc<<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
             k_vis_gather<<<grid_for(m.neles, 256), 256, 0, st>>>(m, s);
+        } else if (HP_VISC_SPLIT) {
+            k_visc8<<<grid_for(8ll * m.neles, 128), 128, 0, st>>>(m, s, P);
         } else {
             k_visc4<<<g4, 128, 0, st>>>(m, s, P);
         }
