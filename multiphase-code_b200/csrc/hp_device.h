@@ -56,6 +56,9 @@ struct DevMesh {
     const unsigned* fk;     // [ld] face kind nibbles
     const int* iblank;      // [ld]
     const double *xc, *yc, *zc, *vol, *dl, *dd;   // [ld]
+    // limiter epsilon^2 = (K dl)^3 per cell (src/sr_VK.F90:34), evaluated
+    // once at set-up with the host's pow, as the reference evaluates it
+    const double* eps2;     // [ld]
     const double* sc;       // [12][ld] face area vectors sc1x..sc4z
     const double* fch;      // [12][ld] face centroids, 0.3333 factor (HLLC, VK)
     const double* fcv;      // [12][ld] face centroids, /3 (viscous)

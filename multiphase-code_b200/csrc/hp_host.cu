@@ -179,6 +179,7 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     m.fk = (unsigned*)a.take(ld * sizeof(unsigned)); m.iblank = (int*)a.take(ld * I);
     m.xc = (double*)a.take(ld * D); m.yc = (double*)a.take(ld * D); m.zc = (double*)a.take(ld * D);
     m.vol = (double*)a.take(ld * D); m.dl = (double*)a.take(ld * D); m.dd = (double*)a.take(ld * D);
+    m.eps2 = (double*)a.take(ld * D);
     m.sc = (double*)a.take(12 * ld * D); m.fch = (double*)a.take(12 * ld * D);
     m.fcv = (double*)a.take(12 * ld * D);
     m.lsqa = (double*)a.take(11 * ld * D);
@@ -222,11 +223,11 @@ struct Layout {
     long long ld = 0;
     std::vector<int> nc, snb, ib, gpar, gid, gtyp, perm, ghost_id;
     std::vector<unsigned> fk;
-    std::vector<double> x, y, z, vol, dl, dd, sc, fch, fcv, la, lb;
+    std::vector<double> x, y, z, vol, dl, dd, eps2, sc, fch, fcv, la, lb;
     Layout(int ne, int ng) : neles(ne), nghosts(ng), ld(((long long)ne + ng + 63) / 64 * 64) {
         nc.assign(4 * ld, 0); snb.assign(4 * ld, 0); ib.assign(ld, 0); fk.assign(ld, 0u);
         gpar.assign(ng, 0); gid.assign(ng, 0); gtyp.assign(ng, 0); perm.assign(ne, 0); ghost_id.assign(ng, 0);
-        for (auto* v : {&x, &y, &z, &vol, &dl, &dd}) v->assign(ld, 0.0);
+        for (auto* v : {&x, &y, &z, &vol, &dl, &dd, &eps2}) v->assign(ld, 0.0);
         for (auto* v : {&sc, &fch, &fcv}) v->assign(12 * ld, 0.0);
         la.assign(11 * ld, 0.0); lb.assign(11 * ld, 0.0);
     }
@@ -673,7 +674,12 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     if (e == cudaSuccess) e = up(m.yc, L.y.data(), ld * D);
     if (e == cudaSuccess) e = up(m.zc, L.z.data(), ld * D);
     if (e == cudaSuccess) e = up(m.vol, L.vol.data(), ld * D);
+    // the limiter's (K dl)^3 with the host's pow (src/sr_VK.F90:34): a
+    // device cube rounds differently from pow in rare near-tie cases
+#pragma omp parallel for schedule(static)
+    for (long long t = 0; t < ld; t++) L.eps2[t] = std::pow(P.venkat_k * L.dl[t], 3.0);
     if (e == cudaSuccess) e = up(m.dl, L.dl.data(), ld * D);
+    if (e == cudaSuccess) e = up(m.eps2, L.eps2.data(), ld * D);
     if (e == cudaSuccess) e = up(m.dd, L.dd.data(), ld * D);
     if (e == cudaSuccess) e = up(m.sc, L.sc.data(), 12 * ld * D);
     if (e == cudaSuccess) e = up(m.fch, L.fch.data(), 12 * ld * D);

@@ -40,18 +40,6 @@ __device__ __forceinline__ T fvenkat(T delp, T delm, T epssq) {
             (delp * delp + T(2) * delm * delm + delp * delm + epssq)) / delm;
 }
 
-// (K dl)^3 rounded once: Dekker's exact product splits a*a and (a*a)*a into
-// head + tail with fma, then one final rounding of the sum.  Matches a
-// correctly rounded pow(a, 3) except in near-tie cases.
-__device__ __forceinline__ double cube_rn(double a) {
-    double p = a * a;
-    double pe = fma(a, a, -p);
-    double h = p * a;
-    double he = fma(p, a, -h);
-    return h + (he + pe * a);
-}
-__device__ __forceinline__ float cube_rn(float a) { return (float)cube_rn((double)a); }
-
 template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 
 // Minimum resident 128-thread blocks per SM of the 4-lanes-per-cell kernels
@@ -808,7 +796,7 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParam
         COL(s.gr, 3 * v + 2)[i] = gv[v][2];
     }
     // limiter: phi_i = min over {pg, pp, rog, rop} x 4 faces
-    const R epssq = (R)cube_rn((double)(P.venkat_k * ldg(m.dl + i)));
+    const R epssq = (R)ldg(m.eps2 + i);
     R fx[4], fy[4], fz[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) {
@@ -1528,7 +1516,7 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
     R fx0 = qshfl(sg[0], src), fy0 = qshfl(sg[1], src), fz0 = qshfl(sg[2], src);
     if (q >= 2) { lg[0] = fx0; lg[1] = fy0; lg[2] = fz0; }
     const int lcol = q == 0 ? P_PG : q == 1 ? P_PP : q == 2 ? P_ROG : P_ROP;
-    const R epssq = (R)cube_rn((double)(P.venkat_k * ldg(m.dl + i)));
+    const R epssq = (R)ldg(m.eps2 + i);
     const R* qq = COL(s.prr, lcol);
     R qi = qq[i];
     R vmax = mx2(mx2(mx2(mx2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
