@@ -80,6 +80,14 @@ typedef struct hp_params {
                                 [64, 512]; hydraphase.tune picks it */
     int32_t use_graph;       /* 1: capture each step in a CUDA graph */
     double pad_[4];
+    /* --- five-phase model (the reference's FIVE_PHASE build): three
+     * dispersed, incompressible phases q, r, s with mass and momentum each,
+     * so 22 conserved variables (src/main.F90:114-124); flow.in groups
+     * 19-21 (src/sr_Read_flow.F90:214-250), read when present --------- */
+    int32_t five_phase;      /* 1: 22 conserved variables (cu(1:22)) */
+    double rhoq, rhor, rhos; /* dispersed-phase densities */
+    double radq, radr, rads; /* particle radii */
+    double phiginit, phipinit, phiqinit, phirinit, phisinit;  /* start fractions */
 } hp_params;
 
 /* Mesh as the reference reads it (src/sr_geometry.F90:101-139):

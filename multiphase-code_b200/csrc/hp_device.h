@@ -39,6 +39,9 @@ struct DevParams {
     double r_emm, r_gm1, r_gamap, r_prg, r_prp;
     int rk_scheme, inviscid, myorder, nstage;
     int myflux;   // 1 HLLC-Zien, 2 HLLC-Batten (src/mod_Fluxmodule.F90:8-11)
+    // five-phase model: dispersed phases q, r, s (conserved columns 10-21)
+    int five_phase;
+    double rhod[3], radd[3], vold[3];   // densities, radii, particle volumes
 };
 
 // A handle holds one case or a batch of cases whose meshes are concatenated:
@@ -120,6 +123,11 @@ struct DevState {
     double *anu, *d2q;       // [2][ld], [10][ld]
     double *d24, *vis;       // [10][ld], [8][ld]
     double* egt;             // [2][ld] ghost egtotal/eptotal (aliased meshes)
+    // five-phase model only (null otherwise): cn, cu, cn1, d2q and d24 then
+    // hold 22 columns
+    double* qpr;             // [12][ld] phi, u, v, w of q, r, s
+    double* anuq;            // [3][ld] their JST switches
+    double* qdrag;           // [9][ld] drag of q, r, s on the liquid (x, y, z)
     R* ff;                   // [nface][FACE_REC] face records (face-based
                              // variants): 10 flux components, the wall flag
                              // (1: pressure terms only), one pad
@@ -132,7 +140,7 @@ struct DevState {
 enum KernelKind {
     KK_PRIM_START = 0, KK_STEP_BEGIN, KK_SMOOTH1, KK_SMOOTH2, KK_BC_VISC, KK_VISC,
     KK_PRIM_STAGE, KK_BC, KK_GRAD, KK_FLUX, KK_PRIM_END, KK_STEP_END, KK_SERIAL,
-    KK_OVERSET, KK_HALO, KK_COUNT
+    KK_OVERSET, KK_HALO, KK_QRS, KK_COUNT
 };
 
 // Optional hook called before every launch (and with KK_COUNT after the

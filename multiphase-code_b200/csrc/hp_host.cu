@@ -102,6 +102,7 @@ struct hp_handle {
     bool started = false, have_state = false;
     std::vector<char> state_set;   // per case: state uploaded
     int aliased = 0;
+    int neq = 10;               // conserved variables: 10, or 22 with the five-phase model
     int max_diag = 4096;
     std::string err;
     double* h_diag = nullptr;   // pinned
@@ -187,14 +188,21 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     m.g_par = (int*)a.take((nghosts + 1) * (size_t)I); m.g_id = (int*)a.take((nghosts + 1) * (size_t)I);
     m.g_type = (int*)a.take((nghosts + 1) * (size_t)I);
     DevState<double>& s = h->ds;
-    s.cn = (double*)a.take(10 * ld * D); s.cu = (double*)a.take(10 * ld * D);
-    s.cn1 = (double*)a.take(10 * ld * D); s.pr = (double*)a.take(NPR * ld * D);
+    const long long nq = h->neq;
+    s.cn = (double*)a.take(nq * ld * D); s.cu = (double*)a.take(nq * ld * D);
+    s.cn1 = (double*)a.take(nq * ld * D); s.pr = (double*)a.take(NPR * ld * D);
     // primitives in the arithmetic of the gradients and fluxes: a float copy
     // for the FP32-arithmetic variants, the FP64 columns themselves otherwise
     s.prr = gb == D ? s.pr : (double*)a.take(NPR * ld * gb);
     s.gr = (double*)a.take(NGR * ld * gb); s.phi = (double*)a.take(ld * D);
-    s.anu = (double*)a.take(2 * ld * D); s.d2q = (double*)a.take(10 * ld * D);
-    s.d24 = (double*)a.take(10 * ld * D); s.vis = (double*)a.take(8 * ld * D);
+    s.anu = (double*)a.take(2 * ld * D); s.d2q = (double*)a.take(nq * ld * D);
+    s.d24 = (double*)a.take(nq * ld * D); s.vis = (double*)a.take(8 * ld * D);
+    if (h->neq == 22) {
+        s.qpr = (double*)a.take(12 * ld * D); s.anuq = (double*)a.take(3 * ld * D);
+        s.qdrag = (double*)a.take(9 * ld * D);
+    } else {
+        s.qpr = s.anuq = s.qdrag = nullptr;
+    }
     s.egt = (double*)a.take(2 * ld * D);
     s.s = (DevScalars*)a.take(ncase * sizeof(DevScalars));
     s.diag = (double*)a.take((size_t)ncase * h->max_diag * 8 * D);
@@ -508,6 +516,13 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
         return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
     if (params->block_size != 0 && (params->block_size < 64 || params->block_size > 512 || params->block_size % 32))
         return fail(nullptr, HP_E_ARG, "block_size must be 0 or a multiple of 32 in [64, 512]");
+    if (params->five_phase) {
+        if (!(params->rhoq > 0 && params->rhor > 0 && params->rhos > 0 && params->radq > 0 && params->radr > 0 &&
+              params->rads > 0))
+            return fail(nullptr, HP_E_ARG, "five-phase model: rhoq, rhor, rhos, radq, radr, rads must be positive");
+        if (params->precision == HP_PREC_FP32)
+            return fail(nullptr, HP_E_UNSUPPORTED, "five-phase model: not in the all-FP32 variant");
+    }
     long long etot = 0, gtot = 0;
     for (int c = 0; c < ncase; c++) {
         const hp_mesh* mesh = meshes + c;
@@ -567,6 +582,17 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     P.fsd = 4.0 * p.surfacetension / p.diap;
     P.cfl = p.cfl; P.venkat_k = p.venkat_k > 0 ? p.venkat_k : 0.3; P.twall = p.twall; P.amup = 0.001;
     P.rk_scheme = p.rk_scheme; P.inviscid = p.inviscid; P.myorder = p.myorder; P.myflux = p.myflux;
+    P.five_phase = p.five_phase ? 1 : 0;
+    if (P.five_phase) {
+        if (h->aliased) { delete h; return fail(nullptr, HP_E_UNSUPPORTED, "five-phase model: aliased ghost ids"); }
+        const double rho[3] = {p.rhoq, p.rhor, p.rhos}, rad[3] = {p.radq, p.radr, p.rads};
+        for (int d = 0; d < 3; d++) {   // src/main.F90:352-354
+            P.rhod[d] = rho[d];
+            P.radd[d] = rad[d];
+            P.vold[d] = (4.0 / 3.0) * 3.1415926 * (rad[d] * rad[d] * rad[d]);
+        }
+        h->neq = 22;
+    }
     P.r_emm = 1.0 / (P.emax - P.emin);
     P.r_gm1 = 1.0 / (P.gamag - 1.0);
     P.r_gamap = 1.0 / P.gamap;
@@ -837,11 +863,13 @@ static int upload_state(hp_handle* h, int c, double time, const double* cu_elem,
     const int ne = cr.ne, ng = cr.ng, gs = h->neles + cr.g0;
     cudaStream_t st = h->stream;
     CUDA_OK(h, cudaStreamSynchronize(st));
-    CUDA_OK(h, cudaMemcpyAsync(h->ds.cn1, cu_elem, 10 * (size_t)ne * sizeof(double), cudaMemcpyHostToDevice, st));
-    if (ng) k_fill_cols<<<blocks_for(10LL * ng, 256), 256, 0, st>>>(h->ds.cu, ld, 10, gs, ng, 0.0);
-    k_scatter_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cn1, ne, 10, h->d_perm + cr.e0, h->ds.cu, ld);
-    k_copy_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cn, h->ds.cu, ld, 10, cr.e0, ne);
-    if (ng) k_copy_cols<<<blocks_for(10LL * ng, 256), 256, 0, st>>>(h->ds.cn, h->ds.cu, ld, 10, gs, ng);
+    const int nq = h->neq;
+    CUDA_OK(h, cudaMemcpyAsync(h->ds.cn1, cu_elem, nq * (size_t)ne * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (ng) k_fill_cols<<<blocks_for((long long)nq * ng, 256), 256, 0, st>>>(h->ds.cu, ld, nq, gs, ng, 0.0);
+    k_scatter_cols<<<blocks_for((long long)nq * ne, 256), 256, 0, st>>>(h->ds.cn1, ne, nq, h->d_perm + cr.e0,
+                                                                         h->ds.cu, ld);
+    k_copy_cols<<<blocks_for((long long)nq * ne, 256), 256, 0, st>>>(h->ds.cn, h->ds.cu, ld, nq, cr.e0, ne);
+    if (ng) k_copy_cols<<<blocks_for((long long)nq * ng, 256), 256, 0, st>>>(h->ds.cn, h->ds.cu, ld, nq, gs, ng);
     // primitives: zero, then the restart's ghost values (src/main.F90:433-438)
     k_fill_cols<<<blocks_for((long long)NPR * ne, 256), 256, 0, st>>>(h->ds.pr, ld, NPR, cr.e0, ne, 0.0);
     if (ng) k_fill_cols<<<blocks_for((long long)NPR * ng, 256), 256, 0, st>>>(h->ds.pr, ld, NPR, gs, ng, 0.0);
@@ -896,11 +924,24 @@ extern "C" int hp_init_uniform(hp_handle* h) {
     double v[10] = {phig * rogmin, phig * rogmin * p.ugmin, phig * rogmin * p.vgmin, phig * rogmin * p.wgmin,
                     phig * rogmin * egtmin, phip * ropmin, phip * ropmin * p.upmin, phip * ropmin * p.vpmin,
                     phip * ropmin * p.wpmin, phip * ropmin * eptmin};
+    double vq[12] = {};
+    if (h->neq == 22) {   // src/sr_init_cond.F90:180-208
+        phig = 1 - phip - p.epslninf - p.epslninf - p.epslninf;
+        v[0] = phig * rogmin; v[1] = phig * rogmin * p.ugmin; v[2] = phig * rogmin * p.vgmin;
+        v[3] = phig * rogmin * p.wgmin; v[4] = phig * rogmin * egtmin;
+        const double rho[3] = {p.rhoq, p.rhor, p.rhos}, ini[3] = {p.phiqinit, p.phirinit, p.phisinit};
+        for (int d = 0; d < 3; d++) {
+            vq[4 * d] = ini[d] * rho[d];
+            vq[4 * d + 1] = ini[d] * rho[d] * p.upmin;
+            vq[4 * d + 2] = ini[d] * rho[d] * p.vpmin;
+            vq[4 * d + 3] = ini[d] * rho[d] * p.wpmin;
+        }
+    }
     for (int c = 0; c < h->ncase; c++) {
         const int ne = h->cases[c].ne;
-        cu.assign(10 * (size_t)ne, 0.0);
-        for (int k = 0; k < 10; k++)
-            for (int i = 0; i < ne; i++) cu[(size_t)k * ne + i] = v[k];
+        cu.assign(h->neq * (size_t)ne, 0.0);
+        for (int k = 0; k < h->neq; k++)
+            for (int i = 0; i < ne; i++) cu[(size_t)k * ne + i] = k < 10 ? v[k] : vq[k - 10];
         rc = upload_state(h, c, 0.0, cu.data(), nullptr);
         if (rc) return rc;
     }
@@ -1061,6 +1102,7 @@ extern "C" int hp_profile_steps(hp_handle* h, int32_t nsteps, double* ms_per_kin
 
 extern "C" int hp_set_overset(hp_handle* h, const hp_overset* ov) {
     if (!h || !ov) return HP_E_ARG;
+    if (h->neq == 22) return fail(h, HP_E_UNSUPPORTED, "five-phase model: no overset fringe tables");
     if (h->ncase != 1) return fail(h, HP_E_UNSUPPORTED, "overset tables: single-case handles only");
     const int nf = ov->nfringe, ne = h->neles;
     if (nf < 0 || (nf > 0 && (!ov->fringe || !ov->donor || !ov->weight)))
@@ -1119,6 +1161,7 @@ static int slot_of(const hp_handle* h, int c, int e) {
 extern "C" int hp_set_halo(hp_handle* h, int32_t n, const int32_t* dst_case, const int32_t* dst_elem,
                            const int32_t* src_case, const int32_t* src_elem) {
     if (!h || n < 0 || (n > 0 && (!dst_case || !dst_elem || !src_case || !src_elem))) return HP_E_ARG;
+    if (h->neq == 22) return fail(h, HP_E_UNSUPPORTED, "five-phase model: no partition halos");
     if (h->started) return fail(h, HP_E_STATE, "hp_set_halo after the first step");
     std::vector<int> iv(2 * (size_t)n);
     std::vector<char> role(h->neles, 0);   // 1 destination, 2 source
@@ -1153,6 +1196,7 @@ extern "C" int hp_set_halo(hp_handle* h, int32_t n, const int32_t* dst_case, con
 
 extern "C" int hp_set_exchange(hp_handle* h, hp_exchange_fn fn, void* user) {
     if (!h) return HP_E_ARG;
+    if (h->neq == 22) return fail(h, HP_E_UNSUPPORTED, "five-phase model: no partition exchange");
     if (fn && h->ncase != 1) return fail(h, HP_E_UNSUPPORTED, "exchange callbacks: single-case handles only");
     h->xfn = fn;
     h->xuser = user;
@@ -1163,6 +1207,7 @@ extern "C" int hp_set_exchange(hp_handle* h, hp_exchange_fn fn, void* user) {
 extern "C" int hp_set_halo_lists(hp_handle* h, int32_t nsend, const int32_t* send_elem, int32_t nrecv,
                                  const int32_t* recv_elem) {
     if (!h || nsend < 0 || nrecv < 0 || (nsend && !send_elem) || (nrecv && !recv_elem)) return HP_E_ARG;
+    if (h->neq == 22) return fail(h, HP_E_UNSUPPORTED, "five-phase model: no partition exchange");
     if (h->ncase != 1) return fail(h, HP_E_UNSUPPORTED, "halo lists: single-case handles only");
     std::vector<int> iv((size_t)nsend + nrecv);
     for (int t = 0; t < nsend + nrecv; t++) {
@@ -1230,6 +1275,7 @@ extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, i
                                                                                                 : sizeof(double);
     Arena probe;
     const int nface = gb == sizeof(double) || params->face_mode ? 0 : (int)((4LL * mesh->neles + mesh->nghosts) / 2);
+    probe_h.neq = params->five_phase ? 22 : 10;
     plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb, 1, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
@@ -1250,6 +1296,7 @@ extern "C" int hp_estimate_batch_bytes(const hp_mesh* meshes, int32_t ncase, con
                                                                                                 : sizeof(double);
     Arena probe;
     const int nface = gb == sizeof(double) || params->face_mode ? 0 : (int)((4 * ne + ng) / 2);
+    probe_h.neq = params->five_phase ? 22 : 10;
     plan_arena(&probe_h, probe, (int)ne, (int)ng, ld, gb, ncase, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
@@ -1291,10 +1338,11 @@ extern "C" int hp_get_state_case(hp_handle* h, int32_t c, double* time, double* 
         CUDA_OK(h, cudaMemcpyAsync(h->h_scal, h->ds.s + c, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
     }
     if (cu_elem) {
-        k_gather_cols<<<blocks_for(10LL * ne, 256), 256, 0, st>>>(h->ds.cu, ld, 0, ne, 10, h->d_perm + cr.e0,
-                                                                  h->ds.cn1);
+        const int nq = h->neq;
+        k_gather_cols<<<blocks_for((long long)nq * ne, 256), 256, 0, st>>>(h->ds.cu, ld, 0, ne, nq,
+                                                                            h->d_perm + cr.e0, h->ds.cn1);
         CUDA_OK(h, cudaGetLastError());
-        CUDA_OK(h, cudaMemcpyAsync(cu_elem, h->ds.cn1, 10 * (size_t)ne * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(h, cudaMemcpyAsync(cu_elem, h->ds.cn1, nq * (size_t)ne * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
     if (ghost_prims && ng) {
         k_gather_ghost_prims<<<blocks_for(6LL * ng, 256), 256, 0, st>>>(h->ds.pr, ld, GHOST_COLS, ng,
@@ -1323,6 +1371,7 @@ cudaError_t launch_tecplot_fields(const double* cu, long long ld, int ne, const 
 extern "C" int hp_output_async(hp_handle* h, int32_t c, const hp_mesh* mesh, const char* restart_path,
                                const char* tecplot_path, int32_t* ticket) {
     if (!h || !ticket || (!restart_path && !tecplot_path)) return HP_E_ARG;
+    if (h->neq == 22) return fail(h, HP_E_UNSUPPORTED, "five-phase model: no asynchronous restart/Tecplot output (two-phase layout)");
     if (c < 0 || c >= h->ncase) return fail(h, HP_E_ARG, "case index out of range");
     const CaseRange& cr = h->cases[c];
     if (tecplot_path && (!mesh || mesh->neles != cr.ne || !mesh->elem || !mesh->x || !mesh->y || !mesh->z))
@@ -1426,6 +1475,7 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
         if (h->dm.nface > 0 && !h->prm.inviscid && h->var->face_visc) n += 1;   // k_vis_gather
         n += (int64_t)h->dp.nstage * per_stage + 3;
         if (h->aliased) n += 2;
+        if (h->neq == 22) n += 2 + (int64_t)h->dp.nstage * (2 + (h->nghosts ? 1 : 0));   // k_qrs_*
         *kernels_per_step = n;
     }
     if (device_bytes) *device_bytes = (int64_t)h->arena.size;

@@ -142,13 +142,23 @@ extern "C" int hp_read_flow(const char* path, hp_params* out) {
         {{'i', &p.istart}, {'d', &p.diap}},
         {{'d', &p.surfacetension}, {'i', &p.myflux}},
         {{'i', &p.myorder}, {'d', &p.as}, {'d', &p.ts}},
+        // read by the five-phase model only; a flow.in may end before them
+        {{'d', &p.rhoq}, {'d', &p.rhor}, {'d', &p.rhos}},
+        {{'d', &p.radq}, {'d', &p.radr}, {'d', &p.rads}},
+        {{'d', &p.phiginit}, {'d', &p.phipinit}, {'d', &p.phiqinit}, {'d', &p.phirinit}, {'d', &p.phisinit}},
     };
+    const size_t nrequired = groups.size() - 3;
     std::string line;
     std::vector<std::string> tok;
+    size_t gi = 0;
     for (auto& g : groups) {
         bool done = false;
+        const bool optional = gi++ >= nrequired;
         while (!done) {
-            if (!r.next(line)) return HP_E_IO;   // flow.in ended early
+            if (!r.next(line)) {
+                if (optional) goto end_of_file;
+                return HP_E_IO;   // flow.in ended early
+            }
             if (line.find_first_not_of(" \t") == std::string::npos || line[0] == '#') continue;
             size_t c = line.find('#');
             if (c != std::string::npos) line = line.substr(0, c);
@@ -162,6 +172,7 @@ extern "C" int hp_read_flow(const char* path, hp_params* out) {
             done = ok;
         }
     }
+end_of_file:
     p.venkat_k = 0.3;
     p.precision = HP_PREC_FP64_PARITY;
     p.renumber = 1;

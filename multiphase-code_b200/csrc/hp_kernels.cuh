@@ -203,7 +203,10 @@ __device__ __forceinline__ void blend_phases(const DevParams& P, S& phig, S& phi
     }
 }
 
-__device__ __forceinline__ void prim_full(double cd[10], PrimV& q, const DevParams& P) {
+// qm: the dispersed masses cn(11), cn(15), cn(19) of the five-phase model
+// (src/sr_primitive.F90:56-80), or null for the two-phase model
+__device__ __forceinline__ void prim_full(double cd[10], PrimV& q, const DevParams& P,
+                                          const double* qm = nullptr) {
     S c[10];
 #pragma unroll
     for (int k = 0; k < 10; k++) c[k] = (S)cd[k];
@@ -214,16 +217,36 @@ __device__ __forceinline__ void prim_full(double cd[10], PrimV& q, const DevPara
     q.up = div_rn(c[6], c[5], r5); q.vp = div_rn(c[7], c[5], r5); q.wp = div_rn(c[8], c[5], r5);
     S eg = div_rn(c[4], c[0], r0) - S(0.5) * (q.ug * q.ug + q.vg * q.vg + q.wg * q.wg);
     S ep = div_rn(c[9], c[5], r5) - S(0.5) * (q.up * q.up + q.vp * q.vp + q.wp * q.wp);
-    S bbb = (fsd + pinf * gamap) - (c[0] * (gamag - S(1.0)) * eg) - (c[5] * (gamap - S(1.0)) * ep);
-    S ccc = c[0] * (gamag - S(1.0)) * eg * (fsd + pinf * gamap);
-    q.pg = (-bbb + sqrt(bbb * bbb + S(4.0) * ccc)) * S(0.5);
-    q.pp = q.pg + fsd;
-    q.phig = (c[0] * (gamag - S(1.0)) * eg) / q.pg;
-    q.phip = S(1.0) - q.phig;
-    q.rog = c[0] / q.phig;
-    q.rop = c[5] / q.phip;
-    q.tg = q.pg / (q.rog * rrg);
-    q.tp = ((q.pp + pinf) * gamap) / ((gamap - S(1.0)) * q.rop * cpp);
+    if (qm) {
+        // the dispersed phases take their share of the volume out of the
+        // pressure-equilibrium quadratic; densities from the energies
+        const S emin = (S)P.emin;
+        const S phq = mn2(mx2((S)qm[0] / (S)P.rhod[0], emin), S(1.0) - emin);
+        const S phr = mn2(mx2((S)qm[1] / (S)P.rhod[1], emin), S(1.0) - emin);
+        const S phs = mn2(mx2((S)qm[2] / (S)P.rhod[2], emin), S(1.0) - emin);
+        const S aaa = mn2(mx2(S(1.0) - phq - phr - phs, emin), S(1.0) - emin);
+        S bbb = (aaa * pinf * gamap) - (c[0] * (gamag - S(1.0)) * eg) - (c[5] * (gamap - S(1.0)) * ep);
+        S ccc = (c[0] * (gamag - S(1.0)) * eg * (gamap * pinf));
+        q.pg = (-bbb + sqrt(bbb * bbb + S(4.0) * aaa * ccc)) / (S(2.0) * aaa);
+        q.pp = q.pg + fsd;
+        q.rog = q.pg / ((gamag - S(1.0)) * eg);
+        q.rop = (q.pp + pinf * gamap) / ((gamap - S(1.0)) * ep);
+        q.tg = q.pg / (q.rog * rrg);
+        q.tp = ((q.pp + pinf) * gamap) / ((gamap - S(1.0)) * q.rop * cpp);
+        q.phig = mn2(mx2(c[0] / q.rog, emin), S(1.0) - emin);
+        q.phip = mn2(mx2(c[5] / q.rop, emin), S(1.0) - emin);
+    } else {
+        S bbb = (fsd + pinf * gamap) - (c[0] * (gamag - S(1.0)) * eg) - (c[5] * (gamap - S(1.0)) * ep);
+        S ccc = c[0] * (gamag - S(1.0)) * eg * (fsd + pinf * gamap);
+        q.pg = (-bbb + sqrt(bbb * bbb + S(4.0) * ccc)) * S(0.5);
+        q.pp = q.pg + fsd;
+        q.phig = (c[0] * (gamag - S(1.0)) * eg) / q.pg;
+        q.phip = S(1.0) - q.phig;
+        q.rog = c[0] / q.phig;
+        q.rop = c[5] / q.phip;
+        q.tg = q.pg / (q.rog * rrg);
+        q.tp = ((q.pp + pinf) * gamap) / ((gamap - S(1.0)) * q.rop * cpp);
+    }
     blend_phases(P, q.phig, q.phip, q.ug, q.vg, q.wg, q.tg, q.pg, q.up, q.vp, q.wp, q.tp, q.pp);
     q.rog = q.pg / (rrg * q.tg);
     q.rop = (q.pp + pinf) * gamap / ((gamap - S(1.0)) * cpp * q.tp);
@@ -290,7 +313,11 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
             for (int k = 0; k < 10; k++) u[k] = COL(s.cu, k)[i];
         }
         PrimV q;
-        prim_full(c, q, P);
+        double qm[3];
+        if (P.five_phase) {
+            qm[0] = COL(s.cn, 10)[i]; qm[1] = COL(s.cn, 14)[i]; qm[2] = COL(s.cn, 18)[i];
+        }
+        prim_full(c, q, P, P.five_phase ? qm : nullptr);
 #pragma unroll
         for (int k = 0; k < 10; k++) COL(s.cn, k)[i] = c[k];
         store_prims(m, s.pr, i, q);
@@ -313,6 +340,13 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
                 }
                 bad |= (c[k] != c[k]);
                 COL(s.cu, k)[i] = c[k];
+            }
+            if (P.five_phase) {   // cu = cn over all 22 variables (src/main.F90:619-625)
+                for (int k = 10; k < 22; k++) {
+                    const double v = COL(s.cn, k)[i];
+                    bad |= (v != v);
+                    COL(s.cu, k)[i] = v;
+                }
             }
             // halo cells are counted by the part that owns them
             nanc = (bad && ldg(m.iblank + i) < HP_IBLANK_HALO1) ? 1 : 0;
@@ -434,7 +468,10 @@ __device__ __forceinline__ void bc_one(const DevMesh& m, double* pr, double* egt
     const double rrg = P.rrg, gamag = P.gamag, gamap = P.gamap, pinf = P.pinf, cpp = P.cpp;
     if (nt == 2) {
         phip[ng] = P.phipzero;
-        phig[ng] = 1.0 - phip[ng];
+        // five-phase: the dispersed fractions at the inflow are epslnmin
+        // (src/sr_primitiveplusbc.F90:210-216, src/sr_viscousgp.F90:83-88)
+        if (P.five_phase) phig[ng] = 1.0 - phip[ng] - P.emin - P.emin - P.emin;
+        else phig[ng] = 1.0 - phip[ng];
         ug[ng] = P.ugmin; vg[ng] = P.vgmin; wg[ng] = P.wgmin;
         tg[ng] = P.tgmin;
         pg[ng] = pg[np];
@@ -1407,6 +1444,14 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
         rhs[8] = rhs[8] + (double)((fdgz + pint * dpz) * voli) - COL(vis, 6)[i];
         rhs[9] = rhs[9] + (double)(en * voli) - COL(vis, 7)[i];
     }
+    // five-phase: drag of q, r, s on the liquid, in the order
+    // src/sr_sourceqrs.F90 adds it
+    if (P.five_phase) {
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) rhs[6 + c] = rhs[6 + c] + COL(s.qdrag, 3 * d + c)[i];
+    }
     // RK stage update (FP64)
     const double dtbyvol = s.s[case_of(m, i)].dt / ldg(m.vol + i);
 #pragma unroll
@@ -1707,6 +1752,13 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         rhs[7] = rhs[7] + (S)((fdgy + pint * dpy) * voli) - (S)COL(vis, 5)[i];
         rhs[8] = rhs[8] + (S)((fdgz + pint * dpz) * voli) - (S)COL(vis, 6)[i];
         rhs[9] = rhs[9] + (S)(en * voli) - (S)COL(vis, 7)[i];
+    }
+    // five-phase: drag of q, r, s on the liquid (see k_flux)
+    if (P.five_phase) {
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) rhs[6 + c] = rhs[6 + c] + (S)COL(s.qdrag, 3 * d + c)[i];
     }
     if constexpr (F == 1) {
         if (__any_sync(0xffffffffu, bad)) return false;
@@ -2135,6 +2187,251 @@ __global__ void __launch_bounds__(256) k_halo(DevMesh m, DevState<R> s) {
     for (int k = 0; k < 10; k++) COL(s.cn, k)[i] = COL(s.cn, k)[j];
 }
 
+// ---------------------------------------------------------------------------
+// Five-phase model: three dispersed, incompressible phases q, r, s (conserved
+// columns 10-13, 14-17, 18-21: mass and momentum at densities rhod), carried
+// by central fluxes with JST dissipation and coupled to the liquid by drag
+// (src/sr_jamesonqrs.F90, src/sr_dissipationqrs.F90, src/sr_sourceqrs.F90).
+// FP64 in every variant that accepts the model.
+
+// JST switches (liquid pressure, liquid mass and each dispersed mass) and
+// the Laplacian of columns 10-21, src/sr_dissipationqrs.F90:16-52; ghost
+// neighbours read their parent through snb, as the reference copies them.
+__global__ void __launch_bounds__(256) k_qrs_diss1(DevMesh m, DevState<R> s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles) return;
+    const int a = ldg(COL(m.snb, 0) + i), b = ldg(COL(m.snb, 1) + i);
+    const int c = ldg(COL(m.snb, 2) + i), d = ldg(COL(m.snb, 3) + i);
+    const double e16 = (double)1.0e-16f;      // a REAL(4) literal in the reference
+    const double* pp = COL(s.pr, P_PP);
+    const double ppi = pp[i], ppa = pp[a], ppb = pp[b], ppc = pp[c], ppd = pp[d];
+    double anun = fabs(ppa - ppi) + fabs(ppb - ppi) + fabs(ppc - ppi) + fabs(ppd - ppi);
+    double anud = fabs(ppa + ppi) + fabs(ppb + ppi) + fabs(ppc + ppi) + fabs(ppd + ppi);
+    double anupp = anun / anud;
+    double sw[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        const double* col = COL(s.cn, t == 0 ? 5 : 6 + 4 * t);    // cn(:,6), cn(:,11), cn(:,15), cn(:,19)
+        const double v0 = col[i], v1 = col[a], v2 = col[b], v3 = col[c], v4 = col[d];
+        anun = fabs(v1 - v0) + fabs(v2 - v0) + fabs(v3 - v0) + fabs(v4 - v0);
+        anud = fabs(v1 + v0) + fabs(v2 + v0) + fabs(v3 + v0) + fabs(v4 + v0);
+        sw[t] = anun / (anud + e16);
+    }
+    anupp = anupp + sw[0];
+    double lap[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        const double* col = COL(s.cn, 10 + k);
+        const double v0 = col[i];
+        lap[k] = col[a] - v0 + col[b] - v0 + col[c] - v0 + col[d] - v0;
+    }
+#pragma unroll
+    for (int k = 0; k < 12; k++) COL(s.d2q, 10 + k)[i] = lap[k];
+#pragma unroll
+    for (int t = 0; t < 3; t++) COL(s.anuq, t)[i] = anupp + sw[1 + t];
+}
+
+// d24 of columns 10-21, src/sr_dissipationqrs.F90:62-157.
+__global__ void __launch_bounds__(256) k_qrs_diss2(DevMesh m, DevState<R> s, DevParams P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles) return;
+    const double dt = s.s[case_of(m, i)].dt;
+    int nb[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) nb[f] = ldg(COL(m.snb, f) + i);
+    const double vi = ldg(m.vol + i) / dt;
+    double d24nc[4], out[12];
+#pragma unroll
+    for (int f = 0; f < 4; f++) d24nc[f] = 0.5 * (vi + ldg(m.vol + nb[f]) / dt);
+#pragma unroll
+    for (int set = 0; set < 3; set++) {
+        const double* anu = COL(s.anuq, set);
+        const double ai = anu[i];
+        double d2c[4], d4c[4];
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            const double e2 = P.co2 * mx2(ai, anu[nb[f]]);
+            const double e4 = mx2(0.0, P.co4 - e2);
+            d2c[f] = e2 * d24nc[f];
+            d4c[f] = e4 * d24nc[f];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const double* cn = COL(s.cn, 10 + 4 * set + k);
+            const double* dq = COL(s.d2q, 10 + 4 * set + k);
+            const double ci = cn[i], qi = dq[i];
+            const double d2 = d2c[0] * (cn[nb[0]] - ci) + d2c[1] * (cn[nb[1]] - ci) + d2c[2] * (cn[nb[2]] - ci) +
+                              d2c[3] * (cn[nb[3]] - ci);
+            const double d4 = d4c[0] * (dq[nb[0]] - qi) + d4c[1] * (dq[nb[1]] - qi) + d4c[2] * (dq[nb[2]] - qi) +
+                              d4c[3] * (dq[nb[3]] - qi);
+            out[4 * set + k] = d2 - d4;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 12; k++) COL(s.d24, 10 + k)[i] = out[k];
+}
+
+// src/sr_jamesonqrs.F90:21-60: dispersed fractions from their masses,
+// renormalised with the two-phase fractions of this stage, velocities, and
+// the masses and momenta rewritten from them; active elements.  (The
+// reference also renormalises phig and phip there; nothing reads those
+// values before the next primitive recovery overwrites them.)
+__global__ void __launch_bounds__(256) k_qrs_prim(DevMesh m, DevState<R> s, DevParams P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles || ldg(m.iblank + i) != 1) return;
+    const double emin = P.emin;
+    double phd[3], u[3], v[3], w[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) phd[d] = mn2(mx2(COL(s.cn, 10 + 4 * d)[i] / P.rhod[d], emin), 1.0 - emin);
+    const double phitotal = COL(s.pr, P_PHIG)[i] + COL(s.pr, P_PHIP)[i] + phd[0] + phd[1] + phd[2];
+#pragma unroll
+    for (int d = 0; d < 3; d++) phd[d] = phd[d] / phitotal;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double mass = COL(s.cn, 10 + 4 * d)[i];
+        u[d] = COL(s.cn, 11 + 4 * d)[i] / mass;
+        v[d] = COL(s.cn, 12 + 4 * d)[i] / mass;
+        w[d] = COL(s.cn, 13 + 4 * d)[i] / mass;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double r = P.rhod[d];
+        COL(s.cn, 10 + 4 * d)[i] = phd[d] * r;
+        COL(s.cn, 11 + 4 * d)[i] = phd[d] * r * u[d];
+        COL(s.cn, 12 + 4 * d)[i] = phd[d] * r * v[d];
+        COL(s.cn, 13 + 4 * d)[i] = phd[d] * r * w[d];
+        COL(s.qpr, 4 * d)[i] = phd[d];
+        COL(s.qpr, 4 * d + 1)[i] = u[d];
+        COL(s.qpr, 4 * d + 2)[i] = v[d];
+        COL(s.qpr, 4 * d + 3)[i] = w[d];
+    }
+}
+
+// src/sr_jamesonqrs.F90:67-147: ghost states of the dispersed phases (inflow
+// 2: fraction epslnmin at the liquid's ghost velocity; outflow 3: the
+// parent's; wall 5: the parent's fraction, velocity reversed; other types
+// keep their previous ghost state) and the ghost masses and momenta.  One
+// thread per ghost (meshes without aliased ghost ids).
+__global__ void __launch_bounds__(256) k_qrs_bc(DevMesh m, DevState<R> s, DevParams P) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= m.nghosts) return;
+    const int np = m.g_par[g], ng = m.g_id[g], nt = m.g_type[g];
+#pragma unroll
+    for (int k = 10; k < 22; k++) COL(s.cn, k)[ng] = COL(s.cn, k)[np];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        double* ph = COL(s.qpr, 4 * d);
+        double* u = COL(s.qpr, 4 * d + 1);
+        double* v = COL(s.qpr, 4 * d + 2);
+        double* w = COL(s.qpr, 4 * d + 3);
+        if (nt == 2) {
+            ph[ng] = P.emin;
+            u[ng] = COL(s.pr, P_UP)[ng]; v[ng] = COL(s.pr, P_VP)[ng]; w[ng] = COL(s.pr, P_WP)[ng];
+        } else if (nt == 3) {
+            ph[ng] = ph[np]; u[ng] = u[np]; v[ng] = v[np]; w[ng] = w[np];
+        } else if (nt == 5) {
+            ph[ng] = ph[np]; u[ng] = -u[np]; v[ng] = -v[np]; w[ng] = -w[np];
+        }
+        const double r = P.rhod[d];
+        COL(s.cn, 10 + 4 * d)[ng] = ph[ng] * r;
+        COL(s.cn, 11 + 4 * d)[ng] = ph[ng] * r * u[ng];
+        COL(s.cn, 12 + 4 * d)[ng] = ph[ng] * r * v[ng];
+        COL(s.cn, 13 + 4 * d)[ng] = ph[ng] * r * w[ng];
+    }
+}
+
+// Central fluxes of the dispersed phases over the 4 faces in face order (none
+// through type-5 walls), src/sr_jamesonqrs.F90:151-330; their drag with the
+// liquid, src/sr_sourceqrs.F90:42-199 (constant liquid viscosity 0.001 of the
+// AMUP_CONSTANT build), whose liquid-momentum terms go to qdrag for the flux
+// kernel to add in the reference's order; then the RK stage update of
+// columns 10-21 (src/sr_RK.F90).  Active elements.
+__global__ void __launch_bounds__(128) k_qrs_flux(DevMesh m, DevState<R> s, DevParams P, int stage) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.neles || ldg(m.iblank + i) != 1) return;
+    const unsigned kinds = ldg(m.fk + i);
+    double rhs[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) rhs[k] = 0.0;
+    double phi[3], ui[3], vi[3], wi[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        phi[d] = COL(s.qpr, 4 * d)[i]; ui[d] = COL(s.qpr, 4 * d + 1)[i];
+        vi[d] = COL(s.qpr, 4 * d + 2)[i]; wi[d] = COL(s.qpr, 4 * d + 3)[i];
+    }
+#pragma unroll 1
+    for (int f = 0; f < 4; f++) {
+        if ((kinds >> (4 * f)) & FK_WALL) continue;
+        const int n = ldg(COL(m.nc, f) + i);
+        const double scx = ldg(COL(m.sc, 3 * f) + i), scy = ldg(COL(m.sc, 3 * f + 1) + i),
+                     scz = ldg(COL(m.sc, 3 * f + 2) + i);
+        const double area = sqrt(scx * scx + scy * scy + scz * scz);
+        const double enx = scx / area, eny = scy / area, enz = scz / area;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double un = COL(s.qpr, 4 * d + 1)[n], vn = COL(s.qpr, 4 * d + 2)[n], wn = COL(s.qpr, 4 * d + 3)[n];
+            const double qnl = ui[d] * enx + vi[d] * eny + wi[d] * enz;
+            const double qnr = un * enx + vn * eny + wn * enz;
+            const double phih = (phi[d] + COL(s.qpr, 4 * d)[n]) * 0.5;
+            const double roh = (P.rhod[d] + P.rhod[d]) * 0.5;
+            const double uh = (ui[d] + un) * 0.5, vh = (vi[d] + vn) * 0.5, wh = (wi[d] + wn) * 0.5;
+            const double qh = (qnl + qnr) * 0.5;
+            rhs[4 * d] = rhs[4 * d] + (phih * roh * qh) * area;
+            rhs[4 * d + 1] = rhs[4 * d + 1] + (phih * roh * qh * uh) * area;
+            rhs[4 * d + 2] = rhs[4 * d + 2] + (phih * roh * qh * vh) * area;
+            rhs[4 * d + 3] = rhs[4 * d + 3] + (phih * roh * qh * wh) * area;
+        }
+    }
+    // drag (Schiller-Naumann-type coefficient of the reference)
+    const double voli = ldg(m.vol + i);
+    const double up = COL(s.pr, P_UP)[i], vp = COL(s.pr, P_VP)[i], wp = COL(s.pr, P_WP)[i];
+    const double amup = 0.001, gravity = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double du = up - ui[d], dv = vp - vi[d], dw = wp - wi[d];
+        const double reyn = mx2(P.rhod[d] * 2.0 * P.radd[d] * sqrt(du * du + dv * dv + dw * dw) / amup, 0.001);
+        const double relv = sqrt(du * du + dv * dv + dw * dw);
+        double cd;
+        if (reyn < 0.1) cd = 24.0 / reyn;
+        else if (reyn < 1000.0) cd = 0.48 + 28.0 / pow(reyn, 0.85);
+        else cd = 0.48;
+        const double drag = 0.5 * cd * P.rhod[d] * 3.1415926 * P.radd[d] * P.radd[d] * relv * (phi[d] / P.vold[d]);
+        rhs[4 * d + 1] = rhs[4 * d + 1] - drag * du * voli;
+        rhs[4 * d + 2] = rhs[4 * d + 2] - drag * dv * voli - phi[d] * P.rhod[d] * gravity * voli;
+        rhs[4 * d + 3] = rhs[4 * d + 3] - drag * dw * voli;
+        COL(s.qdrag, 3 * d)[i] = drag * du * voli;
+        COL(s.qdrag, 3 * d + 1)[i] = drag * dv * voli;
+        COL(s.qdrag, 3 * d + 2)[i] = drag * dw * voli;
+    }
+    const double dtbyvol = s.s[case_of(m, i)].dt / voli;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        const int j = 10 + k;
+        const double r = rhs[k] - COL(s.d24, j)[i];
+        const double cu = COL(s.cu, j)[i];
+        double* cnp = COL(s.cn, j) + i;
+        if (P.rk_scheme == 0) {
+            if (stage == 1) {
+                const double v = cu - (11.0 / 20.0) * dtbyvol * r;
+                *cnp = v;
+                COL(s.cn1, j)[i] = v;
+            } else {
+                const double upd = *cnp - (11.0 / 20.0) * dtbyvol * r;
+                if (stage == 2) *cnp = (3.0 / 8.0) * cu + (5.0 / 8.0) * upd;
+                else if (stage == 3) *cnp = (4.0 / 9.0) * cu + (5.0 / 9.0) * upd;
+                else *cnp = (111.0 / 1331.0) * cu + (260.0 / 1331.0) * COL(s.cn1, j)[i] + (960.0 / 1331.0) * upd;
+            }
+        } else {
+            if (stage == 1) *cnp = cu - dtbyvol * r;
+            else {
+                const double upd = *cnp - dtbyvol * r;
+                if (stage == 2) *cnp = 0.75 * cu + 0.25 * upd;
+                else *cnp = (1.0 / 3.0) * cu + (2.0 / 3.0) * upd;
+            }
+        }
+    }
+}
+
 static inline unsigned grid_for(long long n, int block) {
     return (unsigned)((n + block - 1) / block);
 }
@@ -2190,6 +2487,11 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
     if (m.aliased) { MARK(KK_SERIAL); k_smooth_copy_serial<<<1, 1, 0, st>>>(m, s, 1); }
     MARK(KK_SMOOTH2);
     k_smooth2<<<ge, cb, 0, st>>>(m, s, P);
+    if (P.five_phase) {   // src/main.F90:570-572
+        MARK(KK_QRS);
+        k_qrs_diss1<<<grid_for(m.neles, 256), 256, 0, st>>>(m, s);
+        k_qrs_diss2<<<grid_for(m.neles, 256), 256, 0, st>>>(m, s, P);
+    }
     // viscous fluxes, src/sr_viscousgp.F90 (stage 1 of each step)
     if (m.nghosts > 0) {
         MARK(KK_BC_VISC);
@@ -2225,6 +2527,12 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             else if (sizeof(R) != sizeof(double)) k_grad<true><<<gf, b, 0, st>>>(m, s, P);
             else k_grad4<<<g4, 128, 0, st>>>(m, s, P);
             if (m.aliased) { MARK(KK_SERIAL); k_phi_copy_serial<<<1, 1, 0, st>>>(m, s); }
+        }
+        if (P.five_phase) {   // src/mod_Fluxmodule.F90:18-20: jamesonqrs (and sourceqrs)
+            MARK(KK_QRS);
+            k_qrs_prim<<<grid_for(m.neles, 256), 256, 0, st>>>(m, s, P);
+            if (m.nghosts > 0) k_qrs_bc<<<grid_for(m.nghosts, 256), 256, 0, st>>>(m, s, P);
+            k_qrs_flux<<<grid_for(m.neles, 128), 128, 0, st>>>(m, s, P, stage);
         }
         MARK(KK_FLUX);
         if (P.myflux == 1) enqueue_flux<1>(m, s, P, st, stage, hook);

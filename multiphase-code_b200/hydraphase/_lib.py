@@ -39,7 +39,10 @@ class HpParams(ctypes.Structure):
         ("niter", _I), ("itersub", _I), ("istart", _I), ("diap", _D), ("surfacetension", _D),
         ("myflux", _I), ("myorder", _I), ("as_", _D), ("ts", _D), ("face_mode", _I),
         ("venkat_k", _D), ("rk_scheme", _I), ("inviscid", _I), ("twall", _D), ("precision", _I),
-        ("renumber", _I), ("block_size", _I), ("use_graph", _I), ("pad_", _D * 4)]
+        ("renumber", _I), ("block_size", _I), ("use_graph", _I), ("pad_", _D * 4),
+        ("five_phase", _I)] + [(n, _D) for n in (
+        "rhoq", "rhor", "rhos", "radq", "radr", "rads", "phiginit", "phipinit", "phiqinit", "phirinit",
+        "phisinit")]
 
 
 class HpMesh(ctypes.Structure):
@@ -141,7 +144,7 @@ def lib():
 
 
 KERNEL_KINDS = ("prim_start", "step_begin", "smooth1", "smooth2", "bc_visc", "visc", "prim_stage",
-                "bc", "grad", "flux", "prim_end", "step_end", "serial", "overset", "halo")
+                "bc", "grad", "flux", "prim_end", "step_end", "serial", "overset", "halo", "qrs")
 
 EXPORTED_SYMBOLS = (
     "hp_create", "hp_destroy", "hp_last_error", "hp_create_error", "hp_init_uniform",

@@ -330,6 +330,38 @@ def _cylinder_flow(b: Built, name, ndrop=32, seed=1, mach=0.3, re_d=150.0, t_inf
     return CaseSpec(name, b.mesh, flow, cu, gp, 1000, extra)
 
 
+def with_dispersed(spec: CaseSpec, fractions=(2.0e-3, 1.0e-3, 5.0e-4), rho=(2500.0, 1950.0, 2700.0),
+                   rad=(5.0e-6, 20.0e-6, 7.5e-6), slip=0.02) -> CaseSpec:
+    """The five-phase form of a two-phase case: three dispersed phases q, r,
+    s (particles of density rho and radius rad, the reference's FIVE_PHASE
+    model, flow.in groups 19-20) whose volume fractions vary smoothly around
+    `fractions` over the domain, moving with the liquid velocity plus a small
+    slip (so their drag is not zero).  The gas and liquid fractions are
+    scaled by the volume left to them, so the five fractions sum to one and
+    the pressure recovered by the five-phase equation of state is the case's
+    own.  Variables 11-22 of cu: mass and momentum of q, r, s."""
+    m = spec.mesh
+    el = m.elem[:, :4] - 1
+    xc = np.stack([m.x[el].mean(1), m.y[el].mean(1), m.z[el].mean(1)], axis=1)
+    lo, hi = xc.min(axis=0), xc.max(axis=0)
+    t = (xc - lo) / np.maximum(hi - lo, 1e-30)
+    phd = [f * (1.0 + 0.5 * np.sin(2 * np.pi * (k + 1) * t[:, k % 3]) * np.cos(np.pi * t[:, (k + 1) % 3]))
+           for k, f in enumerate(fractions)]
+    aaa = 1.0 - phd[0] - phd[1] - phd[2]
+    cu2 = spec.cu.copy() * aaa[None, :]
+    up = cu2[6:9] / cu2[5][None, :]
+    cu = np.empty((22, m.neles))
+    cu[:10] = cu2
+    for d in range(3):
+        ud = up * (1.0 + slip * (d + 1))
+        cu[10 + 4 * d] = phd[d] * rho[d]
+        cu[11 + 4 * d:14 + 4 * d] = (phd[d] * rho[d])[None, :] * ud
+    flow = dict(spec.flow, rhoq=rho[0], rhor=rho[1], rhos=rho[2], radq=rad[0], radr=rad[1], rads=rad[2],
+                phiqinit=fractions[0], phirinit=fractions[1], phisinit=fractions[2])
+    return CaseSpec(spec.name + "_five_phase", m, flow, cu, spec.ghost_prims, spec.steps,
+                    dict(spec.extra, five_phase=1))
+
+
 def union_mesh(a: Built, b: Built) -> tuple[Built, np.ndarray]:
     """One element list of two meshes: a's elements, then b's; ghosts of a,
     then of b, all after the elements (so no ghost id aliases an element id,

@@ -180,6 +180,7 @@ class Case:
         self.h = h
         self.neles = mesh.neles
         self.nghosts = mesh.nghosts
+        self.neq = 22 if params.five_phase else 10
 
     def close(self):
         if getattr(self, "h", None):
@@ -203,8 +204,8 @@ class Case:
 
     def set_state(self, time: float, cu: np.ndarray, ghost_prims: np.ndarray | None = None):
         cu = np.ascontiguousarray(cu, np.float64).reshape(-1)
-        if cu.size != 10 * self.neles:
-            raise ValueError("cu must hold 10 x neles values")
+        if cu.size != self.neq * self.neles:
+            raise ValueError(f"cu must hold {self.neq} x neles values")
         gp = None if ghost_prims is None else np.ascontiguousarray(ghost_prims, np.float64).reshape(-1)
         _check(self.L.hp_set_state(self.h, float(time), _dp(cu), _dp(gp)), self.h)
 
@@ -252,20 +253,21 @@ class Case:
         return {"kinds": list(KERNEL_KINDS), "ms": ms.tolist(), "launches": cnt.tolist()}
 
     def state(self, out=None):
-        """(time, cu (10, neles), ghost primitives (6, nghosts)).  out =
-        (cu, gp): caller buffers (C-contiguous float64 of 10 * neles and at
-        least 6 * nghosts values, e.g. pinned memory) to fill instead."""
+        """(time, cu (neq, neles), ghost primitives (6, nghosts)); neq is 10,
+        or 22 with the five-phase model.  out = (cu, gp): caller buffers
+        (C-contiguous float64 of neq * neles and at least 6 * nghosts values,
+        e.g. pinned memory) to fill instead."""
         t = ctypes.c_double()
         if out is None:
-            cu = np.zeros(10 * self.neles)
+            cu = np.zeros(self.neq * self.neles)
             gp = np.zeros(6 * max(self.nghosts, 1))
         else:
             cu, gp = out
             if (cu.dtype != np.float64 or gp.dtype != np.float64 or not cu.flags.c_contiguous
-                    or not gp.flags.c_contiguous or cu.size != 10 * self.neles or gp.size < 6 * self.nghosts):
-                raise ValueError("out must be C-contiguous float64 buffers of 10*neles and 6*nghosts values")
+                    or not gp.flags.c_contiguous or cu.size != self.neq * self.neles or gp.size < 6 * self.nghosts):
+                raise ValueError("out must be C-contiguous float64 buffers of neq*neles and 6*nghosts values")
         _check(self.L.hp_get_state(self.h, ctypes.byref(t), _dp(cu), _dp(gp)), self.h)
-        return t.value, cu.reshape(10, self.neles), gp.reshape(-1)[:6 * self.nghosts].reshape(6, self.nghosts)
+        return t.value, cu.reshape(self.neq, self.neles), gp.reshape(-1)[:6 * self.nghosts].reshape(6, self.nghosts)
 
     def output_async(self, restart_path=None, tecplot_path=None, mesh: MeshArrays | None = None) -> int:
         """Start writing the current state (after the steps enqueued so far)
@@ -357,6 +359,7 @@ class Batch:
         _check(self.L.hp_create_batch(arr, len(meshes), ctypes.byref(params), ctypes.byref(h)))
         self.h = h
         self.neles = [m.neles for m in meshes]
+        self.neq = 22 if params.five_phase else 10
         self.nghosts = [m.nghosts for m in meshes]
 
     @property
@@ -382,8 +385,8 @@ class Batch:
 
     def set_state(self, c: int, time: float, cu: np.ndarray, ghost_prims: np.ndarray | None = None):
         cu = np.ascontiguousarray(cu, np.float64).reshape(-1)
-        if cu.size != 10 * self.neles[c]:
-            raise ValueError("cu must hold 10 x neles values of case %d" % c)
+        if cu.size != self.neq * self.neles[c]:
+            raise ValueError("cu must hold %d x neles values of case %d" % (self.neq, c))
         gp = None if ghost_prims is None else np.ascontiguousarray(ghost_prims, np.float64).reshape(-1)
         _check(self.L.hp_set_state_case(self.h, int(c), float(time), _dp(cu), _dp(gp)), self.h)
 
@@ -414,7 +417,7 @@ class Batch:
     def state(self, c: int):
         t = ctypes.c_double()
         ne, ng = self.neles[c], self.nghosts[c]
-        cu = np.zeros(10 * ne)
+        cu = np.zeros(self.neq * ne)
         gp = np.zeros(6 * max(ng, 1))
         _check(self.L.hp_get_state_case(self.h, int(c), ctypes.byref(t), _dp(cu), _dp(gp)), self.h)
-        return t.value, cu.reshape(10, ne), gp[:6 * ng].reshape(6, ng)
+        return t.value, cu.reshape(self.neq, ne), gp[:6 * ng].reshape(6, ng)

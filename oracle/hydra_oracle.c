@@ -40,6 +40,10 @@ struct or_case {
     double *ug, *vg, *wg, *pg, *pp, *tg, *phig, *up, *vp, *wp, *phip, *tp;
     double *rop, *rog, *ag, *ap, *egtotal, *eptotal, *phi;
     double *cn, *cu, *cn1, *rhs, *d24, *d2q, *anu;
+    int neq;                                 /* 10, or 22 with the five-phase model */
+    /* five-phase model: dispersed-phase primitives (phi, u, v, w of q, r, s) */
+    double *phiq, *phir, *phis, *uq, *vq, *wq, *ur, *vr, *wr, *us, *vs, *ws;
+    double volq, volr, vols;                 /* particle volumes, src/main.F90:352-354 */
     double *vis[8];                          /* ug,vg,wg,tg,up,vp,wp,tp */
     double *g[NGRAD];
     double xmax, ymax, zmax, ymin, zmin;
@@ -254,10 +258,19 @@ or_case *or_create(const or_params *p, int32_t nodes, int32_t neles,
                         &S->up, &S->vp, &S->wp, &S->phip, &S->tp, &S->rop, &S->rog,
                         &S->ag, &S->ap, &S->egtotal, &S->eptotal, &S->phi};
     for (size_t k = 0; k < sizeof(prims) / sizeof(prims[0]); k++) *prims[k] = dalloc(nt1);
-    size_t nn = (size_t)S->ntot * NEQ;
+    S->neq = p->five_phase ? 22 : NEQ;          /* src/main.F90:114-124 */
+    size_t nn = (size_t)S->ntot * S->neq;
     S->cn = dalloc(nn); S->cu = dalloc(nn); S->cn1 = dalloc(nn); S->d2q = dalloc(nn);
     S->anu = dalloc((size_t)S->ntot * 3);
-    S->rhs = dalloc((size_t)neles * NEQ); S->d24 = dalloc((size_t)neles * NEQ);
+    S->rhs = dalloc((size_t)neles * S->neq); S->d24 = dalloc((size_t)neles * S->neq);
+    if (p->five_phase) {
+        double **q[] = {&S->phiq, &S->phir, &S->phis, &S->uq, &S->vq, &S->wq,
+                        &S->ur, &S->vr, &S->wr, &S->us, &S->vs, &S->ws};
+        for (size_t k = 0; k < sizeof(q) / sizeof(q[0]); k++) *q[k] = dalloc(nt1);
+        S->volq = (4.0 / 3.0) * 3.1415926 * (p->radq * p->radq * p->radq);
+        S->volr = (4.0 / 3.0) * 3.1415926 * (p->radr * p->radr * p->radr);
+        S->vols = (4.0 / 3.0) * 3.1415926 * (p->rads * p->rads * p->rads);
+    }
     for (int k = 0; k < 8; k++) S->vis[k] = dalloc((size_t)neles + 1);
     for (int k = 0; k < NGRAD; k++) S->g[k] = dalloc(nt1);
 
@@ -298,6 +311,8 @@ void or_destroy(or_case *S) {
     for (size_t k = 0; k < sizeof(prims) / sizeof(prims[0]); k++) free(prims[k]);
     free(S->cn); free(S->cu); free(S->cn1); free(S->d2q); free(S->anu);
     free(S->rhs); free(S->d24);
+    free(S->phiq); free(S->phir); free(S->phis); free(S->uq); free(S->vq); free(S->wq);
+    free(S->ur); free(S->vr); free(S->wr); free(S->us); free(S->vs); free(S->ws);
     for (int k = 0; k < 8; k++) free(S->vis[k]);
     for (int k = 0; k < NGRAD; k++) free(S->g[k]);
     free(S->ofr); free(S->odon); free(S->ow);
@@ -320,14 +335,30 @@ void or_init_uniform(or_case *S) {
         CU(i, 8) = phip * S->ropmin * p->vpmin;
         CU(i, 9) = phip * S->ropmin * p->wpmin;
         CU(i, 10) = phip * S->ropmin * S->eptotalmin;
+        if (p->five_phase) {   /* src/sr_init_cond.F90:180-208 */
+            phig = 1 - phip - p->epslninf - p->epslninf - p->epslninf;
+            CU(i, 1) = phig * S->rogmin;
+            CU(i, 2) = phig * S->rogmin * p->ugmin;
+            CU(i, 3) = phig * S->rogmin * p->vgmin;
+            CU(i, 4) = phig * S->rogmin * p->wgmin;
+            CU(i, 5) = phig * S->rogmin * S->egtotalmin;
+            const double rho[3] = {p->rhoq, p->rhor, p->rhos};
+            const double ini[3] = {p->phiqinit, p->phirinit, p->phisinit};
+            for (int d = 0; d < 3; d++) {
+                CU(i, 11 + 4 * d) = ini[d] * rho[d];
+                CU(i, 12 + 4 * d) = ini[d] * rho[d] * p->upmin;
+                CU(i, 13 + 4 * d) = ini[d] * rho[d] * p->vpmin;
+                CU(i, 14 + 4 * d) = ini[d] * rho[d] * p->wpmin;
+            }
+        }
     }
-    memcpy(S->cn, S->cu, sizeof(double) * (size_t)S->ntot * NEQ);
+    memcpy(S->cn, S->cu, sizeof(double) * (size_t)S->ntot * S->neq);
 }
 
 void or_set_state(or_case *S, double time, const double *cu_elem,
                   const double *ghost_prims) {
     S->time = time;
-    for (int k = 1; k <= NEQ; k++)
+    for (int k = 1; k <= S->neq; k++)
         for (int i = 1; i <= S->neles; i++)
             CU(i, k) = cu_elem[(size_t)(k - 1) * S->neles + (i - 1)];
     if (ghost_prims) {
@@ -336,7 +367,7 @@ void or_set_state(or_case *S, double time, const double *cu_elem,
             for (int i = 1; i <= S->nghosts; i++)
                 dst[v][S->nghost[i]] = ghost_prims[(size_t)v * S->nghosts + (i - 1)];
     }
-    memcpy(S->cn, S->cu, sizeof(double) * (size_t)S->ntot * NEQ);
+    memcpy(S->cn, S->cu, sizeof(double) * (size_t)S->ntot * S->neq);
 }
 
 /* ------------------------------------------------------------------ */
@@ -407,6 +438,30 @@ static void prim_head(or_case *S, int i, int with_sound) {
     double eg = CN(i, 5) / CN(i, 1) - 0.5 * (sq(S->ug[i]) + sq(S->vg[i]) + sq(S->wg[i]));
     double ep = CN(i, 10) / CN(i, 6) - 0.5 * (sq(S->up[i]) + sq(S->vp[i]) + sq(S->wp[i]));
     double fs = S->foursigmabyd;
+    if (p->five_phase) {
+        /* src/sr_primitive.F90:56-80: the dispersed phases take their share
+         * of the volume out of the pressure-equilibrium quadratic */
+        double emin = p->epslnmin;
+        double phq = mn2(mx2(CN(i, 11) / p->rhoq, emin), 1.0 - emin);
+        double phr = mn2(mx2(CN(i, 15) / p->rhor, emin), 1.0 - emin);
+        double phs = mn2(mx2(CN(i, 19) / p->rhos, emin), 1.0 - emin);
+        double aaa = mn2(mx2(1.0 - phq - phr - phs, emin), 1.0 - emin);
+        double bbb = (aaa * pinf * gamap) - (CN(i, 1) * (gamag - 1.0) * eg) - (CN(i, 6) * (gamap - 1.0) * ep);
+        double ccc = (CN(i, 1) * (gamag - 1.0) * eg * (gamap * pinf));
+        S->pg[i] = (-bbb + sqrt(sq(bbb) + 4.0 * aaa * ccc)) / (2.0 * aaa);
+        S->pp[i] = S->pg[i] + fs;
+        S->rog[i] = S->pg[i] / ((gamag - 1.0) * eg);
+        S->rop[i] = (S->pp[i] + pinf * gamap) / ((gamap - 1.0) * ep);
+        S->tg[i] = S->pg[i] / (S->rog[i] * S->rrg);
+        S->tp[i] = ((S->pp[i] + pinf) * gamap) / ((gamap - 1.0) * S->rop[i] * p->cpp);
+        S->phig[i] = mn2(mx2(CN(i, 1) / S->rog[i], emin), 1.0 - emin);
+        S->phip[i] = mn2(mx2(CN(i, 6) / S->rop[i], emin), 1.0 - emin);
+        if (with_sound) {
+            S->ag[i] = sqrt((gamag * S->pg[i]) / S->rog[i]);
+            S->ap[i] = sqrt((gamap * (S->pp[i] + pinf)) / S->rop[i]);
+        }
+        return;
+    }
     double bbb = (fs + pinf * gamap) - (CN(i, 1) * (gamag - 1.0) * eg) -
                  (CN(i, 6) * (gamap - 1.0) * ep);
     double ccc = CN(i, 1) * (gamag - 1.0) * eg * (fs + pinf * gamap);
@@ -450,8 +505,14 @@ static void bc_fill(or_case *S, int viscous) {
     /* type 2: subsonic inflow */
     for (int ii = 1; ii <= S->nbc[0]; ii++) {
         int i = S->bcl[0][ii], np = S->nparent[i], ng = S->nghost[i];
-        S->phip[ng] = p->phipzero;
-        S->phig[ng] = 1.0 - S->phip[ng];
+        if (p->five_phase) {   /* sr_primitiveplusbc.F90:210-216, sr_viscousgp.F90:83-88 */
+            S->phiq[ng] = p->epslnmin; S->phir[ng] = p->epslnmin; S->phis[ng] = p->epslnmin;
+            S->phip[ng] = p->phipzero;
+            S->phig[ng] = 1.0 - S->phip[ng] - S->phiq[ng] - S->phir[ng] - S->phis[ng];
+        } else {
+            S->phip[ng] = p->phipzero;
+            S->phig[ng] = 1.0 - S->phip[ng];
+        }
         S->ug[ng] = p->ugmin; S->vg[ng] = p->vgmin; S->wg[ng] = p->wgmin;
         S->tg[ng] = p->tgmin;
         S->pg[ng] = S->pg[np];
@@ -1101,6 +1162,200 @@ static void hllc_zien_face(double *F, double area, double enx, double eny, doubl
     }
 }
 
+/* ------------------------------------------------------------------ */
+/* Five-phase model: three dispersed phases q, r, s (variables 11-14,
+ * 15-18, 19-22: mass and momentum, incompressible at rhoq, rhor, rhos). */
+
+/* JST dissipation of variables 11-22, src/sr_dissipationqrs.F90:16-157:
+ * switches from the liquid pressure, the liquid mass and each dispersed
+ * mass; called after or_smooth, so ANU(:,1..3) may be reused. */
+static void dissipation_qrs(or_case *S) {
+    for (int i = 1; i <= S->nghosts; i++) {
+        int ng = S->nghost[i], np = S->nparent[i];
+        S->pp[ng] = S->pp[np];
+        for (int k = 11; k <= 22; k++) CN(ng, k) = CN(np, k);
+    }
+    const double e16 = R4(1.0e-16);   /* 1.0E-16 is a REAL(4) literal */
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
+    for (int i = 1; i <= S->neles; i++) {
+        int a = S->nc[0][i], b = S->nc[1][i], c = S->nc[2][i], d = S->nc[3][i];
+        double *pp = S->pp;
+        double anun = fabs(pp[a] - pp[i]) + fabs(pp[b] - pp[i]) + fabs(pp[c] - pp[i]) + fabs(pp[d] - pp[i]);
+        double anud = fabs(pp[a] + pp[i]) + fabs(pp[b] + pp[i]) + fabs(pp[c] + pp[i]) + fabs(pp[d] + pp[i]);
+        double anupp = anun / anud;
+#define SW(K)                                                                          \
+    anun = fabs(CN(a, K) - CN(i, K)) + fabs(CN(b, K) - CN(i, K)) + fabs(CN(c, K) - CN(i, K)) + \
+           fabs(CN(d, K) - CN(i, K));                                                  \
+    anud = fabs(CN(a, K) + CN(i, K)) + fabs(CN(b, K) + CN(i, K)) + fabs(CN(c, K) + CN(i, K)) + \
+           fabs(CN(d, K) + CN(i, K));
+        SW(6);
+        anupp = anupp + anun / (anud + e16);
+        SW(11);
+        ANU(i, 1) = anupp + anun / (anud + e16);
+        SW(15);
+        ANU(i, 2) = anupp + anun / (anud + e16);
+        SW(19);
+        ANU(i, 3) = anupp + anun / (anud + e16);
+#undef SW
+        for (int k = 11; k <= 22; k++)
+            D2Q(i, k) = CN(a, k) - CN(i, k) + CN(b, k) - CN(i, k) + CN(c, k) - CN(i, k) +
+                        CN(d, k) - CN(i, k);
+    }
+    for (int i = 1; i <= S->nghosts; i++) {
+        int ng = S->nghost[i], np = S->nparent[i];
+        for (int k = 11; k <= 22; k++) D2Q(ng, k) = D2Q(np, k);
+        ANU(ng, 1) = ANU(np, 1);
+        ANU(ng, 2) = ANU(np, 2);
+        ANU(ng, 3) = ANU(np, 3);
+    }
+    double dt = S->dt;
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
+    for (int i = 1; i <= S->neles; i++) {
+        int nb[4] = {S->nc[0][i], S->nc[1][i], S->nc[2][i], S->nc[3][i]};
+        double d24nc[4];
+        for (int f = 0; f < 4; f++) d24nc[f] = 0.5 * (S->vol[i] / dt + S->vol[nb[f]] / dt);
+        for (int set = 0; set < 3; set++) {
+            double d2c[4], d4c[4];
+            for (int f = 0; f < 4; f++) {
+                double e2 = S->co2 * mx2(ANU(i, set + 1), ANU(nb[f], set + 1));
+                double e4 = mx2(0.0, S->co4 - e2);
+                d2c[f] = e2 * d24nc[f];
+                d4c[f] = e4 * d24nc[f];
+            }
+            for (int k = 11 + 4 * set; k <= 14 + 4 * set; k++) {
+                double d2 = d2c[0] * (CN(nb[0], k) - CN(i, k)) + d2c[1] * (CN(nb[1], k) - CN(i, k)) +
+                            d2c[2] * (CN(nb[2], k) - CN(i, k)) + d2c[3] * (CN(nb[3], k) - CN(i, k));
+                double d4 = d4c[0] * (D2Q(nb[0], k) - D2Q(i, k)) + d4c[1] * (D2Q(nb[1], k) - D2Q(i, k)) +
+                            d4c[2] * (D2Q(nb[2], k) - D2Q(i, k)) + d4c[3] * (D2Q(nb[3], k) - D2Q(i, k));
+                D24(i, k) = d2 - d4;
+            }
+        }
+    }
+}
+
+/* Drag of the dispersed phases on the liquid, src/sr_sourceqrs.F90:42-199
+ * with the constant liquid viscosity of the AMUP_CONSTANT build; every
+ * element (the reference does not skip iblank != 1 here). */
+static void source_qrs(or_case *S) {
+    const or_params *p = &S->p;
+    const double rho[3] = {p->rhoq, p->rhor, p->rhos}, rad[3] = {p->radq, p->radr, p->rads};
+    const double vold[3] = {S->volq, S->volr, S->vols};
+    double *phd[3] = {S->phiq, S->phir, S->phis};
+    double *ud[3] = {S->uq, S->ur, S->us}, *vd[3] = {S->vq, S->vr, S->vs}, *wd[3] = {S->wq, S->wr, S->ws};
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
+    for (int i = 1; i <= S->neles; i++) {
+        double voli = S->vol[i];
+        double amup = 0.001;
+        for (int d = 0; d < 3; d++) {
+            double du = S->up[i] - ud[d][i], dv = S->vp[i] - vd[d][i], dw = S->wp[i] - wd[d][i];
+            double reyn = mx2(rho[d] * 2.0 * rad[d] * sqrt(sq(du) + sq(dv) + sq(dw)) / amup, 0.001);
+            double relv = sqrt(sq(du) + sq(dv) + sq(dw));
+            double cd;
+            if (reyn < 0.1) cd = 24.0 / reyn;
+            else if (reyn < 1000.0) cd = 0.48 + 28.0 / pow(reyn, 0.85);
+            else cd = 0.48;
+            double drag = 0.5 * cd * rho[d] * 3.1415926 * rad[d] * rad[d] * relv * (phd[d][i] / vold[d]);
+            int k = 12 + 4 * d;
+            RHS(i, k) = RHS(i, k) - drag * du * voli;
+            RHS(i, k + 1) = RHS(i, k + 1) - drag * dv * voli - phd[d][i] * rho[d] * S->gravity * voli;
+            RHS(i, k + 2) = RHS(i, k + 2) - drag * dw * voli;
+            RHS(i, 7) = RHS(i, 7) + drag * du * voli;
+            RHS(i, 8) = RHS(i, 8) + drag * dv * voli;
+            RHS(i, 9) = RHS(i, 9) + drag * dw * voli;
+        }
+    }
+}
+
+/* Central fluxes of the dispersed phases, src/sr_jamesonqrs.F90:21-333:
+ * volume fractions from their masses, renormalised with the two-phase
+ * fractions; velocities; cn rewritten; ghost states for types 2, 3, 5; then
+ * the face loop (no flux through type-5 walls) and sourceqrs. */
+static void jameson_qrs(or_case *S) {
+    const or_params *p = &S->p;
+    const double emin = p->epslnmin;
+    const double rho[3] = {p->rhoq, p->rhor, p->rhos};
+    double *phd[3] = {S->phiq, S->phir, S->phis};
+    double *ud[3] = {S->uq, S->ur, S->us}, *vd[3] = {S->vq, S->vr, S->vs}, *wd[3] = {S->wq, S->wr, S->ws};
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
+    for (int i = 1; i <= S->neles; i++) {
+        if (S->iblank[i] != 1) continue;
+        for (int d = 0; d < 3; d++) phd[d][i] = mn2(mx2(CN(i, 11 + 4 * d) / rho[d], emin), 1.0 - emin);
+        double phitotal = S->phig[i] + S->phip[i] + S->phiq[i] + S->phir[i] + S->phis[i];
+        S->phig[i] = S->phig[i] / phitotal;
+        S->phip[i] = S->phip[i] / phitotal;
+        for (int d = 0; d < 3; d++) phd[d][i] = phd[d][i] / phitotal;
+        for (int d = 0; d < 3; d++) {
+            int k = 11 + 4 * d;
+            ud[d][i] = CN(i, k + 1) / CN(i, k);
+            vd[d][i] = CN(i, k + 2) / CN(i, k);
+            wd[d][i] = CN(i, k + 3) / CN(i, k);
+        }
+        for (int d = 0; d < 3; d++) {
+            int k = 11 + 4 * d;
+            CN(i, k) = phd[d][i] * rho[d];
+            CN(i, k + 1) = phd[d][i] * rho[d] * ud[d][i];
+            CN(i, k + 2) = phd[d][i] * rho[d] * vd[d][i];
+            CN(i, k + 3) = phd[d][i] * rho[d] * wd[d][i];
+        }
+    }
+    for (int g = 1; g <= S->nghosts; g++) {
+        int np = S->nparent[g], ng = S->nghost[g], nt = S->ntype[g];
+        for (int k = 11; k <= 22; k++) CN(ng, k) = CN(np, k);
+        if (nt == 2) {
+            S->phip[ng] = emin;
+            for (int d = 0; d < 3; d++) phd[d][ng] = emin;
+            S->phig[ng] = 1.0 - S->phip[ng] - S->phiq[ng] - S->phir[ng] - S->phis[ng];
+            for (int d = 0; d < 3; d++) { ud[d][ng] = S->up[ng]; vd[d][ng] = S->vp[ng]; wd[d][ng] = S->wp[ng]; }
+        } else if (nt == 3) {
+            S->phip[ng] = emin;
+            for (int d = 0; d < 3; d++) phd[d][ng] = phd[d][np];
+            S->phig[ng] = 1.0 - S->phip[ng] - S->phiq[ng] - S->phir[ng] - S->phis[ng];
+            for (int d = 0; d < 3; d++) { ud[d][ng] = ud[d][np]; vd[d][ng] = vd[d][np]; wd[d][ng] = wd[d][np]; }
+        } else if (nt == 5) {
+            for (int d = 0; d < 3; d++) phd[d][ng] = phd[d][np];
+            for (int d = 0; d < 3; d++) { ud[d][ng] = -ud[d][np]; vd[d][ng] = -vd[d][np]; wd[d][ng] = -wd[d][np]; }
+        }
+        for (int d = 0; d < 3; d++) {
+            int k = 11 + 4 * d;
+            CN(ng, k) = phd[d][ng] * rho[d];
+            CN(ng, k + 1) = phd[d][ng] * rho[d] * ud[d][ng];
+            CN(ng, k + 2) = phd[d][ng] * rho[d] * vd[d][ng];
+            CN(ng, k + 3) = phd[d][ng] * rho[d] * wd[d][ng];
+        }
+    }
+    int neles = S->neles;
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
+    for (int i = 1; i <= neles; i++) {
+        if (S->iblank[i] != 1) continue;
+        for (int k = 11; k <= 22; k++) RHS(i, k) = 0.0;
+        for (int f = 0; f < 4; f++) {
+            int neigh = S->nc[f][i];
+            double scx = S->sc[3 * f][i], scy = S->sc[3 * f + 1][i], scz = S->sc[3 * f + 2][i];
+            double area = sqrt(scx * scx + scy * scy + scz * scz);
+            double enx = scx / area, eny = scy / area, enz = scz / area;
+            int nt = 0;
+            if (neigh > neles) nt = S->ntype[neigh - neles];
+            if (nt == 5) continue;
+            for (int d = 0; d < 3; d++) {
+                double qnl = ud[d][i] * enx + vd[d][i] * eny + wd[d][i] * enz;
+                double qnr = ud[d][neigh] * enx + vd[d][neigh] * eny + wd[d][neigh] * enz;
+                double phih = (phd[d][i] + phd[d][neigh]) * 0.5;
+                double roh = (rho[d] + rho[d]) * 0.5;
+                double uh = (ud[d][i] + ud[d][neigh]) * 0.5;
+                double vh = (vd[d][i] + vd[d][neigh]) * 0.5;
+                double wh = (wd[d][i] + wd[d][neigh]) * 0.5;
+                double qh = (qnl + qnr) * 0.5;
+                int k = 11 + 4 * d;
+                RHS(i, k) = RHS(i, k) + (phih * roh * qh) * area;
+                RHS(i, k + 1) = RHS(i, k + 1) + (phih * roh * qh * uh) * area;
+                RHS(i, k + 2) = RHS(i, k + 2) + (phih * roh * qh * vh) * area;
+                RHS(i, k + 3) = RHS(i, k + 3) + (phih * roh * qh * wh) * area;
+            }
+        }
+    }
+    source_qrs(S);
+}
+
 /* Interphase sources, src/sr_source.F90:42-178 */
 static void source(or_case *S) {
     const or_params *p = &S->p;
@@ -1168,6 +1423,7 @@ void or_flux(or_case *S) {
     if (S->p.myorder == 2) { or_derivative(S); or_venkat(S); }
     hllc_faces(S, S->p.myflux == 1);
     source(S);
+    if (S->p.five_phase) jameson_qrs(S);    /* src/mod_Fluxmodule.F90:18-20 */
 }
 
 /* ------------------------------------------------------------------ */
@@ -1285,7 +1541,7 @@ static void stage(or_case *S, int st) {
     for (int i = 1; i <= ne; i++) {
         if (S->iblank[i] != 1) continue;
         double dtbyvol = S->dt / S->vol[i];
-        for (int j = 1; j <= NEQ; j++) {
+        for (int j = 1; j <= S->neq; j++) {
             double r = RHS(i, j) - D24(i, j);
             if (S->p.rk_scheme == 0) {
                 double upd = CN(i, j) - (11.0 / 20.0) * dtbyvol * r;
@@ -1351,6 +1607,7 @@ static void one_step(or_case *S, double *diff4, double *velmag) {
     S->dt = S->dtmin * p->cfl;
     S->time = S->time + S->dt;
     or_smooth(S);
+    if (p->five_phase) dissipation_qrs(S);   /* src/main.F90:570-572 */
     rk(S);
     or_primitive(S);
     double dp = 0, du = 0, dv = 0, dw = 0;
@@ -1360,7 +1617,7 @@ static void one_step(or_case *S, double *diff4, double *velmag) {
         dv = mx2(dv, fabs(CN(i, 3) - CU(i, 3)));
         dw = mx2(dw, fabs(CN(i, 4) - CU(i, 4)));
     }
-    memcpy(S->cu, S->cn, sizeof(double) * (size_t)S->ntot * NEQ);
+    memcpy(S->cu, S->cn, sizeof(double) * (size_t)S->ntot * S->neq);
     if (diff4) { diff4[0] = dp; diff4[1] = du; diff4[2] = dv; diff4[3] = dw; }
     if (velmag) *velmag = sqrt(sq(S->ug[1]) + sq(S->vg[1]) + sq(S->wg[1]));
 }
@@ -1383,10 +1640,10 @@ double or_time(const or_case *S) { return S->time; }
 double or_last_dt(const or_case *S) { return S->dt; }
 int32_t or_ntot(const or_case *S) { return S->ntot; }
 void or_get_cu(const or_case *S, double *out) {
-    memcpy(out, S->cu, sizeof(double) * (size_t)S->ntot * NEQ);
+    memcpy(out, S->cu, sizeof(double) * (size_t)S->ntot * S->neq);
 }
 void or_get_cn(const or_case *S, double *out) {
-    memcpy(out, S->cn, sizeof(double) * (size_t)S->ntot * NEQ);
+    memcpy(out, S->cn, sizeof(double) * (size_t)S->ntot * S->neq);
 }
 /* ug,vg,wg,pg,pp,tg,phig,up,vp,wp,phip,tp,rop,rog,ag,ap */
 void or_get_prims(const or_case *S, double *out) {
@@ -1411,10 +1668,10 @@ void or_get_ghost_restart(const or_case *S, double *out) {
         for (int i = 1; i <= S->nghosts; i++) out[(size_t)v * S->nghosts + i - 1] = a[v][S->nghost[i]];
 }
 void or_get_rhs(const or_case *S, double *out) {
-    memcpy(out, S->rhs, sizeof(double) * (size_t)S->neles * NEQ);
+    memcpy(out, S->rhs, sizeof(double) * (size_t)S->neles * S->neq);
 }
 void or_get_d24(const or_case *S, double *out) {
-    memcpy(out, S->d24, sizeof(double) * (size_t)S->neles * NEQ);
+    memcpy(out, S->d24, sizeof(double) * (size_t)S->neles * S->neq);
 }
 void or_get_vis(const or_case *S, double *out) {
     for (int v = 0; v < 8; v++)

@@ -49,6 +49,13 @@ typedef struct or_params {
     int32_t inviscid;   /* 1: skip the viscous face fluxes (vis* = 0) */
     double twall;       /* isothermal wall temperature for BC type 6 */
     double pad_[3];
+    /* five-phase model (the reference's FIVE_PHASE build): three dispersed,
+     * incompressible phases q, r, s with mass and momentum each, so
+     * neq = 22.  flow.in groups 19-21 (src/sr_Read_flow.F90:214-250). */
+    int32_t five_phase;
+    double rhoq, rhor, rhos;            /* phase densities */
+    double radq, radr, rads;            /* particle radii */
+    double phiqinit, phirinit, phisinit;/* volume fractions of the uniform start */
 } or_params;
 
 typedef struct or_case or_case;

@@ -46,6 +46,13 @@ FLOW_GROUPS = [
     (("surfacetension", "myflux"), (float, int)),
     (("myorder", "as_", "ts"), (int, float, float)),
 ]
+# groups read only by the five-phase model; optional (the two-phase build
+# stops reading after myorder, as, ts)
+FLOW_GROUPS_OPT = [
+    (("rhoq", "rhor", "rhos"), (float, float, float)),
+    (("radq", "radr", "rads"), (float, float, float)),
+    (("phiginit", "phipinit", "phiqinit", "phirinit", "phisinit"), (float,) * 5),
+]
 
 
 class OrParams(ctypes.Structure):
@@ -60,7 +67,11 @@ class OrParams(ctypes.Structure):
         ("myorder", ctypes.c_int32), ("as_", ctypes.c_double), ("ts", ctypes.c_double),
         ("nan_mode", ctypes.c_int32), ("venkat_k", ctypes.c_double),
         ("rk_scheme", ctypes.c_int32), ("inviscid", ctypes.c_int32),
-        ("twall", ctypes.c_double), ("pad_", ctypes.c_double * 3)]
+        ("twall", ctypes.c_double), ("pad_", ctypes.c_double * 3),
+        ("five_phase", ctypes.c_int32), ("rhoq", ctypes.c_double), ("rhor", ctypes.c_double),
+        ("rhos", ctypes.c_double), ("radq", ctypes.c_double), ("radr", ctypes.c_double),
+        ("rads", ctypes.c_double), ("phiqinit", ctypes.c_double), ("phirinit", ctypes.c_double),
+        ("phisinit", ctypes.c_double)]
 
 
 def _fortran_value(tok: str, typ):
@@ -76,9 +87,11 @@ def parse_flow_in(text: str) -> dict:
     lines = text.splitlines()
     pos = 0
     out: dict = {}
-    for names, types in FLOW_GROUPS:
+    for names, types in FLOW_GROUPS + FLOW_GROUPS_OPT:
         while True:
             if pos >= len(lines):
+                if (names, types) in FLOW_GROUPS_OPT:
+                    return out
                 raise ValueError(f"flow.in ended before {names}")
             line = lines[pos]
             pos += 1
@@ -330,9 +343,13 @@ class Oracle:
     def init_uniform(self):
         self.L.or_init_uniform(self.h)
 
+    @property
+    def neq(self) -> int:
+        return 22 if self.params.five_phase else 10
+
     def set_state(self, time: float, cu_elem: np.ndarray, ghost_prims=None):
         cu = np.ascontiguousarray(cu_elem, np.float64).ravel()
-        assert cu.size == 10 * self.neles
+        assert cu.size == self.neq * self.neles
         gp = None if ghost_prims is None else np.ascontiguousarray(ghost_prims, np.float64).ravel()
         self.L.or_set_state(self.h, float(time), _dp(cu), _dp(gp) if gp is not None else None)
 
@@ -347,10 +364,10 @@ class Oracle:
         return out.reshape(shape)
 
     def cu(self):
-        return self._get("or_get_cu", (10, self.ntot))
+        return self._get("or_get_cu", (self.neq, self.ntot))
 
     def cn(self):
-        return self._get("or_get_cn", (10, self.ntot))
+        return self._get("or_get_cn", (self.neq, self.ntot))
 
     def prims(self):
         return self._get("or_get_prims", (16, self.ntot))
@@ -362,10 +379,10 @@ class Oracle:
         return self._get("or_get_ghost_restart", (6, self.nghosts))
 
     def rhs(self):
-        return self._get("or_get_rhs", (10, self.neles))
+        return self._get("or_get_rhs", (self.neq, self.neles))
 
     def d24(self):
-        return self._get("or_get_d24", (10, self.neles))
+        return self._get("or_get_d24", (self.neq, self.neles))
 
     def vis(self):
         return self._get("or_get_vis", (8, self.neles))

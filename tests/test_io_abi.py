@@ -85,6 +85,12 @@ def test_shipped_mesh_through_reference_format(tmp_path):
     (g / "proc_bc0000.in").write_text("           0           0\n")
     p = read_flow(str(tmp_path / "flow.in"))
     assert (p.myflux, p.myorder, p.niter, p.itersub) == (2, 2, 2, 5)
+    # the dispersed-phase groups the five-phase model reads (flow.in lines
+    # after myorder, as, ts)
+    assert (p.rhoq, p.rhor, p.rhos) == (2500.0, 1950.0, 2700.0)
+    assert (p.radq, p.radr, p.rads) == (5.0e-6, 20.0e-6, 7.50e-6)
+    assert (p.phiqinit, p.phirinit, p.phisinit) == (0.4600, 0.1550, 0.1180)
+    assert flow["rhoq"] == p.rhoq and flow["phisinit"] == p.phisinit
     m = read_mesh(str(tmp_path))
     for k in ("x", "y", "z", "elem", "ghost"):
         np.testing.assert_array_equal(getattr(m, k), getattr(om, k), err_msg=k)
@@ -191,13 +197,24 @@ def test_no_gpu_fails_loudly():
     assert e.value.code == HP_E_CUDA
 
 
-def test_params_layout_matches_header():
-    # hp_params is shared by the C++ driver, the Python mirror and Fortran
-    # bind(C) interfaces: fixed size and offsets
-    assert ctypes.sizeof(HpParams) == 376
+def test_params_layout_matches_header(tmp_path):
+    """hp_params is shared by C callers, the Python mirror and Fortran bind(C)
+    interfaces: the C compiler's size and every field offset equal the
+    mirror's."""
     assert HpParams.cfl.offset == 29 * 8
     assert HpParams.face_mode.offset == 296
-    assert HpParams.venkat_k.offset == HpParams.face_mode.offset + 8
+    names = [f[0] for f in HpParams._fields_]
+    cname = {"as_": "as"}
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"hydraphase.h\"\nint main(void) {\n"
+                   "  printf(\"%zu\\n\", sizeof(hp_params));\n" +
+                   "".join(f'  printf("%zu\\n", offsetof(hp_params, {cname.get(n, n)}));\n' for n in names) +
+                   "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert vals[0] == ctypes.sizeof(HpParams)
+    assert vals[1:] == [getattr(HpParams, n).offset for n in names]
 
 
 def test_host_thread_share():
