@@ -66,9 +66,14 @@ typedef struct hp_params {
     double as, ts;           /* Sutherland constants */
     /* --- additions; zero-initialised values reproduce the reference --- */
     int32_t face_mode;       /* FP32-arithmetic variants: 0 = fluxes evaluated
-                                once per face where the mesh allows, 1 = once
-                                from each side (four lanes per cell);
-                                hydraphase.tune picks it */
+                                once per face where the mesh allows, stored as
+                                face records and gathered per cell in face
+                                order; 1 = once from each side (four lanes per
+                                cell); 2 = once per face, added to per-cell sums
+                                colour by colour (no atomics, fixed order);
+                                3 = once per face with atomic adds (the last
+                                bits vary from run to run); hydraphase.tune
+                                picks it */
     double venkat_k;         /* limiter eps^2 = (K*dl)^3; 0 selects 0.3 */
     int32_t rk_scheme;       /* 0: reference 4-stage ESSPRK; 1: SSP-RK3 */
     int32_t inviscid;        /* 1: viscous face fluxes off */

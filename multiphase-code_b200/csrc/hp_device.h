@@ -15,7 +15,7 @@
 
 namespace hp {
 
-enum { NEQ = 10, NPR = 14, NGR = 33 };
+enum { NEQ = 10, NPR = 14, NGR = 33, NLSQ = 16 };
 
 // primitive columns (the reference's ug,vg,wg,tg,pg,pp,phig,phip,up,vp,wp,
 // tp,rog,rop of src/mod_GlobalVariables.F90:13)
@@ -67,11 +67,12 @@ struct DevMesh {
     const double* fcv;      // [12][ld] face centroids, /3 (viscous)
     // geometry-only least-squares terms, evaluated once at set-up with the
     // reference's expressions: [0..3] weights, [4..9] a1 a2 a3 b1 b2 b3,
-    // [10] the determinant; LSQA for the 1/r^2 cell gradients
-    // (src/sr_derivative.F90:163-176,255), LSQB for the 1/r gradient of
-    // alpha_g in the sources (src/sr_source.F90:100-117)
-    const double* lsqa;     // [11][ld]
-    const double* lsqb;     // [11][ld]
+    // [10] the determinant, [11..14] and [15] the correctly rounded
+    // reciprocals of the weights and of the determinant; LSQA for the 1/r^2
+    // cell gradients (src/sr_derivative.F90:163-176,255), LSQB for the 1/r
+    // gradient of alpha_g in the sources (src/sr_source.F90:100-117)
+    const double* lsqa;     // [NLSQ][ld]
+    const double* lsqb;     // [NLSQ][ld]
     const int *g_par, *g_id, *g_type;   // [nghosts] ghost list (reference order)
     // overset fringe (nfringe = 0: none): cells, 4 donor cells each and
     // barycentric weights, [4][nfringe] column-major
@@ -83,6 +84,15 @@ struct DevMesh {
     const int* f_i;
     const int* f_code;      // local face of the owner (bits 0-1)
     const int* cface;       // [4][ld]
+    // face modes 2 (colouring) and 3 (atomics): the face fluxes are added
+    // to a per-cell accumulator instead of stored as records.  Mode 2 takes
+    // the faces colour by colour (no two faces of a colour share a cell, so
+    // each colour adds without atomics, in a fixed order); fcolor lists the
+    // face ids colour by colour, colour c at [fcoff[c], fcoff[c + 1]).
+    int face_mode;
+    int ncolor;
+    const int* fcolor;      // [nface]
+    int fcoff[33];
     int nfringe;
     const int* fr;
     const int* fdon;
@@ -128,6 +138,7 @@ struct DevState {
     double* qpr;             // [12][ld] phi, u, v, w of q, r, s
     double* anuq;            // [3][ld] their JST switches
     double* qdrag;           // [9][ld] drag of q, r, s on the liquid (x, y, z)
+    double* racc;            // [10][ld] face modes 2, 3: the cells' face sums
     R* ff;                   // [nface][FACE_REC] face records (face-based
                              // variants): 10 flux components, the wall flag
                              // (1: pressure terms only), one pad

@@ -183,8 +183,8 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     m.eps2 = (double*)a.take(ld * D);
     m.sc = (double*)a.take(12 * ld * D); m.fch = (double*)a.take(12 * ld * D);
     m.fcv = (double*)a.take(12 * ld * D);
-    m.lsqa = (double*)a.take(11 * ld * D);
-    m.lsqb = (double*)a.take(11 * ld * D);
+    m.lsqa = (double*)a.take(NLSQ * ld * D);
+    m.lsqb = (double*)a.take(NLSQ * ld * D);
     m.g_par = (int*)a.take((nghosts + 1) * (size_t)I); m.g_id = (int*)a.take((nghosts + 1) * (size_t)I);
     m.g_type = (int*)a.take((nghosts + 1) * (size_t)I);
     DevState<double>& s = h->ds;
@@ -210,11 +210,17 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     m.cid = ncase > 1 ? (const int*)a.take((size_t)neles * I) : nullptr;
     m.nface = nface;
     m.fld = ((long long)nface + 63) / 64 * 64;
+    s.racc = nullptr;
+    m.fcolor = nullptr;
     if (nface > 0) {
         m.f_i = (const int*)a.take((size_t)nface * I);
         m.f_code = (const int*)a.take((size_t)nface * I);
         m.cface = (const int*)a.take(4 * (size_t)ld * I);
         s.ff = (double*)a.take((size_t)FACE_REC * (size_t)m.fld * gb);
+        if (h->prm.face_mode >= 2) {   // colouring or atomics: per-cell face sums
+            s.racc = (double*)a.take(10 * (size_t)ld * D);
+            m.fcolor = (const int*)a.take((size_t)nface * I);
+        }
     } else {
         m.f_i = m.f_code = m.cface = nullptr;
         s.ff = nullptr;
@@ -237,7 +243,7 @@ struct Layout {
         gpar.assign(ng, 0); gid.assign(ng, 0); gtyp.assign(ng, 0); perm.assign(ne, 0); ghost_id.assign(ng, 0);
         for (auto* v : {&x, &y, &z, &vol, &dl, &dd, &eps2}) v->assign(ld, 0.0);
         for (auto* v : {&sc, &fch, &fcv}) v->assign(12 * ld, 0.0);
-        la.assign(11 * ld, 0.0); lb.assign(11 * ld, 0.0);
+        la.assign(NLSQ * ld, 0.0); lb.assign(NLSQ * ld, 0.0);
     }
 };
 
@@ -369,7 +375,7 @@ static int fill_case(const hp_mesh* mesh, const hp_params* params, Layout& L, Ca
         }
     }
     // --- static least-squares terms of the gradient and source operators ---
-    std::vector<double> lsqa(11 * (size_t)(neles + 1), 0.0), lsqb(11 * (size_t)(neles + 1), 0.0);
+    std::vector<double> lsqa(NLSQ * (size_t)(neles + 1), 0.0), lsqb(NLSQ * (size_t)(neles + 1), 0.0);
     auto LA = [&](int k, int i) -> double& { return lsqa[(size_t)k * (neles + 1) + i]; };
     auto LB = [&](int k, int i) -> double& { return lsqb[(size_t)k * (neles + 1) + i]; };
 #pragma omp parallel for schedule(static)
@@ -393,6 +399,10 @@ static int fill_case(const hp_mesh* mesh, const hp_params* params, Layout& L, Ca
         for (int f = 0; f < 4; f++) LA(f, i) = wa[f];
         LA(4, i) = a1; LA(5, i) = a2; LA(6, i) = a3; LA(7, i) = b1; LA(8, i) = b2; LA(9, i) = b3;
         LA(10, i) = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+        // the correctly rounded reciprocals of the weights and the
+        // determinant, which the device's shared-reciprocal division takes
+        for (int f = 0; f < 4; f++) LA(11 + f, i) = 1.0 / wa[f];
+        LA(15, i) = 1.0 / LA(10, i);
         // src/sr_source.F90:100-117
         a1 = sq(xa[0]) / wb[0] + sq(xa[1]) / wb[1] + sq(xa[2]) / wb[2] + sq(xa[3]) / wb[3];
         a2 = sq(ya[0]) / wb[0] + sq(ya[1]) / wb[1] + sq(ya[2]) / wb[2] + sq(ya[3]) / wb[3];
@@ -403,6 +413,8 @@ static int fill_case(const hp_mesh* mesh, const hp_params* params, Layout& L, Ca
         for (int f = 0; f < 4; f++) LB(f, i) = wb[f];
         LB(4, i) = a1; LB(5, i) = a2; LB(6, i) = a3; LB(7, i) = b1; LB(8, i) = b2; LB(9, i) = b3;
         LB(10, i) = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
+        for (int f = 0; f < 4; f++) LB(11 + f, i) = 1.0 / wb[f];
+        LB(15, i) = 1.0 / LB(10, i);
     }
     // --- aliasing: ghost slots that are elements, repeated, or ghost parents ---
     {
@@ -492,7 +504,7 @@ static int fill_case(const hp_mesh* mesh, const hp_params* params, Layout& L, Ca
             for (int k = 0; k < 12; k++) {
                 hsc[k * ld + t] = SC(k, i); hfch[k * ld + t] = FCH(k, i); hfcv[k * ld + t] = FCV(k, i);
             }
-            for (int k = 0; k < 11; k++) { hla[k * ld + t] = LA(k, i); hlb[k * ld + t] = LB(k, i); }
+            for (int k = 0; k < NLSQ; k++) { hla[k * ld + t] = LA(k, i); hlb[k * ld + t] = LB(k, i); }
         } else {
             for (int k = 0; k < 4; k++) { hnc[k * ld + t] = map(nc[k][i]); hsnb[k * ld + t] = map(nc[k][i]); }
         }
@@ -516,6 +528,8 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
         return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
     if (params->block_size != 0 && (params->block_size < 64 || params->block_size > 512 || params->block_size % 32))
         return fail(nullptr, HP_E_ARG, "block_size must be 0 or a multiple of 32 in [64, 512]");
+    if (params->face_mode < 0 || params->face_mode > 3)
+        return fail(nullptr, HP_E_ARG, "face_mode must be 0 (face records), 1 (each side), 2 (colouring) or 3 (atomics)");
     if (params->five_phase) {
         if (!(params->rhoq > 0 && params->rhor > 0 && params->rhos > 0 && params->radq > 0 && params->radr > 0 &&
               params->rads > 0))
@@ -620,7 +634,7 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     // when the other side is a ghost); meshes whose neighbour lists are not
     // mutual, and aliased meshes, keep the cell-centric fluxes ---
     std::vector<int> hf_i, hf_code, hcface;
-    if (gb != D && !h->aliased && h->prm.face_mode == 0) {
+    if (gb != D && !h->aliased && h->prm.face_mode != 1) {
         hcface.assign(4 * (size_t)ld, 0);
         bool mutual = true;
         for (int t = 0; t < neles && mutual; t++)
@@ -641,6 +655,31 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
         if (!mutual) { hf_i.clear(); hf_code.clear(); hcface.clear(); }
     }
     const int nface = (int)hf_i.size();
+    // face mode 2: greedy colouring of the faces in id order, so that no two
+    // faces of a colour touch the same element (tets: at most 7 colours)
+    std::vector<int> hf_color;
+    int ncolor = 0, fcoff[33] = {0};
+    if (nface > 0 && h->prm.face_mode == 2) {
+        std::vector<uint32_t> used((size_t)ld, 0u);
+        std::vector<int> col(nface);
+        for (int t = 0; t < nface; t++) {
+            const int i = hf_i[t], j = L.nc[(size_t)hf_code[t] * ld + i];
+            uint32_t busy = used[i] | (j < neles ? used[j] : 0u);
+            int c = 0;
+            while (c < 31 && (busy & (1u << c))) c++;   // a tet face meets at most 6 others
+            col[t] = c;
+            used[i] |= 1u << c;
+            if (j < neles) used[j] |= 1u << c;
+            ncolor = std::max(ncolor, c + 1);
+        }
+        for (int t = 0; t < nface; t++) fcoff[col[t] + 1]++;
+        for (int c = 0; c < ncolor; c++) fcoff[c + 1] += fcoff[c];
+        hf_color.assign(nface, 0);
+        std::vector<int> pos(fcoff, fcoff + ncolor);
+        for (int t = 0; t < nface; t++) hf_color[pos[col[t]]++] = t;
+    } else if (nface > 0 && h->prm.face_mode == 3) {
+        hf_color.assign(nface, 0);   // unused by the atomic scatter; keeps the array defined
+    }
     Arena& A = h->arena;
     auto plan = [&](Arena& a) { plan_arena(h, a, neles, nghosts, ld, gb, ncase, nface); };
     Arena probe;
@@ -710,8 +749,8 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     if (e == cudaSuccess) e = up(m.sc, L.sc.data(), 12 * ld * D);
     if (e == cudaSuccess) e = up(m.fch, L.fch.data(), 12 * ld * D);
     if (e == cudaSuccess) e = up(m.fcv, L.fcv.data(), 12 * ld * D);
-    if (e == cudaSuccess) e = up(m.lsqa, L.la.data(), 11 * ld * D);
-    if (e == cudaSuccess) e = up(m.lsqb, L.lb.data(), 11 * ld * D);
+    if (e == cudaSuccess) e = up(m.lsqa, L.la.data(), NLSQ * ld * D);
+    if (e == cudaSuccess) e = up(m.lsqb, L.lb.data(), NLSQ * ld * D);
     if (e == cudaSuccess && nghosts) e = up(m.g_par, L.gpar.data(), nghosts * (size_t)I);
     if (e == cudaSuccess && nghosts) e = up(m.g_id, L.gid.data(), nghosts * (size_t)I);
     if (e == cudaSuccess && nghosts) e = up(m.g_type, L.gtyp.data(), nghosts * (size_t)I);
@@ -720,6 +759,10 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     if (e == cudaSuccess && nface) e = up(m.f_i, hf_i.data(), nface * (size_t)I);
     if (e == cudaSuccess && nface) e = up(m.f_code, hf_code.data(), nface * (size_t)I);
     if (e == cudaSuccess && nface) e = up(m.cface, hcface.data(), 4 * (size_t)ld * I);
+    m.face_mode = nface > 0 ? h->prm.face_mode : 0;
+    m.ncolor = ncolor;
+    for (int c = 0; c <= ncolor; c++) m.fcoff[c] = fcoff[c];
+    if (e == cudaSuccess && nface && m.fcolor) e = up(m.fcolor, hf_color.data(), nface * (size_t)I);
     if (e == cudaSuccess && ncase > 1) {
         std::vector<int> cid(neles);
         for (int c = 0; c < ncase; c++)
@@ -1274,8 +1317,10 @@ extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, i
     const size_t gb = (params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32) ? sizeof(float)
                                                                                                 : sizeof(double);
     Arena probe;
-    const int nface = gb == sizeof(double) || params->face_mode ? 0 : (int)((4LL * mesh->neles + mesh->nghosts) / 2);
+    const int nface = gb == sizeof(double) || params->face_mode == 1 ? 0
+                                                                      : (int)((4LL * mesh->neles + mesh->nghosts) / 2);
     probe_h.neq = params->five_phase ? 22 : 10;
+    probe_h.prm.face_mode = params->face_mode;
     plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb, 1, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
@@ -1295,8 +1340,9 @@ extern "C" int hp_estimate_batch_bytes(const hp_mesh* meshes, int32_t ncase, con
     const size_t gb = (params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32) ? sizeof(float)
                                                                                                 : sizeof(double);
     Arena probe;
-    const int nface = gb == sizeof(double) || params->face_mode ? 0 : (int)((4 * ne + ng) / 2);
+    const int nface = gb == sizeof(double) || params->face_mode == 1 ? 0 : (int)((4 * ne + ng) / 2);
     probe_h.neq = params->five_phase ? 22 : 10;
+    probe_h.prm.face_mode = params->face_mode;
     plan_arena(&probe_h, probe, (int)ne, (int)ng, ld, gb, ncase, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
@@ -1471,7 +1517,8 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
         int64_t per_stage = 1 + (h->nghosts ? 1 : 0) + (h->prm.myorder == 2 ? 1 : 0) + 1;
         if (h->aliased) per_stage += (h->prm.myorder == 2 ? 1 : 0) + 1;
         if (h->dm.nfringe > 0) per_stage += 1;
-        if (h->dm.nface > 0) per_stage += 1;   // k_faceflux
+        if (h->dm.nface > 0)   // k_faceflux; or the scatter kernels of face modes 2 (one per colour), 3
+            per_stage += h->dm.face_mode == 2 ? h->dm.ncolor : 1;
         if (h->dm.nface > 0 && !h->prm.inviscid && h->var->face_visc) n += 1;   // k_vis_gather
         n += (int64_t)h->dp.nstage * per_stage + 3;
         if (h->aliased) n += 2;

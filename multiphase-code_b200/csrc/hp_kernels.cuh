@@ -116,6 +116,23 @@ __device__ __forceinline__ double mrcp(double b, unsigned& bad) {
         return 1.0 / b;
     }
 }
+// mrcp with the reciprocal taken from a set-up table (rbt = RN(1/b)
+// computed on the host): the same value and the same range flag, without
+// the division
+template <int F>
+__device__ __forceinline__ double mrcp_tab(double b, double rbt, unsigned& bad) {
+    if constexpr (F == 0) {
+        (void)b; (void)rbt; (void)bad;
+        return 0.0;
+    } else {
+        const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
+        bad |= (unsigned)(eb - 923u > 200u);
+        return rbt;
+    }
+}
+template <int F> __device__ __forceinline__ float mrcp_tab(float b, float, unsigned& bad) {
+    return mrcp<F>(b, bad);
+}
 // the mixed variant divides approximately
 template <int F> __device__ __forceinline__ float mdiv(float a, float b, float rb, unsigned&) { return a * rb; }
 template <int F> __device__ __forceinline__ float mrcp(float b, unsigned&) { return 1.0f / b; }
@@ -1304,7 +1321,7 @@ __global__ void k_flux_carry(DevMesh m, DevState<R> s, DevParams P) {
 // RK stage update of src/sr_RK.F90 fused; iblank == 1 cells.
 // FACE: the four face fluxes are gathered from k_faceflux's output (face-
 // based variants) instead of evaluated here.
-template <bool ALIASED, bool FACE, int Z>
+template <bool ALIASED, bool FACE, int Z, bool ACC = false>
 __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParams P, int stage) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
@@ -1314,7 +1331,11 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
     for (int k = 0; k < 10; k++) rhs[k] = 0.0;
     R Fg[5] = {R(0), R(0), R(0), R(0), R(0)}, Fp[5] = {R(0), R(0), R(0), R(0), R(0)};
     bool haveg = false, havep = false;
-    if constexpr (FACE) {
+    if constexpr (ACC) {
+        // face modes 2 and 3: the face sums were accumulated per cell
+#pragma unroll
+        for (int k = 0; k < 10; k++) rhs[k] = COL(s.racc, k)[i];
+    } else if constexpr (FACE) {
 #pragma unroll
         for (int f = 0; f < 4; f++) {
             const int code = ldg(COL(m.cface, f) + i);
@@ -1334,7 +1355,7 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
         }
     }
 #pragma unroll 1
-    for (int f = 0; f < 4 && !FACE; f++) {
+    for (int f = 0; f < 4 && !FACE && !ACC; f++) {
         FaceOut o;
         unsigned bad_ = 0;
         face_eval<0, Z>(m, s, P, i, f, o, bad_, s.pr);
@@ -1509,10 +1530,14 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
 #define DW(x, f) mdiv<F>((x), wt[f], rw[f], bad)
 #if HP_LSQ_TABLE
 #pragma unroll
-    for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqa, f) + i); rw[f] = mrcp<F>(wt[f], bad); }
+    for (int f = 0; f < 4; f++) {
+        wt[f] = (R)ldg(COL(m.lsqa, f) + i);
+        rw[f] = mrcp_tab<F>(wt[f], (R)ldg(COL(m.lsqa, 11 + f) + i), bad);
+    }
     const R a1 = (R)ldg(COL(m.lsqa, 4) + i), a2 = (R)ldg(COL(m.lsqa, 5) + i), a3 = (R)ldg(COL(m.lsqa, 6) + i);
     const R b1 = (R)ldg(COL(m.lsqa, 7) + i), b2 = (R)ldg(COL(m.lsqa, 8) + i), b3 = (R)ldg(COL(m.lsqa, 9) + i);
     const R dnr = (R)ldg(COL(m.lsqa, 10) + i);
+    const R rdnr_tab = (R)ldg(COL(m.lsqa, 15) + i);
 #else
 #pragma unroll
     for (int f = 0; f < 4; f++) { wt[f] = xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]; rw[f] = mrcp<F>(wt[f], bad); }
@@ -1524,7 +1549,11 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
     const R b3 = DW(za[0] * ya[0], 0) + DW(za[1] * ya[1], 1) + DW(za[2] * ya[2], 2) + DW(za[3] * ya[3], 3);
     const R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
 #endif
+#if HP_LSQ_TABLE
+    const R rdnr = mrcp_tab<F>(dnr, rdnr_tab, bad);
+#else
     const R rdnr = mrcp<F>(dnr, bad);
+#endif
     const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
     // limiter field of this lane: pg (grad field 8), pp (9), rog (11), rop (12)
     R lg[3] = {R(0), R(0), R(0)};     // gradient of the lane's limiter field
@@ -1709,7 +1738,10 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
 #define DW(x, f) mdiv<F>((x), wt[f], rw[f], bad)
 #if HP_LSQ_TABLE
 #pragma unroll
-        for (int f = 0; f < 4; f++) { wt[f] = (R)ldg(COL(m.lsqb, f) + i); rw[f] = mrcp<F>(wt[f], bad); }
+        for (int f = 0; f < 4; f++) {
+            wt[f] = (R)ldg(COL(m.lsqb, f) + i);
+            rw[f] = mrcp_tab<F>(wt[f], (R)ldg(COL(m.lsqb, 11 + f) + i), bad);
+        }
         const R a1 = (R)ldg(COL(m.lsqb, 4) + i), a2 = (R)ldg(COL(m.lsqb, 5) + i), a3 = (R)ldg(COL(m.lsqb, 6) + i);
         const R b1 = (R)ldg(COL(m.lsqb, 7) + i), b2 = (R)ldg(COL(m.lsqb, 8) + i), b3 = (R)ldg(COL(m.lsqb, 9) + i);
 #else
@@ -1737,7 +1769,12 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         const R A11 = q == 0 ? c1 : a1, A21 = q == 0 ? c2 : b1, A31 = q == 0 ? c3 : b2;
         const R A12 = q == 1 ? c1 : b1, A22 = q == 1 ? c2 : a2, A32 = q == 1 ? c3 : b3;
         const R A13 = q >= 2 ? c1 : b2, A23 = q >= 2 ? c2 : b3, A33 = q >= 2 ? c3 : a3;
+#if HP_LSQ_TABLE
+        const R rdnr = mrcp_tab<F>(dnr, (R)ldg(COL(m.lsqb, 15) + i), bad);
+        const R dq = mdiv<F>(det3(A11, A21, A31, A12, A22, A32, A13, A23, A33), dnr, rdnr, bad);
+#else
         const R dq = det3(A11, A21, A31, A12, A22, A32, A13, A23, A33) / dnr;
+#endif
         const R dpx = qshfl(dq, 0), dpy = qshfl(dq, 1), dpz = qshfl(dq, 2);
 #undef DW
 #define DW(x, f) div_rn((x), wt[f], rw[f])
@@ -1835,6 +1872,46 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_faceflux(DevMesh m, DevS
     rec[10] = o.wall ? R(1) : R(0);
     rec[11] = R(0);
     store_frec(s.ff + (size_t)FACE_REC * (size_t)t, rec);
+}
+
+// Face modes 2 and 3: each face evaluated once, its flux added to the owner's
+// accumulator and subtracted from the other cell's (a ghost has none).
+// ATOMIC = false: the faces fids[0, n) of one colour, which share no cell;
+// ATOMIC = true: every face, with atomic adds (the order of the additions,
+// and so the last bits of the sums, vary from run to run).
+template <int Z, bool ATOMIC>
+__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_facescatter(DevMesh m, DevState<R> s, DevParams P,
+                                                                     const int* fids, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int fid = ATOMIC ? t : ldg(fids + t);
+    const int i = ldg(m.f_i + fid), f = ldg(m.f_code + fid) & 3;
+    const int j = ldg(COL(m.nc, f) + i);
+    FaceOut o{};
+    unsigned bad = 0;
+    face_eval<0, Z>(m, s, P, i, f, o, bad, s.prr);
+    double e[10];
+    if (o.wall) {
+#pragma unroll
+        for (int k = 0; k < 10; k++) e[k] = 0.0;
+        e[1] = o.w[0]; e[2] = o.w[1]; e[3] = o.w[2];
+        e[6] = o.w[3]; e[7] = o.w[4]; e[8] = o.w[5];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 10; k++) e[k] = (double)o.F[k];
+    }
+    const bool other = j < m.neles;
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+        double* acc = COL(s.racc, k);
+        if (ATOMIC) {
+            atomicAdd(acc + i, e[k]);
+            if (other) atomicAdd(acc + j, -e[k]);
+        } else {
+            acc[i] = acc[i] + e[k];
+            if (other) acc[j] = acc[j] - e[k];
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2449,6 +2526,17 @@ static void enqueue_flux(const DevMesh& m, const DevState<R>& s, const DevParams
         k_flux<true, false, Z><<<gf, b, 0, st>>>(m, s, P, stage);
         MARK(KK_SERIAL);
         k_flux_carry<Z><<<1, 1, 0, st>>>(m, s, P);
+    } else if (sizeof(R) != sizeof(double) && m.nface > 0 && m.face_mode >= 2) {
+        cudaMemsetAsync(s.racc, 0, 10 * (size_t)m.ld * sizeof(double), st);
+        if (m.face_mode == 3) {
+            k_facescatter<Z, true><<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P, m.fcolor, m.nface);
+        } else {
+            for (int c = 0; c < m.ncolor; c++) {
+                const int n = m.fcoff[c + 1] - m.fcoff[c];
+                k_facescatter<Z, false><<<grid_for(n, 128), 128, 0, st>>>(m, s, P, m.fcolor + m.fcoff[c], n);
+            }
+        }
+        k_flux<false, false, Z, true><<<gf, 128, 0, st>>>(m, s, P, stage);
     } else if (sizeof(R) != sizeof(double) && m.nface > 0) {
         k_faceflux<Z><<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
         k_flux<false, true, Z><<<gf, 128, 0, st>>>(m, s, P, stage);

@@ -6,10 +6,13 @@ Two levels are tuned:
 * **Kernels** (`tune_block_size`, `tune_face_mode`). These are the threads
   per block of the one-thread-per-cell kernels (primitive recovery, JST
   smoothing, ghost fill, and the gradients and face gathers of the
-  FP32-arithmetic variants) and, for those variants, whether the HLLC and
-  viscous fluxes are evaluated once per face (a face list, one thread per
-  face, then a per-cell gather) or once from each side (four lanes per cell,
-  one kernel fewer per stage). Every candidate runs device-timed steps (CUDA
+  FP32-arithmetic variants) and, for those variants, how the HLLC fluxes
+  reach the cells: once per face with the face records gathered per cell in
+  face order (mode 0), once from each side with four lanes per cell (mode 1,
+  one kernel fewer per stage), once per face added to per-cell sums colour by
+  colour so that no two faces of a launch share a cell (mode 2: colouring, no
+  atomics, a fixed order) or, when the caller accepts sums whose last bits
+  vary between runs, with atomic adds (mode 3). Every candidate runs device-timed steps (CUDA
   events) of a representative case of the class: the best of three runs from
   the initial state, each of at least 20 ms (up to 200 steps).  The fastest
   is kept. The four-lane kernels have their block size fixed by their launch
@@ -119,19 +122,23 @@ def tune_block_size(spec, precision: int = PREC_MIXED, candidates=BLOCK_CANDIDAT
 
 
 def tune_face_mode(spec, precision: int = PREC_MIXED, block_size: int = 0, steps: int = 6,
-                   use_cache: bool = True) -> tuple[int, dict]:
+                   use_cache: bool = True, deterministic: bool = True) -> tuple[int, dict]:
     """hp_params.face_mode for the size class of `spec` in the
-    FP32-arithmetic variants: 0 (once per face) or 1 (once from each side);
-    returns (best, {mode: ms per step}).  The FP64 variants have one mode."""
+    FP32-arithmetic variants: 0 (once per face, records gathered per cell),
+    1 (once from each side), 2 (once per face, per-cell sums colour by
+    colour) and, unless `deterministic`, 3 (once per face, atomic sums, whose
+    last bits vary between runs); returns (best, {mode: ms per step}).  The
+    FP64 variants have one mode."""
     if precision not in (PREC_MIXED, PREC_FP32):
         return 0, {}
-    key = _key(precision, size_class(spec.mesh.neles), f"face_mode_b{block_size}")
+    modes = (0, 1, 2) if deterministic else (0, 1, 2, 3)
+    key = _key(precision, size_class(spec.mesh.neles), f"face_mode_b{block_size}" + ("" if deterministic else "_a"))
     if use_cache:
         hit = _load().get(key)
         if hit:
             return int(hit["best"]), {int(k): v for k, v in hit["ms"].items()}
     ms = {}
-    for mode in (0, 1):
+    for mode in modes:
         with Case(spec.mesh, spec.params(precision=precision, block_size=int(block_size), face_mode=mode)) as c:
             ms[mode] = _ms_per_step(c, spec, steps)
     best = min(ms, key=ms.get)

@@ -148,6 +148,24 @@ def test_mixed_within_tolerance(face_mode):
     assert err[4] < 1e-5, err
 
 
+@pytest.mark.parametrize("face_mode", [2, 3])
+def test_mixed_colouring_and_atomics_within_tolerance(face_mode):
+    """Face modes 2 (per-cell sums colour by colour) and 3 (atomic sums):
+    each face once in FP32, summed in another order than face order; the
+    mixed bar of the gather mode holds.  Mode 2 is deterministic: two runs
+    are bit-identical."""
+    spec = SPECS["cylinder"]()
+    _, _, _, cu_o, _ = _oracle_run(spec, 5)
+    _, _, cu_g, _ = _gpu_run(spec, 5, PREC_MIXED, face_mode=face_mode)
+    rho_o, rho_g = cu_o[0] + cu_o[5], cu_g[0] + cu_g[5]
+    assert np.linalg.norm(rho_g - rho_o) / np.linalg.norm(rho_o) < 1e-5
+    err = _rel_l2(cu_g, cu_o)
+    assert err[4] < 1e-5, err
+    if face_mode == 2:
+        _, _, cu_2, _ = _gpu_run(spec, 5, PREC_MIXED, face_mode=face_mode)
+        np.testing.assert_array_equal(cu_2, cu_g)
+
+
 def test_graph_and_eager_identical():
     spec = SPECS["shock_bubble_ref"]()
     _, _, a, _ = _gpu_run(spec, 4, PREC_FP64_PARITY, use_graph=1)

@@ -103,6 +103,9 @@ def test_face_mode_tuner_measures_and_caches(tmp_path, monkeypatch):
     monkeypatch.setenv("HYDRAPHASE_TUNE_CACHE", str(tmp_path / "t.json"))
     spec = cases.shock_bubble(n=8, alpha_min=0.1)
     best, ms = tune.tune_face_mode(spec, steps=2)
+    assert set(ms) == {0, 1, 2}                     # gather, each side, colouring
+    _, ms_a = tune.tune_face_mode(spec, steps=2, deterministic=False)
+    assert set(ms_a) == {0, 1, 2, 3}                # and atomics
     assert best in (0, 1) and set(ms) == {0, 1}
     assert tune.tune_face_mode(spec, steps=2) == (best, ms)
     assert tune.tune_face_mode(spec, precision=PREC_FP64_PARITY) == (0, {})
