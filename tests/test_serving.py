@@ -106,6 +106,6 @@ def test_face_mode_tuner_measures_and_caches(tmp_path, monkeypatch):
     assert set(ms) == {0, 1, 2}                     # gather, each side, colouring
     _, ms_a = tune.tune_face_mode(spec, steps=2, deterministic=False)
     assert set(ms_a) == {0, 1, 2, 3}                # and atomics
-    assert best in (0, 1) and set(ms) == {0, 1}
+    assert best in (0, 1, 2)
     assert tune.tune_face_mode(spec, steps=2) == (best, ms)
     assert tune.tune_face_mode(spec, precision=PREC_FP64_PARITY) == (0, {})
