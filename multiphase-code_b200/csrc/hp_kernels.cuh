@@ -79,6 +79,11 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 #ifndef HP_FACE_VISC
 #define HP_FACE_VISC 1
 #endif
+// FP64 gradients and limiter with eight lanes per cell (k_grad8) instead of
+// four (k_grad4)
+#ifndef HP_GRAD_SPLIT
+#define HP_GRAD_SPLIT 1
+#endif
 // viscous fluxes of the cell-centric variants with eight lanes per cell (one
 // phase each, k_visc8) instead of four (k_visc4)
 #ifndef HP_VISC_SPLIT
@@ -1060,10 +1065,17 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     // variants therefore start from the cell's own alpha_p (recovered in FP64)
     // and subtract the reconstruction increment of alpha_g, which is the same
     // quantity mathematically and keeps alpha_p to FP32 relative precision.
+    // With dispersed phases alpha_g + alpha_p = 1 - their fractions, and the
+    // reference still takes 1 - alpha_g: formed here in FP64 from alpha_g.
     R phipL = R(0), phipR = R(0);
     if constexpr (sizeof(R) == 4) {
-        phipL = (R)PLD(COL(pr, P_PHIP) + i);
-        phipR = (R)PLD(COL(pr, P_PHIP) + neigh);
+        if (P.five_phase) {
+            phipL = (R)(1.0 - PLD(COL(s.pr, P_PHIG) + i));
+            phipR = (R)(1.0 - PLD(COL(s.pr, P_PHIG) + neigh));
+        } else {
+            phipL = (R)PLD(COL(pr, P_PHIP) + i);
+            phipR = (R)PLD(COL(pr, P_PHIP) + neigh);
+        }
     }
     if (P.myorder == 2 && (kind & FK_RECON)) {
         const R phimin = (R)mn2(PLD(s.phi + i), PLD(s.phi + neigh));
@@ -1399,12 +1411,16 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
         // alpha_g (alpha_g - 1) and 1 - alpha_g in the reference's form in
         // FP64; from alpha_p in FP32, where the differences would cancel
         // (see face_eval)
-        R drag;
-        if constexpr (sizeof(R) == 4)
-            drag = -(R(0.44) * phig * phip) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
-        else
+        // (with dispersed phases alpha_p is not 1 - alpha_g, which FP32 then
+        // forms in FP64)
+        R drag, omg;
+        if constexpr (sizeof(R) == 4) {
+            omg = P.five_phase ? (R)(1.0 - COL(s.pr, P_PHIG)[i]) : phip;
+            drag = -(R(0.44) * phig * omg) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        } else {
+            omg = R(1) - phig;
             drag = R(0.44) * phig * (phig - R(1)) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
-        const R omg = sizeof(R) == 4 ? phip : R(1) - phig;
+        }
         const R fdgx = drag * du, fdgy = drag * dv, fdgz = drag * dw;
         const R qsource = R(6) * phip * amug * (R)P.cpg * R(2) * (tp - tg) / ((R)P.prg * (dl * dl));
         const R delpstar = R(2) * (phig * rog * phip * rop) / (phig * rop + phip * rog) *
@@ -1631,6 +1647,118 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
     }
 }
 
+// Value of lane q of this thread's group of eight consecutive lanes.
+template <class T>
+__device__ __forceinline__ T oshfl(T v, int q) {
+    return __shfl_sync(0xffffffffu, v, (int)((threadIdx.x & 31) & ~7u) + q);
+}
+
+// k_grad4 with eight lanes per cell: lane L computes the gradients of fields
+// L and L + 8 (pg, pp, phig, rog, rop for L = 0..4), and lanes 0, 1, 3, 4 the
+// limiter of the second of them (pg, pp, rog, rop); phi is the minimum in
+// that field order, as in k_grad4.  Each field's gradient and each limiter
+// value is formed exactly as in grad4_body; half of a lane's work, so about
+// half of its live state.
+#ifndef HP_GRAD8_MINB
+#define HP_GRAD8_MINB 5
+#endif
+template <int F>
+__device__ __forceinline__ unsigned grad8_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int i,
+                                               int L, bool active) {
+    unsigned bad = 0;
+    int n[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
+    const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
+    R xa[4], ya[4], za[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        xa[f] = (R)(ldg(m.xc + n[f]) - x0);
+        ya[f] = (R)(ldg(m.yc + n[f]) - y0);
+        za[f] = (R)(ldg(m.zc + n[f]) - z0);
+    }
+    R wt[4], rw[4];
+#undef DW
+#define DW(x, f) mdiv<F>((x), wt[f], rw[f], bad)
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        wt[f] = (R)ldg(COL(m.lsqa, f) + i);
+        rw[f] = mrcp_tab<F>(wt[f], (R)ldg(COL(m.lsqa, 11 + f) + i), bad);
+    }
+    const R a1 = (R)ldg(COL(m.lsqa, 4) + i), a2 = (R)ldg(COL(m.lsqa, 5) + i), a3 = (R)ldg(COL(m.lsqa, 6) + i);
+    const R b1 = (R)ldg(COL(m.lsqa, 7) + i), b2 = (R)ldg(COL(m.lsqa, 8) + i), b3 = (R)ldg(COL(m.lsqa, 9) + i);
+    const R dnr = (R)ldg(COL(m.lsqa, 10) + i);
+    const R rdnr = mrcp_tab<F>(dnr, (R)ldg(COL(m.lsqa, 15) + i), bad);
+    const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
+    R lg[3] = {R(0), R(0), R(0)};     // gradient of the lane's limiter field
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int v = L + 8 * r;
+        if (v >= 13) break;
+        const R* qq = COL(s.prr, pcol[v]);
+        R qi = qq[i];
+        R qa = (R)(qq[n[0]] - qi), qb = (R)(qq[n[1]] - qi), qc = (R)(qq[n[2]] - qi), qd = (R)(qq[n[3]] - qi);
+        R c1 = DW(qa * xa[0], 0) + DW(qb * xa[1], 1) + DW(qc * xa[2], 2) + DW(qd * xa[3], 3);
+        R c2;
+        if (v == 7)   // cTp2 lacks the /wt4 (src/sr_derivative.F90:225)
+            c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + qd * ya[3];
+        else
+            c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + DW(qd * ya[3], 3);
+        R c3 = DW(qa * za[0], 0) + DW(qb * za[1], 1) + DW(qc * za[2], 2) + DW(qd * za[3], 3);
+        R gx = mdiv<F>(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr, bad);
+        R gy = mdiv<F>(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr, bad);
+        R gz = mdiv<F>(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr, bad);
+        if (v < 11 && active) {
+            COL(s.gr, 3 * v + 0)[i] = gx;
+            COL(s.gr, 3 * v + 1)[i] = gy;
+            COL(s.gr, 3 * v + 2)[i] = gz;
+        }
+        if (r == 1) { lg[0] = gx; lg[1] = gy; lg[2] = gz; }
+    }
+#undef DW
+#define DW(x, f) div_rn((x), wt[f], rw[f])
+    R phl = R(1);
+    if (L <= 4 && L != 2) {
+        const int lcol = L == 0 ? P_PG : L == 1 ? P_PP : L == 3 ? P_ROG : P_ROP;
+        const R epssq = (R)ldg(m.eps2 + i);
+        const R* qq = COL(s.prr, lcol);
+        R qi = qq[i];
+        R vmax = mx2(mx2(mx2(mx2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
+        R vmin = mn2(mn2(mn2(mn2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
+        R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            R fx = (R)(ldg(COL(m.fch, f) + i) - x0);
+            R fy = (R)(ldg(COL(m.fch, 4 + f) + i) - y0);
+            R fz = (R)(ldg(COL(m.fch, 8 + f) + i) - z0);
+            R d = fx * lg[0] + fy * lg[1] + fz * lg[2];
+            R ph;
+            if (d > R(0)) ph = fvenkat(dmax, d, epssq);
+            else if (d < R(0)) ph = fvenkat(dmin, d, epssq);
+            else ph = R(1);
+            phl = (f == 0) ? ph : mn2(phl, ph);
+        }
+    }
+    R p0 = oshfl(phl, 0), p1 = oshfl(phl, 1), p3 = oshfl(phl, 3), p4 = oshfl(phl, 4);
+    if (L == 0 && active) s.phi[i] = (double)mn2(mn2(mn2(p0, p1), p3), p4);
+    return bad;
+}
+
+__global__ void __launch_bounds__(128, HP_GRAD8_MINB) k_grad8(DevMesh m, DevState<R> s, DevParams P) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int L = (int)(gt & 7);
+    int i = (int)(gt >> 3);
+    const bool valid = i < m.neles;
+    if (!valid) i = m.neles - 1;
+    const bool active = valid && grad_cell(ldg(m.iblank + i));
+    if constexpr (HP_FAST(1)) {
+        const unsigned bad = grad8_body<1>(m, s, P, i, L, active);
+        if (__any_sync(0xffffffffu, bad)) grad8_body<0>(m, s, P, i, L, active);
+    } else {
+        grad8_body<0>(m, s, P, i, L, active);
+    }
+}
+
 // Residual + sources + RK update with four lanes per cell: lane q evaluates
 // face q; every lane re-assembles the residual in face order and computes
 // the sources; lane q writes variables q, q+4, q+8.  F selects the division
@@ -1713,12 +1841,16 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         // alpha_g (alpha_g - 1) and 1 - alpha_g in the reference's form in
         // FP64; from alpha_p in FP32, where the differences would cancel
         // (see face_eval)
-        R drag;
-        if constexpr (sizeof(R) == 4)
-            drag = -(R(0.44) * phig * phip) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
-        else
+        // (with dispersed phases alpha_p is not 1 - alpha_g, which FP32 then
+        // forms in FP64)
+        R drag, omg;
+        if constexpr (sizeof(R) == 4) {
+            omg = P.five_phase ? (R)(1.0 - COL(s.pr, P_PHIG)[i]) : phip;
+            drag = -(R(0.44) * phig * omg) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
+        } else {
+            omg = R(1) - phig;
             drag = R(0.44) * phig * (phig - R(1)) * rog * sqrt(du * du + dv * dv + dw * dw) * dl;
-        const R omg = sizeof(R) == 4 ? phip : R(1) - phig;
+        }
         const R fdgx = drag * du, fdgy = drag * dv, fdgz = drag * dw;
         const R qsource = R(6) * phip * amug * (R)P.cpg * R(2) * (tp - tg) / ((R)P.prg * (dl * dl));
         const R delpstar = R(2) * (phig * rog * phip * rop) / (phig * rop + phip * rog) *
@@ -2613,6 +2745,7 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             MARK(KK_GRAD);
             if (m.aliased) k_grad<false><<<gf, b, 0, st>>>(m, s, P);
             else if (sizeof(R) != sizeof(double)) k_grad<true><<<gf, b, 0, st>>>(m, s, P);
+            else if (HP_GRAD_SPLIT && HP_LSQ_TABLE) k_grad8<<<grid_for(8ll * m.neles, 128), 128, 0, st>>>(m, s, P);
             else k_grad4<<<g4, 128, 0, st>>>(m, s, P);
             if (m.aliased) { MARK(KK_SERIAL); k_phi_copy_serial<<<1, 1, 0, st>>>(m, s); }
         }

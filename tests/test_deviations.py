@@ -15,7 +15,10 @@ finite.
 Config 2 (viscous cylinder): with the reference's convective time step
 (src/main.F90:541-555) the first cell layer at the no-slip wall goes NaN at
 CFL 0.5.  A reduced O-grid of the same wall spacing (40 x 64 x 4 hexes,
-61,440 tets) shows it at step 157; at CFL 0.25 it stays finite.
+61,440 tets) shows it at step 157; at CFL 0.25 it stays finite.  Its
+droplets as stated (alpha_w = 1 - 1e-6 inside, 1e-6 outside) give NaN cells
+in the first step on the full 4,915,200-cell mesh, at CFL 0.25 too, all of
+them inside droplets: the same interface contrast as config 1.
 """
 import os
 
@@ -128,3 +131,21 @@ def test_cylinder_cfl025_stays_finite():
     orc = _oracle(spec, threads=os.cpu_count() or 1, cfl=0.25)
     assert _first_nan_step(orc, spec.mesh.neles, 320) is None
     orc.close()
+
+
+@pytest.mark.slow
+def test_cylinder_stated_droplets_fail_in_first_step():
+    spec = cases.cylinder()
+    assert spec.mesh.neles == 4915200
+    spec.flow["cfl"] = 0.25
+    orc = _oracle(spec, threads=os.cpu_count() or 1)
+    orc.run(1)
+    bad = _nan_cells(orc, spec.mesh.neles)
+    orc.close()
+    assert bad.sum() > 10
+    # the droplet centres of cases.cylinder (seed 1, 32 droplets of radius 0.1)
+    rng = np.random.default_rng(1)
+    dc = np.stack([rng.uniform(-8, -3, 32), rng.uniform(-2, 2, 32), rng.uniform(0.1, 3.9, 32)], axis=1)
+    xc = _centroids(spec.mesh)[bad]
+    dist = np.sqrt(((xc[:, None, :] - dc[None]) ** 2).sum(-1)).min(axis=1)
+    assert np.all(dist < 0.1)
