@@ -111,6 +111,9 @@ class ClockSampler:
 # from the wall outwards), while CFL 0.25 runs 1000 steps. The cost of a step
 # does not depend on the CFL.
 CYL_CFL = 0.25
+# FP64 wall layers of the second mixed measurement (hp_params.wall_fp64_layers):
+# breadth-first tet layers from the cylinder wall
+MIXED_WALL_LAYERS = 96
 
 
 def make_workload(name: str, seed_offset: int = 0):
@@ -421,20 +424,30 @@ def stress_measure(steps: int) -> dict:
             "cells": spec.mesh.neles, "steps": steps, **res}
 
 
-def accuracy_run(spec, steps: int) -> dict:
-    """The mixed variant against the FP64 parity variant after `steps` steps
-    from the same initial state, on the timed workload (rel L2 of mixture
-    density, alpha_g and the conserved variables), with the NaN cells of
-    both final states."""
-    from hydraphase import PREC_FP64_PARITY, PREC_MIXED, Case
+def accuracy_run(spec, steps: int, wall_layers: int = 0) -> dict:
+    """The mixed variant (and, with wall_layers > 0, the mixed variant with
+    that many FP64 wall layers) against the FP64 parity variant after
+    `steps` steps from the same initial state, on the timed workload (rel L2
+    of mixture density, alpha_g and the conserved variables), with the FP64
+    FMA variant's distance as the rounding floor and the NaN cells of every
+    final state."""
+    from hydraphase import PREC_FP64, PREC_FP64_PARITY, PREC_MIXED, Case
+    runs = [("fp64", PREC_FP64_PARITY, {}), ("fp64_fma", PREC_FP64, {}), ("mixed", PREC_MIXED, {})]
+    if wall_layers > 0:
+        runs.append(("mixed_wall", PREC_MIXED, {"wall_fp64_layers": wall_layers}))
     states = {}
-    for name, prec in (("fp64", PREC_FP64_PARITY), ("mixed", PREC_MIXED)):
-        with Case(spec.mesh, spec.params(precision=prec)) as c:
+    for name, prec, over in runs:
+        with Case(spec.mesh, spec.params(precision=prec, **over)) as c:
             c.set_state(0.0, spec.cu, spec.ghost_prims)
             c.step(steps, diagnostics=False)
             _, states[name], _ = c.state()
-    return {"steps": steps, "rel_l2_vs_fp64": accuracy(states["mixed"], states["fp64"], spec.flow),
-            "nan_cells": {k: int((~np.isfinite(v)).any(axis=0).sum()) for k, v in states.items()}}
+    out = {"steps": steps, "rel_l2_vs_fp64": accuracy(states["mixed"], states["fp64"], spec.flow),
+           "fma_floor_rel_l2_vs_fp64": accuracy(states["fp64_fma"], states["fp64"], spec.flow),
+           "nan_cells": {k: int((~np.isfinite(v)).any(axis=0).sum()) for k, v in states.items()}}
+    if wall_layers > 0:
+        out["wall_layers"] = wall_layers
+        out["mixed_wall_rel_l2_vs_fp64"] = accuracy(states["mixed_wall"], states["fp64"], spec.flow)
+    return out
 
 
 def output_measure(steps: int = 300) -> dict:
@@ -499,11 +512,11 @@ def run_reference_arm(args, world, rank, pg):
     return 0
 
 
-def measure_variant(spec, precision, steps, warmup, pg, device):
+def measure_variant(spec, precision, steps, warmup, pg, device, **over):
     """Device-timed steps of one precision variant; returns numbers and the
     final state (for accuracy comparison)."""
     from hydraphase import Case
-    p = spec.params(precision=precision)
+    p = spec.params(precision=precision, **over)
     c = Case(spec.mesh, p)
     c.set_state(0.0, spec.cu, spec.ghost_prims)
     c.step(warmup, diagnostics=False)
@@ -551,6 +564,12 @@ def run_ours(args, world, rank, local, pg):
     tmx = barrier_max(pg, msmx, device) / 1e3
     value_mx = barrier_sum(pg, float(cells * stages * args.steps), device) / tmx
     acc_mx = accuracy(cumx, cu64, spec.flow)
+    # the same with the cells near the walls in FP64
+    wl = args.mixed_wall_layers
+    if wl > 0:
+        msmw, infomw, _, cumw, _ = measure_variant(spec, PREC_MIXED, args.steps, args.warmup, pg, device,
+                                                   wall_fp64_layers=wl)
+        value_mw = barrier_sum(pg, float(cells * stages * args.steps), device) / (barrier_max(pg, msmw, device) / 1e3)
 
     # --- end to end through the public API with host buffers -------------
     # inputs and results in pinned host memory, as a caller that streams
@@ -617,10 +636,16 @@ def run_ours(args, world, rank, local, pg):
                   "dtype": "f32 fluxes/gradients, f64 state/EOS/reductions"},
         "nan_cells_after": float(d64["nan_cells"][0]),
     }
+    if wl > 0:
+        line["mixed_wall"] = {"wall_fp64_layers": wl, "value": value_mw, "ms_per_step": msmw / args.steps,
+                              "speedup_vs_fp64": value_mw / value,
+                              "rel_l2_vs_fp64_after_steps": accuracy(cumw, cu64, spec.flow),
+                              "kernels_per_step": infomw["kernels_per_step"],
+                              "dtype": "mixed; FP64 in the cells within wall_fp64_layers layers of the wall"}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(spec, args.workload, os.cpu_count() or 1)
     if world == 1 and rank == 0 and args.accuracy_steps > 0:
-        line["mixed"]["accuracy"] = accuracy_run(spec, args.accuracy_steps)
+        line["mixed"]["accuracy"] = accuracy_run(spec, args.accuracy_steps, wl)
     if world == 1 and rank == 0 and not args.no_overset:
         line["overset"] = overset_measure(max(args.steps // 2, 5))
     if world == 1 and rank == 0 and args.partition_parts > 1:
@@ -710,6 +735,8 @@ def main():
                          "(instead of one replica per rank)")
     ap.add_argument("--stress-steps", type=int, default=2000,
                     help="steps of the config-5 precision stress run in three precisions (0: skip)")
+    ap.add_argument("--mixed-wall-layers", type=int, default=MIXED_WALL_LAYERS,
+                    help="FP64 wall layers of the second mixed measurement (0: skip it)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy run on the timed workload (0: skip)")
     args = ap.parse_args()

@@ -93,6 +93,11 @@ typedef struct hp_params {
     double rhoq, rhor, rhos; /* dispersed-phase densities */
     double radq, radr, rads; /* particle radii */
     double phiginit, phipinit, phiqinit, phirinit, phisinit;  /* start fractions */
+    /* FP32-arithmetic precisions (mixed, fp32): the cells within this many
+     * layers of a wall ghost (types 5 and 6) take their viscous terms,
+     * fluxes, sources and RK update from the FP64 kernels (0: none).  Not
+     * with aliased ghost ids.  The FP64 precisions ignore it. */
+    int32_t wall_fp64_layers;
 } hp_params;
 
 /* Mesh as the reference reads it (src/sr_geometry.F90:101-139):

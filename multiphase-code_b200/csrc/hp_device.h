@@ -103,6 +103,16 @@ struct DevMesh {
     int nhalo;
     const int* hdst;
     const int* hsrc;
+    // FP64 wall layers of the FP32-arithmetic variants (nwall = 0: none):
+    // the cells within a few layers of a wall ghost (wcells, ascending) take
+    // their viscous terms, fluxes, sources and RK update from the FP64
+    // kernels over these lists; gcells adds their interior neighbours, whose
+    // FP64 gradients those fluxes reconstruct from; wclass[i] = 1 marks the
+    // cells of wcells, which the FP32 kernels leave alone
+    int nwall, ngwall;
+    const int* wcells;
+    const int* gcells;
+    const unsigned char* wclass;   // [ld]
 };
 
 // Per-case scalars (one entry per case of the handle).
@@ -145,7 +155,31 @@ struct DevState {
     DevScalars* s;
     double* diag;            // [max_steps][8]
     int max_diag;
+    double* gr64;            // [33][ld] FP64 gradients of the wall layers
+                             // (FP32 variants with nwall > 0; else null)
 };
+
+// The FP64 view of an FP32-arithmetic state for the wall-layer kernels: the
+// FP64 primitives as their primitives and gr64 as their gradients; every
+// other array is shared.
+template <class R>
+inline DevState<double> fp64_view(const DevState<R>& s) {
+    DevState<double> v;
+    v.cn = s.cn; v.cu = s.cu; v.cn1 = s.cn1; v.pr = s.pr; v.prr = s.pr; v.gr = s.gr64; v.phi = s.phi;
+    v.anu = s.anu; v.d2q = s.d2q; v.d24 = s.d24; v.vis = s.vis; v.egt = s.egt;
+    v.qpr = s.qpr; v.anuq = s.anuq; v.qdrag = s.qdrag; v.racc = s.racc; v.ff = nullptr;
+    v.s = s.s; v.diag = s.diag; v.max_diag = s.max_diag; v.gr64 = s.gr64;
+    return v;
+}
+
+// FP64 kernels over the wall-layer lists, provided by the FP64 variant and
+// called by the FP32-arithmetic variants' step.
+struct WallFp64 {
+    void (*visc)(const DevMesh&, const DevState<double>&, const DevParams&, cudaStream_t);
+    void (*grad)(const DevMesh&, const DevState<double>&, const DevParams&, cudaStream_t);
+    void (*flux)(const DevMesh&, const DevState<double>&, const DevParams&, cudaStream_t, int stage);
+};
+extern const WallFp64 wall_fp64;
 
 // Kernel kinds, for per-kernel timing (hp_profile_steps).
 enum KernelKind {

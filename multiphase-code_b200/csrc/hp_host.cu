@@ -103,6 +103,7 @@ struct hp_handle {
     std::vector<char> state_set;   // per case: state uploaded
     int aliased = 0;
     int neq = 10;               // conserved variables: 10, or 22 with the five-phase model
+    int nwall = 0, ngwall = 0;  // FP64 wall-layer cells and their gradient cells
     int max_diag = 4096;
     std::string err;
     double* h_diag = nullptr;   // pinned
@@ -208,6 +209,17 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     s.diag = (double*)a.take((size_t)ncase * h->max_diag * 8 * D);
     s.max_diag = h->max_diag;
     m.cid = ncase > 1 ? (const int*)a.take((size_t)neles * I) : nullptr;
+    m.nwall = h->nwall; m.ngwall = h->ngwall;
+    if (h->nwall > 0) {
+        m.wcells = (const int*)a.take((size_t)h->nwall * I);
+        m.gcells = (const int*)a.take((size_t)h->ngwall * I);
+        m.wclass = (const unsigned char*)a.take((size_t)ld);
+        s.gr64 = (double*)a.take(NGR * ld * D);
+    } else {
+        m.wcells = m.gcells = nullptr;
+        m.wclass = nullptr;
+        s.gr64 = nullptr;
+    }
     m.nface = nface;
     m.fld = ((long long)nface + 63) / 64 * 64;
     s.racc = nullptr;
@@ -246,6 +258,52 @@ struct Layout {
         la.assign(NLSQ * ld, 0.0); lb.assign(NLSQ * ld, 0.0);
     }
 };
+
+// Cells within `layers` layers of a wall ghost (types 5 and 6), breadth
+// first over the interior neighbours: wall (ascending), the same with their
+// interior neighbours added (grad, ascending), and the per-slot class (1:
+// wall layer).
+static void wall_layers(const Layout& L, int neles, int nghosts, long long ld, int layers,
+                        std::vector<int>& wall, std::vector<int>& grad, std::vector<unsigned char>& cls) {
+    std::vector<int> gtype((size_t)nghosts, 0);
+    for (int g = 0; g < nghosts; g++) {
+        const int t = L.gid[g];
+        if (t >= neles && t < neles + nghosts) gtype[t - neles] = L.gtyp[g];
+    }
+    std::vector<int> layer((size_t)neles, 0), front;
+    for (int t = 0; t < neles; t++)
+        for (int f = 0; f < 4; f++) {
+            const int j = L.nc[(size_t)f * ld + t];
+            if (j >= neles && j < neles + nghosts && (gtype[j - neles] == 5 || gtype[j - neles] == 6)) {
+                layer[t] = 1;
+                front.push_back(t);
+                break;
+            }
+        }
+    for (int k = 2; k <= layers && !front.empty(); k++) {
+        std::vector<int> next;
+        for (int t : front)
+            for (int f = 0; f < 4; f++) {
+                const int j = L.nc[(size_t)f * ld + t];
+                if (j < neles && layer[j] == 0) { layer[j] = k; next.push_back(j); }
+            }
+        front.swap(next);
+    }
+    cls.assign((size_t)ld, 0);
+    std::vector<unsigned char> ing((size_t)neles, 0);
+    for (int t = 0; t < neles; t++)
+        if (layer[t] > 0) {
+            wall.push_back(t);
+            cls[t] = 1;
+            ing[t] = 1;
+            for (int f = 0; f < 4; f++) {
+                const int j = L.nc[(size_t)f * ld + t];
+                if (j < neles) ing[j] = 1;
+            }
+        }
+    for (int t = 0; t < neles; t++)
+        if (ing[t]) grad.push_back(t);
+}
 
 // One case of a handle: validates its connectivity, computes its geometry
 // and static least-squares terms, picks its internal cell order and writes
@@ -530,6 +588,7 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
         return fail(nullptr, HP_E_ARG, "block_size must be 0 or a multiple of 32 in [64, 512]");
     if (params->face_mode < 0 || params->face_mode > 3)
         return fail(nullptr, HP_E_ARG, "face_mode must be 0 (face records), 1 (each side), 2 (colouring) or 3 (atomics)");
+    if (params->wall_fp64_layers < 0) return fail(nullptr, HP_E_ARG, "wall_fp64_layers must be >= 0");
     if (params->five_phase) {
         if (!(params->rhoq > 0 && params->rhor > 0 && params->rhos > 0 && params->radq > 0 && params->radr > 0 &&
               params->rads > 0))
@@ -680,6 +739,18 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     } else if (nface > 0 && h->prm.face_mode == 3) {
         hf_color.assign(nface, 0);   // unused by the atomic scatter; keeps the array defined
     }
+    // --- FP64 wall layers of the FP32-arithmetic variants ---
+    std::vector<int> hwall, hgwall;
+    std::vector<unsigned char> hwclass;
+    if (gb != D && p.wall_fp64_layers > 0) {
+        if (h->aliased) {
+            delete h;
+            return fail(nullptr, HP_E_UNSUPPORTED, "FP64 wall layers: aliased ghost ids");
+        }
+        wall_layers(L, neles, nghosts, ld, p.wall_fp64_layers, hwall, hgwall, hwclass);
+    }
+    h->nwall = (int)hwall.size();
+    h->ngwall = (int)hgwall.size();
     Arena& A = h->arena;
     auto plan = [&](Arena& a) { plan_arena(h, a, neles, nghosts, ld, gb, ncase, nface); };
     Arena probe;
@@ -763,6 +834,11 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     m.ncolor = ncolor;
     for (int c = 0; c <= ncolor; c++) m.fcoff[c] = fcoff[c];
     if (e == cudaSuccess && nface && m.fcolor) e = up(m.fcolor, hf_color.data(), nface * (size_t)I);
+    if (e == cudaSuccess && h->nwall) e = up(m.wcells, hwall.data(), hwall.size() * (size_t)I);
+    if (e == cudaSuccess && h->nwall) e = up(m.gcells, hgwall.data(), hgwall.size() * (size_t)I);
+    if (e == cudaSuccess && h->nwall) e = up(m.wclass, hwclass.data(), (size_t)ld);
+    // hwall, hgwall and hwclass are local vectors
+    if (e == cudaSuccess && h->nwall) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess && ncase > 1) {
         std::vector<int> cid(neles);
         for (int c = 0; c < ncase; c++)
@@ -1321,6 +1397,8 @@ extern "C" int hp_estimate_bytes(const hp_mesh* mesh, const hp_params* params, i
                                                                       : (int)((4LL * mesh->neles + mesh->nghosts) / 2);
     probe_h.neq = params->five_phase ? 22 : 10;
     probe_h.prm.face_mode = params->face_mode;
+    if (gb != sizeof(double) && params->wall_fp64_layers > 0)   // bound: every cell in the layers
+        probe_h.nwall = probe_h.ngwall = mesh->neles;
     plan_arena(&probe_h, probe, mesh->neles, mesh->nghosts, ld, gb, 1, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
@@ -1343,6 +1421,8 @@ extern "C" int hp_estimate_batch_bytes(const hp_mesh* meshes, int32_t ncase, con
     const int nface = gb == sizeof(double) || params->face_mode == 1 ? 0 : (int)((4 * ne + ng) / 2);
     probe_h.neq = params->five_phase ? 22 : 10;
     probe_h.prm.face_mode = params->face_mode;
+    if (gb != sizeof(double) && params->wall_fp64_layers > 0)   // bound: every cell in the layers
+        probe_h.nwall = probe_h.ngwall = (int)ne;
     plan_arena(&probe_h, probe, (int)ne, (int)ng, ld, gb, ncase, nface);
     *bytes = (int64_t)(probe.used + 256);
     return HP_OK;
@@ -1523,6 +1603,8 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
         n += (int64_t)h->dp.nstage * per_stage + 3;
         if (h->aliased) n += 2;
         if (h->neq == 22) n += 2 + (int64_t)h->dp.nstage * (2 + (h->nghosts ? 1 : 0));   // k_qrs_*
+        if (h->nwall > 0)   // FP64 wall layers: viscous once, gradients and fluxes per stage
+            n += (h->prm.inviscid ? 0 : 1) + (int64_t)h->dp.nstage * ((h->prm.myorder == 2 ? 1 : 0) + 1);
         *kernels_per_step = n;
     }
     if (device_bytes) *device_bytes = (int64_t)h->arena.size;

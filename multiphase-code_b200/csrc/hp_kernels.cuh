@@ -79,11 +79,6 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 #ifndef HP_FACE_VISC
 #define HP_FACE_VISC 1
 #endif
-// FP64 gradients and limiter with eight lanes per cell (k_grad8) instead of
-// four (k_grad4)
-#ifndef HP_GRAD_SPLIT
-#define HP_GRAD_SPLIT 1
-#endif
 // viscous fluxes of the cell-centric variants with eight lanes per cell (one
 // phase each, k_visc8) instead of four (k_visc4)
 #ifndef HP_VISC_SPLIT
@@ -1338,6 +1333,8 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     if (ldg(m.iblank + i) != 1) return;
+    // cells of the FP64 wall layers: updated by the FP64 kernels
+    if (sizeof(R) != sizeof(double) && m.nwall > 0 && ldg(m.wclass + i)) return;
     double rhs[10];
 #pragma unroll
     for (int k = 0; k < 10; k++) rhs[k] = 0.0;
@@ -1630,12 +1627,17 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
     return bad;
 }
 
+// LIST = 1: the cells of m.gcells (the FP64 wall layers and their
+// neighbours) instead of all cells.
+template <int LIST>
 __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevState<R> s, DevParams P) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
-    int i = (int)(gt >> 2);
-    const bool valid = i < m.neles;
-    if (!valid) i = m.neles - 1;
+    const int ncell = LIST ? m.ngwall : m.neles;
+    const long long c = gt >> 2;
+    const bool valid = c < ncell;
+    const int k = valid ? (int)c : ncell - 1;
+    const int i = LIST ? ldg(m.gcells + k) : k;
     const bool active = valid && grad_cell(ldg(m.iblank + i));
     if constexpr (HP_FAST(1)) {
         // the outputs are not inputs of this kernel, so a warp that flagged
@@ -1644,118 +1646,6 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
         if (__any_sync(0xffffffffu, bad)) grad4_body<0>(m, s, P, i, q, active);
     } else {
         grad4_body<0>(m, s, P, i, q, active);
-    }
-}
-
-// Value of lane q of this thread's group of eight consecutive lanes.
-template <class T>
-__device__ __forceinline__ T oshfl(T v, int q) {
-    return __shfl_sync(0xffffffffu, v, (int)((threadIdx.x & 31) & ~7u) + q);
-}
-
-// k_grad4 with eight lanes per cell: lane L computes the gradients of fields
-// L and L + 8 (pg, pp, phig, rog, rop for L = 0..4), and lanes 0, 1, 3, 4 the
-// limiter of the second of them (pg, pp, rog, rop); phi is the minimum in
-// that field order, as in k_grad4.  Each field's gradient and each limiter
-// value is formed exactly as in grad4_body; half of a lane's work, so about
-// half of its live state.
-#ifndef HP_GRAD8_MINB
-#define HP_GRAD8_MINB 5
-#endif
-template <int F>
-__device__ __forceinline__ unsigned grad8_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int i,
-                                               int L, bool active) {
-    unsigned bad = 0;
-    int n[4];
-#pragma unroll
-    for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
-    const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
-    R xa[4], ya[4], za[4];
-#pragma unroll
-    for (int f = 0; f < 4; f++) {
-        xa[f] = (R)(ldg(m.xc + n[f]) - x0);
-        ya[f] = (R)(ldg(m.yc + n[f]) - y0);
-        za[f] = (R)(ldg(m.zc + n[f]) - z0);
-    }
-    R wt[4], rw[4];
-#undef DW
-#define DW(x, f) mdiv<F>((x), wt[f], rw[f], bad)
-#pragma unroll
-    for (int f = 0; f < 4; f++) {
-        wt[f] = (R)ldg(COL(m.lsqa, f) + i);
-        rw[f] = mrcp_tab<F>(wt[f], (R)ldg(COL(m.lsqa, 11 + f) + i), bad);
-    }
-    const R a1 = (R)ldg(COL(m.lsqa, 4) + i), a2 = (R)ldg(COL(m.lsqa, 5) + i), a3 = (R)ldg(COL(m.lsqa, 6) + i);
-    const R b1 = (R)ldg(COL(m.lsqa, 7) + i), b2 = (R)ldg(COL(m.lsqa, 8) + i), b3 = (R)ldg(COL(m.lsqa, 9) + i);
-    const R dnr = (R)ldg(COL(m.lsqa, 10) + i);
-    const R rdnr = mrcp_tab<F>(dnr, (R)ldg(COL(m.lsqa, 15) + i), bad);
-    const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
-    R lg[3] = {R(0), R(0), R(0)};     // gradient of the lane's limiter field
-#pragma unroll
-    for (int r = 0; r < 2; r++) {
-        const int v = L + 8 * r;
-        if (v >= 13) break;
-        const R* qq = COL(s.prr, pcol[v]);
-        R qi = qq[i];
-        R qa = (R)(qq[n[0]] - qi), qb = (R)(qq[n[1]] - qi), qc = (R)(qq[n[2]] - qi), qd = (R)(qq[n[3]] - qi);
-        R c1 = DW(qa * xa[0], 0) + DW(qb * xa[1], 1) + DW(qc * xa[2], 2) + DW(qd * xa[3], 3);
-        R c2;
-        if (v == 7)   // cTp2 lacks the /wt4 (src/sr_derivative.F90:225)
-            c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + qd * ya[3];
-        else
-            c2 = DW(qa * ya[0], 0) + DW(qb * ya[1], 1) + DW(qc * ya[2], 2) + DW(qd * ya[3], 3);
-        R c3 = DW(qa * za[0], 0) + DW(qb * za[1], 1) + DW(qc * za[2], 2) + DW(qd * za[3], 3);
-        R gx = mdiv<F>(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr, bad);
-        R gy = mdiv<F>(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr, bad);
-        R gz = mdiv<F>(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr, bad);
-        if (v < 11 && active) {
-            COL(s.gr, 3 * v + 0)[i] = gx;
-            COL(s.gr, 3 * v + 1)[i] = gy;
-            COL(s.gr, 3 * v + 2)[i] = gz;
-        }
-        if (r == 1) { lg[0] = gx; lg[1] = gy; lg[2] = gz; }
-    }
-#undef DW
-#define DW(x, f) div_rn((x), wt[f], rw[f])
-    R phl = R(1);
-    if (L <= 4 && L != 2) {
-        const int lcol = L == 0 ? P_PG : L == 1 ? P_PP : L == 3 ? P_ROG : P_ROP;
-        const R epssq = (R)ldg(m.eps2 + i);
-        const R* qq = COL(s.prr, lcol);
-        R qi = qq[i];
-        R vmax = mx2(mx2(mx2(mx2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
-        R vmin = mn2(mn2(mn2(mn2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
-        R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
-#pragma unroll
-        for (int f = 0; f < 4; f++) {
-            R fx = (R)(ldg(COL(m.fch, f) + i) - x0);
-            R fy = (R)(ldg(COL(m.fch, 4 + f) + i) - y0);
-            R fz = (R)(ldg(COL(m.fch, 8 + f) + i) - z0);
-            R d = fx * lg[0] + fy * lg[1] + fz * lg[2];
-            R ph;
-            if (d > R(0)) ph = fvenkat(dmax, d, epssq);
-            else if (d < R(0)) ph = fvenkat(dmin, d, epssq);
-            else ph = R(1);
-            phl = (f == 0) ? ph : mn2(phl, ph);
-        }
-    }
-    R p0 = oshfl(phl, 0), p1 = oshfl(phl, 1), p3 = oshfl(phl, 3), p4 = oshfl(phl, 4);
-    if (L == 0 && active) s.phi[i] = (double)mn2(mn2(mn2(p0, p1), p3), p4);
-    return bad;
-}
-
-__global__ void __launch_bounds__(128, HP_GRAD8_MINB) k_grad8(DevMesh m, DevState<R> s, DevParams P) {
-    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int L = (int)(gt & 7);
-    int i = (int)(gt >> 3);
-    const bool valid = i < m.neles;
-    if (!valid) i = m.neles - 1;
-    const bool active = valid && grad_cell(ldg(m.iblank + i));
-    if constexpr (HP_FAST(1)) {
-        const unsigned bad = grad8_body<1>(m, s, P, i, L, active);
-        if (__any_sync(0xffffffffu, bad)) grad8_body<0>(m, s, P, i, L, active);
-    } else {
-        grad8_body<0>(m, s, P, i, L, active);
     }
 }
 
@@ -1964,14 +1854,20 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     return true;
 }
 
-template <int Z>
+// LIST = 1: the cells of m.wcells (the FP64 wall layers) instead of all
+// cells.  The FP32 variants leave the cells of the wall layers (wclass) to
+// those FP64 kernels.
+template <int Z, int LIST>
 __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
-    int i = (int)(gt >> 2);
-    const bool valid = i < m.neles;
-    if (!valid) i = m.neles - 1;
-    const bool active = valid && ldg(m.iblank + i) == 1;
+    const int ncell = LIST ? m.nwall : m.neles;
+    const long long c = gt >> 2;
+    const bool valid = c < ncell;
+    const int k = valid ? (int)c : ncell - 1;
+    const int i = LIST ? ldg(m.wcells + k) : k;
+    bool active = valid && ldg(m.iblank + i) == 1;
+    if (sizeof(R) != sizeof(double) && m.nwall > 0) active = active && !ldg(m.wclass + i);
     if constexpr (HP_FAST(2)) {
         if (!flux4_body<1, Z>(m, s, P, stage, i, q, active)) flux4_body<0, Z>(m, s, P, stage, i, q, active);
     } else {
@@ -2290,13 +2186,18 @@ __global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevStat
 // The per-cell sums over faces 1..4 are assembled with shuffles as in
 // k_visc4, so vis is identical to k_visc4's.  Splitting the phases halves
 // each lane's live state, which raises the resident warps.
+// LIST = 1: the cells of m.wcells (the FP64 wall layers) instead of all
+// cells.
+template <int LIST>
 __global__ void __launch_bounds__(128, HP_VISC8_MINB) k_visc8(DevMesh m, DevState<R> s, DevParams P) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
     const int ph = (int)((gt >> 5) & 1);
-    int i = (int)(((gt >> 6) << 3) + ((gt & 31) >> 2));
-    const bool valid = i < m.neles;
-    if (!valid) i = m.neles - 1;
+    const int ncell = LIST ? m.nwall : m.neles;
+    const long long c = ((gt >> 6) << 3) + ((gt & 31) >> 2);
+    const bool valid = c < ncell;
+    const int k = valid ? (int)c : ncell - 1;
+    const int i = LIST ? ldg(m.wcells + k) : k;
     const bool active = valid && ldg(m.iblank + i) == 1;
     int nci[4];
 #pragma unroll
@@ -2673,7 +2574,7 @@ static void enqueue_flux(const DevMesh& m, const DevState<R>& s, const DevParams
         k_faceflux<Z><<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
         k_flux<false, true, Z><<<gf, 128, 0, st>>>(m, s, P, stage);
     } else {
-        k_flux4<Z><<<g4, 128, 0, st>>>(m, s, P, stage);
+        k_flux4<Z, 0><<<g4, 128, 0, st>>>(m, s, P, stage);
     }
 }
 
@@ -2727,10 +2628,12 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             k_facevisc<<<grid_for(m.nface, 128), 128, 0, st>>>(m, s, P);
             k_vis_gather<<<grid_for(m.neles, 256), 256, 0, st>>>(m, s);
         } else if (HP_VISC_SPLIT) {
-            k_visc8<<<grid_for(8ll * m.neles, 128), 128, 0, st>>>(m, s, P);
+            k_visc8<0><<<grid_for(8ll * m.neles, 128), 128, 0, st>>>(m, s, P);
         } else {
             k_visc4<<<g4, 128, 0, st>>>(m, s, P);
         }
+        // FP64 wall layers: their viscous sums replaced by FP64 ones
+        if (sizeof(R) != sizeof(double) && m.nwall > 0) wall_fp64.visc(m, fp64_view(s), P, st);
     }
     for (int stage = 1; stage <= P.nstage; stage++) {
         // src/sr_hllcbatten.F90:29-33: primitiveplusbc, derivative, limiter
@@ -2745,9 +2648,11 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             MARK(KK_GRAD);
             if (m.aliased) k_grad<false><<<gf, b, 0, st>>>(m, s, P);
             else if (sizeof(R) != sizeof(double)) k_grad<true><<<gf, b, 0, st>>>(m, s, P);
-            else if (HP_GRAD_SPLIT && HP_LSQ_TABLE) k_grad8<<<grid_for(8ll * m.neles, 128), 128, 0, st>>>(m, s, P);
-            else k_grad4<<<g4, 128, 0, st>>>(m, s, P);
+            else k_grad4<0><<<g4, 128, 0, st>>>(m, s, P);
             if (m.aliased) { MARK(KK_SERIAL); k_phi_copy_serial<<<1, 1, 0, st>>>(m, s); }
+            // FP64 wall layers: FP64 gradients and limiter of those cells and
+            // their neighbours, for the FP64 fluxes below
+            if (sizeof(R) != sizeof(double) && m.nwall > 0) wall_fp64.grad(m, fp64_view(s), P, st);
         }
         if (P.five_phase) {   // src/mod_Fluxmodule.F90:18-20: jamesonqrs (and sourceqrs)
             MARK(KK_QRS);
@@ -2758,6 +2663,9 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
         MARK(KK_FLUX);
         if (P.myflux == 1) enqueue_flux<1>(m, s, P, st, stage, hook);
         else enqueue_flux<0>(m, s, P, st, stage, hook);
+        // FP64 wall layers: their fluxes, sources and RK update (the FP32
+        // kernels above left those cells alone)
+        if (sizeof(R) != sizeof(double) && m.nwall > 0) wall_fp64.flux(m, fp64_view(s), P, st, stage);
         if (m.nfringe > 0) {
             MARK(KK_OVERSET);
             k_overset<<<grid_for(m.nfringe, 256), 256, 0, st>>>(m, s);

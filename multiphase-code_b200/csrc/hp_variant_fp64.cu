@@ -25,4 +25,22 @@
 
 namespace hp {
 const Variant variant_fp64 = {"fp64", sizeof(double), &v_fp64::enqueue_start, &v_fp64::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0};
+
+// The FP64 (FMA) kernels over the wall-layer cell lists, for the steps of the
+// FP32-arithmetic variants (same compile flags as theirs: -fmad=true).
+namespace v_fp64 {
+static void wall_visc(const DevMesh& m, const DevState<double>& s, const DevParams& P, cudaStream_t st) {
+    if (m.nwall > 0) k_visc8<1><<<grid_for(8ll * m.nwall, 128), 128, 0, st>>>(m, s, P);
+}
+static void wall_grad(const DevMesh& m, const DevState<double>& s, const DevParams& P, cudaStream_t st) {
+    if (m.ngwall > 0) k_grad4<1><<<grid_for(4ll * m.ngwall, 128), 128, 0, st>>>(m, s, P);
+}
+static void wall_flux(const DevMesh& m, const DevState<double>& s, const DevParams& P, cudaStream_t st,
+                      int stage) {
+    if (m.nwall <= 0) return;
+    if (P.myflux == 1) k_flux4<1, 1><<<grid_for(4ll * m.nwall, 128), 128, 0, st>>>(m, s, P, stage);
+    else k_flux4<0, 1><<<grid_for(4ll * m.nwall, 128), 128, 0, st>>>(m, s, P, stage);
+}
+}  // namespace v_fp64
+const WallFp64 wall_fp64 = {&v_fp64::wall_visc, &v_fp64::wall_grad, &v_fp64::wall_flux};
 }

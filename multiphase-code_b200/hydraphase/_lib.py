@@ -42,7 +42,7 @@ class HpParams(ctypes.Structure):
         ("renumber", _I), ("block_size", _I), ("use_graph", _I), ("pad_", _D * 4),
         ("five_phase", _I)] + [(n, _D) for n in (
         "rhoq", "rhor", "rhos", "radq", "radr", "rads", "phiginit", "phipinit", "phiqinit", "phirinit",
-        "phisinit")]
+        "phisinit")] + [("wall_fp64_layers", _I)]
 
 
 class HpMesh(ctypes.Structure):

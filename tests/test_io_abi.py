@@ -171,6 +171,9 @@ def test_create_rejects_bad_meshes():
     with pytest.raises(HydraError) as e:
         Case(m, spec.params(face_mode=4))
     assert e.value.code == HP_E_ARG and "face_mode" in str(e.value)
+    with pytest.raises(HydraError) as e:
+        Case(m, spec.params(wall_fp64_layers=-1))
+    assert e.value.code == HP_E_ARG and "wall_fp64_layers" in str(e.value)
 
 
 def test_partition_ghosts_unsupported():
