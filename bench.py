@@ -286,14 +286,16 @@ def serving_measure(n_cases: int, steps: int, repeats: int = 3):
            "cells_total": int(sum(r.spec.mesh.neles for r in reqs)), "generation_s": round(gen_s, 2)}
     reports = {}
     for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64_PARITY)):
-        blocks, modes = {}, {}
+        blocks, modes, smodes = {}, {}, {}
         for r in reqs:
             cls = tune.size_class(r.spec.mesh.neles)
             if cls not in blocks:
                 blocks[cls] = tune.tune_block_size(r.spec, precision=prec, steps=4)[0]
                 modes[cls] = tune.tune_face_mode(r.spec, precision=prec, block_size=blocks[cls], steps=4)[0]
+                smodes[cls] = tune.tune_step_mode(r.spec, precision=prec, block_size=blocks[cls],
+                                                  face_mode=modes[cls], steps=4)[0]
         server = Server(150 << 30, precision=prec, max_active=16, chunk=25, chunk_cell_steps=10_000_000,
-                        batch_cells=200000, block_size=blocks, face_mode=modes, keep_state=True)
+                        batch_cells=200000, block_size=blocks, face_mode=modes, step_mode=smodes, keep_state=True)
         # warm-up (untimed): every case of the stream for 25 steps, all
         # arriving at once, so the measured run pays no first-use costs
         # (module loading, pool growth to the stream's peak, worker start-up)
@@ -302,7 +304,8 @@ def serving_measure(n_cases: int, steps: int, repeats: int = 3):
         rates = [r.summary()["updates_per_s"] for r in runs]
         rep_ = runs[int(np.argsort(rates)[len(rates) // 2])]          # the median run
         reports[name] = rep_
-        out[name] = {**rep_.summary(), "block_size": blocks, "face_mode": modes, "runs": len(runs),
+        out[name] = {**rep_.summary(), "block_size": blocks, "face_mode": modes,
+                     "step_mode": {k: ("fused" if v == 2 else "graph") for k, v in smodes.items()}, "runs": len(runs),
                      "updates_per_s_range": [min(rates), max(rates)]}
     out["speedup_mixed_vs_fp64"] = out["mixed"]["updates_per_s"] / out["fp64"]["updates_per_s"]
     # each served mixed result against the served FP64 result of the same case

@@ -83,7 +83,12 @@ typedef struct hp_params {
     int32_t block_size;      /* threads per block of the one-thread-per-cell
                                 kernels: 0 (= 256) or a multiple of 32 in
                                 [64, 512]; hydraphase.tune picks it */
-    int32_t use_graph;       /* 1: capture each step in a CUDA graph */
+    int32_t use_graph;       /* 1: capture each step in a CUDA graph; 2: one
+                                fused cooperative kernel per step (precision
+                                HP_PREC_FP64_PARITY on plain meshes: not aliased,
+                                two-phase, no overset fringe or partition halo;
+                                every other handle runs as with 1); 0: launch
+                                each kernel */
     double pad_[4];
     /* --- five-phase model (the reference's FIVE_PHASE build): three
      * dispersed, incompressible phases q, r, s with mass and momentum each,

@@ -181,6 +181,15 @@ struct WallFp64 {
 };
 extern const WallFp64 wall_fp64;
 
+// Grid-wide barrier of the fused step kernel (zeroed at set-up): arrivals,
+// generation, and a flag set when a wait gave up (its spin is bounded).
+struct GridSync {
+    unsigned count;
+    unsigned gen;
+    int err;
+    int pad;
+};
+
 // Kernel kinds, for per-kernel timing (hp_profile_steps).
 enum KernelKind {
     KK_PRIM_START = 0, KK_STEP_BEGIN, KK_SMOOTH1, KK_SMOOTH2, KK_BC_VISC, KK_VISC,
@@ -212,6 +221,11 @@ struct Variant {
     // 1 when the viscous fluxes are evaluated once per face on meshes with a
     // face list (k_facevisc + k_vis_gather instead of one kernel)
     int face_visc;
+    // fused step (one cooperative launch per step): the grid it runs with on
+    // this device (blocks of 128 threads), and the launch of one step
+    int (*fused_grid)(const DevMesh&, const DevParams&);
+    cudaError_t (*enqueue_fused)(const DevMesh&, const void* st, const DevParams&, cudaStream_t,
+                                 GridSync* sync, int grid);
 };
 
 extern const Variant variant_fp64_parity;

@@ -82,6 +82,8 @@ struct hp_handle {
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    GridSync* d_sync = nullptr;  // fused step (use_graph = 2): its grid barrier
+    int fused = 0;               // blocks of the fused step; 0: not this handle
     Arena arena;
     int device = 0;
     int neles = 0, nghosts = 0, ntot = 0;
@@ -108,6 +110,7 @@ struct hp_handle {
     std::string err;
     double* h_diag = nullptr;   // pinned
     DevScalars* h_scal = nullptr;
+    GridSync* h_sync = nullptr;     // pinned copy of d_sync (its error flag)
     OutSlot out[2];             // asynchronous output, two requests in flight
     cudaStream_t ostream = nullptr;
     int next_ticket = 1;
@@ -237,6 +240,7 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
         m.f_i = m.f_code = m.cface = nullptr;
         s.ff = nullptr;
     }
+    h->d_sync = (GridSync*)a.take(sizeof(GridSync));
     h->d_perm = (int*)a.take((neles + 1) * (size_t)I);
     h->d_gid = (int*)a.take((nghosts + 1) * (size_t)I);
     h->d_gstage = (double*)a.take(6 * (nghosts + 1) * D);
@@ -586,6 +590,8 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
         return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
     if (params->block_size != 0 && (params->block_size < 64 || params->block_size > 512 || params->block_size % 32))
         return fail(nullptr, HP_E_ARG, "block_size must be 0 or a multiple of 32 in [64, 512]");
+    if (params->use_graph < 0 || params->use_graph > 2)
+        return fail(nullptr, HP_E_ARG, "use_graph must be 0 (launches), 1 (graph) or 2 (fused step)");
     if (params->face_mode < 0 || params->face_mode > 3)
         return fail(nullptr, HP_E_ARG, "face_mode must be 0 (face records), 1 (each side), 2 (colouring) or 3 (atomics)");
     if (params->wall_fp64_layers < 0) return fail(nullptr, HP_E_ARG, "wall_fp64_layers must be >= 0");
@@ -848,6 +854,20 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     }
     if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_diag, (size_t)h->max_diag * 8 * D * ncase);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_scal, sizeof(DevScalars));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_sync, sizeof(GridSync));
+    // the fused step: plain two-phase meshes on a device with cooperative
+    // launch, in the parity variant.  The variants built with FMA contraction
+    // keep the graph: the fused kernel is another compilation of the same
+    // bodies, whose contractions (and so roundings) may differ from those of
+    // the separate kernels, and a case must give the same result whichever
+    // way it runs (alone or in a batch of another size class).
+    if (e == cudaSuccess && h->prm.use_graph == 2 && h->var == &variant_fp64_parity && !h->aliased &&
+        h->neq == 10 && h->nwall == 0 && !(m.nface > 0 && m.face_mode >= 2)) {
+        int coop = 0;
+        if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop)
+            h->fused = h->var->fused_grid(m, P);
+        cudaGetLastError();
+    }
     for (int c = 0; c < ncase && e == cudaSuccess; c++) {
         DevScalars s0{};
         double v = 1.0e8;
@@ -900,6 +920,7 @@ extern "C" int hp_destroy(hp_handle* h) {
     }
     if (h->h_diag) cudaFreeHost(h->h_diag);
     if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->h_sync) cudaFreeHost(h->h_sync);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return HP_OK;
@@ -1098,7 +1119,13 @@ static int run_steps(hp_handle* h, int n) {
         h->var->enqueue_start(h->dm, &h->ds, h->dp, st, block, nullptr);
         h->started = true;
     }
-    if (h->xfn) {
+    // the fused step needs a plain mesh: no exchange callback, overset
+    // fringe or halo (set after creation), nothing else it leaves out
+    const bool fused = h->prm.use_graph == 2 && h->fused > 0 && !h->xfn && h->dm.nfringe == 0 && h->dm.nhalo == 0;
+    if (fused) {
+        for (int k = 0; k < n; k++)
+            CUDA_OK(h, h->var->enqueue_fused(h->dm, &h->ds, h->dp, st, h->d_sync, h->fused));
+    } else if (h->xfn) {
         const StepHook hook{nullptr, nullptr, exchange_point, h};
         for (int k = 0; k < n; k++) h->var->enqueue_step(h->dm, &h->ds, h->dp, st, block, &hook);
     } else if (h->prm.use_graph) {
@@ -1114,6 +1141,17 @@ static int run_steps(hp_handle* h, int n) {
     }
     CUDA_OK(h, cudaGetLastError());
     return HP_OK;
+}
+
+// After fused steps that the caller waits for anyway: a grid barrier whose
+// wait gave up (bounded spin) is reported, and the barrier is reset.
+static int check_fused(hp_handle* h) {
+    if (h->fused <= 0 || h->prm.use_graph != 2) return HP_OK;
+    CUDA_OK(h, cudaMemcpyAsync(h->h_sync, h->d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OK(h, cudaStreamSynchronize(h->stream));
+    if (h->h_sync->err == 0) return HP_OK;
+    CUDA_OK(h, cudaMemsetAsync(h->d_sync, 0, sizeof(GridSync), h->stream));
+    return fail(h, HP_E_CUDA, "fused step: a grid barrier wait gave up; the step did not complete");
 }
 
 extern "C" int hp_step(hp_handle* h, int32_t nsteps, hp_diag* diag) {
@@ -1133,6 +1171,7 @@ extern "C" int hp_step(hp_handle* h, int32_t nsteps, hp_diag* diag) {
                                            h->ds.diag + (size_t)c * h->max_diag * 8,
                                            (size_t)chunk * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CUDA_OK(h, cudaStreamSynchronize(h->stream));
+            if (int frc = check_fused(h)) return frc;
             for (int c = 0; c < h->ncase; c++)
                 for (int k = 0; k < chunk; k++) {
                     const double* d = h->h_diag + ((size_t)c * h->max_diag + k) * 8;
@@ -1167,7 +1206,8 @@ extern "C" int hp_step_timed(hp_handle* h, int32_t nsteps, double* device_ms) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     *device_ms = ms;
-    return rc;
+    if (rc) return rc;
+    return check_fused(h);
 }
 
 namespace {
@@ -1605,6 +1645,8 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
         if (h->neq == 22) n += 2 + (int64_t)h->dp.nstage * (2 + (h->nghosts ? 1 : 0));   // k_qrs_*
         if (h->nwall > 0)   // FP64 wall layers: viscous once, gradients and fluxes per stage
             n += (h->prm.inviscid ? 0 : 1) + (int64_t)h->dp.nstage * ((h->prm.myorder == 2 ? 1 : 0) + 1);
+        if (h->prm.use_graph == 2 && h->fused > 0 && !h->xfn && h->dm.nfringe == 0 && h->dm.nhalo == 0)
+            n = 1;   // the fused step
         *kernels_per_step = n;
     }
     if (device_bytes) *device_bytes = (int64_t)h->arena.size;

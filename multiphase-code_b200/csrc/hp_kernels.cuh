@@ -11,6 +11,7 @@
 // reference's per-cell summation order (src/sr_hllcbatten.F90:77-555), so the
 // parity variant (compiled with -fmad=false) reproduces the CPU reference
 // bit for bit, and it needs no atomics.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <type_traits>
@@ -138,17 +139,22 @@ template <int F> __device__ __forceinline__ float mdiv(float a, float b, float r
 template <int F> __device__ __forceinline__ float mrcp(float b, unsigned&) { return 1.0f / b; }
 
 // One face record (FACE_REC values of R) of the face-based variants; the
-// record of face t starts at FACE_REC * t, 16-byte aligned in FP32.
+// record of face t starts at FACE_REC * t, 16-byte aligned in FP32.  NC:
+// through the read-only (non-coherent) data path, which a kernel may use
+// only for data it does not write itself; the fused step, which writes the
+// records in an earlier phase, reads them with plain loads.
+template <bool NC = true>
 __device__ __forceinline__ void load_frec(const float* p, float e[FACE_REC]) {
     const float4* q = reinterpret_cast<const float4*>(p);
-    const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    const float4 a = NC ? __ldg(q) : q[0], b = NC ? __ldg(q + 1) : q[1], c = NC ? __ldg(q + 2) : q[2];
     e[0] = a.x; e[1] = a.y; e[2] = a.z; e[3] = a.w;
     e[4] = b.x; e[5] = b.y; e[6] = b.z; e[7] = b.w;
     e[8] = c.x; e[9] = c.y; e[10] = c.z; e[11] = c.w;
 }
+template <bool NC = true>
 __device__ __forceinline__ void load_frec(const double* p, double e[FACE_REC]) {
 #pragma unroll
-    for (int k = 0; k < FACE_REC; k++) e[k] = __ldg(p + k);
+    for (int k = 0; k < FACE_REC; k++) e[k] = NC ? __ldg(p + k) : p[k];
 }
 __device__ __forceinline__ void store_frec(float* p, const float e[FACE_REC]) {
     float4* q = reinterpret_cast<float4*>(p);
@@ -314,9 +320,9 @@ enum { PM_STAGE = 0, PM_START = 1, PM_END = 2 };
 // src/main.F90:529-546; PM_END adds the max-norm residual of :605-611, the
 // cu = cn copy of :619-625 and |u_g(1)| of :641.
 template <int MODE>
-__global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParams P) {
+__device__ __forceinline__ void k_prim_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
     __shared__ unsigned long long red[4][16];
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = bid * blockDim.x + threadIdx.x;
     unsigned long long kmin = ~0ull, kd[4] = {0, 0, 0, 0}, nanc = 0;
     if (i < m.neles) {
         double c[10], u[10];
@@ -374,7 +380,7 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
     if (MODE == PM_STAGE) return;
     // a block whose cells belong to two cases of a batch reduces per thread
     // (block-uniform branch: cases occupy contiguous element ranges)
-    const int b0 = blockIdx.x * blockDim.x;
+    const int b0 = bid * blockDim.x;
     const int c0 = case_of(m, b0), c1 = case_of(m, min(b0 + (int)blockDim.x, m.neles) - 1);
     if (c0 != c1) {
         if (i < m.neles) {
@@ -423,6 +429,10 @@ __global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParam
         }
     }
 }
+template <int MODE>
+__global__ void __launch_bounds__(512) k_prim(DevMesh m, DevState<R> s, DevParams P) {
+    k_prim_body<MODE>(m, s, P, blockIdx.x);
+}
 
 // dt = cfl * dtmin, time += dt (src/main.F90:521-556); one thread per case.
 __device__ __forceinline__ void step_begin_case(DevScalars* sc, const DevParams& P, unsigned long long bits) {
@@ -451,8 +461,8 @@ __global__ void k_step_begin(DevState<R> s, DevParams P, int ncase, int coupled)
 
 // per-step diagnostics and reset of the residual accumulators; one thread
 // per case (diag rows of case c start at c * max_diag).
-__global__ void k_step_end(DevState<R> s, int ncase) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_step_end_body(DevState<R> s, int ncase, int bid) {
+    const int c = bid * blockDim.x + threadIdx.x;
     if (c >= ncase) return;
     DevScalars* sc = s.s + c;
     int k = sc->step_in_call;
@@ -465,6 +475,9 @@ __global__ void k_step_end(DevState<R> s, int ncase) {
     sc->step_in_call = k + 1;
     for (int j = 0; j < 4; j++) sc->diff_bits[j] = 0ull;
     sc->nan_count = 0ull;
+}
+__global__ void k_step_end(DevState<R> s, int ncase) {
+    k_step_end_body(s, ncase, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -613,8 +626,8 @@ __device__ __forceinline__ void ghost_cn_one(const DevMesh& m, double* pr, doubl
 // Parallel ghost fill: valid when every ghost id is its own slot and every
 // parent is an element (no aliasing), so ghost entries are independent.
 template <bool VISC>
-__global__ void __launch_bounds__(512) k_bc(DevMesh m, DevState<R> s, DevParams P) {
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_bc_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
+    int g = bid * blockDim.x + threadIdx.x;
     if (g >= m.nghosts) return;
     const DevScalars& sc = s.s[case_of(m, m.g_par[g])];
     bc_one<VISC>(m, s.pr, nullptr, P, g, sc.dt, sc.total);
@@ -623,6 +636,10 @@ __global__ void __launch_bounds__(512) k_bc(DevMesh m, DevState<R> s, DevParams 
 #pragma unroll
         for (int k = 0; k < NPR; k++) COL(s.prr, k)[ng] = (R)COL(s.pr, k)[ng];
     }
+}
+template <bool VISC>
+__global__ void __launch_bounds__(512) k_bc(DevMesh m, DevState<R> s, DevParams P) {
+    k_bc_body<VISC>(m, s, P, blockIdx.x);
 }
 
 // Sequential ghost fill in the reference's exact order (type lists 2, 3, 5,
@@ -664,8 +681,8 @@ __global__ void k_phi_copy_serial(DevMesh m, DevState<R> s) {
 
 // ---------------------------------------------------------------------------
 // JST dissipation, src/sr_smooth.F90:52-154: switches anu and Laplacian d2q.
-__global__ void __launch_bounds__(512) k_smooth1(DevMesh m, DevState<R> s) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_smooth1_body(DevMesh m, DevState<R> s, int bid) {
+    int i = bid * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     const int a = ldg(COL(m.snb, 0) + i), b = ldg(COL(m.snb, 1) + i);
     const int c = ldg(COL(m.snb, 2) + i), d = ldg(COL(m.snb, 3) + i);
@@ -704,6 +721,9 @@ __global__ void __launch_bounds__(512) k_smooth1(DevMesh m, DevState<R> s) {
     for (int k = 0; k < 10; k++) COL(s.d2q, k)[i] = lap[k];
     COL(s.anu, 0)[i] = anu1;
     COL(s.anu, 1)[i] = anu2;
+}
+__global__ void __launch_bounds__(512) k_smooth1(DevMesh m, DevState<R> s) {
+    k_smooth1_body(m, s, blockIdx.x);
 }
 
 // src/sr_smooth.F90:200-374: blended 2nd/4th difference d24.  F selects the
@@ -750,8 +770,8 @@ __device__ __forceinline__ unsigned smooth2_body(const DevMesh& m, const DevStat
     return bad;
 }
 
-__global__ void __launch_bounds__(512) k_smooth2(DevMesh m, DevState<R> s, DevParams P) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_smooth2_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
+    int i = bid * blockDim.x + threadIdx.x;
     const bool valid = i < m.neles;
     if (!valid) i = m.neles - 1;      // keep the warp whole for the vote below
     if constexpr (HP_FAST(8)) {
@@ -761,6 +781,9 @@ __global__ void __launch_bounds__(512) k_smooth2(DevMesh m, DevState<R> s, DevPa
     } else {
         if (valid) smooth2_body<0>(m, s, P, i);
     }
+}
+__global__ void __launch_bounds__(512) k_smooth2(DevMesh m, DevState<R> s, DevParams P) {
+    k_smooth2_body(m, s, P, blockIdx.x);
 }
 
 // Cells whose gradients and limiter are evaluated: active cells and the
@@ -774,10 +797,10 @@ __device__ __forceinline__ bool grad_cell(int ib) { return ib == 1 || ib == HP_I
 // FPR: read the primitives in R (the float copy of the FP32-arithmetic
 // variants) instead of the FP64 columns; false on aliased meshes.
 template <bool FPR>
-__global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParams P) {
+__device__ __forceinline__ void k_grad_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
     using PT = typename std::conditional<FPR, R, double>::type;
     const PT* const prb = reinterpret_cast<const PT*>(FPR ? (const void*)s.prr : (const void*)s.pr);
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = bid * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     if (!grad_cell(ldg(m.iblank + i))) return;
     int n[4];
@@ -879,6 +902,10 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParam
         }
     }
     s.phi[i] = (double)phi;
+}
+template <bool FPR>
+__global__ void __launch_bounds__(128) k_grad(DevMesh m, DevState<R> s, DevParams P) {
+    k_grad_body<FPR>(m, s, P, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1026,15 +1053,12 @@ __device__ __forceinline__ void zien_flux(FaceOut& o, unsigned& bad, R area, R e
 #ifndef HP_FACE_LDG
 #define HP_FACE_LDG 1
 #endif
-#if HP_FACE_LDG
-#define PLD(p) ldg(p)
-#else
-#define PLD(p) (*(p))
-#endif
+// (NC = false: plain loads, for the fused step, which writes these arrays)
+#define PLD(p) ((HP_FACE_LDG && NC) ? ldg(p) : *(p))
 // F selects the division form (see mdiv); bad collects its out-of-range flag.
 // Z selects the Riemann solver: 0 HLLC-Batten (src/sr_hllcbatten.F90:338-529),
 // 1 HLLC-Zien (src/sr_hllczien.F90:348-487).
-template <int F, int Z, class PT>
+template <int F, int Z, class PT, bool NC = true>
 __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s, const DevParams& P,
                                           int i, int f, FaceOut& o, unsigned& bad, const PT* pr) {
     const int neigh = ldg(COL(m.nc, f) + i);
@@ -1328,9 +1352,9 @@ __global__ void k_flux_carry(DevMesh m, DevState<R> s, DevParams P) {
 // RK stage update of src/sr_RK.F90 fused; iblank == 1 cells.
 // FACE: the four face fluxes are gathered from k_faceflux's output (face-
 // based variants) instead of evaluated here.
-template <bool ALIASED, bool FACE, int Z, bool ACC = false>
-__global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParams P, int stage) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+template <bool ALIASED, bool FACE, int Z, bool ACC = false, bool NC = true>
+__device__ __forceinline__ void k_flux_body(DevMesh m, DevState<R> s, DevParams P, int stage, int bid) {
+    int i = bid * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     if (ldg(m.iblank + i) != 1) return;
     // cells of the FP64 wall layers: updated by the FP64 kernels
@@ -1351,7 +1375,7 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
             const int fid = (code > 0 ? code : -code) - 1;
             const R sg = code > 0 ? R(1) : R(-1);
             R e[FACE_REC];
-            load_frec(s.ff + (size_t)FACE_REC * (size_t)fid, e);
+            load_frec<NC>(s.ff + (size_t)FACE_REC * (size_t)fid, e);
 #pragma unroll
             for (int k = 0; k < 10; k++) e[k] = sg * e[k];
             if (e[10] != R(0)) {
@@ -1514,6 +1538,10 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
         }
     }
 }
+template <bool ALIASED, bool FACE, int Z, bool ACC = false>
+__global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParams P, int stage) {
+    k_flux_body<ALIASED, FACE, Z, ACC>(m, s, P, stage, blockIdx.x);
+}
 
 // ---------------------------------------------------------------------------
 // k_grad with four lanes per cell: lane q computes the LSQ gradients of
@@ -1630,8 +1658,8 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
 // LIST = 1: the cells of m.gcells (the FP64 wall layers and their
 // neighbours) instead of all cells.
 template <int LIST>
-__global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevState<R> s, DevParams P) {
-    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_grad4_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
+    const long long gt = (long long)bid * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
     const int ncell = LIST ? m.ngwall : m.neles;
     const long long c = gt >> 2;
@@ -1648,6 +1676,10 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
         grad4_body<0>(m, s, P, i, q, active);
     }
 }
+template <int LIST>
+__global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevState<R> s, DevParams P) {
+    k_grad4_body<LIST>(m, s, P, blockIdx.x);
+}
 
 // Residual + sources + RK update with four lanes per cell: lane q evaluates
 // face q; every lane re-assembles the residual in face order and computes
@@ -1655,7 +1687,7 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
 // form (see mdiv).  The fast form returns false, before any store, when a lane
 // of the warp flagged an operand (cn is read and written here, so the stores
 // must wait for that vote).
-template <int F, int Z>
+template <int F, int Z, bool NC = true>
 __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int stage,
                                            int i, int q, bool active) {
     unsigned bad = 0;
@@ -1665,7 +1697,7 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     int flags;
     {
         FaceOut o;
-        face_eval<F, Z>(m, s, P, i, q, o, bad, s.prr);
+        face_eval<F, Z, R, NC>(m, s, P, i, q, o, bad, s.prr);
         if (o.wall) {
 #pragma unroll
             for (int k = 0; k < 10; k++) eff[k] = R(0);
@@ -1857,9 +1889,9 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
 // LIST = 1: the cells of m.wcells (the FP64 wall layers) instead of all
 // cells.  The FP32 variants leave the cells of the wall layers (wclass) to
 // those FP64 kernels.
-template <int Z, int LIST>
-__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
-    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+template <int Z, int LIST, bool NC = true>
+__device__ __forceinline__ void k_flux4_body(DevMesh m, DevState<R> s, DevParams P, int stage, int bid) {
+    const long long gt = (long long)bid * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
     const int ncell = LIST ? m.nwall : m.neles;
     const long long c = gt >> 2;
@@ -1869,24 +1901,28 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevStat
     bool active = valid && ldg(m.iblank + i) == 1;
     if (sizeof(R) != sizeof(double) && m.nwall > 0) active = active && !ldg(m.wclass + i);
     if constexpr (HP_FAST(2)) {
-        if (!flux4_body<1, Z>(m, s, P, stage, i, q, active)) flux4_body<0, Z>(m, s, P, stage, i, q, active);
+        if (!flux4_body<1, Z, NC>(m, s, P, stage, i, q, active)) flux4_body<0, Z, NC>(m, s, P, stage, i, q, active);
     } else {
-        flux4_body<0, Z>(m, s, P, stage, i, q, active);
+        flux4_body<0, Z, NC>(m, s, P, stage, i, q, active);
     }
+}
+template <int Z, int LIST>
+__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_flux4(DevMesh m, DevState<R> s, DevParams P, int stage) {
+    k_flux4_body<Z, LIST>(m, s, P, stage, blockIdx.x);
 }
 
 // Face-based fluxes (FP32-arithmetic variants on meshes without aliased
 // ghosts): every face is evaluated once, in its owner cell's orientation,
 // instead of once from each side.  Phases with no HLLC branch taken (only
 // with NaN states) contribute zero here.
-template <int Z>
-__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_faceflux(DevMesh m, DevState<R> s, DevParams P) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+template <int Z, bool NC = true>
+__device__ __forceinline__ void k_faceflux_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
+    const int t = bid * blockDim.x + threadIdx.x;
     if (t >= m.nface) return;
     const int i = ldg(m.f_i + t), f = ldg(m.f_code + t) & 3;
     FaceOut o{};
     unsigned bad = 0;
-    face_eval<0, Z>(m, s, P, i, f, o, bad, s.prr);
+    face_eval<0, Z, R, NC>(m, s, P, i, f, o, bad, s.prr);
     R rec[FACE_REC];
     if (o.wall) {
 #pragma unroll
@@ -1901,6 +1937,10 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_faceflux(DevMesh m, DevS
     rec[11] = R(0);
     store_frec(s.ff + (size_t)FACE_REC * (size_t)t, rec);
 }
+template <int Z>
+__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_faceflux(DevMesh m, DevState<R> s, DevParams P) {
+    k_faceflux_body<Z>(m, s, P, blockIdx.x);
+}
 
 // Face modes 2 and 3: each face evaluated once, its flux added to the owner's
 // accumulator and subtracted from the other cell's (a ghost has none).
@@ -1908,9 +1948,9 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_faceflux(DevMesh m, DevS
 // ATOMIC = true: every face, with atomic adds (the order of the additions,
 // and so the last bits of the sums, vary from run to run).
 template <int Z, bool ATOMIC>
-__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_facescatter(DevMesh m, DevState<R> s, DevParams P,
-                                                                     const int* fids, int n) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_facescatter_body(DevMesh m, DevState<R> s, DevParams P,
+                                                                     const int* fids, int n, int bid) {
+    const int t = bid * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int fid = ATOMIC ? t : ldg(fids + t);
     const int i = ldg(m.f_i + fid), f = ldg(m.f_code + fid) & 3;
@@ -1940,6 +1980,11 @@ __global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_facescatter(DevMesh m, D
             if (other) acc[j] = acc[j] - e[k];
         }
     }
+}
+template <int Z, bool ATOMIC>
+__global__ void __launch_bounds__(128, HP_FLUX4_MINB) k_facescatter(DevMesh m, DevState<R> s, DevParams P,
+                                                                     const int* fids, int n) {
+    k_facescatter_body<Z, ATOMIC>(m, s, P, fids, n, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -2149,8 +2194,8 @@ __global__ void __launch_bounds__(128) k_visc(DevMesh m, DevState<R> s, DevParam
 // of a warp reach every shuffle (out-of-range lanes replay the last cell and
 // do not write).
 
-__global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevState<R> s, DevParams P) {
-    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_visc4_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
+    const long long gt = (long long)bid * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
     int i = (int)(gt >> 2);
     const bool valid = i < m.neles;
@@ -2180,6 +2225,9 @@ __global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevStat
         if (!__any_sync(0xffffffffu, bad)) break;
     }
 }
+__global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevState<R> s, DevParams P) {
+    k_visc4_body(m, s, P, blockIdx.x);
+}
 
 // Eight lanes per cell: each warp takes one phase of 8 cells (warps 2w and
 // 2w+1 the gas and the liquid of the same cells), lane q of a cell face q.
@@ -2189,8 +2237,8 @@ __global__ void __launch_bounds__(128, HP_VISC4_MINB) k_visc4(DevMesh m, DevStat
 // LIST = 1: the cells of m.wcells (the FP64 wall layers) instead of all
 // cells.
 template <int LIST>
-__global__ void __launch_bounds__(128, HP_VISC8_MINB) k_visc8(DevMesh m, DevState<R> s, DevParams P) {
-    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_visc8_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
+    const long long gt = (long long)bid * blockDim.x + threadIdx.x;
     const int q = (int)(gt & 3);
     const int ph = (int)((gt >> 5) & 1);
     const int ncell = LIST ? m.nwall : m.neles;
@@ -2218,14 +2266,18 @@ __global__ void __launch_bounds__(128, HP_VISC8_MINB) k_visc8(DevMesh m, DevStat
         if (!__any_sync(0xffffffffu, bad)) break;
     }
 }
+template <int LIST>
+__global__ void __launch_bounds__(128, HP_VISC8_MINB) k_visc8(DevMesh m, DevState<R> s, DevParams P) {
+    k_visc8_body<LIST>(m, s, P, blockIdx.x);
+}
 
 // Viscous fluxes once per face (FP32-arithmetic variants with a face list):
 // the owner's contribution goes to the face record's first 8 values (the
 // records are free until the first stage's k_faceflux); the other cell of an interior face takes its negative,
 // since the face-centred stencil (both cells' neighbours), the face averages
 // and the face vector are the same from either side up to the vector's sign.
-__global__ void __launch_bounds__(128, HP_VISC4_MINB) k_facevisc(DevMesh m, DevState<R> s, DevParams P) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_facevisc_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
+    const int t = bid * blockDim.x + threadIdx.x;
     if (t >= m.nface) return;
     const int i = ldg(m.f_i + t), f = ldg(m.f_code + t) & 3;
     int nci[4];
@@ -2241,10 +2293,14 @@ __global__ void __launch_bounds__(128, HP_VISC4_MINB) k_facevisc(DevMesh m, DevS
     for (int k = 8; k < FACE_REC; k++) rec[k] = R(0);
     store_frec(s.ff + (size_t)FACE_REC * (size_t)t, rec);
 }
+__global__ void __launch_bounds__(128, HP_VISC4_MINB) k_facevisc(DevMesh m, DevState<R> s, DevParams P) {
+    k_facevisc_body(m, s, P, blockIdx.x);
+}
 
 // Per-cell viscous sums from k_facevisc's face values, in face order 1..4.
-__global__ void __launch_bounds__(256) k_vis_gather(DevMesh m, DevState<R> s) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+template <bool NC = true>
+__device__ __forceinline__ void k_vis_gather_body(DevMesh m, DevState<R> s, int bid) {
+    const int i = bid * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     if (ldg(m.iblank + i) != 1) return;
     double acc[8];
@@ -2256,12 +2312,15 @@ __global__ void __launch_bounds__(256) k_vis_gather(DevMesh m, DevState<R> s) {
         const size_t fid = (size_t)((code > 0 ? code : -code) - 1);
         const double sg = code > 0 ? 1.0 : -1.0;
         R rec[FACE_REC];
-        load_frec(s.ff + (size_t)FACE_REC * fid, rec);
+        load_frec<NC>(s.ff + (size_t)FACE_REC * fid, rec);
 #pragma unroll
         for (int k = 0; k < 8; k++) acc[k] = acc[k] + sg * (double)rec[k];
     }
 #pragma unroll
     for (int k = 0; k < 8; k++) COL(s.vis, k)[i] = acc[k];
+}
+__global__ void __launch_bounds__(256) k_vis_gather(DevMesh m, DevState<R> s) {
+    k_vis_gather_body<true>(m, s, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -2688,6 +2747,157 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
 }
 #undef MARK
 #undef EXCHANGE
+
+// ---------------------------------------------------------------------------
+// Fused step: one cooperative launch runs a whole time step.  The kernels of
+// enqueue_step run as phases, in the same order and with the same bodies,
+// over virtual blocks of 128 threads; a grid-wide barrier separates the
+// phases.  Results are those of the separate launches bit for bit (every
+// reduction is order-free: min, max, integer sums).  For small meshes, where
+// the fixed cost of ~20 dependent launches is a large part of a step.
+// Not for aliased meshes, the five-phase model, face modes 2 and 3, overset
+// fringes, partition halos or FP64 wall layers (the host keeps the graph).
+// Built in the parity variant only (HP_FUSED_STEP): without FMA contraction
+// the bodies round the same inlined here as in their own kernels.
+
+#if HP_FUSED_STEP
+#ifndef HP_FUSED_MINB
+#define HP_FUSED_MINB 4
+#endif
+// spins of a barrier wait (each with a 64 ns sleep) before it gives up
+#ifndef HP_SYNC_SPIN_LIMIT
+#define HP_SYNC_SPIN_LIMIT (1ll << 24)
+#endif
+
+// Every block of the grid arrives; false once any wait of any block gave up
+// (then every block returns at its next barrier, whose waits are bounded).
+__device__ __forceinline__ bool grid_sync(GridSync* g) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &g->gen;
+        const unsigned gen0 = *vgen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(&g->count, 1u) == gridDim.x - 1) {
+            atomicExch(&g->count, 0u);
+            __threadfence();
+            atomicAdd(&g->gen, 1u);
+        } else {
+            long long it = 0;
+            while (*vgen == gen0) {
+                if (++it > HP_SYNC_SPIN_LIMIT) {
+                    atomicExch(&g->err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_s = ok && *(volatile int*)&g->err == 0;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+template <int Z>
+__global__ void __launch_bounds__(128, HP_FUSED_MINB) k_step_fused(DevMesh m, DevState<R> s, DevParams P,
+                                                                   GridSync* g) {
+    const int nb = gridDim.x;
+#define PHASE(nthreads, CALL) \
+    for (int vb = blockIdx.x; vb < (int)(((long long)(nthreads) + 127) / 128); vb += nb) { CALL; }
+#define SYNC \
+    if (!grid_sync(g)) return;
+    // src/main.F90:521-556: dt and time of every case
+    PHASE(m.ncase, { const int c = vb * 128 + threadIdx.x; if (c < m.ncase) step_begin_case(s.s + c, P, s.s[c].dtmin_bits); })
+    SYNC
+    PHASE(m.neles, k_smooth1_body(m, s, vb))
+    SYNC
+    PHASE(m.neles, k_smooth2_body(m, s, P, vb))
+    SYNC
+    if (m.nghosts > 0) {
+        PHASE(m.nghosts, k_bc_body<true>(m, s, P, vb))
+        SYNC
+    }
+    if (!P.inviscid) {
+        if (sizeof(R) != sizeof(double) && HP_FACE_VISC && m.nface > 0) {
+            PHASE(m.nface, k_facevisc_body(m, s, P, vb))
+            SYNC
+            PHASE(m.neles, k_vis_gather_body<false>(m, s, vb))
+        } else if (HP_VISC_SPLIT) {
+            PHASE(8ll * m.neles, k_visc8_body<0>(m, s, P, vb))
+        } else {
+            PHASE(4ll * m.neles, k_visc4_body(m, s, P, vb))
+        }
+        SYNC
+    }
+    for (int stage = 1; stage <= P.nstage; stage++) {
+        // the primitive pass reduces through shared memory: a block barrier
+        // between its virtual blocks
+        PHASE(m.neles, { k_prim_body<PM_STAGE>(m, s, P, vb); __syncthreads(); })
+        SYNC
+        if (m.nghosts > 0) {
+            PHASE(m.nghosts, k_bc_body<false>(m, s, P, vb))
+            SYNC
+        }
+        if (P.myorder == 2) {
+            if (sizeof(R) != sizeof(double)) {
+                PHASE(m.neles, k_grad_body<true>(m, s, P, vb))
+            } else {
+                PHASE(4ll * m.neles, k_grad4_body<0>(m, s, P, vb))
+            }
+            SYNC
+        }
+        if (sizeof(R) != sizeof(double) && m.nface > 0) {
+            PHASE(m.nface, (k_faceflux_body<Z, false>(m, s, P, vb)))
+            SYNC
+            PHASE(m.neles, (k_flux_body<false, true, Z, false, false>(m, s, P, stage, vb)))
+        } else {
+            PHASE(4ll * m.neles, (k_flux4_body<Z, 0, false>(m, s, P, stage, vb)))
+        }
+        SYNC
+    }
+    PHASE(m.neles, { k_prim_body<PM_END>(m, s, P, vb); __syncthreads(); })
+    SYNC
+    PHASE(m.ncase, k_step_end_body(s, m.ncase, vb))
+    SYNC
+    PHASE(m.neles, { k_prim_body<PM_START>(m, s, P, vb); __syncthreads(); })
+#undef PHASE
+#undef SYNC
+}
+
+// Blocks of the fused step on this device: as many as are co-resident
+// (cooperative launch), at most the largest phase's virtual blocks.
+static int fused_grid(const DevMesh& m, const DevParams& P) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    cudaError_t e = P.myflux == 1
+                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_fused<1>, 128, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_fused<0>, 128, 0);
+    if (e != cudaSuccess || per_sm < 1) return 0;
+    const long long need = (8ll * m.neles + 127) / 128;
+    return (int)std::min<long long>((long long)sms * per_sm, std::max(need, 1ll));
+}
+
+static cudaError_t enqueue_fused(const DevMesh& m, const void* stp, const DevParams& P, cudaStream_t st,
+                                 GridSync* sync, int grid) {
+    DevState<R> s = *static_cast<const DevState<R>*>(stp);
+    DevMesh mm = m;
+    DevParams pp = P;
+    void* args[] = {&mm, &s, &pp, &sync};
+    return P.myflux == 1 ? cudaLaunchCooperativeKernel((void*)k_step_fused<1>, grid, 128, args, 0, st)
+                         : cudaLaunchCooperativeKernel((void*)k_step_fused<0>, grid, 128, args, 0, st);
+}
+#else
+// variants without the fused step (built with FMA contraction)
+static int fused_grid(const DevMesh&, const DevParams&) { return 0; }
+static cudaError_t enqueue_fused(const DevMesh&, const void*, const DevParams&, cudaStream_t, GridSync*, int) {
+    return cudaErrorNotSupported;
+}
+#endif
 
 }  // namespace HP_NS
 }  // namespace hp

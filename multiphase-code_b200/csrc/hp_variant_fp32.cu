@@ -22,5 +22,6 @@
 #include "hp_kernels.cuh"
 
 namespace hp {
-const Variant variant_fp32 = {"fp32", sizeof(float), &v_fp32::enqueue_start, &v_fp32::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0};
+const Variant variant_fp32 = {"fp32", sizeof(float), &v_fp32::enqueue_start, &v_fp32::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0,
+    &v_fp32::fused_grid, &v_fp32::enqueue_fused};
 }

@@ -24,7 +24,8 @@
 #include "hp_kernels.cuh"
 
 namespace hp {
-const Variant variant_fp64 = {"fp64", sizeof(double), &v_fp64::enqueue_start, &v_fp64::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0};
+const Variant variant_fp64 = {"fp64", sizeof(double), &v_fp64::enqueue_start, &v_fp64::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0,
+    &v_fp64::fused_grid, &v_fp64::enqueue_fused};
 
 // The FP64 (FMA) kernels over the wall-layer cell lists, for the steps of the
 // FP32-arithmetic variants (same compile flags as theirs: -fmad=true).

@@ -21,8 +21,11 @@
 #ifndef HP_VISC4_MINB
 #define HP_VISC4_MINB 3
 #endif
+// the fused step kernel (one cooperative launch per step)
+#define HP_FUSED_STEP 1
 #include "hp_kernels.cuh"
 
 namespace hp {
-const Variant variant_fp64_parity = {"fp64_parity", sizeof(double), &v_fp64_parity::enqueue_start, &v_fp64_parity::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0};
+const Variant variant_fp64_parity = {"fp64_parity", sizeof(double), &v_fp64_parity::enqueue_start, &v_fp64_parity::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0,
+    &v_fp64_parity::fused_grid, &v_fp64_parity::enqueue_fused};
 }

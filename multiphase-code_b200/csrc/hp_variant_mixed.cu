@@ -19,5 +19,6 @@
 #include "hp_kernels.cuh"
 
 namespace hp {
-const Variant variant_mixed = {"mixed", sizeof(float), &v_mixed::enqueue_start, &v_mixed::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0};
+const Variant variant_mixed = {"mixed", sizeof(float), &v_mixed::enqueue_start, &v_mixed::enqueue_step, (HP_FACE_VISC && sizeof(HP_R) != sizeof(double)) ? 1 : 0,
+    &v_mixed::fused_grid, &v_mixed::enqueue_fused};
 }

@@ -124,6 +124,8 @@ class Server:
     block_size: threads per block of the per-cell kernels: an int, a dict
         from hydraphase.tune.size_class() to an int, or None (256)
     face_mode: hp_params.face_mode, an int or a dict by size class (None: 0)
+    step_mode: hp_params.use_graph (1: graph, 2: fused step), an int or a
+        dict by size class (None: 1)
     host_threads: OpenMP threads of each set-up worker's hp_create (None: the
         cores divided among the workers, so that concurrent set-ups do not
         oversubscribe the host and delay the loop that feeds the GPU)
@@ -132,7 +134,7 @@ class Server:
     def __init__(self, hbm_budget: int, precision: int = PREC_MIXED, max_active: int = 12, chunk: int = 25,
                  setup_workers: int = 8, keep_state: bool = True, param_overrides: dict | None = None,
                  batch_cells: int = 0, max_batch: int = 64, block_size=None, face_mode=None,
-                 chunk_cell_steps: int | None = None, host_threads: int | None = None):
+                 chunk_cell_steps: int | None = None, host_threads: int | None = None, step_mode=None):
         self.budget = int(hbm_budget)
         self.precision = precision
         self.max_active = max_active
@@ -144,6 +146,7 @@ class Server:
         self.max_batch = int(max_batch)
         self.block_size = block_size
         self.face_mode = face_mode
+        self.step_mode = step_mode
         self.chunk_cell_steps = chunk_cell_steps
         self.host_threads = host_threads
 
@@ -159,6 +162,11 @@ class Server:
             over["block_size"] = int(b)
         if fm and "face_mode" not in over:
             over["face_mode"] = int(fm)
+        sm = self.step_mode
+        if isinstance(sm, dict):
+            sm = sm.get(size_class(cells))
+        if sm and "use_graph" not in over:
+            over["use_graph"] = int(sm)
         return spec.params(precision=self.precision, **over)
 
     @staticmethod

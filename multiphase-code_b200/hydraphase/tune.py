@@ -3,7 +3,7 @@ for each mesh-size class, and caches the choices.
 
 Two levels are tuned:
 
-* **Kernels** (`tune_block_size`, `tune_face_mode`). These are the threads
+* **Kernels** (`tune_block_size`, `tune_face_mode`, `tune_step_mode`). These are the threads
   per block of the one-thread-per-cell kernels (primitive recovery, JST
   smoothing, ghost fill, and the gradients and face gathers of the
   FP32-arithmetic variants) and, for those variants, how the HLLC fluxes
@@ -16,7 +16,10 @@ Two levels are tuned:
   events) of a representative case of the class: the best of three runs from
   the initial state, each of at least 20 ms (up to 200 steps).  The fastest
   is kept. The four-lane kernels have their block size fixed by their launch
-  bounds, tuned per precision variant at build time.
+  bounds, tuned per precision variant at build time. Last, whether a step
+  replays its ~20 kernels from a CUDA graph or runs as one fused cooperative
+  kernel (grid-wide barriers between the phases), which saves the fixed
+  cost of the launches on small meshes.
 * **Serving** (`tune_serving`). These are the units in flight, the
   multi-mesh batch size and the steps enqueued per turn. Every candidate
   serves a short sample of the stream with all cases arriving at once, and
@@ -34,7 +37,7 @@ import math
 import os
 import time
 
-from ._lib import PREC_FP32, PREC_MIXED
+from ._lib import PREC_FP32, PREC_FP64_PARITY, PREC_MIXED
 from .engine import Case
 
 SIZE_CLASSES = ((0, 20000, "xs"), (20000, 100000, "s"), (100000, 400000, "m"), (400000, 1 << 62, "l"))
@@ -140,6 +143,33 @@ def tune_face_mode(spec, precision: int = PREC_MIXED, block_size: int = 0, steps
     ms = {}
     for mode in modes:
         with Case(spec.mesh, spec.params(precision=precision, block_size=int(block_size), face_mode=mode)) as c:
+            ms[mode] = _ms_per_step(c, spec, steps)
+    best = min(ms, key=ms.get)
+    data = _load()
+    data[key] = {"best": best, "ms": {str(k): v for k, v in ms.items()}, "cells": spec.mesh.neles,
+                 "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+    _store(data)
+    return best, ms
+
+
+def tune_step_mode(spec, precision: int = PREC_MIXED, block_size: int = 0, face_mode: int = 0, steps: int = 6,
+                   use_cache: bool = True) -> tuple[int, dict]:
+    """hp_params.use_graph for the size class of `spec`: 1 (the step's
+    kernels replayed from a CUDA graph) or 2 (the fused step, one
+    cooperative kernel per step); returns (best, {mode: ms per step}).
+    Only the FP64 parity variant has the fused step (the variants built with
+    FMA contraction keep the graph), so the others return (1, {})."""
+    if precision != PREC_FP64_PARITY:
+        return 1, {}
+    key = _key(precision, size_class(spec.mesh.neles), f"step_mode_b{block_size}_f{face_mode}")
+    if use_cache:
+        hit = _load().get(key)
+        if hit:
+            return int(hit["best"]), {int(k): v for k, v in hit["ms"].items()}
+    ms = {}
+    for mode in (1, 2):
+        with Case(spec.mesh, spec.params(precision=precision, block_size=int(block_size), face_mode=int(face_mode),
+                                         use_graph=mode)) as c:
             ms[mode] = _ms_per_step(c, spec, steps)
     best = min(ms, key=ms.get)
     data = _load()

@@ -109,3 +109,29 @@ def test_face_mode_tuner_measures_and_caches(tmp_path, monkeypatch):
     assert best in (0, 1, 2)
     assert tune.tune_face_mode(spec, steps=2) == (best, ms)
     assert tune.tune_face_mode(spec, precision=PREC_FP64_PARITY) == (0, {})
+
+
+@pytest.mark.gpu
+def test_step_mode_tuner_measures_and_caches(tmp_path, monkeypatch):
+    from hydraphase import PREC_FP64_PARITY, tune
+    monkeypatch.setenv("HYDRAPHASE_TUNE_CACHE", str(tmp_path / "t.json"))
+    spec = cases.shock_bubble(n=8, alpha_min=0.1)
+    best, ms = tune.tune_step_mode(spec, precision=PREC_FP64_PARITY, steps=2)
+    assert set(ms) == {1, 2} and best in (1, 2)      # graph, fused step
+    assert tune.tune_step_mode(spec, precision=PREC_FP64_PARITY, steps=2) == (best, ms)
+    assert tune.tune_step_mode(spec, precision=PREC_MIXED) == (1, {})
+
+
+@pytest.mark.gpu
+def test_served_fused_results_equal_graph_results():
+    from hydraphase.serve import Server
+    reqs = cases.serving_stream(n_cases=6, rate=1000.0, steps=20, cells=(3000, 30000), seed=5)
+    outs = []
+    for mode in (1, 2):
+        server = Server(hbm_budget=8 << 30, precision=PREC_FP64_PARITY, max_active=3, chunk=10,
+                        batch_cells=60000, step_mode=mode)
+        rep = server.run(reqs, realtime=False)
+        assert all(r.error is None for r in rep.results)
+        outs.append({r.rid: r.cu for r in rep.results})
+    for rid in outs[0]:
+        np.testing.assert_array_equal(outs[1][rid], outs[0][rid])
