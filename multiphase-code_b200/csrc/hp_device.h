@@ -107,8 +107,9 @@ struct DevMesh {
     // the cells within a few layers of a wall ghost (wcells, ascending) take
     // their viscous terms, fluxes, sources and RK update from the FP64
     // kernels over these lists; gcells adds their interior neighbours, whose
-    // FP64 gradients those fluxes reconstruct from; wclass[i] = 1 marks the
-    // cells of wcells, which the FP32 kernels leave alone
+    // FP64 gradients those fluxes reconstruct from; wclass[i] != 0 marks the
+    // cells of wcells, which the FP32 kernels leave alone (2: no neighbour
+    // outside the layers, so not even their FP32 gradients are read)
     int nwall, ngwall;
     const int* wcells;
     const int* gcells;

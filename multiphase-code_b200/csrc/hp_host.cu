@@ -265,8 +265,8 @@ struct Layout {
 
 // Cells within `layers` layers of a wall ghost (types 5 and 6), breadth
 // first over the interior neighbours: wall (ascending), the same with their
-// interior neighbours added (grad, ascending), and the per-slot class (1:
-// wall layer).
+// interior neighbours added (grad, ascending), and the per-slot class (1: a
+// layer cell with a neighbour outside the layers, 2: one without).
 static void wall_layers(const Layout& L, int neles, int nghosts, long long ld, int layers,
                         std::vector<int>& wall, std::vector<int>& grad, std::vector<unsigned char>& cls) {
     std::vector<int> gtype((size_t)nghosts, 0);
@@ -307,6 +307,16 @@ static void wall_layers(const Layout& L, int neles, int nghosts, long long ld, i
         }
     for (int t = 0; t < neles; t++)
         if (ing[t]) grad.push_back(t);
+    // class 2: every interior neighbour is a layer cell too, so no FP32 face
+    // needs the cell's FP32 gradients
+    for (int t : wall) {
+        bool inner = true;
+        for (int f = 0; f < 4 && inner; f++) {
+            const int j = L.nc[(size_t)f * ld + t];
+            if (j < neles && layer[j] == 0) inner = false;
+        }
+        if (inner) cls[t] = 2;
+    }
 }
 
 // One case of a handle: validates its connectivity, computes its geometry

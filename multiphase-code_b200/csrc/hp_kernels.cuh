@@ -796,6 +796,15 @@ __device__ __forceinline__ bool grad_cell(int ib) { return ib == 1 || ib == HP_I
 // Venkatakrishnan limiter (src/sr_VK.F90:32-272).  grad_cell() cells.
 // FPR: read the primitives in R (the float copy of the FP32-arithmetic
 // variants) instead of the FP64 columns; false on aliased meshes.
+// FP64 wall layers of the FP32 variants: a face whose two cells are layer
+// cells (or a layer cell's boundary face) feeds only FP64 kernels, so the
+// FP32 face kernels skip it.
+__device__ __forceinline__ bool wall_face(const DevMesh& m, int i, int f) {
+    if (sizeof(R) == sizeof(double) || m.nwall == 0 || !ldg(m.wclass + i)) return false;
+    const int j = ldg(COL(m.nc, f) + i);
+    return j >= m.neles || ldg(m.wclass + j) != 0;
+}
+
 template <bool FPR>
 __device__ __forceinline__ void k_grad_body(DevMesh m, DevState<R> s, DevParams P, int bid) {
     using PT = typename std::conditional<FPR, R, double>::type;
@@ -803,6 +812,9 @@ __device__ __forceinline__ void k_grad_body(DevMesh m, DevState<R> s, DevParams 
     int i = bid * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     if (!grad_cell(ldg(m.iblank + i))) return;
+    // FP64 wall layers: no FP32 face reads the gradients of a layer cell
+    // whose neighbours are all layer cells (class 2)
+    if (sizeof(R) != sizeof(double) && m.nwall > 0 && ldg(m.wclass + i) == 2) return;
     int n[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
@@ -1155,7 +1167,9 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     }
     const R eps8 = (R)(double)1.0e-8f, eps6 = (R)(double)1.0e-6f;
     const R rgm1 = (R)P.r_gm1, rgamap = (R)P.r_gamap;
-    const R rropL = mrcp<F>(ropL, bad), rropR = mrcp<F>(ropR, bad);
+    // the gas phase's wave speeds and HLLC first, then the liquid's: each
+    // phase's quantities are live only while it is evaluated (the values and
+    // their order of evaluation are those of src/sr_hllcbatten.F90:338-529)
     R egL = mdiv<F>(rrg * tgL, gamag - R(1), rgm1, bad) + R(0.5) * (ugL * ugL + vgL * vgL + wgL * wgL);
     const R rrogL = mrcp<F>(rogL, bad), rrogR = mrcp<F>(rogR, bad);
     R hgL = egL + mdiv<F>(pgL, rogL, rrogL, bad);
@@ -1165,32 +1179,30 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
     R hgR = egR + mdiv<F>(pgR, rogR, rrogR, bad);
     R qgR = ugR * enx + vgR * eny + wgR * enz;
     R agR = sqrt(mdiv<F>(gamag * pgR, rogR, rrogR, bad));
-    R epL = mdiv<F>(cpp * tpL, gamap, rgamap, bad) + mdiv<F>(pinf, ropL, rropL, bad) +
-            R(0.5) * (upL * upL + vpL * vpL + wpL * wpL);
-    R hpL = epL + mdiv<F>(ppL, ropL, rropL, bad);
-    R qpL = upL * enx + vpL * eny + wpL * enz;
-    R apL = sqrt(mdiv<F>(gamap * (ppL + pinf), ropL, rropL, bad));
-    R epR = mdiv<F>(cpp * tpR, gamap, rgamap, bad) + mdiv<F>(pinf, ropR, rropR, bad) +
-            R(0.5) * (upR * upR + vpR * vpR + wpR * wpR);
-    R hpR = epR + mdiv<F>(ppR, ropR, rropR, bad);
-    R qpR = upR * enx + vpR * eny + wpR * enz;
+#define HP_LIQUID_WAVES \
+    const R rropL = mrcp<F>(ropL, bad), rropR = mrcp<F>(ropR, bad); \
+    R epL = mdiv<F>(cpp * tpL, gamap, rgamap, bad) + mdiv<F>(pinf, ropL, rropL, bad) + \
+            R(0.5) * (upL * upL + vpL * vpL + wpL * wpL); \
+    R hpL = epL + mdiv<F>(ppL, ropL, rropL, bad); \
+    R qpL = upL * enx + vpL * eny + wpL * enz; \
+    R apL = sqrt(mdiv<F>(gamap * (ppL + pinf), ropL, rropL, bad)); \
+    R epR = mdiv<F>(cpp * tpR, gamap, rgamap, bad) + mdiv<F>(pinf, ropR, rropR, bad) + \
+            R(0.5) * (upR * upR + vpR * vpR + wpR * wpR); \
+    R hpR = epR + mdiv<F>(ppR, ropR, rropR, bad); \
+    R qpR = upR * enx + vpR * eny + wpR * enz; \
     R apR = sqrt(mdiv<F>(gamap * (ppR + pinf), ropR, rropR, bad));
     if constexpr (Z == 1) {
+        HP_LIQUID_WAVES
         zien_flux<F>(o, bad, area, enx, eny, enz, phigL, phipL, rogL, ropL, ugL, vgL, wgL, upL, vpL, wpL, pgL,
                      ppL, egL, hgL, qgL, agL, epL, hpL, qpL, apL, phigR, phipR, rogR, ropR, ugR, vgR, wgR, upR,
                      vpR, wpR, pgR, ppR, egR, hgR, qgR, agR, epR, hpR, qpR, apR);
         return;
     }
     R sgl = mn2(mn2(qgL - agL, qgR - agR), eps8);
-    R spl = mn2(mn2(qpL - apL, qpR - apR), eps8);
     R sgr = mx2(mx2(qgL + agL, qgR + agR), eps8);
-    R spr = mx2(mx2(qpL + apL, qpR + apR), eps8);
     R sgstar = (pgR - pgL + rogL * qgL * (sgl - qgL) - rogR * qgR * (sgr - qgR)) /
                ((rogL * (sgl - qgL) - rogR * (sgr - qgR)) + eps8);
-    R spstar = (ppR - ppL + ropL * qpL * (spl - qpL) - ropR * qpR * (spr - qpR)) /
-               ((ropL * (spl - qpL) - ropR * (spr - qpR)) + eps8);
     R pgstar = mx2(pgL + rogL * (qgL - sgl) * (qgL - sgstar), eps6 * mn2(pgL, pgR));
-    R ppstar = mx2(ppL + ropL * (qpL - spl) * (qpL - spstar), eps6 * mn2(ppL, ppR));
     // gas phase
     {
         int br = (sgl > R(0)) ? 1 : (sgl <= R(0) && sgstar > R(0)) ? 2
@@ -1248,6 +1260,13 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
             }
         }
     }
+    HP_LIQUID_WAVES
+#undef HP_LIQUID_WAVES
+    R spl = mn2(mn2(qpL - apL, qpR - apR), eps8);
+    R spr = mx2(mx2(qpL + apL, qpR + apR), eps8);
+    R spstar = (ppR - ppL + ropL * qpL * (spl - qpL) - ropR * qpR * (spr - qpR)) /
+               ((ropL * (spl - qpL) - ropR * (spr - qpR)) + eps8);
+    R ppstar = mx2(ppL + ropL * (qpL - spl) * (qpL - spstar), eps6 * mn2(ppL, ppR));
     // liquid phase
     {
         int br = (spl > R(0)) ? 1 : (spl <= R(0) && spstar > R(0)) ? 2
@@ -1920,6 +1939,7 @@ __device__ __forceinline__ void k_faceflux_body(DevMesh m, DevState<R> s, DevPar
     const int t = bid * blockDim.x + threadIdx.x;
     if (t >= m.nface) return;
     const int i = ldg(m.f_i + t), f = ldg(m.f_code + t) & 3;
+    if (wall_face(m, i, f)) return;
     FaceOut o{};
     unsigned bad = 0;
     face_eval<0, Z, R, NC>(m, s, P, i, f, o, bad, s.prr);
@@ -2280,6 +2300,7 @@ __device__ __forceinline__ void k_facevisc_body(DevMesh m, DevState<R> s, DevPar
     const int t = bid * blockDim.x + threadIdx.x;
     if (t >= m.nface) return;
     const int i = ldg(m.f_i + t), f = ldg(m.f_code + t) & 3;
+    if (wall_face(m, i, f)) return;
     int nci[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) nci[k] = ldg(COL(m.nc, k) + i);
@@ -2303,6 +2324,7 @@ __device__ __forceinline__ void k_vis_gather_body(DevMesh m, DevState<R> s, int 
     const int i = bid * blockDim.x + threadIdx.x;
     if (i >= m.neles) return;
     if (ldg(m.iblank + i) != 1) return;
+    if (sizeof(R) != sizeof(double) && m.nwall > 0 && ldg(m.wclass + i)) return;   // FP64 wall layers
     double acc[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) acc[k] = 0.0;
