@@ -233,6 +233,23 @@ def profiled_traffic_per_cell(kernel: str):
     return None
 
 
+def profiled_pipes(kernel: str):
+    """FP64-pipe and issue activity (fractions of peak over active cycles) of
+    `kernel` from its committed ncu summary (lines 'fp64_pipe_active: X' and
+    'issue_active: Y', percent), or None: what bounds a kernel that is not
+    DRAM-bound."""
+    import glob
+    import re
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", kernel + "_*.md"))):
+        t = open(path).read()
+        a = re.search(r"fp64_pipe_active:\s*([0-9.]+)", t)
+        b = re.search(r"issue_active:\s*([0-9.]+)", t)
+        if a and b:
+            return {"fp64_pipe_active": float(a.group(1)) / 100, "issue_active": float(b.group(1)) / 100,
+                    "source": "profiles/" + os.path.basename(path)}
+    return None
+
+
 def cpu_oracle_run(spec, threads: int, warmup: int, steps: int | None = None,
                    seconds_target: float | None = None):
     """The CPU restatement of the reference (oracle/, FP64, OpenMP over cells
@@ -626,6 +643,7 @@ def run_ours(args, world, rank, local, pg):
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "peak_source": peak_src, "bytes_per_cell": fb, "traffic": traffic,
                      "traffic_source": (f"profiles/{tp[1]}: ncu dram bytes per cell x {cells} cells" if tp else None),
+                     "pipes": profiled_pipes("k_flux4"),
                      "launch_ms": flux_ms,
                      "step_level": {"bytes_per_cell_stage": STEP_BYTES_FP64, "achieved": achieved_step,
                                     "frac": achieved_step / hbm_peak}},

@@ -71,6 +71,8 @@ struct DevMesh {
     // reciprocals of the weights and of the determinant; LSQA for the 1/r^2
     // cell gradients (src/sr_derivative.F90:163-176,255), LSQB for the 1/r
     // gradient of alpha_g in the sources (src/sr_source.F90:100-117)
+    const double* dxn;      // [12][ld] centroid of neighbour f minus the
+                            // cell's (x, y, z of face 1, then 2, 3, 4)
     const double* lsqa;     // [NLSQ][ld]
     const double* lsqb;     // [NLSQ][ld]
     const int *g_par, *g_id, *g_type;   // [nghosts] ghost list (reference order)

@@ -187,6 +187,7 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     m.eps2 = (double*)a.take(ld * D);
     m.sc = (double*)a.take(12 * ld * D); m.fch = (double*)a.take(12 * ld * D);
     m.fcv = (double*)a.take(12 * ld * D);
+    m.dxn = (double*)a.take(12 * ld * D);
     m.lsqa = (double*)a.take(NLSQ * ld * D);
     m.lsqb = (double*)a.take(NLSQ * ld * D);
     m.g_par = (int*)a.take((nghosts + 1) * (size_t)I); m.g_id = (int*)a.take((nghosts + 1) * (size_t)I);
@@ -836,6 +837,18 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     if (e == cudaSuccess) e = up(m.sc, L.sc.data(), 12 * ld * D);
     if (e == cudaSuccess) e = up(m.fch, L.fch.data(), 12 * ld * D);
     if (e == cudaSuccess) e = up(m.fcv, L.fcv.data(), 12 * ld * D);
+    // neighbour centroid differences of the FP64 gradient and source LSQ
+    // (the subtraction the kernels would do on the gathered centroids)
+    std::vector<double> hdxn(12 * (size_t)ld, 0.0);
+#pragma omp parallel for schedule(static)
+    for (long long t = 0; t < neles; t++)
+        for (int f = 0; f < 4; f++) {
+            const int j = L.nc[(size_t)f * ld + t];
+            hdxn[(size_t)(3 * f) * ld + t] = L.x[j] - L.x[t];
+            hdxn[(size_t)(3 * f + 1) * ld + t] = L.y[j] - L.y[t];
+            hdxn[(size_t)(3 * f + 2) * ld + t] = L.z[j] - L.z[t];
+        }
+    if (e == cudaSuccess) e = up(m.dxn, hdxn.data(), 12 * ld * D);
     if (e == cudaSuccess) e = up(m.lsqa, L.la.data(), NLSQ * ld * D);
     if (e == cudaSuccess) e = up(m.lsqb, L.lb.data(), NLSQ * ld * D);
     if (e == cudaSuccess && nghosts) e = up(m.g_par, L.gpar.data(), nghosts * (size_t)I);

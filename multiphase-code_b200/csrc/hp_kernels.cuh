@@ -82,6 +82,11 @@ template <class T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p
 #endif
 // viscous fluxes of the cell-centric variants with eight lanes per cell (one
 // phase each, k_visc8) instead of four (k_visc4)
+// FP64 four-lane kernels: neighbour centroid differences from the set-up
+// table m.dxn instead of gathered centroids
+#ifndef HP_DXN_TABLE
+#define HP_DXN_TABLE 1
+#endif
 #ifndef HP_VISC_SPLIT
 #define HP_VISC_SPLIT 1
 #endif
@@ -1579,9 +1584,16 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
     R xa[4], ya[4], za[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) {
+#if HP_DXN_TABLE
+        // the centroid differences, formed at set-up (the same subtraction)
+        xa[f] = (R)ldg(COL(m.dxn, 3 * f) + i);
+        ya[f] = (R)ldg(COL(m.dxn, 3 * f + 1) + i);
+        za[f] = (R)ldg(COL(m.dxn, 3 * f + 2) + i);
+#else
         xa[f] = (R)(ldg(m.xc + n[f]) - x0);
         ya[f] = (R)(ldg(m.yc + n[f]) - y0);
         za[f] = (R)(ldg(m.zc + n[f]) - z0);
+#endif
     }
     // geometry-only terms (wt, a1..b3, dnr of src/sr_derivative.F90:163-176,
     // 255), evaluated once at set-up with the same expressions
@@ -1731,7 +1743,12 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     // neighbour data for the alpha_g gradient of the sources
     const int nq = ldg(COL(m.nc, q) + i);
     const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
+#if HP_DXN_TABLE
+    const R xq = (R)ldg(COL(m.dxn, 3 * q) + i), yq = (R)ldg(COL(m.dxn, 3 * q + 1) + i),
+            zq = (R)ldg(COL(m.dxn, 3 * q + 2) + i);
+#else
     const R xq = (R)(ldg(m.xc + nq) - x0), yq = (R)(ldg(m.yc + nq) - y0), zq = (R)(ldg(m.zc + nq) - z0);
+#endif
     // alpha_g differences from the FP64 primitives (see k_grad)
     const R pq = (R)(COL(s.pr, P_PHIG)[nq] - COL(s.pr, P_PHIG)[i]);
     // residual in face order 1..4 (src/sr_hllcbatten.F90:534-552)
