@@ -1567,6 +1567,90 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
     k_flux_body<ALIASED, FACE, Z, ACC>(m, s, P, stage, blockIdx.x);
 }
 
+// Asynchronous global-to-shared copies: 16 bytes through L2 only (the tail
+// prefetch of the four-lane flux kernel), 8 bytes through L1 (the limiter
+// prefetch of the four-lane gradient kernel).
+#ifndef HP_FLUX4_PREFETCH
+#define HP_FLUX4_PREFETCH 0
+#endif
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+#ifndef HP_GRAD4_LIMPF
+#define HP_GRAD4_LIMPF 0
+#endif
+// GPF (with LIMPF and SMEM): the gradient fields' values at the cell and its
+// neighbours are copied to shared memory too, one group per field
+#ifndef HP_GRAD4_GPF
+#define HP_GRAD4_GPF 0
+#endif
+enum { LIM_LD = 128, LIMC_N = 13, LIMC_LD = 32 };
+
+// ---------------------------------------------------------------------------
+// Venkatakrishnan limiter of the four-lane gradient kernel: lane q limits
+// pg, pp, rog or rop from the gradient it holds (lg) or receives (sg of
+// another lane), over its four faces; lane 0 stores the cell's minimum.
+// lp, lc (LIMPF, below): the limiter field of the lane's cell and of its
+// four neighbours (lp[k * LIM_LD], k = 0 the cell) and the cell's face
+// centroids and epsilon^2 (lc[k * LIMC_LD], k = 0..11 fch, 12 eps2), copied
+// to shared memory when the kernel started; null: read from global memory
+__device__ __forceinline__ unsigned grad4_limiter(const DevMesh& m, const DevState<R>& s, const DevParams& P,
+                                                  int i, int q, bool active, const int n[4], double x0,
+                                                  double y0, double z0, R lg[3], const R sg[3],
+                                                  const double* lp, const double* lc) {
+    // lane 2 takes rog from lane 3, lane 3 takes rop from lane 0
+    const int src = q == 2 ? 3 : (q == 3 ? 0 : q);
+    R fx0 = qshfl(sg[0], src), fy0 = qshfl(sg[1], src), fz0 = qshfl(sg[2], src);
+    if (q >= 2) { lg[0] = fx0; lg[1] = fy0; lg[2] = fz0; }
+    const int lcol = q == 0 ? P_PG : q == 1 ? P_PP : q == 2 ? P_ROG : P_ROP;
+    if (lp) {
+        cp_async_wait_all();
+        __syncwarp();
+    }
+    const R epssq = lc ? (R)lc[12 * LIMC_LD] : (R)ldg(m.eps2 + i);
+    const R* qq = COL(s.prr, lcol);
+    R qi = lp ? (R)lp[0] : qq[i];
+    R q0 = lp ? (R)lp[LIM_LD] : qq[n[0]], q1 = lp ? (R)lp[2 * LIM_LD] : qq[n[1]];
+    R q2 = lp ? (R)lp[3 * LIM_LD] : qq[n[2]], q3 = lp ? (R)lp[4 * LIM_LD] : qq[n[3]];
+    R vmax = mx2(mx2(mx2(mx2(qi, q0), q1), q2), q3);
+    R vmin = mn2(mn2(mn2(mn2(qi, q0), q1), q2), q3);
+    R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
+    R phl = R(0);
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        R fx = (R)((lc ? lc[f * LIMC_LD] : ldg(COL(m.fch, f) + i)) - x0);
+        R fy = (R)((lc ? lc[(4 + f) * LIMC_LD] : ldg(COL(m.fch, 4 + f) + i)) - y0);
+        R fz = (R)((lc ? lc[(8 + f) * LIMC_LD] : ldg(COL(m.fch, 8 + f) + i)) - z0);
+        R d = fx * lg[0] + fy * lg[1] + fz * lg[2];
+        R ph;
+        if (d > R(0)) ph = fvenkat(dmax, d, epssq);
+        else if (d < R(0)) ph = fvenkat(dmin, d, epssq);
+        else ph = R(1);
+        phl = (f == 0) ? ph : mn2(phl, ph);
+    }
+    R p0 = qshfl(phl, 0), p1 = qshfl(phl, 1), p2 = qshfl(phl, 2), p3 = qshfl(phl, 3);
+    if (q == 0 && active) s.phi[i] = (double)mn2(mn2(mn2(p0, p1), p2), p3);
+    return 0u;
+}
+
+// Shared-memory staging of the cell geometry of the four-lane gradient
+// kernel: the 12 centroid differences and the 16 least-squares terms of the
+// block's 32 cells, [28][32] doubles, so that the field loop reads them from
+// shared memory instead of holding 28 doubles per lane in registers.
+#ifndef HP_GRAD4_SMEM
+#define HP_GRAD4_SMEM 0
+#endif
+enum { GEO_N = 28, GEO_LD = 32 };
+
 // ---------------------------------------------------------------------------
 // k_grad with four lanes per cell: lane q computes the LSQ gradients of
 // fields q, q+4, q+8, q+12 and the limiter of one of pg, pp, rog, rop; phi is
@@ -1575,12 +1659,80 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
 // the fast form's out-of-range flag.
 template <int F>
 __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int i,
-                                               int q, bool active) {
+                                               int q, bool active, const double* geo, const double* lp,
+                                               const double* lc, const double* gp) {
     unsigned bad = 0;
     int n[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
     const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
+#if HP_GRAD4_SMEM && HP_DXN_TABLE && HP_LSQ_TABLE
+    if constexpr (sizeof(R) == sizeof(double)) {
+        // geo[k * GEO_LD]: k < 12 the centroid differences (x, y, z of faces
+        // 1..4), 12 + j column j of the LSQA table
+#define GX(f) geo[(3 * (f)) * GEO_LD]
+#define GY(f) geo[(3 * (f) + 1) * GEO_LD]
+#define GZ(f) geo[(3 * (f) + 2) * GEO_LD]
+#define GT(j) geo[(12 + (j)) * GEO_LD]
+#undef DW
+#define DW(x, f) mdiv<F>((x), GT(f), GT(11 + (f)), bad)
+#pragma unroll
+        for (int f = 0; f < 4; f++) (void)mrcp_tab<F>(GT(f), GT(11 + f), bad);
+        (void)mrcp_tab<F>(GT(10), GT(15), bad);
+        const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
+        R lg[3] = {R(0), R(0), R(0)};
+        R sg[3] = {R(0), R(0), R(0)};
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int v = q + 4 * r;
+            if (v >= 13) break;
+            R qi, qa, qb, qc, qd;
+            if (gp) {
+                // this lane's copies of field v at the cell and its neighbours
+                // (group r of the GPF prefetch; the limiter's group follows)
+                if (r == 0) cp_async_wait_group<4>();
+                else if (r == 1) cp_async_wait_group<3>();
+                else if (r == 2) cp_async_wait_group<2>();
+                else cp_async_wait_group<1>();
+                const double* g = gp + 5 * r * LIM_LD;
+                qi = (R)g[0];
+                qa = (R)(g[LIM_LD] - qi); qb = (R)(g[2 * LIM_LD] - qi);
+                qc = (R)(g[3 * LIM_LD] - qi); qd = (R)(g[4 * LIM_LD] - qi);
+            } else {
+                const R* qq = COL(s.prr, pcol[v]);
+                qi = qq[i];
+                qa = (R)(qq[n[0]] - qi); qb = (R)(qq[n[1]] - qi); qc = (R)(qq[n[2]] - qi); qd = (R)(qq[n[3]] - qi);
+            }
+            R c1 = DW(qa * GX(0), 0) + DW(qb * GX(1), 1) + DW(qc * GX(2), 2) + DW(qd * GX(3), 3);
+            R c2;
+            if (v == 7)   // cTp2 lacks the /wt4 (src/sr_derivative.F90:225)
+                c2 = DW(qa * GY(0), 0) + DW(qb * GY(1), 1) + DW(qc * GY(2), 2) + qd * GY(3);
+            else
+                c2 = DW(qa * GY(0), 0) + DW(qb * GY(1), 1) + DW(qc * GY(2), 2) + DW(qd * GY(3), 3);
+            R c3 = DW(qa * GZ(0), 0) + DW(qb * GZ(1), 1) + DW(qc * GZ(2), 2) + DW(qd * GZ(3), 3);
+            const R a1 = GT(4), a2 = GT(5), a3 = GT(6), b1 = GT(7), b2 = GT(8), b3 = GT(9);
+            const R dnr = GT(10), rdnr = GT(15);
+            R gx = mdiv<F>(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr, bad);
+            R gy = mdiv<F>(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr, bad);
+            R gz = mdiv<F>(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr, bad);
+            if (v < 11 && active) {
+                COL(s.gr, 3 * v + 0)[i] = gx;
+                COL(s.gr, 3 * v + 1)[i] = gy;
+                COL(s.gr, 3 * v + 2)[i] = gz;
+            }
+            if (v == 8 || v == 9) { lg[0] = gx; lg[1] = gy; lg[2] = gz; }
+            if (v == 11 || v == 12) { sg[0] = gx; sg[1] = gy; sg[2] = gz; }
+        }
+#undef DW
+#undef GX
+#undef GY
+#undef GZ
+#undef GT
+#define DW(x, f) div_rn((x), wt[f], rw[f])
+        return bad | grad4_limiter(m, s, P, i, q, active, n, x0, y0, z0, lg, sg, lp, lc);
+    }
+#endif
+    (void)geo; (void)gp;
     R xa[4], ya[4], za[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) {
@@ -1657,34 +1809,9 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
     }
 #undef DW
 #define DW(x, f) div_rn((x), wt[f], rw[f])
-    // lane 2 takes rog from lane 3, lane 3 takes rop from lane 0
-    const int src = q == 2 ? 3 : (q == 3 ? 0 : q);
-    R fx0 = qshfl(sg[0], src), fy0 = qshfl(sg[1], src), fz0 = qshfl(sg[2], src);
-    if (q >= 2) { lg[0] = fx0; lg[1] = fy0; lg[2] = fz0; }
-    const int lcol = q == 0 ? P_PG : q == 1 ? P_PP : q == 2 ? P_ROG : P_ROP;
-    const R epssq = (R)ldg(m.eps2 + i);
-    const R* qq = COL(s.prr, lcol);
-    R qi = qq[i];
-    R vmax = mx2(mx2(mx2(mx2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
-    R vmin = mn2(mn2(mn2(mn2(qi, qq[n[0]]), qq[n[1]]), qq[n[2]]), qq[n[3]]);
-    R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
-    R phl = R(0);
-#pragma unroll
-    for (int f = 0; f < 4; f++) {
-        R fx = (R)(ldg(COL(m.fch, f) + i) - x0);
-        R fy = (R)(ldg(COL(m.fch, 4 + f) + i) - y0);
-        R fz = (R)(ldg(COL(m.fch, 8 + f) + i) - z0);
-        R d = fx * lg[0] + fy * lg[1] + fz * lg[2];
-        R ph;
-        if (d > R(0)) ph = fvenkat(dmax, d, epssq);
-        else if (d < R(0)) ph = fvenkat(dmin, d, epssq);
-        else ph = R(1);
-        phl = (f == 0) ? ph : mn2(phl, ph);
-    }
-    R p0 = qshfl(phl, 0), p1 = qshfl(phl, 1), p2 = qshfl(phl, 2), p3 = qshfl(phl, 3);
-    if (q == 0 && active) s.phi[i] = (double)mn2(mn2(mn2(p0, p1), p2), p3);
-    return bad;
+    return bad | grad4_limiter(m, s, P, i, q, active, n, x0, y0, z0, lg, sg, lp, lc);
 }
+
 
 // LIST = 1: the cells of m.gcells (the FP64 wall layers and their
 // neighbours) instead of all cells.
@@ -1698,18 +1825,98 @@ __device__ __forceinline__ void k_grad4_body(DevMesh m, DevState<R> s, DevParams
     const int k = valid ? (int)c : ncell - 1;
     const int i = LIST ? ldg(m.gcells + k) : k;
     const bool active = valid && grad_cell(ldg(m.iblank + i));
+    const double* geo = nullptr;
+#if HP_GRAD4_SMEM && HP_DXN_TABLE && HP_LSQ_TABLE
+    // the 28 geometry values of the block's 32 cells; lane q stages values
+    // q, q + 4, ... of its cell (a warp's 8 cells are its own, so a warp
+    // barrier orders the stores before the loads)
+    __shared__ double sgeo[GEO_N * GEO_LD];
+    const int cs = (int)(threadIdx.x >> 2) & (GEO_LD - 1);
+#pragma unroll
+    for (int k = q; k < GEO_N; k += 4)
+        sgeo[k * GEO_LD + cs] = k < 12 ? ldg(COL(m.dxn, k) + i) : ldg(COL(m.lsqa, k - 12) + i);
+    __syncwarp();
+    geo = sgeo + cs;
+#endif
+    const double *lp = nullptr, *lc = nullptr, *gp = nullptr;
+#if HP_GRAD4_LIMPF
+    if constexpr (sizeof(R) == sizeof(double)) {
+        // start copying what the limiter reads (see grad4_limiter): the
+        // lane's limiter field at the cell and its 4 neighbours, and face
+        // centroid columns q, 4 + q, 8 + q (lane 0 also epsilon^2)
+        __shared__ __align__(16) double slim[5 * LIM_LD];
+        __shared__ __align__(16) double slimc[LIMC_N * LIMC_LD];
+        const int tid = (int)threadIdx.x & (LIM_LD - 1), cl = (int)(threadIdx.x >> 2) & (LIMC_LD - 1);
+#if HP_GRAD4_GPF && HP_GRAD4_SMEM && HP_DXN_TABLE && HP_LSQ_TABLE
+        {
+            // fields q, q + 4, q + 8, q + 12 at the cell and its neighbours,
+            // one commit group per field (empty when the lane has no field)
+            __shared__ __align__(16) double sgat[4 * 5 * LIM_LD];
+            const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
+            int nn[4];
+#pragma unroll
+            for (int f = 0; f < 4; f++) nn[f] = ldg(COL(m.nc, f) + i);
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int v = q + 4 * r;
+                if (v < 13) {
+                    const double* qv = reinterpret_cast<const double*>(COL(s.prr, pcol[v]));
+                    double* g = sgat + 5 * r * LIM_LD + tid;
+                    cp_async8(g, qv + i);
+#pragma unroll
+                    for (int f = 0; f < 4; f++) cp_async8(g + (1 + f) * LIM_LD, qv + nn[f]);
+                }
+                cp_async_commit();
+            }
+            gp = sgat + tid;
+        }
+#endif
+        const int lcol = q == 0 ? P_PG : q == 1 ? P_PP : q == 2 ? P_ROG : P_ROP;
+        const double* qq = reinterpret_cast<const double*>(COL(s.prr, lcol));
+        cp_async8(slim + tid, qq + i);
+#pragma unroll
+        for (int f = 0; f < 4; f++) cp_async8(slim + (1 + f) * LIM_LD + tid, qq + ldg(COL(m.nc, f) + i));
+#pragma unroll
+        for (int d = 0; d < 3; d++) cp_async8(slimc + (4 * d + q) * LIMC_LD + cl, COL(m.fch, 4 * d + q) + i);
+        if (q == 0) cp_async8(slimc + 12 * LIMC_LD + cl, m.eps2 + i);
+        cp_async_commit();
+        lp = slim + tid;
+        lc = slimc + cl;
+    }
+#endif
     if constexpr (HP_FAST(1)) {
         // the outputs are not inputs of this kernel, so a warp that flagged
         // an operand simply recomputes and overwrites them
-        const unsigned bad = grad4_body<1>(m, s, P, i, q, active);
-        if (__any_sync(0xffffffffu, bad)) grad4_body<0>(m, s, P, i, q, active);
+        const unsigned bad = grad4_body<1>(m, s, P, i, q, active, geo, lp, lc, gp);
+        if (__any_sync(0xffffffffu, bad)) grad4_body<0>(m, s, P, i, q, active, geo, lp, lc, gp);
     } else {
-        grad4_body<0>(m, s, P, i, q, active);
+        grad4_body<0>(m, s, P, i, q, active, geo, lp, lc, gp);
     }
+#if (HP_GRAD4_SMEM && HP_DXN_TABLE && HP_LSQ_TABLE) || HP_GRAD4_LIMPF
+    // the fused step reuses the arrays for its next virtual block
+    __syncwarp();
+#endif
 }
 template <int LIST>
 __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevState<R> s, DevParams P) {
     k_grad4_body<LIST>(m, s, P, blockIdx.x);
+}
+
+// Columns of the tail prefetch: the 14 primitives, dl, vol, the 16 LSQB
+// terms, vis, d24, cu, cn and the 12 centroid differences; TAIL_LD cells
+// (one 128-thread block) per column.
+enum { TAIL_DL = 14, TAIL_VOL = 15, TAIL_LSQB = 16, TAIL_VIS = 32, TAIL_D24 = 40, TAIL_CU = 50, TAIL_CN = 60,
+       TAIL_DXN = 70, TAIL_N = 82, TAIL_LD = 32 };
+__device__ __forceinline__ const double* tail_col(const DevMesh& m, const DevState<R>& s, int k) {
+    if (k < TAIL_DL) return s.pr + (size_t)k * m.ld;
+    if (k == TAIL_DL) return m.dl;
+    if (k == TAIL_VOL) return m.vol;
+    if (k < TAIL_VIS) return m.lsqb + (size_t)(k - TAIL_LSQB) * m.ld;
+    if (k < TAIL_D24) return s.vis + (size_t)(k - TAIL_VIS) * m.ld;
+    if (k < TAIL_CU) return s.d24 + (size_t)(k - TAIL_D24) * m.ld;
+    if (k < TAIL_CN) return s.cu + (size_t)(k - TAIL_CU) * m.ld;
+    if (k < TAIL_DXN) return s.cn + (size_t)(k - TAIL_CN) * m.ld;
+    return m.dxn + (size_t)(k - TAIL_DXN) * m.ld;
 }
 
 // Residual + sources + RK update with four lanes per cell: lane q evaluates
@@ -1718,11 +1925,16 @@ __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevStat
 // form (see mdiv).  The fast form returns false, before any store, when a lane
 // of the warp flagged an operand (cn is read and written here, so the stores
 // must wait for that vote).
-template <int F, int Z, bool NC = true>
+template <int F, int Z, bool NC = true, bool PF = false>
 __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int stage,
-                                           int i, int q, bool active) {
+                                           int i, int q, bool active, const double* pf = nullptr) {
     unsigned bad = 0;
     const R* pr = s.prr;
+    // PF: the cell's own values after the face evaluation come from the
+    // shared-memory copy that k_flux4_body started (pf[k * TAIL_LD], column
+    // k of the TAIL_* map)
+#define TL(k, expr) (PF ? (R)pf[(k) * TAIL_LD] : (R)(expr))
+#define TLS(k, expr) (PF ? (S)pf[(k) * TAIL_LD] : (S)(expr))
     // this lane's face
     R eff[10];
     int flags;
@@ -1740,12 +1952,17 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         }
         flags = (o.wall ? 1 : 0) | (o.takeg ? 2 : 0) | (o.takep ? 4 : 0);
     }
+    if constexpr (PF) {
+        cp_async_wait_all();
+        __syncwarp();
+    }
     // neighbour data for the alpha_g gradient of the sources
     const int nq = ldg(COL(m.nc, q) + i);
     const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
 #if HP_DXN_TABLE
-    const R xq = (R)ldg(COL(m.dxn, 3 * q) + i), yq = (R)ldg(COL(m.dxn, 3 * q + 1) + i),
-            zq = (R)ldg(COL(m.dxn, 3 * q + 2) + i);
+    const R xq = TL(TAIL_DXN + 3 * q, ldg(COL(m.dxn, 3 * q) + i)),
+            yq = TL(TAIL_DXN + 3 * q + 1, ldg(COL(m.dxn, 3 * q + 1) + i)),
+            zq = TL(TAIL_DXN + 3 * q + 2, ldg(COL(m.dxn, 3 * q + 2) + i));
 #else
     const R xq = (R)(ldg(m.xc + nq) - x0), yq = (R)(ldg(m.yc + nq) - y0), zq = (R)(ldg(m.zc + nq) - z0);
 #endif
@@ -1788,12 +2005,13 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     }
     // interphase sources (src/sr_source.F90:46-155)
     {
-        const R tg = (R)COL(pr, P_TG)[i], phig = (R)COL(pr, P_PHIG)[i], rog = (R)COL(pr, P_ROG)[i];
-        const R rop = (R)COL(pr, P_ROP)[i], phip = (R)COL(pr, P_PHIP)[i];
-        const R ug = (R)COL(pr, P_UG)[i], vg = (R)COL(pr, P_VG)[i], wg = (R)COL(pr, P_WG)[i];
-        const R up = (R)COL(pr, P_UP)[i], vp = (R)COL(pr, P_VP)[i], wp = (R)COL(pr, P_WP)[i];
-        const R tp = (R)COL(pr, P_TP)[i], pg = (R)COL(pr, P_PG)[i];
-        const R dl = (R)ldg(m.dl + i), voli = (R)ldg(m.vol + i);
+        const R tg = TL(P_TG, COL(pr, P_TG)[i]), phig = TL(P_PHIG, COL(pr, P_PHIG)[i]),
+                rog = TL(P_ROG, COL(pr, P_ROG)[i]);
+        const R rop = TL(P_ROP, COL(pr, P_ROP)[i]), phip = TL(P_PHIP, COL(pr, P_PHIP)[i]);
+        const R ug = TL(P_UG, COL(pr, P_UG)[i]), vg = TL(P_VG, COL(pr, P_VG)[i]), wg = TL(P_WG, COL(pr, P_WG)[i]);
+        const R up = TL(P_UP, COL(pr, P_UP)[i]), vp = TL(P_VP, COL(pr, P_VP)[i]), wp = TL(P_WP, COL(pr, P_WP)[i]);
+        const R tp = TL(P_TP, COL(pr, P_TP)[i]), pg = TL(P_PG, COL(pr, P_PG)[i]);
+        const R dl = TL(TAIL_DL, ldg(m.dl + i)), voli = TL(TAIL_VOL, ldg(m.vol + i));
         const R amug = (R)P.as * sqrt(tg) / (R(1) + (R)P.ts / tg);
         const R du = ug - up, dv = vg - vp, dw = wg - wp;
         // alpha_g (alpha_g - 1) and 1 - alpha_g in the reference's form in
@@ -1827,13 +2045,14 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
 #undef DW
 #define DW(x, f) mdiv<F>((x), wt[f], rw[f], bad)
 #if HP_LSQ_TABLE
+#define LB(k) TL(TAIL_LSQB + (k), ldg(COL(m.lsqb, k) + i))
 #pragma unroll
         for (int f = 0; f < 4; f++) {
-            wt[f] = (R)ldg(COL(m.lsqb, f) + i);
-            rw[f] = mrcp_tab<F>(wt[f], (R)ldg(COL(m.lsqb, 11 + f) + i), bad);
+            wt[f] = LB(f);
+            rw[f] = mrcp_tab<F>(wt[f], LB(11 + f), bad);
         }
-        const R a1 = (R)ldg(COL(m.lsqb, 4) + i), a2 = (R)ldg(COL(m.lsqb, 5) + i), a3 = (R)ldg(COL(m.lsqb, 6) + i);
-        const R b1 = (R)ldg(COL(m.lsqb, 7) + i), b2 = (R)ldg(COL(m.lsqb, 8) + i), b3 = (R)ldg(COL(m.lsqb, 9) + i);
+        const R a1 = LB(4), a2 = LB(5), a3 = LB(6);
+        const R b1 = LB(7), b2 = LB(8), b3 = LB(9);
 #else
 #pragma unroll
         for (int f = 0; f < 4; f++) { wt[f] = sqrt(xa[f] * xa[f] + ya[f] * ya[f] + za[f] * za[f]); rw[f] = mrcp<F>(wt[f], bad); }
@@ -1845,7 +2064,7 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         const R b3 = DW(ya[0] * za[0], 0) + DW(ya[1] * za[1], 1) + DW(ya[2] * za[2], 2) + DW(ya[3] * za[3], 3);
 #endif
 #if HP_LSQ_TABLE
-        const R dnr = (R)ldg(COL(m.lsqb, 10) + i);
+        const R dnr = LB(10);
 #else
         const R dnr = det3(a1, b1, b2, b1, a2, b3, b2, b3, a3);
 #endif
@@ -1860,7 +2079,8 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         const R A12 = q == 1 ? c1 : b1, A22 = q == 1 ? c2 : a2, A32 = q == 1 ? c3 : b3;
         const R A13 = q >= 2 ? c1 : b2, A23 = q >= 2 ? c2 : b3, A33 = q >= 2 ? c3 : a3;
 #if HP_LSQ_TABLE
-        const R rdnr = mrcp_tab<F>(dnr, (R)ldg(COL(m.lsqb, 15) + i), bad);
+        const R rdnr = mrcp_tab<F>(dnr, LB(15), bad);
+#undef LB
         const R dq = mdiv<F>(det3(A11, A21, A31, A12, A22, A32, A13, A23, A33), dnr, rdnr, bad);
 #else
         const R dq = det3(A11, A21, A31, A12, A22, A32, A13, A23, A33) / dnr;
@@ -1871,14 +2091,14 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         const R g = R(0);
         R en = pint * (uint_ * dpx + vint * dpy + wint * dpz) + uint_ * fdgx + vint * fdgy + wint * fdgz + qsource;
         const double* vis = s.vis;
-        rhs[1] = rhs[1] - (S)((fdgx + pint * dpx + phig * rog * g) * voli) - (S)COL(vis, 0)[i];
-        rhs[2] = rhs[2] - (S)((fdgy + pint * dpy) * voli) - (S)COL(vis, 1)[i];
-        rhs[3] = rhs[3] - (S)((fdgz + pint * dpz) * voli) - (S)COL(vis, 2)[i];
-        rhs[4] = rhs[4] - (S)(en * voli) - (S)COL(vis, 3)[i];
-        rhs[6] = rhs[6] + (S)((fdgx + pint * dpx - phip * rop * g) * voli) - (S)COL(vis, 4)[i];
-        rhs[7] = rhs[7] + (S)((fdgy + pint * dpy) * voli) - (S)COL(vis, 5)[i];
-        rhs[8] = rhs[8] + (S)((fdgz + pint * dpz) * voli) - (S)COL(vis, 6)[i];
-        rhs[9] = rhs[9] + (S)(en * voli) - (S)COL(vis, 7)[i];
+        rhs[1] = rhs[1] - (S)((fdgx + pint * dpx + phig * rog * g) * voli) - TLS(TAIL_VIS + 0, COL(vis, 0)[i]);
+        rhs[2] = rhs[2] - (S)((fdgy + pint * dpy) * voli) - TLS(TAIL_VIS + 1, COL(vis, 1)[i]);
+        rhs[3] = rhs[3] - (S)((fdgz + pint * dpz) * voli) - TLS(TAIL_VIS + 2, COL(vis, 2)[i]);
+        rhs[4] = rhs[4] - (S)(en * voli) - TLS(TAIL_VIS + 3, COL(vis, 3)[i]);
+        rhs[6] = rhs[6] + (S)((fdgx + pint * dpx - phip * rop * g) * voli) - TLS(TAIL_VIS + 4, COL(vis, 4)[i]);
+        rhs[7] = rhs[7] + (S)((fdgy + pint * dpy) * voli) - TLS(TAIL_VIS + 5, COL(vis, 5)[i]);
+        rhs[8] = rhs[8] + (S)((fdgz + pint * dpz) * voli) - TLS(TAIL_VIS + 6, COL(vis, 6)[i]);
+        rhs[9] = rhs[9] + (S)(en * voli) - TLS(TAIL_VIS + 7, COL(vis, 7)[i]);
     }
     // five-phase: drag of q, r, s on the liquid (see k_flux)
     if (P.five_phase) {
@@ -1891,13 +2111,13 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         if (__any_sync(0xffffffffu, bad)) return false;
     }
     if (!active) return true;
-    const S dtbyvol = (S)s.s[case_of(m, i)].dt / (S)ldg(m.vol + i);
+    const S dtbyvol = (S)s.s[case_of(m, i)].dt / TLS(TAIL_VOL, ldg(m.vol + i));
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         const int j = q + 4 * r;
         if (j >= 10) break;
-        const S rr = rhs[j] - (S)COL(s.d24, j)[i];
-        const S cu = (S)COL(s.cu, j)[i];
+        const S rr = rhs[j] - TLS(TAIL_D24 + j, COL(s.d24, j)[i]);
+        const S cu = TLS(TAIL_CU + j, COL(s.cu, j)[i]);
         double* cnp = COL(s.cn, j) + i;
         if (P.rk_scheme == 0) {
             if (stage == 1) {
@@ -1905,7 +2125,7 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
                 *cnp = v;
                 COL(s.cn1, j)[i] = v;
             } else {
-                S upd = (S)*cnp - S(11.0 / 20.0) * dtbyvol * rr;
+                S upd = TLS(TAIL_CN + j, *cnp) - S(11.0 / 20.0) * dtbyvol * rr;
                 if (stage == 2) *cnp = S(3.0 / 8.0) * cu + S(5.0 / 8.0) * upd;
                 else if (stage == 3) *cnp = S(4.0 / 9.0) * cu + S(5.0 / 9.0) * upd;
                 else *cnp = S(111.0 / 1331.0) * cu + S(260.0 / 1331.0) * (S)COL(s.cn1, j)[i] + S(960.0 / 1331.0) * upd;
@@ -1913,12 +2133,14 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
         } else {
             if (stage == 1) *cnp = cu - dtbyvol * rr;
             else {
-                S upd = (S)*cnp - dtbyvol * rr;
+                S upd = TLS(TAIL_CN + j, *cnp) - dtbyvol * rr;
                 if (stage == 2) *cnp = S(0.75) * cu + S(0.25) * upd;
                 else *cnp = S(1.0 / 3.0) * cu + S(2.0 / 3.0) * upd;
             }
         }
     }
+#undef TL
+#undef TLS
     return true;
 }
 
@@ -1936,6 +2158,29 @@ __device__ __forceinline__ void k_flux4_body(DevMesh m, DevState<R> s, DevParams
     const int i = LIST ? ldg(m.wcells + k) : k;
     bool active = valid && ldg(m.iblank + i) == 1;
     if (sizeof(R) != sizeof(double) && m.nwall > 0) active = active && !ldg(m.wclass + i);
+#if HP_FLUX4_PREFETCH && HP_LSQ_TABLE && HP_DXN_TABLE
+    if constexpr (LIST == 0 && NC && sizeof(R) == sizeof(double)) {
+        // the warp's 8 consecutive cells: start the asynchronous copy of
+        // their values that the sources and the RK update read (TAIL_*),
+        // 64 bytes per column, while the faces are evaluated
+        __shared__ __align__(16) double stail[TAIL_N * TAIL_LD];
+        const int lane = (int)(threadIdx.x & 31), w8 = (int)((threadIdx.x >> 5) * 8);
+        const long long c0 = ((long long)bid * blockDim.x + (threadIdx.x & ~31u)) >> 2;
+        for (int t = lane; t < TAIL_N * 4; t += 32) {
+            const int k = t >> 2, part = t & 3;
+            cp_async16(stail + k * TAIL_LD + w8 + 2 * part, tail_col(m, s, k) + c0 + 2 * part);
+        }
+        cp_async_commit();
+        const double* pf = stail + ((threadIdx.x >> 2) & (TAIL_LD - 1));
+        if constexpr (HP_FAST(2)) {
+            if (!flux4_body<1, Z, NC, true>(m, s, P, stage, i, q, active, pf))
+                flux4_body<0, Z, NC, true>(m, s, P, stage, i, q, active, pf);
+        } else {
+            flux4_body<0, Z, NC, true>(m, s, P, stage, i, q, active, pf);
+        }
+        return;
+    }
+#endif
     if constexpr (HP_FAST(2)) {
         if (!flux4_body<1, Z, NC>(m, s, P, stage, i, q, active)) flux4_body<0, Z, NC>(m, s, P, stage, i, q, active);
     } else {

@@ -12,8 +12,24 @@
 #ifndef HP_FAST_MASK
 #define HP_FAST_MASK 11
 #endif
+// the four-lane gradient kernel stages its cell geometry, its fields' values
+// at the cell and its neighbours and the limiter's inputs in shared memory
+// (asynchronous copies issued when it starts); the flux kernel prefetches
+// what its sources and RK update read the same way
+#ifndef HP_GRAD4_SMEM
+#define HP_GRAD4_SMEM 1
+#endif
+#ifndef HP_GRAD4_GPF
+#define HP_GRAD4_GPF 1
+#endif
+#ifndef HP_GRAD4_LIMPF
+#define HP_GRAD4_LIMPF 1
+#endif
+#ifndef HP_FLUX4_PREFETCH
+#define HP_FLUX4_PREFETCH 1
+#endif
 #ifndef HP_GRAD4_MINB
-#define HP_GRAD4_MINB 6
+#define HP_GRAD4_MINB 5
 #endif
 #ifndef HP_FLUX4_MINB
 #define HP_FLUX4_MINB 4
