@@ -1067,6 +1067,26 @@ __device__ __forceinline__ void zien_flux(FaceOut& o, unsigned& bad, R area, R e
 }
 
 // face-state loads through the read-only data path (1) or plain (0)
+// Asynchronous global-to-shared copies: 16 bytes through L2 only (the tail
+// prefetch of the four-lane flux kernel), 8 bytes through L1 (the staged
+// four-lane gradient kernel).
+#ifndef HP_FLUX4_PREFETCH
+#define HP_FLUX4_PREFETCH 0
+#endif
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+enum { LIM_LD = 128, LIMC_N = 13, LIMC_LD = 32 };
+
 #ifndef HP_FACE_LDG
 #define HP_FACE_LDG 1
 #endif
@@ -1567,42 +1587,16 @@ __global__ void __launch_bounds__(128) k_flux(DevMesh m, DevState<R> s, DevParam
     k_flux_body<ALIASED, FACE, Z, ACC>(m, s, P, stage, blockIdx.x);
 }
 
-// Asynchronous global-to-shared copies: 16 bytes through L2 only (the tail
-// prefetch of the four-lane flux kernel), 8 bytes through L1 (the limiter
-// prefetch of the four-lane gradient kernel).
-#ifndef HP_FLUX4_PREFETCH
-#define HP_FLUX4_PREFETCH 0
-#endif
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-#ifndef HP_GRAD4_LIMPF
-#define HP_GRAD4_LIMPF 0
-#endif
-// GPF (with LIMPF and SMEM): the gradient fields' values at the cell and its
-// neighbours are copied to shared memory too, one group per field
-#ifndef HP_GRAD4_GPF
-#define HP_GRAD4_GPF 0
-#endif
-enum { LIM_LD = 128, LIMC_N = 13, LIMC_LD = 32 };
 
 // ---------------------------------------------------------------------------
 // Venkatakrishnan limiter of the four-lane gradient kernel: lane q limits
 // pg, pp, rog or rop from the gradient it holds (lg) or receives (sg of
 // another lane), over its four faces; lane 0 stores the cell's minimum.
-// lp, lc (LIMPF, below): the limiter field of the lane's cell and of its
-// four neighbours (lp[k * LIM_LD], k = 0 the cell) and the cell's face
-// centroids and epsilon^2 (lc[k * LIMC_LD], k = 0..11 fch, 12 eps2), copied
-// to shared memory when the kernel started; null: read from global memory
+// lp, lc (the staged kernel, below): the limiter field of the lane's cell
+// and of its four neighbours (lp[k * LIM_LD], k = 0 the cell) and the cell's
+// face centroids and epsilon^2 (lc[k * LIMC_LD], k = 0..11 fch, 12 eps2),
+// copied to shared memory when the kernel started; null: read from global
+// memory
 __device__ __forceinline__ unsigned grad4_limiter(const DevMesh& m, const DevState<R>& s, const DevParams& P,
                                                   int i, int q, bool active, const int n[4], double x0,
                                                   double y0, double z0, R lg[3], const R sg[3],
@@ -1642,34 +1636,49 @@ __device__ __forceinline__ unsigned grad4_limiter(const DevMesh& m, const DevSta
     return 0u;
 }
 
-// Shared-memory staging of the cell geometry of the four-lane gradient
-// kernel: the 12 centroid differences and the 16 least-squares terms of the
-// block's 32 cells, [28][32] doubles, so that the field loop reads them from
-// shared memory instead of holding 28 doubles per lane in registers.
-#ifndef HP_GRAD4_SMEM
-#define HP_GRAD4_SMEM 0
+// Staged form of the four-lane gradient kernel (HP_GRAD4_STAGE, FP64
+// variants with set-up tables): when a block starts, each lane issues
+// asynchronous copies into shared memory of
+//   group 0   the 28 geometry values of its cell (12 centroid differences,
+//             the 16 LSQA terms), lane q copying values q, q + 4, ...;
+//   groups 1-4  field q + 4r (r = 0..3) at the cell and its 4 neighbours
+//             (an empty group when the lane has no such field);
+//   group 5   the limiter's inputs (see grad4_limiter).
+// The field loop waits for one group per field, so the gathers of later
+// fields stay in flight while earlier ones are computed, without holding
+// registers.
+#ifndef HP_GRAD4_STAGE
+#define HP_GRAD4_STAGE 0
 #endif
+#define GRAD4_STAGED (HP_GRAD4_STAGE && HP_DXN_TABLE && HP_LSQ_TABLE)
 enum { GEO_N = 28, GEO_LD = 32 };
+struct Grad4Stage {
+    const double* geo;    // geo[k * GEO_LD], k < 12 centroid differences, 12 + j LSQA column j
+    const double* gat;    // gat[(5 r + k) * LIM_LD], field q + 4r at the cell (k = 0) and neighbour k - 1
+    const double* lim;    // see grad4_limiter
+    const double* limc;
+};
 
 // ---------------------------------------------------------------------------
 // k_grad with four lanes per cell: lane q computes the LSQ gradients of
 // fields q, q+4, q+8, q+12 and the limiter of one of pg, pp, rog, rop; phi is
 // the in-order minimum over the lanes (equal to the reference's chain when no
 // value is NaN).  F selects the division form (see mdiv); the return value is
-// the fast form's out-of-range flag.
+// the fast form's out-of-range flag.  st: the staged copies (null: read from
+// global memory).
 template <int F>
 __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<R>& s, const DevParams& P, int i,
-                                               int q, bool active, const double* geo, const double* lp,
-                                               const double* lc, const double* gp) {
+                                               int q, bool active, const Grad4Stage* st) {
     unsigned bad = 0;
     int n[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) n[f] = ldg(COL(m.nc, f) + i);
     const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
-#if HP_GRAD4_SMEM && HP_DXN_TABLE && HP_LSQ_TABLE
+#if GRAD4_STAGED
     if constexpr (sizeof(R) == sizeof(double)) {
-        // geo[k * GEO_LD]: k < 12 the centroid differences (x, y, z of faces
-        // 1..4), 12 + j column j of the LSQA table
+        const double* geo = st->geo;
+        cp_async_wait_group<5>();   // group 0, copied by the cell's four lanes
+        __syncwarp();
 #define GX(f) geo[(3 * (f)) * GEO_LD]
 #define GY(f) geo[(3 * (f) + 1) * GEO_LD]
 #define GZ(f) geo[(3 * (f) + 2) * GEO_LD]
@@ -1679,30 +1688,20 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
 #pragma unroll
         for (int f = 0; f < 4; f++) (void)mrcp_tab<F>(GT(f), GT(11 + f), bad);
         (void)mrcp_tab<F>(GT(10), GT(15), bad);
-        const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
         R lg[3] = {R(0), R(0), R(0)};
         R sg[3] = {R(0), R(0), R(0)};
 #pragma unroll
         for (int r = 0; r < 4; r++) {
             const int v = q + 4 * r;
             if (v >= 13) break;
-            R qi, qa, qb, qc, qd;
-            if (gp) {
-                // this lane's copies of field v at the cell and its neighbours
-                // (group r of the GPF prefetch; the limiter's group follows)
-                if (r == 0) cp_async_wait_group<4>();
-                else if (r == 1) cp_async_wait_group<3>();
-                else if (r == 2) cp_async_wait_group<2>();
-                else cp_async_wait_group<1>();
-                const double* g = gp + 5 * r * LIM_LD;
-                qi = (R)g[0];
-                qa = (R)(g[LIM_LD] - qi); qb = (R)(g[2 * LIM_LD] - qi);
-                qc = (R)(g[3 * LIM_LD] - qi); qd = (R)(g[4 * LIM_LD] - qi);
-            } else {
-                const R* qq = COL(s.prr, pcol[v]);
-                qi = qq[i];
-                qa = (R)(qq[n[0]] - qi); qb = (R)(qq[n[1]] - qi); qc = (R)(qq[n[2]] - qi); qd = (R)(qq[n[3]] - qi);
-            }
+            if (r == 0) cp_async_wait_group<4>();
+            else if (r == 1) cp_async_wait_group<3>();
+            else if (r == 2) cp_async_wait_group<2>();
+            else cp_async_wait_group<1>();
+            const double* g = st->gat + 5 * r * LIM_LD;
+            const R qi = (R)g[0];
+            const R qa = (R)(g[LIM_LD] - qi), qb = (R)(g[2 * LIM_LD] - qi);
+            const R qc = (R)(g[3 * LIM_LD] - qi), qd = (R)(g[4 * LIM_LD] - qi);
             R c1 = DW(qa * GX(0), 0) + DW(qb * GX(1), 1) + DW(qc * GX(2), 2) + DW(qd * GX(3), 3);
             R c2;
             if (v == 7)   // cTp2 lacks the /wt4 (src/sr_derivative.F90:225)
@@ -1729,10 +1728,10 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
 #undef GZ
 #undef GT
 #define DW(x, f) div_rn((x), wt[f], rw[f])
-        return bad | grad4_limiter(m, s, P, i, q, active, n, x0, y0, z0, lg, sg, lp, lc);
+        return bad | grad4_limiter(m, s, P, i, q, active, n, x0, y0, z0, lg, sg, st->lim, st->limc);
     }
 #endif
-    (void)geo; (void)gp;
+    (void)st;
     R xa[4], ya[4], za[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) {
@@ -1809,7 +1808,7 @@ __device__ __forceinline__ unsigned grad4_body(const DevMesh& m, const DevState<
     }
 #undef DW
 #define DW(x, f) div_rn((x), wt[f], rw[f])
-    return bad | grad4_limiter(m, s, P, i, q, active, n, x0, y0, z0, lg, sg, lp, lc);
+    return bad | grad4_limiter(m, s, P, i, q, active, n, x0, y0, z0, lg, sg, nullptr, nullptr);
 }
 
 
@@ -1825,98 +1824,86 @@ __device__ __forceinline__ void k_grad4_body(DevMesh m, DevState<R> s, DevParams
     const int k = valid ? (int)c : ncell - 1;
     const int i = LIST ? ldg(m.gcells + k) : k;
     const bool active = valid && grad_cell(ldg(m.iblank + i));
-    const double* geo = nullptr;
-#if HP_GRAD4_SMEM && HP_DXN_TABLE && HP_LSQ_TABLE
-    // the 28 geometry values of the block's 32 cells; lane q stages values
-    // q, q + 4, ... of its cell (a warp's 8 cells are its own, so a warp
-    // barrier orders the stores before the loads)
-    __shared__ double sgeo[GEO_N * GEO_LD];
-    const int cs = (int)(threadIdx.x >> 2) & (GEO_LD - 1);
-#pragma unroll
-    for (int k = q; k < GEO_N; k += 4)
-        sgeo[k * GEO_LD + cs] = k < 12 ? ldg(COL(m.dxn, k) + i) : ldg(COL(m.lsqa, k - 12) + i);
-    __syncwarp();
-    geo = sgeo + cs;
-#endif
-    const double *lp = nullptr, *lc = nullptr, *gp = nullptr;
-#if HP_GRAD4_LIMPF
+#if GRAD4_STAGED
     if constexpr (sizeof(R) == sizeof(double)) {
-        // start copying what the limiter reads (see grad4_limiter): the
-        // lane's limiter field at the cell and its 4 neighbours, and face
-        // centroid columns q, 4 + q, 8 + q (lane 0 also epsilon^2)
+        __shared__ __align__(16) double sgeo[GEO_N * GEO_LD];
+        __shared__ __align__(16) double sgat[4 * 5 * LIM_LD];
         __shared__ __align__(16) double slim[5 * LIM_LD];
         __shared__ __align__(16) double slimc[LIMC_N * LIMC_LD];
-        const int tid = (int)threadIdx.x & (LIM_LD - 1), cl = (int)(threadIdx.x >> 2) & (LIMC_LD - 1);
-#if HP_GRAD4_GPF && HP_GRAD4_SMEM && HP_DXN_TABLE && HP_LSQ_TABLE
-        {
-            // fields q, q + 4, q + 8, q + 12 at the cell and its neighbours,
-            // one commit group per field (empty when the lane has no field)
-            __shared__ __align__(16) double sgat[4 * 5 * LIM_LD];
-            const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
-            int nn[4];
+        const int tid = (int)threadIdx.x & (LIM_LD - 1), cl = (int)(threadIdx.x >> 2) & (GEO_LD - 1);
+        int nn[4];
 #pragma unroll
-            for (int f = 0; f < 4; f++) nn[f] = ldg(COL(m.nc, f) + i);
+        for (int f = 0; f < 4; f++) nn[f] = ldg(COL(m.nc, f) + i);
+        // group 0: geometry values q, q + 4, ... of the lane's cell
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const int v = q + 4 * r;
-                if (v < 13) {
-                    const double* qv = reinterpret_cast<const double*>(COL(s.prr, pcol[v]));
-                    double* g = sgat + 5 * r * LIM_LD + tid;
-                    cp_async8(g, qv + i);
+        for (int k = q; k < GEO_N; k += 4)
+            cp_async8(sgeo + k * GEO_LD + cl, k < 12 ? COL(m.dxn, k) + i : COL(m.lsqa, k - 12) + i);
+        cp_async_commit();
+        // groups 1-4: fields q, q + 4, q + 8, q + 12
+        const int pcol[13] = {P_UG, P_VG, P_WG, P_TG, P_UP, P_VP, P_WP, P_TP, P_PG, P_PP, P_PHIG, P_ROG, P_ROP};
 #pragma unroll
-                    for (int f = 0; f < 4; f++) cp_async8(g + (1 + f) * LIM_LD, qv + nn[f]);
-                }
-                cp_async_commit();
+        for (int r = 0; r < 4; r++) {
+            const int v = q + 4 * r;
+            if (v < 13) {
+                const double* qv = reinterpret_cast<const double*>(COL(s.prr, pcol[v]));
+                double* g = sgat + 5 * r * LIM_LD + tid;
+                cp_async8(g, qv + i);
+#pragma unroll
+                for (int f = 0; f < 4; f++) cp_async8(g + (1 + f) * LIM_LD, qv + nn[f]);
             }
-            gp = sgat + tid;
+            cp_async_commit();
         }
-#endif
+        // group 5: the limiter field at the cell and its neighbours, face
+        // centroid columns q, 4 + q, 8 + q and (lane 0) epsilon^2
         const int lcol = q == 0 ? P_PG : q == 1 ? P_PP : q == 2 ? P_ROG : P_ROP;
-        const double* qq = reinterpret_cast<const double*>(COL(s.prr, lcol));
-        cp_async8(slim + tid, qq + i);
+        const double* ql = reinterpret_cast<const double*>(COL(s.prr, lcol));
+        cp_async8(slim + tid, ql + i);
 #pragma unroll
-        for (int f = 0; f < 4; f++) cp_async8(slim + (1 + f) * LIM_LD + tid, qq + ldg(COL(m.nc, f) + i));
+        for (int f = 0; f < 4; f++) cp_async8(slim + (1 + f) * LIM_LD + tid, ql + nn[f]);
 #pragma unroll
         for (int d = 0; d < 3; d++) cp_async8(slimc + (4 * d + q) * LIMC_LD + cl, COL(m.fch, 4 * d + q) + i);
         if (q == 0) cp_async8(slimc + 12 * LIMC_LD + cl, m.eps2 + i);
         cp_async_commit();
-        lp = slim + tid;
-        lc = slimc + cl;
+        const Grad4Stage st{sgeo + cl, sgat + tid, slim + tid, slimc + cl};
+        if constexpr (HP_FAST(1)) {
+            const unsigned bad = grad4_body<1>(m, s, P, i, q, active, &st);
+            if (__any_sync(0xffffffffu, bad)) grad4_body<0>(m, s, P, i, q, active, &st);
+        } else {
+            grad4_body<0>(m, s, P, i, q, active, &st);
+        }
+        // the fused step reuses the arrays for its next virtual block
+        __syncwarp();
+        return;
     }
 #endif
     if constexpr (HP_FAST(1)) {
         // the outputs are not inputs of this kernel, so a warp that flagged
         // an operand simply recomputes and overwrites them
-        const unsigned bad = grad4_body<1>(m, s, P, i, q, active, geo, lp, lc, gp);
-        if (__any_sync(0xffffffffu, bad)) grad4_body<0>(m, s, P, i, q, active, geo, lp, lc, gp);
+        const unsigned bad = grad4_body<1>(m, s, P, i, q, active, nullptr);
+        if (__any_sync(0xffffffffu, bad)) grad4_body<0>(m, s, P, i, q, active, nullptr);
     } else {
-        grad4_body<0>(m, s, P, i, q, active, geo, lp, lc, gp);
+        grad4_body<0>(m, s, P, i, q, active, nullptr);
     }
-#if (HP_GRAD4_SMEM && HP_DXN_TABLE && HP_LSQ_TABLE) || HP_GRAD4_LIMPF
-    // the fused step reuses the arrays for its next virtual block
-    __syncwarp();
-#endif
 }
 template <int LIST>
 __global__ void __launch_bounds__(128, HP_GRAD4_MINB) k_grad4(DevMesh m, DevState<R> s, DevParams P) {
     k_grad4_body<LIST>(m, s, P, blockIdx.x);
 }
 
-// Columns of the tail prefetch: the 14 primitives, dl, vol, the 16 LSQB
-// terms, vis, d24, cu, cn and the 12 centroid differences; TAIL_LD cells
-// (one 128-thread block) per column.
-enum { TAIL_DL = 14, TAIL_VOL = 15, TAIL_LSQB = 16, TAIL_VIS = 32, TAIL_D24 = 40, TAIL_CU = 50, TAIL_CN = 60,
-       TAIL_DXN = 70, TAIL_N = 82, TAIL_LD = 32 };
+// Columns of the tail prefetch: dl, vol, the 16 LSQB terms, vis, d24, cu
+// and cn; TAIL_LD cells (one 128-thread block) per column.  (Staging the 14
+// primitives and the 12 centroid differences as well measured 2% slower:
+// the face evaluation has just read the primitives.)
+enum { TAIL_DL = 0, TAIL_VOL = 1, TAIL_LSQB = 2, TAIL_VIS = 18, TAIL_D24 = 26, TAIL_CU = 36, TAIL_CN = 46,
+       TAIL_N = 56, TAIL_LD = 32 };
 __device__ __forceinline__ const double* tail_col(const DevMesh& m, const DevState<R>& s, int k) {
-    if (k < TAIL_DL) return s.pr + (size_t)k * m.ld;
     if (k == TAIL_DL) return m.dl;
     if (k == TAIL_VOL) return m.vol;
     if (k < TAIL_VIS) return m.lsqb + (size_t)(k - TAIL_LSQB) * m.ld;
     if (k < TAIL_D24) return s.vis + (size_t)(k - TAIL_VIS) * m.ld;
     if (k < TAIL_CU) return s.d24 + (size_t)(k - TAIL_D24) * m.ld;
     if (k < TAIL_CN) return s.cu + (size_t)(k - TAIL_CU) * m.ld;
-    if (k < TAIL_DXN) return s.cn + (size_t)(k - TAIL_CN) * m.ld;
-    return m.dxn + (size_t)(k - TAIL_DXN) * m.ld;
+    return s.cn + (size_t)(k - TAIL_CN) * m.ld;
 }
 
 // Residual + sources + RK update with four lanes per cell: lane q evaluates
@@ -1960,9 +1947,8 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     const int nq = ldg(COL(m.nc, q) + i);
     const double x0 = ldg(m.xc + i), y0 = ldg(m.yc + i), z0 = ldg(m.zc + i);
 #if HP_DXN_TABLE
-    const R xq = TL(TAIL_DXN + 3 * q, ldg(COL(m.dxn, 3 * q) + i)),
-            yq = TL(TAIL_DXN + 3 * q + 1, ldg(COL(m.dxn, 3 * q + 1) + i)),
-            zq = TL(TAIL_DXN + 3 * q + 2, ldg(COL(m.dxn, 3 * q + 2) + i));
+    const R xq = (R)ldg(COL(m.dxn, 3 * q) + i), yq = (R)ldg(COL(m.dxn, 3 * q + 1) + i),
+            zq = (R)ldg(COL(m.dxn, 3 * q + 2) + i);
 #else
     const R xq = (R)(ldg(m.xc + nq) - x0), yq = (R)(ldg(m.yc + nq) - y0), zq = (R)(ldg(m.zc + nq) - z0);
 #endif
@@ -2005,12 +1991,12 @@ __device__ __forceinline__ bool flux4_body(const DevMesh& m, const DevState<R>& 
     }
     // interphase sources (src/sr_source.F90:46-155)
     {
-        const R tg = TL(P_TG, COL(pr, P_TG)[i]), phig = TL(P_PHIG, COL(pr, P_PHIG)[i]),
-                rog = TL(P_ROG, COL(pr, P_ROG)[i]);
-        const R rop = TL(P_ROP, COL(pr, P_ROP)[i]), phip = TL(P_PHIP, COL(pr, P_PHIP)[i]);
-        const R ug = TL(P_UG, COL(pr, P_UG)[i]), vg = TL(P_VG, COL(pr, P_VG)[i]), wg = TL(P_WG, COL(pr, P_WG)[i]);
-        const R up = TL(P_UP, COL(pr, P_UP)[i]), vp = TL(P_VP, COL(pr, P_VP)[i]), wp = TL(P_WP, COL(pr, P_WP)[i]);
-        const R tp = TL(P_TP, COL(pr, P_TP)[i]), pg = TL(P_PG, COL(pr, P_PG)[i]);
+        const R tg = (R)COL(pr, P_TG)[i], phig = (R)COL(pr, P_PHIG)[i],
+                rog = (R)COL(pr, P_ROG)[i];
+        const R rop = (R)COL(pr, P_ROP)[i], phip = (R)COL(pr, P_PHIP)[i];
+        const R ug = (R)COL(pr, P_UG)[i], vg = (R)COL(pr, P_VG)[i], wg = (R)COL(pr, P_WG)[i];
+        const R up = (R)COL(pr, P_UP)[i], vp = (R)COL(pr, P_VP)[i], wp = (R)COL(pr, P_WP)[i];
+        const R tp = (R)COL(pr, P_TP)[i], pg = (R)COL(pr, P_PG)[i];
         const R dl = TL(TAIL_DL, ldg(m.dl + i)), voli = TL(TAIL_VOL, ldg(m.vol + i));
         const R amug = (R)P.as * sqrt(tg) / (R(1) + (R)P.ts / tg);
         const R du = ug - up, dv = vg - vp, dw = wg - wp;

@@ -16,14 +16,8 @@
 // at the cell and its neighbours and the limiter's inputs in shared memory
 // (asynchronous copies issued when it starts); the flux kernel prefetches
 // what its sources and RK update read the same way
-#ifndef HP_GRAD4_SMEM
-#define HP_GRAD4_SMEM 1
-#endif
-#ifndef HP_GRAD4_GPF
-#define HP_GRAD4_GPF 1
-#endif
-#ifndef HP_GRAD4_LIMPF
-#define HP_GRAD4_LIMPF 1
+#ifndef HP_GRAD4_STAGE
+#define HP_GRAD4_STAGE 1
 #endif
 #ifndef HP_FLUX4_PREFETCH
 #define HP_FLUX4_PREFETCH 1
