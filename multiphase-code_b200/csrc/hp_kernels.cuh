@@ -2145,16 +2145,22 @@ __device__ __forceinline__ void k_flux4_body(DevMesh m, DevState<R> s, DevParams
     bool active = valid && ldg(m.iblank + i) == 1;
     if (sizeof(R) != sizeof(double) && m.nwall > 0) active = active && !ldg(m.wclass + i);
 #if HP_FLUX4_PREFETCH && HP_LSQ_TABLE && HP_DXN_TABLE
-    if constexpr (LIST == 0 && NC && sizeof(R) == sizeof(double)) {
-        // the warp's 8 consecutive cells: start the asynchronous copy of
-        // their values that the sources and the RK update read (TAIL_*),
-        // 64 bytes per column, while the faces are evaluated
+    if constexpr (NC && sizeof(R) == sizeof(double)) {
+        // start the asynchronous copy of the values that the sources and the
+        // RK update read (TAIL_*) while the faces are evaluated: for all
+        // cells, the warp's 8 consecutive cells, 64 bytes per column; for a
+        // cell list, lane q copies columns q, q + 4, ... of its own cell
         __shared__ __align__(16) double stail[TAIL_N * TAIL_LD];
-        const int lane = (int)(threadIdx.x & 31), w8 = (int)((threadIdx.x >> 5) * 8);
-        const long long c0 = ((long long)bid * blockDim.x + (threadIdx.x & ~31u)) >> 2;
-        for (int t = lane; t < TAIL_N * 4; t += 32) {
-            const int k = t >> 2, part = t & 3;
-            cp_async16(stail + k * TAIL_LD + w8 + 2 * part, tail_col(m, s, k) + c0 + 2 * part);
+        if constexpr (LIST == 0) {
+            const int lane = (int)(threadIdx.x & 31), w8 = (int)((threadIdx.x >> 5) * 8);
+            const long long c0 = ((long long)bid * blockDim.x + (threadIdx.x & ~31u)) >> 2;
+            for (int t = lane; t < TAIL_N * 4; t += 32) {
+                const int k = t >> 2, part = t & 3;
+                cp_async16(stail + k * TAIL_LD + w8 + 2 * part, tail_col(m, s, k) + c0 + 2 * part);
+            }
+        } else {
+            const int cs = (int)(threadIdx.x >> 2) & (TAIL_LD - 1);
+            for (int k = q; k < TAIL_N; k += 4) cp_async8(stail + k * TAIL_LD + cs, tail_col(m, s, k) + i);
         }
         cp_async_commit();
         const double* pf = stail + ((threadIdx.x >> 2) & (TAIL_LD - 1));
