@@ -827,9 +827,16 @@ __device__ __forceinline__ void k_grad_body(DevMesh m, DevState<R> s, DevParams 
     R xa[4], ya[4], za[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) {
-        xa[f] = (R)(ldg(m.xc + n[f]) - x0);
-        ya[f] = (R)(ldg(m.yc + n[f]) - y0);
-        za[f] = (R)(ldg(m.zc + n[f]) - z0);
+        if (FPR && HP_DXN_TABLE) {
+            // the centroid differences, formed at set-up (the same subtraction)
+            xa[f] = (R)ldg(COL(m.dxn, 3 * f) + i);
+            ya[f] = (R)ldg(COL(m.dxn, 3 * f + 1) + i);
+            za[f] = (R)ldg(COL(m.dxn, 3 * f + 2) + i);
+        } else {
+            xa[f] = (R)(ldg(m.xc + n[f]) - x0);
+            ya[f] = (R)(ldg(m.yc + n[f]) - y0);
+            za[f] = (R)(ldg(m.zc + n[f]) - z0);
+        }
     }
     // geometry-only terms (wt, a1..b3, dnr of src/sr_derivative.F90:163-176,
     // 255), evaluated once at set-up with the same expressions
@@ -865,12 +872,14 @@ __device__ __forceinline__ void k_grad_body(DevMesh m, DevState<R> s, DevParams 
             // alpha_p = 1 - alpha_g itself, whose reconstruction uses this
             // gradient
             const double* q = COL(s.pr, P_PHIG);
-            const double qi = q[i];
-            qa = (R)(q[n[0]] - qi); qb = (R)(q[n[1]] - qi); qc = (R)(q[n[2]] - qi); qd = (R)(q[n[3]] - qi);
+            const double qi = ldg(q + i);
+            qa = (R)(ldg(q + n[0]) - qi); qb = (R)(ldg(q + n[1]) - qi);
+            qc = (R)(ldg(q + n[2]) - qi); qd = (R)(ldg(q + n[3]) - qi);
         } else {
             const PT* q = COL(prb, pcol[v]);
-            PT qi = q[i];
-            qa = (R)(q[n[0]] - qi); qb = (R)(q[n[1]] - qi); qc = (R)(q[n[2]] - qi); qd = (R)(q[n[3]] - qi);
+            PT qi = ldg(q + i);
+            qa = (R)(ldg(q + n[0]) - qi); qb = (R)(ldg(q + n[1]) - qi);
+            qc = (R)(ldg(q + n[2]) - qi); qd = (R)(ldg(q + n[3]) - qi);
         }
         R c1 = DW(qa * xa[0], 0) + DW(qb * xa[1], 1) + DW(qc * xa[2], 2) + DW(qd * xa[3], 3);
         R c2;
@@ -882,12 +891,13 @@ __device__ __forceinline__ void k_grad_body(DevMesh m, DevState<R> s, DevParams 
         gv[v][0] = div_rn(det3(c1, c2, c3, b1, a2, b3, b2, b3, a3), dnr, rdnr);
         gv[v][1] = div_rn(det3(a1, b1, b2, c1, c2, c3, b2, b3, a3), dnr, rdnr);
         gv[v][2] = div_rn(det3(a1, b1, b2, b1, a2, b3, c1, c2, c3), dnr, rdnr);
-    }
-#pragma unroll
-    for (int v = 0; v < 11; v++) {
-        COL(s.gr, 3 * v + 0)[i] = gv[v][0];
-        COL(s.gr, 3 * v + 1)[i] = gv[v][1];
-        COL(s.gr, 3 * v + 2)[i] = gv[v][2];
+        // stored at once (the inputs are read through the read-only path,
+        // so the stores do not order them); the limiter keeps 8, 9, 11, 12
+        if (v < 11) {
+            COL(s.gr, 3 * v + 0)[i] = gv[v][0];
+            COL(s.gr, 3 * v + 1)[i] = gv[v][1];
+            COL(s.gr, 3 * v + 2)[i] = gv[v][2];
+        }
     }
     // limiter: phi_i = min over {pg, pp, rog, rop} x 4 faces
     const R epssq = (R)ldg(m.eps2 + i);
@@ -903,9 +913,9 @@ __device__ __forceinline__ void k_grad_body(DevMesh m, DevState<R> s, DevParams 
 #pragma unroll
     for (int t = 0; t < 4; t++) {
         const PT* q = COL(prb, pcol[lv[t]]);
-        PT qi = q[i];
-        PT vmax = mx2(mx2(mx2(mx2(qi, q[n[0]]), q[n[1]]), q[n[2]]), q[n[3]]);
-        PT vmin = mn2(mn2(mn2(mn2(qi, q[n[0]]), q[n[1]]), q[n[2]]), q[n[3]]);
+        PT qi = ldg(q + i), q0 = ldg(q + n[0]), q1 = ldg(q + n[1]), q2 = ldg(q + n[2]), q3 = ldg(q + n[3]);
+        PT vmax = mx2(mx2(mx2(mx2(qi, q0), q1), q2), q3);
+        PT vmin = mn2(mn2(mn2(mn2(qi, q0), q1), q2), q3);
         R dmax = (R)(vmax - qi), dmin = (R)(vmin - qi);
         R gx = gv[lv[t]][0], gy = gv[lv[t]][1], gz = gv[lv[t]][2];
 #pragma unroll
