@@ -112,8 +112,11 @@ class ClockSampler:
 # does not depend on the CFL.
 CYL_CFL = 0.25
 # FP64 wall layers of the second mixed measurement (hp_params.wall_fp64_layers):
-# breadth-first tet layers from the cylinder wall
-MIXED_WALL_LAYERS = 96
+# breadth-first tet layers from the cylinder wall.  On this mesh 80 layers is
+# the smallest count whose density error after 1000 steps equals that of the
+# FP64 variant with FMA contraction (the flow's rounding floor); 64 layers
+# end three times above it.
+MIXED_WALL_LAYERS = 80
 
 
 def make_workload(name: str, seed_offset: int = 0):
