@@ -61,7 +61,7 @@ typedef struct hp_params {
     int32_t istart;
     double diap;
     double surfacetension;
-    int32_t myflux;          /* 1 = HLLC-Zien, 2 = HLLC-Batten (3, Jameson: HP_E_UNSUPPORTED) */
+    int32_t myflux;          /* 1 = HLLC-Zien, 2 = HLLC-Batten, 3 = Jameson central flux */
     int32_t myorder;         /* 1 or 2 */
     double as, ts;           /* Sutherland constants */
     /* --- additions; zero-initialised values reproduce the reference --- */

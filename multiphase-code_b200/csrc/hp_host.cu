@@ -593,10 +593,8 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     g_create_error.clear();
     if (!meshes || !params || !out || ncase < 1) return fail(nullptr, HP_E_ARG, "null argument or no case");
     *out = nullptr;
-    if (params->myflux == 3)
-        return fail(nullptr, HP_E_UNSUPPORTED, "myflux 3 (Jameson central flux) is not built");
-    if (params->myflux != 1 && params->myflux != 2)
-        return fail(nullptr, HP_E_ARG, "myflux must be 1 (HLLC-Zien) or 2 (HLLC-Batten)");
+    if (params->myflux < 1 || params->myflux > 3)
+        return fail(nullptr, HP_E_ARG, "myflux must be 1 (HLLC-Zien), 2 (HLLC-Batten) or 3 (Jameson)");
     if (params->myorder != 1 && params->myorder != 2)
         return fail(nullptr, HP_E_ARG, "myorder must be 1 or 2");
     if (params->block_size != 0 && (params->block_size < 64 || params->block_size > 512 || params->block_size % 32))
@@ -885,7 +883,7 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     // the separate kernels, and a case must give the same result whichever
     // way it runs (alone or in a batch of another size class).
     if (e == cudaSuccess && h->prm.use_graph == 2 && h->var == &variant_fp64_parity && !h->aliased &&
-        h->neq == 10 && h->nwall == 0 && !(m.nface > 0 && m.face_mode >= 2)) {
+        h->neq == 10 && h->nwall == 0 && P.myflux != 3 && !(m.nface > 0 && m.face_mode >= 2)) {
         int coop = 0;
         if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop)
             h->fused = h->var->fused_grid(m, P);

@@ -1103,8 +1103,9 @@ enum { LIM_LD = 128, LIMC_N = 13, LIMC_LD = 32 };
 // (NC = false: plain loads, for the fused step, which writes these arrays)
 #define PLD(p) ((HP_FACE_LDG && NC) ? ldg(p) : *(p))
 // F selects the division form (see mdiv); bad collects its out-of-range flag.
-// Z selects the Riemann solver: 0 HLLC-Batten (src/sr_hllcbatten.F90:338-529),
-// 1 HLLC-Zien (src/sr_hllczien.F90:348-487).
+// Z selects the face flux: 0 HLLC-Batten (src/sr_hllcbatten.F90:338-529),
+// 1 HLLC-Zien (src/sr_hllczien.F90:348-487), 2 the Jameson central flux
+// (src/sr_jameson.F90:126-262).
 template <int F, int Z, class PT, bool NC = true>
 __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s, const DevParams& P,
                                           int i, int f, FaceOut& o, unsigned& bad, const PT* pr) {
@@ -1142,6 +1143,66 @@ __device__ __forceinline__ void face_eval(const DevMesh& m, const DevState<R>& s
             phipL = (R)PLD(COL(pr, P_PHIP) + i);
             phipR = (R)PLD(COL(pr, P_PHIP) + neigh);
         }
+    }
+    if constexpr (Z == 2) {
+        // Jameson central flux (src/sr_jameson.F90:126-262): the two cells'
+        // own values, no reconstruction and no phase blending, the densities
+        // of the primitive recovery; the face flux is the mean of the two
+        // sides' physical fluxes times the area, so both phases always take it
+        if constexpr (sizeof(R) != 4) {
+            phipL = R(1) - phigL;
+            phipR = R(1) - phigR;
+        }
+        o.wall = (kind & FK_WALL) != 0;
+        o.takeg = o.takep = !o.wall;
+        if (o.wall) {   // :185-191
+            o.w[0] = phigL * pgL * enx * area;
+            o.w[1] = phigL * pgL * eny * area;
+            o.w[2] = phigL * pgL * enz * area;
+            o.w[3] = phipL * ppL * enx * area;
+            o.w[4] = phipL * ppL * eny * area;
+            o.w[5] = phipL * ppL * enz * area;
+            return;
+        }
+        const R rrg = (R)P.rrg, gamag = (R)P.gamag, gamap = (R)P.gamap, pinf = (R)P.pinf, cpp = (R)P.cpp;
+        const R rgm1 = (R)P.r_gm1, rgamap = (R)P.r_gamap;
+        const R rogL = (R)PLD(COL(pr, P_ROG) + i), ropL = (R)PLD(COL(pr, P_ROP) + i);
+        const R rogR = (R)PLD(COL(pr, P_ROG) + neigh), ropR = (R)PLD(COL(pr, P_ROP) + neigh);
+        const R rrogL = mrcp<F>(rogL, bad), rrogR = mrcp<F>(rogR, bad);
+        const R rropL = mrcp<F>(ropL, bad), rropR = mrcp<F>(ropR, bad);
+        // :194-212 (the sound speeds formed there enter no flux)
+        const R egL = mdiv<F>(rrg * tgL, gamag - R(1), rgm1, bad) + R(0.5) * (ugL * ugL + vgL * vgL + wgL * wgL);
+        const R hgL = egL + mdiv<F>(pgL, rogL, rrogL, bad);
+        const R qgL = ugL * enx + vgL * eny + wgL * enz;
+        const R egR = mdiv<F>(rrg * tgR, gamag - R(1), rgm1, bad) + R(0.5) * (ugR * ugR + vgR * vgR + wgR * wgR);
+        const R hgR = egR + mdiv<F>(pgR, rogR, rrogR, bad);
+        const R qgR = ugR * enx + vgR * eny + wgR * enz;
+        const R epL = mdiv<F>(cpp * tpL, gamap, rgamap, bad) + mdiv<F>(pinf, ropL, rropL, bad) +
+                      R(0.5) * (upL * upL + vpL * vpL + wpL * wpL);
+        const R hpL = epL + mdiv<F>(ppL, ropL, rropL, bad);
+        const R qpL = upL * enx + vpL * eny + wpL * enz;
+        const R epR = mdiv<F>(cpp * tpR, gamap, rgamap, bad) + mdiv<F>(pinf, ropR, rropR, bad) +
+                      R(0.5) * (upR * upR + vpR * vpR + wpR * wpR);
+        const R hpR = epR + mdiv<F>(ppR, ropR, rropR, bad);
+        const R qpR = upR * enx + vpR * eny + wpR * enz;
+        // :216-261
+        o.F[0] = (phigL * rogL * qgL + phigR * rogR * qgR) * R(0.5) * area;
+        o.F[1] = ((phigL * rogL * qgL * ugL + phigL * pgL * enx) + (phigR * rogR * qgR * ugR + phigR * pgR * enx)) *
+                 R(0.5) * area;
+        o.F[2] = ((phigL * rogL * qgL * vgL + phigL * pgL * eny) + (phigR * rogR * qgR * vgR + phigR * pgR * eny)) *
+                 R(0.5) * area;
+        o.F[3] = ((phigL * rogL * qgL * wgL + phigL * pgL * enz) + (phigR * rogR * qgR * wgR + phigR * pgR * enz)) *
+                 R(0.5) * area;
+        o.F[4] = (phigL * rogL * qgL * hgL + phigR * rogR * qgR * hgR) * R(0.5) * area;
+        o.F[5] = (phipL * ropL * qpL + phipR * ropR * qpR) * R(0.5) * area;
+        o.F[6] = ((phipL * ropL * qpL * upL + phipL * ppL * enx) + (phipR * ropR * qpR * upR + phipR * ppR * enx)) *
+                 R(0.5) * area;
+        o.F[7] = ((phipL * ropL * qpL * vpL + phipL * ppL * eny) + (phipR * ropR * qpR * vpR + phipR * ppR * eny)) *
+                 R(0.5) * area;
+        o.F[8] = ((phipL * ropL * qpL * wpL + phipL * ppL * enz) + (phipR * ropR * qpR * wpR + phipR * ppR * enz)) *
+                 R(0.5) * area;
+        o.F[9] = (phipL * ropL * qpL * hpL + phipR * ropR * qpR * hpR) * R(0.5) * area;
+        return;
     }
     if (P.myorder == 2 && (kind & FK_RECON)) {
         const R phimin = (R)mn2(PLD(s.phi + i), PLD(s.phi + neigh));
@@ -2989,7 +3050,9 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
             if (m.aliased) k_bc_serial<false><<<1, 1, 0, st>>>(m, s, P);
             else k_bc<false><<<gg, cb, 0, st>>>(m, s, P);
         }
-        if (P.myorder == 2) {
+        // (the Jameson flux reads no gradients: src/sr_jameson.F90:24 calls
+        // primitiveplusbc only)
+        if (P.myorder == 2 && P.myflux != 3) {
             MARK(KK_GRAD);
             if (m.aliased) k_grad<false><<<gf, b, 0, st>>>(m, s, P);
             else if (sizeof(R) != sizeof(double)) k_grad<true><<<gf, b, 0, st>>>(m, s, P);
@@ -3007,6 +3070,7 @@ static void enqueue_step(const DevMesh& m, const void* stp, const DevParams& P, 
         }
         MARK(KK_FLUX);
         if (P.myflux == 1) enqueue_flux<1>(m, s, P, st, stage, hook);
+        else if (P.myflux == 3) enqueue_flux<2>(m, s, P, st, stage, hook);
         else enqueue_flux<0>(m, s, P, st, stage, hook);
         // FP64 wall layers: their fluxes, sources and RK update (the FP32
         // kernels above left those cells alone)

@@ -50,6 +50,7 @@ static void wall_flux(const DevMesh& m, const DevState<double>& s, const DevPara
                       int stage) {
     if (m.nwall <= 0) return;
     if (P.myflux == 1) k_flux4<1, 1><<<grid_for(4ll * m.nwall, 128), 128, 0, st>>>(m, s, P, stage);
+    else if (P.myflux == 3) k_flux4<2, 1><<<grid_for(4ll * m.nwall, 128), 128, 0, st>>>(m, s, P, stage);
     else k_flux4<0, 1><<<grid_for(4ll * m.nwall, 128), 128, 0, st>>>(m, s, P, stage);
 }
 }  // namespace v_fp64

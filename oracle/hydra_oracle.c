@@ -213,7 +213,7 @@ static void geometry(or_case *S) {
 or_case *or_create(const or_params *p, int32_t nodes, int32_t neles,
                    int32_t nghosts, const double *x, const double *y,
                    const double *z, const int32_t *elem, const int32_t *ghost) {
-    if (p->myflux != 1 && p->myflux != 2) return NULL;   /* mod_Fluxmodule.F90:14-16 stops */
+    if (p->myflux < 1 || p->myflux > 3) return NULL;   /* mod_Fluxmodule.F90:14-16 stops */
     or_case *S = (or_case *)calloc(1, sizeof(or_case));
     S->p = *p;
     g_nan_mode = p->nan_mode;
@@ -1415,11 +1415,98 @@ static void source(or_case *S) {
     }
 }
 
+/* Jameson central flux, src/sr_jameson.F90:43-282 (two-phase equations).
+ * Cell values on both sides of each face, with no reconstruction and no
+ * phase blending: the face flux is the mean of the two sides' physical
+ * fluxes times the area; a wall face (neighbour ghost of type 5) adds the
+ * phase pressures only (:185-191).  The densities are the primitive arrays'
+ * (:139,:145); the sound speeds the reference forms (:197,:202,:207,:212)
+ * enter no flux and are left out.  The reference does not ship a run of
+ * it: parity is against this restatement only. */
+static void jameson_faces(or_case *S) {
+    const or_params *p = &S->p;
+    double rrg = S->rrg, gamag = p->gamag, gamap = p->gamap, pinf = p->pinf, cpp = p->cpp;
+    int neles = S->neles, nghosts = S->nghosts;
+#pragma omp parallel for num_threads(g_threads) if (PAR(S)) schedule(static)
+    for (int i = 1; i <= neles; i++) {
+        if (S->iblank[i] != 1) continue;
+        for (int k = 1; k <= 10; k++) RHS(i, k) = 0.0;
+        for (int f = 0; f < 4; f++) {
+            int neigh = S->nc[f][i];
+            double scx = S->sc[3 * f][i], scy = S->sc[3 * f + 1][i], scz = S->sc[3 * f + 2][i];
+            double area = sqrt(scx * scx + scy * scy + scz * scz);
+            double enx = scx / area, eny = scy / area, enz = scz / area;
+            int nt = 0;
+            if (neigh > neles && neigh <= neles + nghosts) nt = S->ntype[neigh - neles];
+            double rogL = S->rog[i], ugL = S->ug[i], vgL = S->vg[i], wgL = S->wg[i], tgL = S->tg[i],
+                   phigL = S->phig[i], ropL = S->rop[i], upL = S->up[i], vpL = S->vp[i], wpL = S->wp[i],
+                   tpL = S->tp[i], pgL = S->pg[i], ppL = S->pp[i];
+            double rogR = S->rog[neigh], ugR = S->ug[neigh], vgR = S->vg[neigh], wgR = S->wg[neigh],
+                   tgR = S->tg[neigh], phigR = S->phig[neigh], ropR = S->rop[neigh], upR = S->up[neigh],
+                   vpR = S->vp[neigh], wpR = S->wp[neigh], tpR = S->tp[neigh], pgR = S->pg[neigh],
+                   ppR = S->pp[neigh];
+            double phipL = 1.0 - phigL, phipR = 1.0 - phigR;
+            if (nt == 5) {
+                RHS(i, 2) = RHS(i, 2) + phigL * pgL * enx * area;
+                RHS(i, 3) = RHS(i, 3) + phigL * pgL * eny * area;
+                RHS(i, 4) = RHS(i, 4) + phigL * pgL * enz * area;
+                RHS(i, 7) = RHS(i, 7) + phipL * ppL * enx * area;
+                RHS(i, 8) = RHS(i, 8) + phipL * ppL * eny * area;
+                RHS(i, 9) = RHS(i, 9) + phipL * ppL * enz * area;
+                continue;
+            }
+            double egL = rrg * tgL / (gamag - 1.0) + 0.5 * (sq(ugL) + sq(vgL) + sq(wgL));
+            double hgL = egL + pgL / rogL;
+            double qgL = ugL * enx + vgL * eny + wgL * enz;
+            double egR = rrg * tgR / (gamag - 1.0) + 0.5 * (sq(ugR) + sq(vgR) + sq(wgR));
+            double hgR = egR + pgR / rogR;
+            double qgR = ugR * enx + vgR * eny + wgR * enz;
+            double epL = (cpp * tpL) / gamap + pinf / ropL + 0.5 * (sq(upL) + sq(vpL) + sq(wpL));
+            double hpL = epL + ppL / ropL;
+            double qpL = upL * enx + vpL * eny + wpL * enz;
+            double epR = (cpp * tpR) / gamap + pinf / ropR + 0.5 * (sq(upR) + sq(vpR) + sq(wpR));
+            double hpR = epR + ppR / ropR;
+            double qpR = upR * enx + vpR * eny + wpR * enz;
+            double fl[10], fr[10];
+            fl[0] = phigL * rogL * qgL;
+            fl[1] = phigL * rogL * qgL * ugL + phigL * pgL * enx;
+            fl[2] = phigL * rogL * qgL * vgL + phigL * pgL * eny;
+            fl[3] = phigL * rogL * qgL * wgL + phigL * pgL * enz;
+            fl[4] = phigL * rogL * qgL * hgL;
+            fl[5] = phipL * ropL * qpL;
+            fl[6] = phipL * ropL * qpL * upL + phipL * ppL * enx;
+            fl[7] = phipL * ropL * qpL * vpL + phipL * ppL * eny;
+            fl[8] = phipL * ropL * qpL * wpL + phipL * ppL * enz;
+            fl[9] = phipL * ropL * qpL * hpL;
+            fr[0] = phigR * rogR * qgR;
+            fr[1] = phigR * rogR * qgR * ugR + phigR * pgR * enx;
+            fr[2] = phigR * rogR * qgR * vgR + phigR * pgR * eny;
+            fr[3] = phigR * rogR * qgR * wgR + phigR * pgR * enz;
+            fr[4] = phigR * rogR * qgR * hgR;
+            fr[5] = phipR * ropR * qpR;
+            fr[6] = phipR * ropR * qpR * upR + phipR * ppR * enx;
+            fr[7] = phipR * ropR * qpR * vpR + phipR * ppR * eny;
+            fr[8] = phipR * ropR * qpR * wpR + phipR * ppR * enz;
+            fr[9] = phipR * ropR * qpR * hpR;
+            /* :252-261 */
+            for (int k = 1; k <= 10; k++) RHS(i, k) = RHS(i, k) + (fl[k - 1] + fr[k - 1]) * 0.5 * area;
+        }
+    }
+}
+
 /* CallFluxSolver, src/mod_Fluxmodule.F90:7-21: myflux 1 = HLLC-Zien
  * (src/sr_hllczien.F90:29-506), 2 = HLLC-Batten (src/sr_hllcbatten.F90:
- * 29-560); or_create rejects any other value */
+ * 29-560), 3 = Jameson (src/sr_jameson.F90:1-288: primitiveplusbc, no
+ * gradients or limiter, the central flux, source); or_create rejects any
+ * other value */
 void or_flux(or_case *S) {
     or_primitiveplusbc(S);
+    if (S->p.myflux == 3) {
+        jameson_faces(S);
+        source(S);
+        if (S->p.five_phase) jameson_qrs(S);    /* src/mod_Fluxmodule.F90:18-20 */
+        return;
+    }
     if (S->p.myorder == 2) { or_derivative(S); or_venkat(S); }
     hllc_faces(S, S->p.myflux == 1);
     source(S);

@@ -324,7 +324,7 @@ class Oracle:
         self.h = self.L.or_create(ctypes.byref(params), mesh.nodes, mesh.neles,
                                   mesh.nghosts, _dp(x), _dp(y), _dp(z), _ip(el), _ip(gh))
         if not self.h:
-            raise ValueError(f"myflux must be 1 (HLLC-Zien) or 2 (HLLC-Batten), not {params.myflux}")
+            raise ValueError(f"myflux must be 1 (HLLC-Zien), 2 (HLLC-Batten) or 3 (Jameson), not {params.myflux}")
         self.neles = mesh.neles
         self.nghosts = mesh.nghosts
         self.ntot = mesh.neles + mesh.nghosts
