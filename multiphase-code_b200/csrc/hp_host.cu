@@ -518,6 +518,46 @@ static int fill_case(const hp_mesh* mesh, const hp_params* params, Layout& L, Ca
             for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], p[d]); hi[d] = std::max(hi[d], p[d]); }
         }
         const double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+        // FP64 wall layers of the FP32-arithmetic variants: the cells within
+        // the layers first (group 0), then their other interior neighbours
+        // (group 1), then the rest, each group along the curve.  The
+        // layer kernels' cell lists are then contiguous ranges of the order,
+        // and the FP32 kernels skip whole warps instead of scattered cells.
+        // (The same breadth-first search over interior neighbours from the
+        // cells next to a wall ghost of type 5 or 6 as wall_layers.)
+        std::vector<uint8_t> group(neles + 1, 2);
+        const bool fp32_arith = params->precision == HP_PREC_MIXED || params->precision == HP_PREC_FP32;
+        if (fp32_arith && params->wall_fp64_layers > 0) {
+            std::vector<int> gtype_of(ntot + 1, 0);
+            for (int g = 0; g < nghosts; g++) gtype_of[gid[g]] = gtyp[g];
+            std::vector<int> layer(neles + 1, 0), front;
+            for (int e = 1; e <= neles; e++)
+                for (int k = 0; k < 4; k++) {
+                    const int j = nc[k][e];
+                    if (j > neles && j <= ntot && (gtype_of[j] == 5 || gtype_of[j] == 6)) {
+                        layer[e] = 1;
+                        front.push_back(e);
+                        break;
+                    }
+                }
+            for (int k = 2; k <= params->wall_fp64_layers && !front.empty(); k++) {
+                std::vector<int> next;
+                for (int e : front)
+                    for (int f = 0; f < 4; f++) {
+                        const int j = nc[f][e];
+                        if (j <= neles && layer[j] == 0) { layer[j] = k; next.push_back(j); }
+                    }
+                front.swap(next);
+            }
+            for (int e = 1; e <= neles; e++)
+                if (layer[e] > 0) {
+                    group[e] = 0;
+                    for (int f = 0; f < 4; f++) {
+                        const int j = nc[f][e];
+                        if (j <= neles && layer[j] == 0) group[j] = 1;
+                    }
+                }
+        }
         std::vector<std::pair<uint32_t, int>> key(neles);
 #pragma omp parallel for schedule(static)
         for (int i = 1; i <= neles; i++) {
@@ -527,7 +567,7 @@ static int fill_case(const hp_mesh* mesh, const hp_params* params, Layout& L, Ca
                 double t = ext > 0.0 ? (p[d] - lo[d]) / ext : 0.0;
                 q[d] = (uint32_t)std::min(1023.0, std::max(0.0, t * 1023.0));
             }
-            key[i - 1] = {hilbert10(q[0], q[1], q[2]), i};
+            key[i - 1] = {((uint32_t)group[i] << 30) | hilbert10(q[0], q[1], q[2]), i};
         }
         std::stable_sort(key.begin(), key.end());
         for (int r = 0; r < neles; r++) perm[key[r].second] = r;
@@ -1654,9 +1694,11 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
     if (kernels_per_step) {
         // k_step_begin, smooth x2, bc, visc, stages x (prim, bc, grad, flux), prim end,
         // k_step_end, prim start
+        // (the Jameson flux, myflux 3, computes no gradients)
+        const int grad = h->prm.myorder == 2 && h->prm.myflux != 3 ? 1 : 0;
         int64_t n = 1 + 2 + (h->nghosts ? 1 : 0) + (h->prm.inviscid ? 0 : 1);
-        int64_t per_stage = 1 + (h->nghosts ? 1 : 0) + (h->prm.myorder == 2 ? 1 : 0) + 1;
-        if (h->aliased) per_stage += (h->prm.myorder == 2 ? 1 : 0) + 1;
+        int64_t per_stage = 1 + (h->nghosts ? 1 : 0) + grad + 1;
+        if (h->aliased) per_stage += grad + 1;
         if (h->dm.nfringe > 0) per_stage += 1;
         if (h->dm.nface > 0)   // k_faceflux; or the scatter kernels of face modes 2 (one per colour), 3
             per_stage += h->dm.face_mode == 2 ? h->dm.ncolor : 1;
@@ -1665,7 +1707,7 @@ extern "C" int hp_info(const hp_handle* h, int64_t* kernels_per_step, int64_t* d
         if (h->aliased) n += 2;
         if (h->neq == 22) n += 2 + (int64_t)h->dp.nstage * (2 + (h->nghosts ? 1 : 0));   // k_qrs_*
         if (h->nwall > 0)   // FP64 wall layers: viscous once, gradients and fluxes per stage
-            n += (h->prm.inviscid ? 0 : 1) + (int64_t)h->dp.nstage * ((h->prm.myorder == 2 ? 1 : 0) + 1);
+            n += (h->prm.inviscid ? 0 : 1) + (int64_t)h->dp.nstage * (grad + 1);
         if (h->prm.use_graph == 2 && h->fused > 0 && !h->xfn && h->dm.nfringe == 0 && h->dm.nhalo == 0)
             n = 1;   // the fused step
         *kernels_per_step = n;
