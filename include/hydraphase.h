@@ -170,9 +170,9 @@ int hp_sync(hp_handle *h);
  * measured with CUDA events on the handle's stream. */
 int hp_step_timed(hp_handle *h, int32_t nsteps, double *device_ms);
 /* nsteps launched eagerly with a CUDA event between every two kernels;
- * accumulates device time and launch counts per kernel kind (nkinds >= 14:
+ * accumulates device time and launch counts per kernel kind (nkinds >= 16:
  * prim_start, step_begin, smooth1, smooth2, bc_visc, visc, prim_stage, bc,
- * grad, flux, prim_end, step_end, serial, overset, halo). */
+ * grad, flux, prim_end, step_end, serial, overset, halo, qrs). */
 int hp_profile_steps(hp_handle *h, int32_t nsteps, double *ms_per_kind,
                      int64_t *launches_per_kind, int32_t nkinds);
 
