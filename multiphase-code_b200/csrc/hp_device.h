@@ -113,6 +113,8 @@ struct DevMesh {
     // cells of wcells, which the FP32 kernels leave alone (2: no neighbour
     // outside the layers, so not even their FP32 gradients are read)
     int nwall, ngwall;
+    int wprefix;            // 1: wcells and gcells are 0, 1, ... (the layer
+                            // cells first in the cell order, see hp_host.cu)
     const int* wcells;
     const int* gcells;
     const unsigned char* wclass;   // [ld]

@@ -106,6 +106,7 @@ struct hp_handle {
     int aliased = 0;
     int neq = 10;               // conserved variables: 10, or 22 with the five-phase model
     int nwall = 0, ngwall = 0;  // FP64 wall-layer cells and their gradient cells
+    int wprefix = 0;            // 1: those lists are the first cells of the order
     int max_diag = 4096;
     std::string err;
     double* h_diag = nullptr;   // pinned
@@ -213,7 +214,7 @@ static void plan_arena(hp_handle* h, Arena& a, int neles, int nghosts, long long
     s.diag = (double*)a.take((size_t)ncase * h->max_diag * 8 * D);
     s.max_diag = h->max_diag;
     m.cid = ncase > 1 ? (const int*)a.take((size_t)neles * I) : nullptr;
-    m.nwall = h->nwall; m.ngwall = h->ngwall;
+    m.nwall = h->nwall; m.ngwall = h->ngwall; m.wprefix = h->wprefix;
     if (h->nwall > 0) {
         m.wcells = (const int*)a.take((size_t)h->nwall * I);
         m.gcells = (const int*)a.take((size_t)h->ngwall * I);
@@ -806,6 +807,15 @@ extern "C" int hp_create_batch(const hp_mesh* meshes, int32_t ncase, const hp_pa
     }
     h->nwall = (int)hwall.size();
     h->ngwall = (int)hgwall.size();
+    // with the layer-first cell order (one case, renumbered) both lists are
+    // the leading cells 0, 1, ...: the layer kernels then run as whole-mesh
+    // launches over that prefix
+    {
+        bool pre = h->nwall > 0;
+        for (int k = 0; k < h->ngwall && pre; k++) pre = hgwall[k] == k;
+        for (int k = 0; k < h->nwall && pre; k++) pre = hwall[k] == k;
+        h->wprefix = pre ? 1 : 0;
+    }
     Arena& A = h->arena;
     auto plan = [&](Arena& a) { plan_arena(h, a, neles, nghosts, ld, gb, ncase, nface); };
     Arena probe;

@@ -43,15 +43,34 @@ namespace v_fp64 {
 static void wall_visc(const DevMesh& m, const DevState<double>& s, const DevParams& P, cudaStream_t st) {
     if (m.nwall > 0) k_visc8<1><<<grid_for(8ll * m.nwall, 128), 128, 0, st>>>(m, s, P);
 }
+// With the layer-first cell order (m.wprefix) the lists are the leading
+// cells, and the gradient and flux kernels run their whole-mesh form over a
+// view of the mesh that ends after them: the same per-cell arithmetic, with
+// the coalesced staging of the whole-mesh launches.  (The viscous kernel
+// tells boundary faces by m.neles, so it keeps the list.)
+static DevMesh prefix_view(const DevMesh& m, int n) {
+    DevMesh v = m;
+    v.neles = n;
+    return v;
+}
 static void wall_grad(const DevMesh& m, const DevState<double>& s, const DevParams& P, cudaStream_t st) {
-    if (m.ngwall > 0) k_grad4<1><<<grid_for(4ll * m.ngwall, 128), 128, 0, st>>>(m, s, P);
+    if (m.ngwall <= 0) return;
+    if (m.wprefix) k_grad4<0><<<grid_for(4ll * m.ngwall, 128), 128, 0, st>>>(prefix_view(m, m.ngwall), s, P);
+    else k_grad4<1><<<grid_for(4ll * m.ngwall, 128), 128, 0, st>>>(m, s, P);
+}
+template <int Z>
+static void wall_flux_z(const DevMesh& m, const DevState<double>& s, const DevParams& P, cudaStream_t st,
+                        int stage) {
+    const unsigned g = grid_for(4ll * m.nwall, 128);
+    if (m.wprefix) k_flux4<Z, 0><<<g, 128, 0, st>>>(prefix_view(m, m.nwall), s, P, stage);
+    else k_flux4<Z, 1><<<g, 128, 0, st>>>(m, s, P, stage);
 }
 static void wall_flux(const DevMesh& m, const DevState<double>& s, const DevParams& P, cudaStream_t st,
                       int stage) {
     if (m.nwall <= 0) return;
-    if (P.myflux == 1) k_flux4<1, 1><<<grid_for(4ll * m.nwall, 128), 128, 0, st>>>(m, s, P, stage);
-    else if (P.myflux == 3) k_flux4<2, 1><<<grid_for(4ll * m.nwall, 128), 128, 0, st>>>(m, s, P, stage);
-    else k_flux4<0, 1><<<grid_for(4ll * m.nwall, 128), 128, 0, st>>>(m, s, P, stage);
+    if (P.myflux == 1) wall_flux_z<1>(m, s, P, st, stage);
+    else if (P.myflux == 3) wall_flux_z<2>(m, s, P, st, stage);
+    else wall_flux_z<0>(m, s, P, st, stage);
 }
 }  // namespace v_fp64
 const WallFp64 wall_fp64 = {&v_fp64::wall_visc, &v_fp64::wall_grad, &v_fp64::wall_flux};
